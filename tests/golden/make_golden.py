@@ -1,0 +1,196 @@
+"""Generates the golden fixtures under tests/golden/ by running the upstream DGAmore code itself.
+
+Run in a container that holds the upstream sources at /root/reference (they do not travel to the GPU box; the
+committed .npz files do):
+
+    python tests/golden/make_golden.py
+
+For each small synthetic configuration (``dgamore_b200.synthetic.CONFIGS``: t1, t1b, t2, t3) it builds the
+inputs of one nonlocal pass, then replays the upstream call sequence of ``calculate_self_energy_q``
+(dgamore/nonlocal_sde.py:786-879) with the upstream functions, in FP64 (``IHaveMat.mat`` patched to keep
+complex128), and stores inputs and every intermediate into ``<name>.npz``.
+
+It also copies the upstream's own end-to-end fixtures that pin the bubble (``g_dga.npy``,
+``gchi0_q_rank_0.npy``, ``gchi0_q_inv_rank_0.npy`` from tests/test_data/end_2_end) and the lambda-correction
+fixtures (tests/test_data/lambda_correction/{sp,spch}) into ``upstream_fixtures.npz``, and the upstream BSE
+known-answer case (tests/test_four_point.py:466-532, rng 1234) into ``bse_kat.npz``.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+from copy import deepcopy
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+sys.path.insert(0, REPO)
+
+import _ref_harness as harness  # noqa: E402
+
+harness.install()
+harness.patch_fp64()
+
+from dgamore import config  # noqa: E402
+import dgamore.brillouin_zone as bz  # noqa: E402
+import dgamore.lambda_correction as lc  # noqa: E402
+from dgamore import nonlocal_sde, mpi_utils  # noqa: E402
+from dgamore.bubble_gen import BubbleGenerator  # noqa: E402
+from dgamore.four_point import FourPoint  # noqa: E402
+from dgamore.greens_function import GreensFunction  # noqa: E402
+from dgamore.interaction import LocalInteraction, Interaction  # noqa: E402
+from dgamore.local_four_point import LocalFourPoint  # noqa: E402
+from dgamore.n_point_base import SpinChannel  # noqa: E402
+from dgamore.self_energy import SelfEnergy  # noqa: E402
+
+from dgamore_b200 import synthetic  # noqa: E402
+
+UPSTREAM_DATA = os.path.join(harness.REFERENCE_ROOT, "tests", "test_data")
+
+
+class _Logger:
+    def info(self, *a, **k):
+        pass
+
+    debug = warning = info
+
+    def log_memory_usage(self, *a, **k):
+        pass
+
+
+def _setup_config(cfg: synthetic.DgaConfig, inp: dict):
+    config.logger = _Logger()
+    config.sys.beta = cfg.beta
+    config.sys.n_bands = cfg.n_bands
+    config.sys.mu = inp["mu"]
+    config.box.niw_core = cfg.niw
+    config.box.niv_core = cfg.niv
+    config.box.niv_shell = cfg.niv_shell
+    config.box.niv_full = cfg.niv_full
+    config.lattice.nk = tuple(cfg.nk)
+    config.lattice.nq = tuple(cfg.nk)
+    config.lattice.k_grid = bz.KGrid(tuple(cfg.nk), symmetries=bz.two_dimensional_square_symmetries())
+    config.lattice.q_grid = config.lattice.k_grid
+    config.eliashberg.perform_eliashberg = False
+    config.self_consistency.restrict_chi_phys = False
+    config.lambda_correction.perform_lambda_correction = False
+
+
+def run_reference_pass(name: str) -> dict:
+    cfg = synthetic.CONFIGS[name]
+    inp = synthetic.make_inputs(cfg)
+    _setup_config(cfg, inp)
+    grid = config.lattice.q_grid
+    assert np.array_equal(grid.irrk_ind, inp["irrk_ind"]), "irreducible wedge differs from upstream"
+    assert np.array_equal(grid.irrk_inv.ravel(), inp["irrk_inv"]), "irreducible inverse map differs"
+    assert np.array_equal(grid.irrk_count, inp["irrk_count"]), "irreducible counts differ"
+
+    beta = cfg.beta
+    dist = harness.FakeDistributor(grid.nk_irr)
+    giwk = GreensFunction(inp["g_k"], None, None, True, False, False)
+    u_loc = LocalInteraction(inp["u"])
+    v_full = Interaction(inp["v_q_full"].reshape(*cfg.nk, *inp["v_q_full"].shape[1:]), SpinChannel.NONE, tuple(cfg.nk))
+    irr_q_list = grid.get_irrq_list()
+    v_nonloc = v_full.reduce_q(irr_q_list)
+
+    out = {}
+    # bubble (nonlocal_sde.py:801-809)
+    gchi0_q = BubbleGenerator.create_generalized_chi0_q_fft_cpu(dist, giwk, cfg.niw, cfg.niv_full, grid, beta)
+    out["chi0"] = gchi0_q.mat.copy()
+    # direct-q bubble variant (bubble_gen.py:147-183)
+    gchi0_direct = BubbleGenerator.create_generalized_chi0_q_cpu(giwk, cfg.niw, cfg.niv_full, irr_q_list, grid, beta)
+    out["chi0_direct"] = gchi0_direct.mat.copy()
+
+    # double-counting kernel (nonlocal_sde.py:817-820)
+    f_dc_loc = 2 * LocalFourPoint(inp["f_magn_loc"], SpinChannel.NONE, 1, 2, False, True).permute_orbitals("abcd->cbad")
+    kernel = -nonlocal_sde.calculate_sigma_dc_kernel(f_dc_loc, gchi0_q, u_loc)
+    out["kernel_dc"] = -kernel.mat.copy()
+
+    # chi0 sums and inverse (nonlocal_sde.py:824-835)
+    gchi0_q_full_sum = 1.0 / beta * gchi0_q.sum_over_all_vn(beta)
+    gchi0_q_core = gchi0_q.cut_niv(cfg.niv)
+    gchi0_q_core_inv = deepcopy(gchi0_q_core).invert(False)
+    out["chi0_inv"] = gchi0_q_core_inv.mat.copy()
+    gchi0_q_core_sum = 1.0 / beta * gchi0_q_core.sum_over_all_vn(beta)
+
+    for ch, chan in (("dens", SpinChannel.DENS), ("magn", SpinChannel.MAGN)):
+        gamma_r = LocalFourPoint(inp[f"gamma_{ch}"], chan, 1, 2, False, True)
+        # calculate_sigma_kernel_r_q (nonlocal_sde.py:257-336), both BSE variants
+        aux = nonlocal_sde.create_auxiliary_chi_r_q_sum_v1(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc)
+        aux3 = nonlocal_sde.create_auxiliary_chi_r_q_sum_v3(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc, dist)
+        out[f"chi_aux_sum_{ch}"] = aux.mat.copy()
+        out[f"chi_aux_sum_v3_{ch}"] = aux3.mat.copy()
+        vrg_q = nonlocal_sde.create_vrg_r_q(aux, gchi0_q_core_inv)
+        out[f"vrg_{ch}"] = vrg_q.mat.copy()
+        chi_phys = aux.sum_over_all_vn(beta)
+        chi_phys = nonlocal_sde.create_generalized_chi_q_with_shell_correction(
+            chi_phys, gchi0_q_full_sum, gchi0_q_core_sum, u_loc, v_nonloc
+        )
+        out[f"chi_phys_{ch}_before_lambda"] = chi_phys.mat.copy()
+        if cfg.n_bands == 1:
+            chi_phys, lam = lc.perform_single_lambda_correction(chi_phys, inp[f"chi_loc_sum_{ch}"])
+            out[f"lambda_{ch}"] = np.float64(lam)
+        out[f"chi_phys_{ch}"] = chi_phys.mat.copy()
+        k_r = nonlocal_sde.calculate_kernel_r_q(vrg_q, chi_phys, v_nonloc, u_loc)
+        out[f"kernel_{ch}"] = k_r.mat.copy()
+        kernel += k_r if ch == "dens" else 3 * k_r
+
+    out["kernel"] = kernel.mat.copy()
+    # IBZ -> FBZ and the Sigma contraction through real space (nonlocal_sde.py:861, 874-878)
+    kernel_full = deepcopy(kernel).map_to_full_bz(grid)
+    kernel_full._nq = tuple(cfg.nk)
+    sigma_r = nonlocal_sde.calculate_sigma_from_kernel_fft_cpu(dist, deepcopy(kernel_full), giwk)
+    sigma = sigma_r.ifft().to_full_niv_range()
+    out["sigma"] = sigma.compress_q_dimension().mat.copy()
+    # direct Sigma variant (nonlocal_sde.py:430-469) on the full q list
+    sig_direct = nonlocal_sde.calculate_sigma_from_kernel_cpu(deepcopy(kernel_full), giwk, grid.get_q_list())
+    out["sigma_direct"] = sig_direct.compress_q_dimension().mat.copy()
+
+    save = {k: v for k, v in inp.items() if k not in ("config",)}
+    save.update({f"ref_{k}": v for k, v in out.items()})
+    save["config_name"] = np.array(name)
+    return save
+
+
+def upstream_fixtures() -> dict:
+    e2e = os.path.join(UPSTREAM_DATA, "end_2_end")
+    out = {}
+    for f in ("g_dga", "gchi0_q_rank_0", "gchi0_q_inv_rank_0", "mu_history"):
+        out[f] = np.load(os.path.join(e2e, f + ".npy"))
+    for kind in ("sp", "spch"):
+        d = os.path.join(UPSTREAM_DATA, "lambda_correction", kind)
+        for f in sorted(os.listdir(d)):
+            if f.endswith(".npy"):
+                out[f"lambda_{kind}_{f[:-4]}"] = np.load(os.path.join(d, f))
+    return out
+
+
+def bse_kat() -> dict:
+    """The upstream BSE known-answer input (tests/test_four_point.py:46-63, rng 1234) and its outputs."""
+    rng = np.random.default_rng(1234)
+    nq, o, niw, niv = (4, 4, 1), 2, 3, 3
+    shape = (16, o, o, o, o, 2 * niw + 1, 2 * niv, 2 * niv)
+    mat = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    beta = 11.0
+    fp = FourPoint(mat, SpinChannel.MAGN, nq, 1, 2, True, True, True)
+    v1 = deepcopy(fp).invert_and_sum_over_last_vn(beta).mat
+    v2 = deepcopy(fp).invert_and_sum_over_last_vn_v2(beta).mat
+    # the input is regenerated from default_rng(1234) by the tests; only the outputs are stored
+    return {"beta": beta, "v1": v1, "v2": v2}
+
+
+def main():
+    for name in ("t1", "t1b", "t2", "t3"):
+        data = run_reference_pass(name)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+        print("wrote", name, sorted(data.keys()))
+    np.savez_compressed(os.path.join(HERE, "upstream_fixtures.npz"), **upstream_fixtures())
+    np.savez_compressed(os.path.join(HERE, "bse_kat.npz"), **bse_kat())
+    print("done")
+
+
+if __name__ == "__main__":
+    main()
