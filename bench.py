@@ -1,0 +1,372 @@
+"""Benchmark: (q, w) ladder solves per second of the nonlocal ladder-DGA pass on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c3] [--impl ours|reference]
+
+One step is one full nonlocal pass over the resident inputs of the configuration (bubble -> double-counting
+kernel -> chi0^-1 -> BSE in the density and magnetic channels -> shell-corrected chi -> lambda (single band)
+-> kernel -> Sigma(k, nu)).  One (q, w) ladder solve = one irreducible q x one w >= 0 x one channel, so a step
+of the 3-orbital t2g configuration (32x32, niv = niw = 40, N = 720) is 153 * 41 * 2 = 12,546 solves.
+
+The metric is whole-job throughput over the timed steps (CUDA events on the launching stream, max over
+ranks).  ``e2e`` is the same metric through the public API with host G(k) in and host Sigma out.  Multi-GPU
+runs are independent replicas (the device schedule has no inter-GPU exchange): weak scaling.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+
+def f_solve(N: int, n2: int) -> float:
+    """Real flops of one complex LU with partial pivoting plus n2 right-hand-side solves: 8/3 N^3 + 8 n2 N^2."""
+    return 8.0 / 3.0 * N**3 + 8.0 * n2 * N**2
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons every 200 ms in the background."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+        "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+        "clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
+                    capture_output=True, text=True, timeout=5,
+                ).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=5)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        smax = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for name, val in zip(names, s[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(self.samples),
+        }
+
+
+def dist_setup(n_gpus: int):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def fp64_peak_tflops() -> float:
+    """cuBLAS DGEMM 8192^3 best of 5 on this GPU (the FP64 denominator; MEASURED_PEAKS.json holds bf16 only)."""
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n**3 / best / 1e12
+
+
+def cpu_baseline_sample(inp: dict, n_items: int = 6) -> dict:
+    """The oracle (NumPy restatement of the upstream path) timed on a bounded sample of BSE solves."""
+    from oracle import ladder as oracle
+
+    beta = inp["beta"]
+    nb = inp["u"].shape[0]
+    niv = inp["niv_core"]
+    chi0 = oracle.chi0_q_fft(inp["g_k"], inp["niw"], niv + inp["niv_shell"], inp["irrk_ind"][:1], beta)
+    c0i = oracle.chi0_inv(oracle.cut_niv(chi0, niv, 1))
+    uv = oracle.u_as_channel(inp["u"], "magn")[None] + oracle.v_as_channel(inp["v_q_irr"][:1], "magn")
+    t0 = time.perf_counter()
+    done = 0
+    for w in range(min(n_items, c0i.shape[5])):
+        oracle.bse_sum(c0i[..., w : w + 1, :], inp["gamma_magn"][..., w : w + 1, :, :], uv, beta)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {
+        "value": done / dt,
+        "unit": "(q,w) ladder solves/s",
+        "cores": os.cpu_count(),
+        "kind": "port",
+        "sample": f"{done} BSE solves (N={nb * nb * 2 * niv}) of the oracle (numpy inv + nu' sum, "
+        f"four_point.py:620-642), one q, magn channel",
+    }
+
+
+def run_reference(args, rank: int, world: int):
+    """--impl reference: the upstream CPU path (its NumPy restatement in oracle/) on the host cores."""
+    if rank != 0:
+        return
+    from dgamore_b200 import synthetic
+    from oracle import ladder as oracle
+
+    cfg = synthetic.CONFIGS[args.config]
+    inp = synthetic.make_inputs(cfg)
+    nb, niv = cfg.n_bands, cfg.niv
+    N = nb * nb * 2 * niv
+    beta = cfg.beta
+    chi0 = oracle.chi0_q_fft(inp["g_k"], cfg.niw, cfg.niv_full, inp["irrk_ind"][:1], beta)
+    c0i = oracle.chi0_inv(oracle.cut_niv(chi0, niv, 1))
+    uv = oracle.u_as_channel(inp["u"], "magn")[None] + oracle.v_as_channel(inp["v_q_irr"][:1], "magn")
+    per_step = max(1, min(cfg.niw + 1, args.ref_items))
+    times = []
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for w in range(per_step):
+            oracle.bse_sum(c0i[..., w : w + 1, :], inp["gamma_magn"][..., w : w + 1, :, :], uv, beta)
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = float(np.sum(times))
+    value = per_step * args.steps / t
+    line = {
+        "impl": "reference",
+        "metric": "(q,w) ladder solves/s",
+        "value": value,
+        "unit": "(q,w) ladder solves/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "complex128",
+        "data": "synthetic (seeded model inputs with the configuration's shapes)",
+        "config": {"workload": f"{args.config}: {cfg.n_bands}-orbital {cfg.nk[0]}x{cfg.nk[1]} niv=niw={cfg.niv}, N={N}",
+                   "sample_per_step": f"{per_step} BSE solves"},
+        "cpu_baseline": {"value": value, "unit": "(q,w) ladder solves/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{per_step} BSE solves per step (numpy inv + nu' sum of the oracle)"},
+        "e2e": {"value": value, "unit": "(q,w) ladder solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank: int, world: int, local: int):
+    import torch
+
+    from dgamore_b200 import synthetic
+    from dgamore_b200.pipeline import LadderPass
+
+    cfg = synthetic.CONFIGS[args.config]
+    inp = synthetic.make_inputs(cfg)
+    lp = LadderPass(inp, keep_intermediates=False)
+    sh = lp.sh
+    stream = torch.cuda.current_stream()
+
+    # warm-up
+    for _ in range(args.warmup):
+        lp.run()
+    torch.cuda.synchronize()
+    status = int(lp.bse_status.abs().sum().item()) + int(lp.status.abs().sum().item())
+
+    # timed region: device-resident inputs, K passes; the BSE launch is timed separately on the same stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for k in range(args.steps):
+            lp.status.zero_()
+            lp.bubble()
+            lp.dc_kernel()
+            lp.chi0_prep()
+            ev[k][0].record(stream)
+            lp.bse()
+            ev[k][1].record(stream)
+            lp.chi_phys_stage()
+            chi_r = lp.lambda_stage()
+            lp.kernel_stage(chi_r)
+            lp.sigma_stage()
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    t_local = start.elapsed_time(end) / 1e3
+    t = max_over_ranks(t_local, world)
+    bse_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    value = world * sh.n_solves * args.steps / t
+    kernels_per_pass = 14 if lp.do_lambda else 13
+
+    # end-to-end through the public API: host G(k) -> device pass -> host Sigma
+    for _ in range(1):
+        lp.run_e2e()
+    barrier(world)
+    e_s, e_e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_s.record(stream)
+    for _ in range(args.steps):
+        lp.run_e2e()
+    e_e.record(stream)
+    e_e.synchronize()
+    t_e2e = max_over_ranks(e_s.elapsed_time(e_e) / 1e3, world)
+    e2e_value = world * sh.n_solves * args.steps / t_e2e
+
+    peaks = measured_peaks()
+    fp64_peak = fp64_peak_tflops() if rank == 0 else None
+    flops_launch = sh.n_solves * f_solve(sh.N, sh.n2)
+    achieved = flops_launch / (bse_ms / 1e3) / 1e12
+    line = {
+        "metric": "(q,w) ladder solves/s",
+        "value": value,
+        "unit": "(q,w) ladder solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "complex128",
+        "data": "synthetic (seeded model inputs with the configuration's shapes; see dgamore_b200/synthetic.py)",
+        "config": {
+            "workload": f"{args.config}: {cfg.n_bands}-orbital {cfg.nk[0]}x{cfg.nk[1]} square lattice, "
+            f"niv=niw={cfg.niv}, N={sh.N}, {sh.n_q} irreducible q, {sh.n_solves} solves per pass",
+            "precision": "fp64 drop-in",
+            "step": "one full nonlocal pass (bubble, dc kernel, chi0^-1, BSE dens+magn, chi_phys, lambda, kernel, Sigma)",
+            "l2": "inputs larger than L2 (Gamma_r alone is %.0f MB)" % (lp.gamma_cm.numel() * 16 / 1e6),
+            "parallelism": f"{world} independent replica(s)",
+        },
+        "gpu_launches": kernels_per_pass * args.steps,
+        "e2e": {
+            "value": e2e_value,
+            "unit": "(q,w) ladder solves/s",
+            "h2d_bytes_per_step": lp.h2d_bytes,
+            "d2h_bytes_per_step": lp.d2h_bytes,
+        },
+        "roofline": {
+            "bound": "tensor",
+            "kernel": "bse_solve_sum_fp64_kernel",
+            "achieved": achieved,
+            "peak": fp64_peak,
+            "unit": "TFLOP/s",
+            "frac": (achieved / fp64_peak) if fp64_peak else None,
+            "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has bf16 and HBM only)",
+            "flops_per_launch": flops_launch,
+            "bse_ms_per_launch": bse_ms,
+            "traffic": None,
+        },
+        "bse_status_nonzero": status,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        line["cpu_baseline"] = cpu_baseline_sample(inp, args.cpu_items)
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="c3")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-items", type=int, default=4)
+    ap.add_argument("--ref-items", type=int, default=3)
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,564 @@
+// Batched ladder Bethe-Salpeter solve for every (channel, q, w) work item.
+//
+// For one item the compound-index matrix (row (o1,o2,nu), column (o4,o3,nu'), N = n^2 * 2 niv) is
+//
+//     A = (blockdiag_nu chi0^-1(q,w,nu) + Gamma_r(w) / beta^2) - (U_r + V_r^q) / beta^2
+//
+// (dgamore/nonlocal_sde.py:85-96 assembled through FourPoint.add, four_point.py:332-430), and the result is
+//
+//     X[(o1,o2,nu), (o4,o3)] = sum_nu' (A^-1)[(o1,o2,nu), (o4,o3,nu')] / beta
+//
+// (four_point.py:620-642; equivalently the solve against the n^2 selector right-hand sides of
+// four_point.py:644-684).  Each CTA owns one item at a time (persistent loop over a device work list):
+//
+//   1. form A column-major in the CTA's scratch slot (Gamma_r is pre-permuted to the same column-major
+//      compound layout once per request, so this is a coalesced stream plus a block-diagonal add);
+//   2. blocked right-looking LU with partial pivoting (panel width NB): the panel is factored column by
+//      column with the LAPACK pivot measure |re|+|im| and first-index ties (izamax), the panel's row
+//      interchanges are applied to the other columns, the U12 row block is solved against L11 from shared
+//      memory, and the trailing matrix is updated by a 64x64-tiled complex GEMM from shared memory;
+//   3. the permuted selector right-hand side is solved by blocked forward and back substitution and
+//      written out divided by beta.
+//
+// The same LU core serves the FP64 drop-in (R = double) and the mixed form (R = float for the
+// factorisation, FP64 residuals and refinement; see bse_mixed below).
+#include "dga_common.cuh"
+
+#include <stdio.h>
+
+namespace dga {
+
+constexpr int BSE_THREADS = 256;
+constexpr int BSE_NB = 32;    // panel width
+constexpr int BSE_TILE = 64;  // trailing-update tile edge
+constexpr int BSE_MAX_N = 2048;
+
+// ----------------------------------------------------------------------------------------------
+// Matrix sources: how A(i, j) of a work item is formed
+// ----------------------------------------------------------------------------------------------
+
+// A formed from the resident ladder inputs (structured form of nonlocal_sde.py:85-96).
+struct StructuredSource {
+  const double2* gamma_cm;  // [n_ch][W][N][N]: column-major compound Gamma_r(w): element (i,j) at j*N + i
+  const double2* chi0_inv;  // [Q][W][nv][n2][n2]: chi0^-1 orbital matrices, row (o1,o2), column (o4,o3)
+  const double2* uv;        // [n_ch][Q][n2][n2]: U_r + V_r^q, row (o1,o2), column (o4,o3)
+  int n2, nv, W, Q;
+  double inv_beta2;  // 1 / beta**2 computed on the host exactly as the upstream does
+
+  // Element (i, j) in FP64, with the upstream's order of operations: (chi0inv_diag + Gamma*ib2) + (-(uv*ib2)).
+  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j) const {
+    const double2 g = gamma_cm[((size_t)(ch * W + w) * N + j) * N + i];
+    const int pr = i / nv, vr = i - pr * nv;
+    const int pc = j / nv, vc = j - pc * nv;
+    const double2 u = uv[((size_t)ch * Q + q) * n2 * n2 + pr * n2 + pc];
+    double re = __dmul_rn(g.x, inv_beta2);
+    double im = __dmul_rn(g.y, inv_beta2);
+    if (vr == vc) {
+      const double2 c = chi0_inv[(((size_t)q * W + w) * nv + vr) * n2 * n2 + pr * n2 + pc];
+      re = __dadd_rn(c.x, re);
+      im = __dadd_rn(c.y, im);
+    }
+    re = __dadd_rn(re, -__dmul_rn(u.x, inv_beta2));
+    im = __dadd_rn(im, -__dmul_rn(u.y, inv_beta2));
+    return make_double2(re, im);
+  }
+};
+
+// A given explicitly in the upstream FourPoint layout [q][o1][o2][o3][o4][w][nu][nu'] (the generic
+// FourPoint.invert_and_sum_over_last_vn, four_point.py:620-642).
+struct DenseSource {
+  const double2* mat;  // [Q][n][n][n][n][W][nv][nv]
+  int nb, nv, W, Q;
+
+  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j) const {
+    const int pr = i / nv, vr = i - pr * nv;
+    const int pc = j / nv, vc = j - pc * nv;
+    const int o1 = pr / nb, o2 = pr - o1 * nb;
+    const int o4 = pc / nb, o3 = pc - o4 * nb;
+    size_t idx = ((((size_t)q * nb + o1) * nb + o2) * nb + o3) * nb + o4;
+    idx = ((idx * W + w) * nv + vr) * nv + vc;
+    return mat[idx];
+  }
+};
+
+struct WorkItem {
+  int ch, q, w;
+};
+
+// ----------------------------------------------------------------------------------------------
+// Block-wide arg-max of the pivot measure: larger value wins, ties go to the smaller row index.
+// ----------------------------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void argmax_merge(R& v, int& idx, R ov, int oidx) {
+  if (ov > v || (ov == v && oidx < idx)) {
+    v = ov;
+    idx = oidx;
+  }
+}
+
+template <typename R>
+__device__ int block_argmax(R v, int idx, R* s_val, int* s_idx) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    R ov = __shfl_down_sync(0xffffffffu, v, off);
+    int oi = __shfl_down_sync(0xffffffffu, idx, off);
+    argmax_merge(v, idx, ov, oi);
+  }
+  if (lane == 0) {
+    s_val[warp] = v;
+    s_idx[warp] = idx;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    v = lane < nw ? s_val[lane] : R(-1);
+    idx = lane < nw ? s_idx[lane] : 0x7fffffff;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      R ov = __shfl_down_sync(0xffffffffu, v, off);
+      int oi = __shfl_down_sync(0xffffffffu, idx, off);
+      argmax_merge(v, idx, ov, oi);
+    }
+    if (lane == 0) {
+      s_val[0] = v;
+      s_idx[0] = idx;
+    }
+  }
+  __syncthreads();
+  int r = s_idx[0];
+  __syncthreads();
+  return r;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Shared-memory layout of one CTA
+// ----------------------------------------------------------------------------------------------
+template <typename C>
+struct BseSmem {
+  C Ls[BSE_NB][BSE_TILE];  // L21 tile (k, row)
+  C Us[BSE_NB][BSE_TILE];  // U12 tile (k, col)
+  C L11[BSE_NB][BSE_NB + 1];
+  C row[BSE_NB];
+  double red_val[32];
+  int red_idx[32];
+  int flag;
+};
+
+// ----------------------------------------------------------------------------------------------
+// LU with partial pivoting of the N x N column-major matrix A (leading dimension ld) in place.
+// piv[j] receives the row exchanged with row j.  Returns true if an exact zero pivot was met.
+// ----------------------------------------------------------------------------------------------
+template <typename C>
+__device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ piv, BseSmem<C>& sm) {
+  using R = decltype(C::x);
+  const int tid = threadIdx.x, T = blockDim.x;
+  bool singular = false;
+
+  for (int k0 = 0; k0 < N; k0 += BSE_NB) {
+    const int nb = min(BSE_NB, N - k0);
+    // ---- panel factorisation (columns k0 .. k0+nb-1) ----
+    for (int jj = 0; jj < nb; ++jj) {
+      const int j = k0 + jj;
+      const C* colj = A + (size_t)j * ld;
+      R best = R(-1);
+      int bidx = 0x7fffffff;
+      for (int i = j + tid; i < N; i += T) {
+        R v = cabs1(colj[i]);
+        if (v > best) {
+          best = v;
+          bidx = i;
+        }
+      }
+      // reduce in double precision storage (R may be float)
+      int p;
+      {
+        double dv = (double)best;
+        p = block_argmax<double>(dv, bidx, sm.red_val, sm.red_idx);
+      }
+      if (p >= N) p = j;  // empty range cannot happen (j < N), kept for safety
+      if (tid == 0) piv[j] = p;
+      if (p != j) {
+        for (int c = tid; c < nb; c += T) {
+          C* col = A + (size_t)(k0 + c) * ld;
+          C t = col[j];
+          col[j] = col[p];
+          col[p] = t;
+        }
+      }
+      __syncthreads();
+      const C d = A[(size_t)j * ld + j];
+      const bool zero = (d.x == R(0) && d.y == R(0));
+      if (zero) singular = true;
+      const C rinv = zero ? cmake<C>(R(0), R(0)) : crecip(d);
+      for (int c = tid; c < nb - jj - 1; c += T) sm.row[c] = A[(size_t)(j + 1 + c) * ld + j];
+      __syncthreads();
+      const int ncols = nb - jj - 1;
+      for (int i = j + 1 + tid; i < N; i += T) {
+        C l = A[(size_t)j * ld + i];
+        if (!zero) l = cmul(l, rinv);
+        A[(size_t)j * ld + i] = l;
+        for (int c = 0; c < ncols; ++c) {
+          C* a = A + (size_t)(j + 1 + c) * ld + i;
+          C v = *a;
+          cfms(v, l, sm.row[c]);
+          *a = v;
+        }
+      }
+      __syncthreads();
+    }
+    // ---- L11 to shared memory ----
+    for (int e = tid; e < nb * nb; e += T) {
+      const int r = e % nb, c = e / nb;
+      sm.L11[r][c] = A[(size_t)(k0 + c) * ld + k0 + r];
+    }
+    __syncthreads();
+    // ---- row interchanges on the other columns + U12 = L11^-1 A12 ----
+    const int k1 = k0 + nb;
+    for (int c = tid; c < N; c += T) {
+      if (c >= k0 && c < k1) continue;
+      C* col = A + (size_t)c * ld;
+      for (int jj = 0; jj < nb; ++jj) {
+        const int p = piv[k0 + jj];
+        if (p != k0 + jj) {
+          C t = col[k0 + jj];
+          col[k0 + jj] = col[p];
+          col[p] = t;
+        }
+      }
+      if (c >= k1) {
+        C x[BSE_NB];
+#pragma unroll
+        for (int r = 0; r < BSE_NB; ++r)
+          if (r < nb) x[r] = col[k0 + r];
+#pragma unroll
+        for (int r = 0; r < BSE_NB; ++r) {
+          if (r < nb) {
+#pragma unroll
+            for (int rr = r + 1; rr < BSE_NB; ++rr)
+              if (rr < nb) cfms(x[rr], sm.L11[rr][r], x[r]);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < BSE_NB; ++r)
+          if (r < nb) col[k0 + r] = x[r];
+      }
+    }
+    __syncthreads();
+    // ---- trailing update A22 -= L21 U12 ----
+    const int nt = N - k1;
+    if (nt > 0) {
+      const int tiles = (nt + BSE_TILE - 1) / BSE_TILE;
+      const int ty = tid & 15, tx = tid >> 4;
+      for (int tile = 0; tile < tiles * tiles; ++tile) {
+        const int tr0 = k1 + (tile % tiles) * BSE_TILE;
+        const int tc0 = k1 + (tile / tiles) * BSE_TILE;
+        for (int e = tid; e < nb * BSE_TILE; e += T) {
+          const int k = e / BSE_TILE, r = e % BSE_TILE;
+          sm.Ls[k][r] = (tr0 + r < N) ? A[(size_t)(k0 + k) * ld + tr0 + r] : cmake<C>(R(0), R(0));
+        }
+        for (int e = tid; e < nb * BSE_TILE; e += T) {
+          const int c = e / nb, k = e % nb;
+          sm.Us[k][c] = (tc0 + c < N) ? A[(size_t)(tc0 + c) * ld + k0 + k] : cmake<C>(R(0), R(0));
+        }
+        __syncthreads();
+        C acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = cmake<C>(R(0), R(0));
+        for (int k = 0; k < nb; ++k) {
+          C lv[4], uv[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) lv[a] = sm.Ls[k][ty + 16 * a];
+#pragma unroll
+          for (int b = 0; b < 4; ++b) uv[b] = sm.Us[k][tx + 16 * b];
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) cfma(acc[a][b], lv[a], uv[b]);
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int c = tc0 + tx + 16 * b;
+          if (c < N) {
+            C* col = A + (size_t)c * ld;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+              const int r = tr0 + ty + 16 * a;
+              if (r < N) col[r] = csub(col[r], acc[a][b]);
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  return singular;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Solve (L U) Y = B in place for the n_rhs columns of Y (column-major, leading dimension N), with the LU
+// factors of lu_factor (unit lower L below the diagonal, U on and above).  Blocked by 32 rows.
+// ----------------------------------------------------------------------------------------------
+template <typename C, typename CY>
+__device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __restrict__ Y, int n_rhs,
+                                 BseSmem<C>& sm) {
+  using RY = decltype(CY::x);
+  const int tid = threadIdx.x, T = blockDim.x;
+  // forward: L z = b
+  for (int b0 = 0; b0 < N; b0 += BSE_NB) {
+    const int bn = min(BSE_NB, N - b0);
+    for (int e = tid; e < bn * bn; e += T) {
+      const int r = e % bn, c = e / bn;
+      sm.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
+    }
+    __syncthreads();
+    for (int s = tid; s < n_rhs; s += T) {
+      CY* y = Y + (size_t)s * N + b0;
+      for (int r = 0; r < bn; ++r) {
+        const CY yr = y[r];
+        for (int rr = r + 1; rr < bn; ++rr) {
+          const C l = sm.L11[rr][r];
+          CY lw = cmake<CY>((RY)l.x, (RY)l.y);
+          cfms(y[rr], lw, yr);
+        }
+      }
+    }
+    __syncthreads();
+    const int rows = N - b0 - bn;
+    for (int e = tid; e < rows * n_rhs; e += T) {
+      const int i = b0 + bn + e % rows, s = e / rows;
+      CY* y = Y + (size_t)s * N;
+      CY acc = y[i];
+      for (int r = 0; r < bn; ++r) {
+        const C l = A[(size_t)(b0 + r) * ld + i];
+        cfms(acc, cmake<CY>((RY)l.x, (RY)l.y), y[b0 + r]);
+      }
+      y[i] = acc;
+    }
+    __syncthreads();
+  }
+  // backward: U y = z
+  const int nblk = (N + BSE_NB - 1) / BSE_NB;
+  for (int blk = nblk - 1; blk >= 0; --blk) {
+    const int b0 = blk * BSE_NB;
+    const int bn = min(BSE_NB, N - b0);
+    for (int e = tid; e < bn * bn; e += T) {
+      const int r = e % bn, c = e / bn;
+      sm.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
+    }
+    __syncthreads();
+    for (int s = tid; s < n_rhs; s += T) {
+      CY* y = Y + (size_t)s * N + b0;
+      for (int r = bn - 1; r >= 0; --r) {
+        const C u = sm.L11[r][r];
+        CY yr = cdiv(y[r], cmake<CY>((RY)u.x, (RY)u.y));
+        y[r] = yr;
+        for (int rr = 0; rr < r; ++rr) {
+          const C l = sm.L11[rr][r];
+          cfms(y[rr], cmake<CY>((RY)l.x, (RY)l.y), yr);
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < b0 * n_rhs; e += T) {
+      const int i = e % b0, s = e / b0;
+      CY* y = Y + (size_t)s * N;
+      CY acc = y[i];
+      for (int r = 0; r < bn; ++r) {
+        const C u = A[(size_t)(b0 + r) * ld + i];
+        cfms(acc, cmake<CY>((RY)u.x, (RY)u.y), y[b0 + r]);
+      }
+      y[i] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Y = P * S where S is the n2-column selector (S[j, s] = 1 if the orbital pair of row j is s) and P the
+// row permutation recorded in piv.  perm is shared scratch of N ints.
+template <typename CY>
+__device__ void permuted_selector(CY* __restrict__ Y, int N, int nv, int n_rhs, const int* __restrict__ piv,
+                                  int* __restrict__ perm) {
+  using RY = decltype(CY::x);
+  const int tid = threadIdx.x, T = blockDim.x;
+  for (int i = tid; i < N; i += T) perm[i] = i;
+  __syncthreads();
+  if (tid == 0) {
+    for (int i = 0; i < N; ++i) {
+      const int p = piv[i];
+      if (p != i) {
+        int t = perm[i];
+        perm[i] = perm[p];
+        perm[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < N * n_rhs; e += T) {
+    const int i = e % N, s = e / N;
+    Y[(size_t)s * N + i] = cmake<CY>((perm[i] / nv == s) ? RY(1) : RY(0), RY(0));
+  }
+  __syncthreads();
+}
+
+// ----------------------------------------------------------------------------------------------
+// FP64 kernel: one CTA per work item, persistent over the list.
+// ----------------------------------------------------------------------------------------------
+template <typename Source>
+__global__ void __launch_bounds__(BSE_THREADS, 2)
+    bse_solve_sum_fp64_kernel(Source src, const WorkItem* __restrict__ work, int n_items, int N, int n2,
+                              int nv, int W, int Q, double beta, double2* __restrict__ out,
+                              int* __restrict__ status, double2* __restrict__ scratch, size_t slot_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BseSmem<double2>& sm = *reinterpret_cast<BseSmem<double2>*>(smem_raw);
+  int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<double2>));
+  int* perm = piv + N;
+  double2* A = scratch + (size_t)blockIdx.x * slot_elems;
+  double2* Y = A + (size_t)N * N;
+  const int tid = threadIdx.x, T = blockDim.x;
+
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const WorkItem wi = work[item];
+    for (size_t e = tid; e < (size_t)N * N; e += T) {
+      const int i = (int)(e % N), j = (int)(e / N);
+      A[e] = src.element(wi.ch, wi.q, wi.w, N, i, j);
+    }
+    __syncthreads();
+    const bool singular = lu_factor<double2>(A, N, N, piv, sm);
+    permuted_selector<double2>(Y, N, nv, n2, piv, perm);
+    lu_solve_inplace<double2, double2>(A, N, N, Y, n2, sm);
+    // write X[(ch, q, w)][i][s] = Y[i][s] / beta and check finiteness
+    if (tid == 0) sm.flag = 0;
+    __syncthreads();
+    double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * n2;
+    bool bad = false;
+    for (int e = tid; e < N * n2; e += T) {
+      const int i = e / n2, s = e % n2;
+      double2 y = Y[(size_t)s * N + i];
+      y.x = y.x / beta;
+      y.y = y.y / beta;
+      if (!cfinite(y)) bad = true;
+      o[e] = y;
+    }
+    if (bad) atomicOr(&sm.flag, DGA_ITEM_NONFINITE);
+    __syncthreads();
+    if (tid == 0 && status) status[item] = (singular ? DGA_ITEM_SINGULAR : 0) | sm.flag;
+    __syncthreads();
+  }
+}
+
+}  // namespace dga
+
+using namespace dga;
+
+static size_t bse_smem_bytes(int N) { return sizeof(BseSmem<double2>) + 2 * sizeof(int) * (size_t)N; }
+
+static int bse_grid(int n_items, size_t smem) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bse_solve_sum_fp64_kernel<StructuredSource>,
+                                                BSE_THREADS, smem);
+  if (per_sm < 1) per_sm = 1;
+  int g = sms * per_sm;
+  return n_items < g ? n_items : g;
+}
+
+extern "C" {
+
+// Scratch bytes the FP64 BSE entry points need for a launch over n_items items of compound size N with
+// n2 right-hand sides: one N x N matrix plus N x n2 solution per resident CTA.
+size_t dga_bse_scratch_bytes(int N, int n2, int n_items) {
+  if (N <= 0 || n2 <= 0 || n_items <= 0) return 0;
+  const size_t smem = bse_smem_bytes(N);
+  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<StructuredSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  const int grid = bse_grid(n_items, smem);
+  return (size_t)grid * ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
+}
+
+int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                           const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
+                           int n_items, void* out, int* status, void* scratch, size_t scratch_bytes,
+                           cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0 || N > BSE_MAX_N) {
+    dga_set_error("dga_bse_solve_sum_c128: invalid sizes (n_orb=%d niv=%d niw_half=%d n_q=%d n_ch=%d items=%d)",
+                  n_orb, niv, niw_half, n_q, n_ch, n_items);
+    return DGA_ERR_ARG;
+  }
+  if (!gamma_cm || !chi0_inv || !uv || !work || !out || !scratch) {
+    dga_set_error("dga_bse_solve_sum_c128: null pointer argument");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = bse_smem_bytes(N);
+  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<StructuredSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  const int grid = bse_grid(n_items, smem);
+  const size_t slot = (size_t)N * N + (size_t)N * n2;
+  if (scratch_bytes < (size_t)grid * slot * sizeof(double2)) {
+    dga_set_error("dga_bse_solve_sum_c128: scratch too small (%zu < %zu)", scratch_bytes,
+                  (size_t)grid * slot * sizeof(double2));
+    return DGA_ERR_SCRATCH;
+  }
+  StructuredSource src;
+  src.gamma_cm = (const double2*)gamma_cm;
+  src.chi0_inv = (const double2*)chi0_inv;
+  src.uv = (const double2*)uv;
+  src.n2 = n2;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  src.inv_beta2 = inv_beta2;
+  bse_solve_sum_fp64_kernel<StructuredSource><<<grid, BSE_THREADS, smem, stream>>>(
+      src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, (double2*)out, status,
+      (double2*)scratch, slot);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_bse_solve_sum_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+// Generic FourPoint.invert_and_sum_over_last_vn (four_point.py:620-642): the matrix is given explicitly in
+// the FourPoint layout [q][o1][o2][o3][o4][w][nu][nu'] (half w range); out is [q][w][N][n2].
+int dga_invert_sum_dense_c128(int n_orb, int niv, int niw_half, int n_q, double beta, const void* mat,
+                              const int* work, int n_items, void* out, int* status, void* scratch,
+                              size_t scratch_bytes, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_items <= 0 || N > BSE_MAX_N || !mat || !work ||
+      !out || !scratch) {
+    dga_set_error("dga_invert_sum_dense_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = bse_smem_bytes(N);
+  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<DenseSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  const int grid = bse_grid(n_items, smem);
+  const size_t slot = (size_t)N * N + (size_t)N * n2;
+  if (scratch_bytes < (size_t)grid * slot * sizeof(double2)) {
+    dga_set_error("dga_invert_sum_dense_c128: scratch too small");
+    return DGA_ERR_SCRATCH;
+  }
+  DenseSource src;
+  src.mat = (const double2*)mat;
+  src.nb = n_orb;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  bse_solve_sum_fp64_kernel<DenseSource><<<grid, BSE_THREADS, smem, stream>>>(
+      src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, (double2*)out, status,
+      (double2*)scratch, slot);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_invert_sum_dense_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"

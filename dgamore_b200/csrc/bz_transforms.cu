@@ -1,0 +1,437 @@
+// Brillouin-zone transforms of the ladder hot path, all built on one shared-memory plane DFT:
+//
+//   * dga_dft_planes_c128: batched separable DFT of momentum planes (G(k) -> G(R), Sigma(R) -> Sigma(k));
+//   * dga_bubble_c128:     chi0[q_irr,a,b,c,d,w,nu] = -beta/Nk * IFFT_R[G_ad(R,nu) G_cb(-R,nu-w)]
+//                          (dgamore/bubble_gen.py:33-69), product, inverse transform, irreducible-q pick,
+//                          scaling and the 1e-12 filter (n_point_base.py:205-211) fused in one kernel;
+//   * dga_sigma_partial_c128 / dga_sigma_reduce_c128: Sigma_ij(R,nu) = sum_w sum_ad G_ad(R,nu-w) K_aijd(-R,w,nu)
+//                          (nonlocal_sde.py:544-594), with K(-R) = sum_q K(q) e^{iqR} formed per plane from
+//                          the irreducible kernel through the IBZ -> FBZ map (n_point_base.py:489-494) and the
+//                          w < 0 half from K(q,-w,nu) = conj K(q,w,-nu-1) (local_n_point.py:191-225).
+//
+// A plane (Nk = nx*ny*nz points, C order) sits in shared memory; each axis is a direct DFT against a
+// host-built FP64 twiddle table (e^{2 pi i m / n}, sign folded in), so the transform needs no FFT plan and
+// handles any grid (16, 32, 48, 64, ...).  Work per plane is Nk*(nx+ny+nz) complex FMAs.
+#include "dga_common.cuh"
+
+namespace dga {
+
+constexpr int BZ_THREADS = 256;
+constexpr int BZ_MAX_NK = 4096;
+constexpr int BZ_MAX_AXIS = 128;
+
+struct Grid3 {
+  int nx, ny, nz, nk;
+};
+
+// twiddle tables in shared memory: tw[0..nx) for x, then y, then z
+__device__ __forceinline__ void load_twiddles(double2* s_tw, const double2* tw, const Grid3 g) {
+  for (int i = threadIdx.x; i < g.nx + g.ny + g.nz; i += blockDim.x) s_tw[i] = tw[i];
+}
+
+// out[kx][y][z] = sum_x in[x][y][z] * twx[(kx*x) % nx], then along y, then z (skipped when the axis has
+// length 1).  Result ends in `a` (the input buffer); `b` is work space.  Both buffers hold g.nk points.
+__device__ void plane_dft(double2* a, double2* b, const double2* s_tw, const Grid3 g) {
+  const int T = blockDim.x;
+  const double2* twx = s_tw;
+  const double2* twy = s_tw + g.nx;
+  const double2* twz = s_tw + g.nx + g.ny;
+  const int nyz = g.ny * g.nz;
+  // x axis: a -> b
+  for (int e = threadIdx.x; e < g.nk; e += T) {
+    const int kx = e / nyz, yz = e - kx * nyz;
+    double2 acc = make_double2(0.0, 0.0);
+    int m = 0;
+    for (int x = 0; x < g.nx; ++x) {
+      cfma(acc, a[x * nyz + yz], twx[m]);
+      m += kx;
+      if (m >= g.nx) m -= g.nx;
+    }
+    b[e] = acc;
+  }
+  __syncthreads();
+  // y axis: b -> a
+  for (int e = threadIdx.x; e < g.nk; e += T) {
+    const int kx = e / nyz, r = e - kx * nyz;
+    const int ky = r / g.nz, z = r - ky * g.nz;
+    const double2* row = b + kx * nyz + z;
+    double2 acc = make_double2(0.0, 0.0);
+    int m = 0;
+    for (int y = 0; y < g.ny; ++y) {
+      cfma(acc, row[y * g.nz], twy[m]);
+      m += ky;
+      if (m >= g.ny) m -= g.ny;
+    }
+    a[e] = acc;
+  }
+  __syncthreads();
+  if (g.nz > 1) {
+    for (int e = threadIdx.x; e < g.nk; e += T) {
+      const int base = (e / g.nz) * g.nz, kz = e - base;
+      double2 acc = make_double2(0.0, 0.0);
+      int m = 0;
+      for (int z = 0; z < g.nz; ++z) {
+        cfma(acc, a[base + z], twz[m]);
+        m += kz;
+        if (m >= g.nz) m -= g.nz;
+      }
+      b[e] = acc;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < g.nk; e += T) a[e] = b[e];
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// batched plane DFT with strided input/output addressing:
+//   element (plane p = p_hi * n_lo + p_lo, point R) at p_hi*s_hi + p_lo*s_lo + R*s_r
+// ------------------------------------------------------------------------------------------------
+struct PlaneAddr {
+  long long s_hi, s_lo, s_r;
+  int n_lo;
+  __device__ __forceinline__ long long at(int p, int r) const {
+    const int hi = p / n_lo, lo = p - hi * n_lo;
+    return hi * s_hi + lo * s_lo + (long long)r * s_r;
+  }
+};
+
+__global__ void __launch_bounds__(BZ_THREADS) dft_planes_kernel(const double2* __restrict__ in, PlaneAddr ia,
+                                                                 double2* __restrict__ out, PlaneAddr oa,
+                                                                 int n_planes, Grid3 g,
+                                                                 const double2* __restrict__ tw, double scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* a = reinterpret_cast<double2*>(smem_raw);
+  double2* b = a + g.nk;
+  double2* s_tw = b + g.nk;
+  load_twiddles(s_tw, tw, g);
+  for (int p = blockIdx.x; p < n_planes; p += gridDim.x) {
+    __syncthreads();
+    for (int r = threadIdx.x; r < g.nk; r += blockDim.x) a[r] = in[ia.at(p, r)];
+    __syncthreads();
+    plane_dft(a, b, s_tw, g);
+    for (int r = threadIdx.x; r < g.nk; r += blockDim.x) {
+      double2 v = a[r];
+      out[oa.at(p, r)] = make_double2(v.x * scale, v.y * scale);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// bubble: one CTA per (w, nu, a, d), looping over (c, b)
+//   g_r: [T][n][n][Nk] with slot t = nu_index + niv + niw (nu_index in [-niv-niw, niv))
+// ------------------------------------------------------------------------------------------------
+struct OutStrides7 {
+  long long q, w, v, a, b, c, d;
+};
+
+__global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __restrict__ g_r, int nb, int niv,
+                                                             int niw, Grid3 g, const int* __restrict__ q_irr,
+                                                             int n_qirr, const double2* __restrict__ tw,
+                                                             double beta, double2* __restrict__ out,
+                                                             OutStrides7 os) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* P = reinterpret_cast<double2*>(smem_raw);
+  double2* T1 = P + g.nk;
+  double2* s_tw = T1 + g.nk;
+  int* s_q = reinterpret_cast<int*>(s_tw + g.nx + g.ny + g.nz);
+  load_twiddles(s_tw, tw, g);
+  for (int i = threadIdx.x; i < 3 * n_qirr; i += blockDim.x) s_q[i] = q_irr[i];
+
+  const int nv = 2 * niv, W = niw + 1;
+  const int n2 = nb * nb;
+  const int total = W * nv * n2;
+  const int nyz = g.ny * g.nz;
+  const double inv_nk = 1.0 / (double)g.nk;
+  const double pref = -beta / (double)g.nk;
+  for (int blk = blockIdx.x; blk < total; blk += gridDim.x) {
+    const int ad = blk % n2;
+    const int v = (blk / n2) % nv;
+    const int w = blk / (n2 * nv);
+    const int a = ad / nb, d = ad - a * nb;
+    const int t1 = v + niw;      // G(nu)
+    const int t2 = v + niw - w;  // G(nu - w)
+    const double2* gad = g_r + (((size_t)t1 * nb + a) * nb + d) * g.nk;
+    for (int cb = 0; cb < n2; ++cb) {
+      const int c = cb / nb, b = cb - c * nb;
+      const double2* gcb = g_r + (((size_t)t2 * nb + c) * nb + b) * g.nk;
+      __syncthreads();
+      for (int r = threadIdx.x; r < g.nk; r += blockDim.x) {
+        const int x = r / nyz, rem = r - x * nyz, y = rem / g.nz, z = rem - y * g.nz;
+        const int xm = x ? g.nx - x : 0, ym = y ? g.ny - y : 0, zm = z ? g.nz - z : 0;
+        P[r] = cmul(gad[r], gcb[(xm * g.ny + ym) * g.nz + zm]);
+      }
+      __syncthreads();
+      // x axis in full (P -> T1)
+      {
+        const double2* twx = s_tw;
+        for (int e = threadIdx.x; e < g.nk; e += blockDim.x) {
+          const int kx = e / nyz, yz = e - kx * nyz;
+          double2 acc = make_double2(0.0, 0.0);
+          int m = 0;
+          for (int x = 0; x < g.nx; ++x) {
+            cfma(acc, P[x * nyz + yz], twx[m]);
+            m += kx;
+            if (m >= g.nx) m -= g.nx;
+          }
+          T1[e] = acc;
+        }
+      }
+      __syncthreads();
+      // y and z axes only at the irreducible q points
+      const double2* twy = s_tw + g.nx;
+      const double2* twz = s_tw + g.nx + g.ny;
+      for (int iq = threadIdx.x; iq < n_qirr; iq += blockDim.x) {
+        const int qx = s_q[3 * iq], qy = s_q[3 * iq + 1], qz = s_q[3 * iq + 2];
+        double2 acc = make_double2(0.0, 0.0);
+        int my = 0;
+        for (int y = 0; y < g.ny; ++y) {
+          double2 accz = make_double2(0.0, 0.0);
+          int mz = 0;
+          const double2* row = T1 + qx * nyz + y * g.nz;
+          for (int z = 0; z < g.nz; ++z) {
+            cfma(accz, row[z], twz[mz]);
+            mz += qz;
+            if (mz >= g.nz) mz -= g.nz;
+          }
+          cfma(acc, accz, twy[my]);
+          my += qy;
+          if (my >= g.ny) my -= g.ny;
+        }
+        double re = (acc.x * inv_nk) * pref;
+        double im = (acc.y * inv_nk) * pref;
+        if (fabs(re) < 1e-12 && fabs(im) < 1e-12) {
+          re = 0.0;
+          im = 0.0;
+        }
+        out[iq * os.q + w * os.w + v * os.v + a * os.a + b * os.b + c * os.c + d * os.d] = make_double2(re, im);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Sigma partial sums: CTA per (nu >= 0, i, j, w-chunk)
+//   kern: [Q][W][nv][n2][n2] irreducible kernel, matrix row (a,i), column (d,j); W = niw+1, nv = 2 niv
+//   g_r:  [T][n][n][Nk] with slot t = nu_index + niw, nu_index in [-niw, niv+niw)
+//   part: [n_chunks][niv][n2][Nk]
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(BZ_THREADS) sigma_partial_kernel(const double2* __restrict__ kern,
+                                                                    const double2* __restrict__ g_r, int nb, int niv,
+                                                                    int niw, int Q, Grid3 g,
+                                                                    const int* __restrict__ irrk_inv,
+                                                                    const double2* __restrict__ tw, int n_chunks,
+                                                                    double2* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* Pa = reinterpret_cast<double2*>(smem_raw);
+  double2* Pb = Pa + g.nk;
+  double2* s_tw = Pb + g.nk;
+  int* s_inv = reinterpret_cast<int*>(s_tw + g.nx + g.ny + g.nz);
+  load_twiddles(s_tw, tw, g);
+  for (int i = threadIdx.x; i < g.nk; i += blockDim.x) s_inv[i] = irrk_inv[i];
+
+  const int n2 = nb * nb, nv = 2 * niv, W = niw + 1, nwf = 2 * niw + 1;
+  const int per_chunk = (nwf + n_chunks - 1) / n_chunks;
+  const int total = niv * n2 * n_chunks;
+  constexpr int MAXR = BZ_MAX_NK / BZ_THREADS;
+  for (int blk = blockIdx.x; blk < total; blk += gridDim.x) {
+    const int chunk = blk % n_chunks;
+    const int ij = (blk / n_chunks) % n2;
+    const int v = blk / (n_chunks * n2);
+    const int i = ij / nb, j = ij - i * nb;
+    double2 acc[MAXR];
+#pragma unroll
+    for (int k = 0; k < MAXR; ++k) acc[k] = make_double2(0.0, 0.0);
+    const int wf0 = chunk * per_chunk, wf1 = min(nwf, wf0 + per_chunk);
+    for (int wf = wf0; wf < wf1; ++wf) {
+      const int w = wf - niw;
+      const bool neg = w < 0;
+      const int wa = neg ? -w : w;
+      const int vi = neg ? (niv - 1 - v) : (niv + v);
+      for (int ad = 0; ad < n2; ++ad) {
+        const int a = ad / nb, d = ad - a * nb;
+        const int row = a * nb + i, col = d * nb + j;
+        __syncthreads();
+        for (int r = threadIdx.x; r < g.nk; r += blockDim.x) {
+          double2 kv = kern[((((size_t)s_inv[r] * W + wa) * nv + vi) * n2 + row) * n2 + col];
+          if (neg) kv.y = -kv.y;
+          Pa[r] = kv;
+        }
+        __syncthreads();
+        plane_dft(Pa, Pb, s_tw, g);
+        const double2* gp = g_r + (((size_t)(v - w + niw) * nb + a) * nb + d) * g.nk;
+#pragma unroll
+        for (int k = 0; k < MAXR; ++k) {
+          const int r = threadIdx.x + k * BZ_THREADS;
+          if (r < g.nk) cfma(acc[k], gp[r], Pa[r]);
+        }
+      }
+    }
+    double2* o = part + (((size_t)chunk * niv + v) * n2 + ij) * g.nk;
+#pragma unroll
+    for (int k = 0; k < MAXR; ++k) {
+      const int r = threadIdx.x + k * BZ_THREADS;
+      if (r < g.nk) o[r] = acc[k];
+    }
+  }
+}
+
+// Neumaier-compensated sum over the chunk partials, times -1/2 / (beta Nk): sig_r[niv][n2][Nk]
+__global__ void sigma_reduce_kernel(const double2* __restrict__ part, int n_chunks, long long n_out, double factor,
+                                    double2* __restrict__ sig_r) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n_out;
+       e += (long long)gridDim.x * blockDim.x) {
+    double sr = 0.0, cr = 0.0, si = 0.0, ci = 0.0;
+    for (int c = 0; c < n_chunks; ++c) {
+      const double2 x = part[(size_t)c * n_out + e];
+      double t = sr + x.x;
+      cr += (fabs(sr) >= fabs(x.x)) ? (sr - t) + x.x : (x.x - t) + sr;
+      sr = t;
+      t = si + x.y;
+      ci += (fabs(si) >= fabs(x.y)) ? (si - t) + x.y : (x.y - t) + si;
+      si = t;
+    }
+    sig_r[e] = make_double2((sr + cr) * factor, (si + ci) * factor);
+  }
+}
+
+// Sigma(k) planes [niv][n][n][Nk] -> upstream layout [Nk][n][n][2 niv] with the nu < 0 half as
+// conj(Sigma(k, -nu-1)) (self_energy.py:109-120)
+__global__ void sigma_full_nu_kernel(const double2* __restrict__ sig_k, int nb, int niv, int nk,
+                                     double2* __restrict__ out) {
+  const int n2 = nb * nb;
+  const long long total = (long long)niv * n2 * nk;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e % nk);
+    const int ij = (int)((e / nk) % n2);
+    const int v = (int)(e / ((long long)nk * n2));
+    const double2 s = sig_k[e];
+    double2* o = out + ((size_t)r * n2 + ij) * 2 * niv;
+    o[niv + v] = s;
+    o[niv - 1 - v] = make_double2(s.x, -s.y);
+  }
+}
+
+}  // namespace dga
+
+using namespace dga;
+
+static int check_grid(int nx, int ny, int nz, const char* who) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nx > BZ_MAX_AXIS || ny > BZ_MAX_AXIS || nz > BZ_MAX_AXIS ||
+      nx * ny * nz > BZ_MAX_NK) {
+    dga_set_error("%s: unsupported momentum grid %dx%dx%d (at most %d points, %d per axis)", who, nx, ny, nz,
+                  BZ_MAX_NK, BZ_MAX_AXIS);
+    return DGA_ERR_ARG;
+  }
+  return DGA_OK;
+}
+
+static int launch_status(const char* who) {
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("%s: launch failed: %s", who, cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+static int grid_cap(long long work) {
+  long long g = work < 148LL * 8 ? work : 148LL * 8;
+  return (int)(g > 0 ? g : 1);
+}
+
+extern "C" {
+
+// Batched separable DFT of momentum planes.  tw holds nx + ny + nz FP64 twiddles e^{s 2 pi i m / n}
+// (the caller folds the sign s in); each plane is multiplied by `scale` on output.
+int dga_dft_planes_c128(const void* in, long long in_s_hi, long long in_s_lo, long long in_s_r, void* out,
+                        long long out_s_hi, long long out_s_lo, long long out_s_r, int n_lo, int n_planes, int nx,
+                        int ny, int nz, const void* tw, double scale, cudaStream_t stream) {
+  if (check_grid(nx, ny, nz, "dga_dft_planes_c128")) return DGA_ERR_ARG;
+  if (!in || !out || !tw || n_planes <= 0 || n_lo <= 0) {
+    dga_set_error("dga_dft_planes_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  Grid3 g{nx, ny, nz, nx * ny * nz};
+  PlaneAddr ia{in_s_hi, in_s_lo, in_s_r, n_lo}, oa{out_s_hi, out_s_lo, out_s_r, n_lo};
+  const size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2);
+  cudaFuncSetAttribute(dft_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dft_planes_kernel<<<grid_cap(n_planes), BZ_THREADS, smem, stream>>>((const double2*)in, ia, (double2*)out, oa,
+                                                                      n_planes, g, (const double2*)tw, scale);
+  return launch_status("dga_dft_planes_c128");
+}
+
+// Fused bubble.  g_r: [2 niv + niw][n][n][Nk] forward transforms of G(k) for nu indices [-niv-niw, niv);
+// q_irr: [n_qirr][3] index triples; tw: inverse-transform twiddles (e^{+2 pi i m/n}); out addressed by the
+// seven element strides (q, w, nu, a, b, c, d).
+int dga_bubble_c128(const void* g_r, int n_orb, int niv, int niw, int nx, int ny, int nz, const int* q_irr,
+                    int n_qirr, const void* tw, double beta, void* out, const long long* out_strides,
+                    cudaStream_t stream) {
+  if (check_grid(nx, ny, nz, "dga_bubble_c128")) return DGA_ERR_ARG;
+  if (!g_r || !q_irr || !tw || !out || !out_strides || n_orb <= 0 || niv <= 0 || niw < 0 || n_qirr <= 0) {
+    dga_set_error("dga_bubble_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  Grid3 g{nx, ny, nz, nx * ny * nz};
+  OutStrides7 os{out_strides[0], out_strides[1], out_strides[2], out_strides[3],
+                 out_strides[4], out_strides[5], out_strides[6]};
+  const size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + 3 * sizeof(int) * (size_t)n_qirr;
+  cudaFuncSetAttribute(bubble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long work = (long long)(niw + 1) * 2 * niv * n_orb * n_orb;
+  bubble_kernel<<<(int)(work < 148LL * 64 ? work : 148LL * 64), BZ_THREADS, smem, stream>>>(
+      (const double2*)g_r, n_orb, niv, niw, g, q_irr, n_qirr, (const double2*)tw, beta, (double2*)out, os);
+  return launch_status("dga_bubble_c128");
+}
+
+// Bytes of the partial-sum buffer of dga_sigma_c128.
+size_t dga_sigma_scratch_bytes(int n_orb, int niv, int nk, int n_chunks) {
+  return (size_t)n_chunks * niv * n_orb * n_orb * nk * sizeof(double2) * 2;
+}
+
+// Sigma(k, nu) from the irreducible kernel (nonlocal_sde.py:544-594 and 876-879).
+//   kern:   [Q][niw+1][2 niv][n2][n2] (row (a,i), column (d,j));  irrk_inv: [Nk]
+//   g_r:    [niv + 2 niw][n][n][Nk] forward transforms of G(k) for nu indices [-niw, niv + niw)
+//   tw_inv: e^{+2 pi i m / n} twiddles;  out: [Nk][n][n][2 niv] (upstream SelfEnergy layout)
+//   scratch: dga_sigma_scratch_bytes(n_orb, niv, Nk, n_chunks) bytes
+int dga_sigma_c128(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, int nx, int ny, int nz,
+                   const int* irrk_inv, const void* tw_inv, double beta, int n_chunks, void* out, void* scratch,
+                   size_t scratch_bytes, cudaStream_t stream) {
+  if (check_grid(nx, ny, nz, "dga_sigma_c128")) return DGA_ERR_ARG;
+  if (!kern || !g_r || !irrk_inv || !tw_inv || !out || !scratch || n_orb <= 0 || niv <= 0 || niw < 0 ||
+      n_chunks <= 0) {
+    dga_set_error("dga_sigma_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  Grid3 g{nx, ny, nz, nx * ny * nz};
+  const int n2 = n_orb * n_orb;
+  const size_t need = dga_sigma_scratch_bytes(n_orb, niv, g.nk, n_chunks);
+  if (scratch_bytes < need) {
+    dga_set_error("dga_sigma_c128: scratch too small (%zu < %zu)", scratch_bytes, need);
+    return DGA_ERR_SCRATCH;
+  }
+  double2* part = (double2*)scratch;
+  double2* sig = part + (size_t)n_chunks * niv * n2 * g.nk;
+  size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + sizeof(int) * (size_t)g.nk;
+  cudaFuncSetAttribute(sigma_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long work = (long long)niv * n2 * n_chunks;
+  sigma_partial_kernel<<<grid_cap(work), BZ_THREADS, smem, stream>>>(
+      (const double2*)kern, (const double2*)g_r, n_orb, niv, niw, n_q, g, irrk_inv, (const double2*)tw_inv, n_chunks,
+      part);
+  if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
+  const long long n_out = (long long)niv * n2 * g.nk;
+  const double factor = -0.5 / beta / (double)g.nk;
+  sigma_reduce_kernel<<<grid_cap((n_out + 255) / 256), 256, 0, stream>>>(part, n_chunks, n_out, factor, sig);
+  if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
+  // inverse transform over R (normalised 1/Nk), planes contiguous; result back into `part`
+  smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2);
+  cudaFuncSetAttribute(dft_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  PlaneAddr pa{(long long)g.nk, 0, 1, 1};
+  dft_planes_kernel<<<grid_cap(niv * n2), BZ_THREADS, smem, stream>>>(sig, pa, part, pa, niv * n2, g,
+                                                                      (const double2*)tw_inv, 1.0 / (double)g.nk);
+  if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
+  sigma_full_nu_kernel<<<grid_cap((n_out + 255) / 256), 256, 0, stream>>>(part, n_orb, niv, g.nk, (double2*)out);
+  return launch_status("dga_sigma_c128");
+}
+
+}  // extern "C"

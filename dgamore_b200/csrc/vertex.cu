@@ -1,0 +1,587 @@
+// Small-matrix stages of the ladder pass, all in the compound orbital basis [(o1,o2),(o4,o3)] where the
+// upstream einsums are plain n^2 x n^2 matrix products:
+//
+//   * dga_chi0_prep_c128:    chi0^-1(q,w,nu) per core nu (four_point.py:601-613) and the nu sums
+//                            chi0_full_sum, chi0_core_sum (nonlocal_sde.py:824-835);
+//   * dga_chi_phys_c128:     chi_r(q,w) = [(sum_nu X/beta + chi0_full - chi0_core)^-1 + U_r + V_r^q]^-1
+//                            (nonlocal_sde.py:167-182, 298) from the BSE output X;
+//   * dga_lambda_c128:       FP64 Newton root-find of the lambda-correction and its application
+//                            (lambda_correction.py:13-73);
+//   * dga_kernel_assembly_c128: gamma_r = beta chi0^-1 X (nonlocal_sde.py:159-164) and
+//                            K = -K_dc + K_dens + 3 K_magn with K_r = U_r (gamma - gamma U_r chi_r [- 2/3 1])
+//                            (nonlocal_sde.py:201-215, 841-853);
+//   * dga_dc_kernel_c128:    K_dc = ((U_adcb / beta^2) chi0) . F_dc cut to the core box (nonlocal_sde.py:185-198),
+//                            a batched complex GEMM over w.
+#include "dga_common.cuh"
+
+namespace dga {
+
+constexpr int MAX_N2 = 16;  // up to 4 orbitals
+
+// In-place Gauss-Jordan inverse of an n x n matrix with partial (row) pivoting on |re|+|im|; element (r, c)
+// at m[(r * n + c) * st].  Returns false on an exact zero pivot.
+__device__ bool gj_inverse(double2* m, int n, int st) {
+  int piv[MAX_N2];
+  bool ok = true;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = cabs1(m[(k * n + k) * st]);
+    for (int i = k + 1; i < n; ++i) {
+      const double v = cabs1(m[(i * n + k) * st]);
+      if (v > best) {
+        best = v;
+        p = i;
+      }
+    }
+    piv[k] = p;
+    if (p != k) {
+      for (int j = 0; j < n; ++j) {
+        double2 t = m[(k * n + j) * st];
+        m[(k * n + j) * st] = m[(p * n + j) * st];
+        m[(p * n + j) * st] = t;
+      }
+    }
+    double2 d = m[(k * n + k) * st];
+    if (d.x == 0.0 && d.y == 0.0) {
+      ok = false;
+      continue;
+    }
+    const double2 pinv = crecip(d);
+    m[(k * n + k) * st] = make_double2(1.0, 0.0);
+    for (int j = 0; j < n; ++j) m[(k * n + j) * st] = cmul(m[(k * n + j) * st], pinv);
+    for (int i = 0; i < n; ++i) {
+      if (i == k) continue;
+      const double2 f = m[(i * n + k) * st];
+      m[(i * n + k) * st] = make_double2(0.0, 0.0);
+      for (int j = 0; j < n; ++j) cfms(m[(i * n + j) * st], f, m[(k * n + j) * st]);
+    }
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const int p = piv[k];
+    if (p != k) {
+      for (int i = 0; i < n; ++i) {
+        double2 t = m[(i * n + k) * st];
+        m[(i * n + k) * st] = m[(i * n + p) * st];
+        m[(i * n + p) * st] = t;
+      }
+    }
+  }
+  return ok;
+}
+
+// c = a @ b for n x n matrices (row-major, contiguous)
+__device__ __forceinline__ void matmul_n(const double2* a, const double2* b, double2* c, int n) {
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int k = 0; k < n; ++k) cfma(acc, a[i * n + k], b[k * n + j]);
+      c[i * n + j] = acc;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// chi0 preparation: one thread per (q, w, nu_core); sums: one thread per (q, w)
+//   chi0: [Q][W][nvf][n2][n2] (device layout written by the bubble), core nu window [shell, shell + nv)
+// ------------------------------------------------------------------------------------------------
+__global__ void chi0_inverse_kernel(const double2* __restrict__ chi0, int n2, int nvf, int nv, int shell,
+                                    long long n_mats, double2* __restrict__ chi0_inv, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* s = reinterpret_cast<double2*>(smem_raw);
+  const int nn = n2 * n2;
+  const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const bool active = m < n_mats;
+  double2* mine = s + threadIdx.x;  // element e at mine[e * blockDim.x]
+  if (active) {
+    const long long qw = m / nv;
+    const int v = (int)(m - qw * nv);
+    const double2* src = chi0 + ((size_t)qw * nvf + shell + v) * nn;
+    for (int e = 0; e < nn; ++e) mine[e * blockDim.x] = src[e];
+    const bool ok = gj_inverse(mine, n2, blockDim.x);
+    double2* dst = chi0_inv + (size_t)m * nn;
+    for (int e = 0; e < nn; ++e) dst[e] = mine[e * blockDim.x];
+    if (!ok && status) atomicOr(status, DGA_ITEM_SINGULAR);
+  }
+}
+
+__global__ void chi0_sums_kernel(const double2* __restrict__ chi0, int n2, int nvf, int nv, int shell,
+                                 long long n_qw, double inv_beta, double2* __restrict__ full_sum,
+                                 double2* __restrict__ core_sum) {
+  const int nn = n2 * n2;
+  const long long total = n_qw * nn;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long qw = e / nn;
+    const int el = (int)(e - qw * nn);
+    const double2* base = chi0 + (size_t)qw * nvf * nn + el;
+    double fr = 0.0, fi = 0.0, cr = 0.0, ci = 0.0;
+    for (int v = 0; v < nvf; ++v) {
+      const double2 x = base[(size_t)v * nn];
+      fr += x.x;
+      fi += x.y;
+      if (v >= shell && v < shell + nv) {
+        cr += x.x;
+        ci += x.y;
+      }
+    }
+    // 1/beta * (1/beta * sum)  (nonlocal_sde.py:824, 835 with local_four_point.py:146-162)
+    full_sum[e] = make_double2(inv_beta * (inv_beta * fr), inv_beta * (inv_beta * fi));
+    core_sum[e] = make_double2(inv_beta * (inv_beta * cr), inv_beta * (inv_beta * ci));
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// physical susceptibility: one thread per (ch, q, w)
+//   X: [n_ch][Q][W][N][n2] with row i = p * nv + nu;  uv: [n_ch][Q][n2][n2];  sums: [Q][W][n2][n2]
+//   out: [n_ch][Q][W][n2][n2]
+// ------------------------------------------------------------------------------------------------
+__global__ void chi_phys_kernel(const double2* __restrict__ X, const double2* __restrict__ uv,
+                                const double2* __restrict__ full_sum, const double2* __restrict__ core_sum, int n2,
+                                int nv, int W, int Q, int n_ch, double inv_beta, double2* __restrict__ out,
+                                int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* s = reinterpret_cast<double2*>(smem_raw);
+  const int nn = n2 * n2;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long total = (long long)n_ch * Q * W;
+  if (t >= total) return;
+  const int w = (int)(t % W);
+  const int q = (int)((t / W) % Q);
+  const int ch = (int)(t / ((long long)W * Q));
+  double2* mine = s + threadIdx.x;
+  const int N = n2 * nv;
+  const double2* x = X + (size_t)t * N * n2;
+  const size_t qw = (size_t)q * W + w;
+  for (int p = 0; p < n2; ++p)
+    for (int sidx = 0; sidx < n2; ++sidx) {
+      double sr = 0.0, si = 0.0;
+      for (int v = 0; v < nv; ++v) {
+        const double2 y = x[(size_t)(p * nv + v) * n2 + sidx];
+        sr += y.x;
+        si += y.y;
+      }
+      // (sum / beta + full) - core
+      const double2 f = full_sum[qw * nn + p * n2 + sidx];
+      const double2 c = core_sum[qw * nn + p * n2 + sidx];
+      const double ar = inv_beta * sr + f.x, ai = inv_beta * si + f.y;
+      mine[(p * n2 + sidx) * blockDim.x] = make_double2(ar - c.x, ai - c.y);
+    }
+  bool ok = gj_inverse(mine, n2, blockDim.x);
+  const double2* u = uv + ((size_t)ch * Q + q) * nn;
+  for (int e = 0; e < nn; ++e) mine[e * blockDim.x] = cadd(mine[e * blockDim.x], u[e]);
+  ok = gj_inverse(mine, n2, blockDim.x) && ok;
+  double2* o = out + (size_t)t * nn;
+  for (int e = 0; e < nn; ++e) o[e] = mine[e * blockDim.x];
+  if (!ok && status) atomicOr(status, DGA_ITEM_SINGULAR);
+}
+
+// ------------------------------------------------------------------------------------------------
+// lambda correction (single band): one CTA per channel
+//   chi: [n_ch][Q][W] (n2 = 1), weights = irrk_count, target[ch] complex
+// ------------------------------------------------------------------------------------------------
+__device__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    v = lane < nw ? red[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) red[0] = v;
+  }
+  __syncthreads();
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+__device__ double block_min(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    v = lane < nw ? red[lane] : INFINITY;
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+    if (lane == 0) red[0] = v;
+  }
+  __syncthreads();
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void lambda_kernel(const double2* __restrict__ chi, int Q, int W, const long long* __restrict__ weights,
+                              const double2* __restrict__ target, double beta, double nk_tot, double delta0,
+                              double eps, int maxiter, double* __restrict__ lambda_out, int* __restrict__ iters_out,
+                              int* __restrict__ status, double2* __restrict__ chi_out) {
+  __shared__ double red[32];
+  const int ch = blockIdx.x;
+  const double2* c = chi + (size_t)ch * Q * W;
+  const int niw = W - 1, nwf = 2 * niw + 1;
+  const long long total = (long long)Q * nwf;
+  // lambda_start = -min_q 1 / Re chi(q, w = 0)
+  double mn = INFINITY;
+  for (int q = threadIdx.x; q < Q; q += blockDim.x) mn = fmin(mn, 1.0 / c[(size_t)q * W].x);
+  const double lam0 = -block_min(mn, red);
+  const double factor = 1.0 / beta / nk_tot;
+  const double2 tgt = target[ch];
+  double delta = delta0;
+  double lam = lam0 + delta;
+  double result = lam;
+  int it = 0, converged = 0;
+  for (; it < maxiter; ++it) {
+    double s1r = 0.0, s1i = 0.0, s2r = 0.0, s2i = 0.0;
+    for (long long e = threadIdx.x; e < total; e += blockDim.x) {
+      const int q = (int)(e / nwf);
+      const int wf = (int)(e - (long long)q * nwf);
+      const int w = wf - niw;
+      double2 x = c[(size_t)q * W + (w < 0 ? -w : w)];
+      if (w < 0) x.y = -x.y;
+      // chi_lam = 1 / (1 / chi + lam)
+      double2 inv = crecip(x);
+      inv.x += lam;
+      const double2 cl = crecip(inv);
+      const double wq = (double)weights[q];
+      s1r += wq * cl.x;
+      s1i += wq * cl.y;
+      const double2 cl2 = cmul(cl, cl);
+      s2r += wq * cl2.x;
+      s2i += wq * cl2.y;
+    }
+    s1r = block_sum(s1r, red);
+    s1i = block_sum(s1i, red);
+    s2r = block_sum(s2r, red);
+    s2i = block_sum(s2i, red);
+    const double2 f = make_double2(s1r * factor - tgt.x, s1i * factor - tgt.y);
+    const double2 fp = make_double2(-s2r * factor, -s2i * factor);
+    const double lam_new = lam - cdiv(f, fp).x;
+    if (fabs(f.x) < eps) {
+      result = lam_new;
+      converged = 1;
+      break;
+    }
+    // no root above lambda_start (e.g. a negative target): the Newton steps grow without bound; stop at the
+    // last finite iterate and report non-convergence instead of propagating inf/nan
+    if (!isfinite(lam_new)) break;
+    if (lam_new < lam) {
+      delta *= 0.5;
+      lam = lam0 + delta;
+    } else {
+      lam = lam_new;
+    }
+    result = lam;
+  }
+  if (threadIdx.x == 0) {
+    lambda_out[ch] = result;
+    if (iters_out) iters_out[ch] = it;
+    if (status && !converged) atomicOr(status, DGA_ITEM_NOCONVERGE);
+  }
+  // apply to the half range
+  for (int e = threadIdx.x; e < Q * W; e += blockDim.x) {
+    double2 inv = crecip(c[e]);
+    inv.x += result;
+    chi_out[(size_t)ch * Q * W + e] = crecip(inv);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// kernel assembly: one thread per (q, w, nu)
+//   chi0_inv: [Q][W][nv][n2][n2]; X: [2][Q][W][N][n2]; uv: [2][Q][n2][n2]; chi_phys: [2][Q][W][n2][n2]
+//   k_dc: [Q][W][nv][n2][n2] or null;  out K: [Q][W][nv][n2][n2];  gamma_out (optional): [2][Q][W][nv][n2][n2]
+// ------------------------------------------------------------------------------------------------
+__global__ void kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __restrict__ X,
+                                       const double2* __restrict__ uv, const double2* __restrict__ chi_phys,
+                                       const double2* __restrict__ k_dc, int n2, int nv, int W, int Q, double beta,
+                                       double2* __restrict__ K, double2* __restrict__ gamma_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nn = n2 * n2;
+  double2* s = reinterpret_cast<double2*>(smem_raw) + (size_t)threadIdx.x * 4 * nn;
+  double2* g3 = s;
+  double2* t1 = s + nn;
+  double2* t2 = s + 2 * nn;
+  double2* acc = s + 3 * nn;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long total = (long long)Q * W * nv;
+  if (t >= total) return;
+  const int v = (int)(t % nv);
+  const long long qw = t / nv;
+  const int q = (int)(qw / W);
+  const int N = n2 * nv;
+  const double2* c0i = chi0_inv + (size_t)t * nn;
+  if (k_dc) {
+    for (int e = 0; e < nn; ++e) {
+      const double2 z = k_dc[(size_t)t * nn + e];
+      acc[e] = make_double2(-z.x, -z.y);
+    }
+  } else {
+    for (int e = 0; e < nn; ++e) acc[e] = make_double2(0.0, 0.0);
+  }
+  for (int ch = 0; ch < 2; ++ch) {
+    const double2* x = X + ((size_t)ch * Q * W + qw) * N * n2;
+    // gamma = beta * (chi0_inv @ X_nu)
+    for (int p = 0; p < n2; ++p)
+      for (int sidx = 0; sidx < n2; ++sidx) {
+        double2 a = make_double2(0.0, 0.0);
+        for (int m = 0; m < n2; ++m) cfma(a, c0i[p * n2 + m], x[(size_t)(m * nv + v) * n2 + sidx]);
+        g3[p * n2 + sidx] = make_double2(beta * a.x, beta * a.y);
+      }
+    if (gamma_out) {
+      double2* go = gamma_out + ((size_t)ch * Q * W * nv + t) * nn;
+      for (int e = 0; e < nn; ++e) go[e] = g3[e];
+    }
+    const double2* u = uv + ((size_t)ch * Q + q) * nn;
+    const double2* cp = chi_phys + ((size_t)ch * Q * W + qw) * nn;
+    matmul_n(g3, u, t1, n2);   // gamma @ U_r
+    matmul_n(t1, cp, t2, n2);  // @ chi_r
+    for (int e = 0; e < nn; ++e) t1[e] = csub(g3[e], t2[e]);
+    if (ch == 1)
+      for (int p = 0; p < n2; ++p) t1[p * n2 + p].x += -(2.0 / 3.0);
+    matmul_n(u, t1, t2, n2);  // U_r @ (...)
+    const double f = ch == 0 ? 1.0 : 3.0;
+    for (int e = 0; e < nn; ++e) {
+      acc[e].x += f * t2[e].x;
+      acc[e].y += f * t2[e].y;
+    }
+  }
+  double2* o = K + (size_t)t * nn;
+  for (int e = 0; e < nn; ++e) o[e] = acc[e];
+}
+
+// ------------------------------------------------------------------------------------------------
+// K1 = (U_adcb / beta^2) @ chi0 for every (q, w, nu_full): one thread per matrix
+// ------------------------------------------------------------------------------------------------
+__global__ void dc_left_kernel(const double2* __restrict__ chi0, const double2* __restrict__ u_perm, int n2,
+                               long long n_mats, double2* __restrict__ k1) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_mats) return;
+  const int nn = n2 * n2;
+  const double2* c = chi0 + (size_t)t * nn;
+  double2* o = k1 + (size_t)t * nn;
+  for (int i = 0; i < n2; ++i)
+    for (int j = 0; j < n2; ++j) {
+      double2 a = make_double2(0.0, 0.0);
+      for (int k = 0; k < n2; ++k) cfma(a, u_perm[i * n2 + k], c[k * n2 + j]);
+      o[i * n2 + j] = a;
+    }
+}
+
+// Batched complex GEMM C = A @ B over w with two-level row/column addressing:
+//   A(r, k): r = (q, p) -> q*a_q + p*a_p;  k = (m, nu) -> m*a_m + nu*a_nu   (K1: [Q][W][nvf][n2][n2])
+//   B(k, c): row k = m*nvf + nu, column c = s*nv + nu'  (F_dc compound matrix [W][Nf][Nf], row-major)
+//   C(r, c): r = (q, p), c = (s, nu')  -> K_dc [Q][W][nv][n2][n2]
+struct DcGemmArgs {
+  const double2* k1;
+  const double2* fdc;
+  double2* out;
+  int Q, W, n2, nvf, nv, shell;
+};
+
+constexpr int DG_TM = 64, DG_TN = 64, DG_TK = 16;
+
+__global__ void __launch_bounds__(256) dc_gemm_kernel(DcGemmArgs a) {
+  __shared__ double2 As[DG_TK][DG_TM];
+  __shared__ double2 Bs[DG_TK][DG_TN];
+  const int w = blockIdx.z;
+  const int M = a.Q * a.n2, Kd = a.n2 * a.nvf, Nc = a.n2 * a.nv;
+  const int r0 = blockIdx.y * DG_TM, c0 = blockIdx.x * DG_TN;
+  const int tid = threadIdx.x, ty = tid & 15, tx = tid >> 4;
+  const int Nf = a.n2 * a.nvf;
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+  for (int k0 = 0; k0 < Kd; k0 += DG_TK) {
+    for (int e = tid; e < DG_TK * DG_TM; e += 256) {
+      const int r = e % DG_TM, kk = e / DG_TM;
+      const int row = r0 + r, k = k0 + kk;
+      double2 val = make_double2(0.0, 0.0);
+      if (row < M && k < Kd) {
+        const int q = row / a.n2, p = row - q * a.n2;
+        const int m = k / a.nvf, nu = k - m * a.nvf;
+        val = a.k1[((((size_t)q * a.W + w) * a.nvf + nu) * a.n2 + p) * a.n2 + m];
+      }
+      As[kk][r] = val;
+    }
+    for (int e = tid; e < DG_TK * DG_TN; e += 256) {
+      const int c = e % DG_TN, kk = e / DG_TN;
+      const int col = c0 + c, k = k0 + kk;
+      double2 val = make_double2(0.0, 0.0);
+      if (col < Nc && k < Kd) {
+        const int sidx = col / a.nv, nup = col - sidx * a.nv;
+        val = a.fdc[((size_t)w * Nf + k) * Nf + sidx * a.nvf + a.shell + nup];
+      }
+      Bs[kk][c] = val;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < DG_TK; ++kk) {
+      double2 av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cfma(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = r0 + ty + 16 * i;
+    if (row >= M) continue;
+    const int q = row / a.n2, p = row - q * a.n2;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int col = c0 + tx + 16 * j;
+      if (col >= Nc) continue;
+      const int sidx = col / a.nv, nup = col - sidx * a.nv;
+      a.out[((((size_t)q * a.W + w) * a.nv + nup) * a.n2 + p) * a.n2 + sidx] = acc[i][j];
+    }
+  }
+}
+
+}  // namespace dga
+
+using namespace dga;
+
+static int vstatus(const char* who) {
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("%s: launch failed: %s", who, cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+static int small_threads(int n2) {
+  // one thread per matrix with its n2 x n2 elements in shared memory (<= 96 KB per block)
+  int t = 128;
+  while (t > 32 && (size_t)t * n2 * n2 * sizeof(double2) > 96 * 1024) t >>= 1;
+  return t;
+}
+
+extern "C" {
+
+// chi0_inv: [Q][W][nv][n2][n2]; full_sum/core_sum: [Q][W][n2][n2]; chi0: [Q][W][nvf][n2][n2]
+int dga_chi0_prep_c128(const void* chi0, int n_orb, int niv_core, int niv_shell, int niw_half, int n_q, double beta,
+                       void* chi0_inv, void* full_sum, void* core_sum, int* status, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv_core, nvf = 2 * (niv_core + niv_shell);
+  if (!chi0 || !chi0_inv || !full_sum || !core_sum || n2 > MAX_N2 || n_orb <= 0 || niv_core <= 0 || n_q <= 0 ||
+      niw_half <= 0 || niv_shell < 0) {
+    dga_set_error("dga_chi0_prep_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const long long n_mats = (long long)n_q * niw_half * nv;
+  const int th = small_threads(n2);
+  const size_t smem = (size_t)th * n2 * n2 * sizeof(double2);
+  cudaFuncSetAttribute(chi0_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  chi0_inverse_kernel<<<(int)((n_mats + th - 1) / th), th, smem, stream>>>(
+      (const double2*)chi0, n2, nvf, nv, niv_shell, n_mats, (double2*)chi0_inv, status);
+  if (vstatus("dga_chi0_prep_c128")) return DGA_ERR_LAUNCH;
+  const long long n_qw = (long long)n_q * niw_half;
+  const long long work = n_qw * n2 * n2;
+  int blocks = (int)((work + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  chi0_sums_kernel<<<blocks, 256, 0, stream>>>((const double2*)chi0, n2, nvf, nv, niv_shell, n_qw, 1.0 / beta,
+                                               (double2*)full_sum, (double2*)core_sum);
+  return vstatus("dga_chi0_prep_c128");
+}
+
+int dga_chi_phys_c128(const void* X, const void* uv, const void* full_sum, const void* core_sum, int n_orb,
+                      int niv_core, int niw_half, int n_q, int n_ch, double beta, void* out, int* status,
+                      cudaStream_t stream) {
+  const int n2 = n_orb * n_orb;
+  if (!X || !uv || !full_sum || !core_sum || !out || n2 > MAX_N2 || n_orb <= 0 || n_ch <= 0) {
+    dga_set_error("dga_chi_phys_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const long long total = (long long)n_ch * n_q * niw_half;
+  const int th = small_threads(n2);
+  const size_t smem = (size_t)th * n2 * n2 * sizeof(double2);
+  cudaFuncSetAttribute(chi_phys_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  chi_phys_kernel<<<(int)((total + th - 1) / th), th, smem, stream>>>(
+      (const double2*)X, (const double2*)uv, (const double2*)full_sum, (const double2*)core_sum, n2, 2 * niv_core,
+      niw_half, n_q, n_ch, 1.0 / beta, (double2*)out, status);
+  return vstatus("dga_chi_phys_c128");
+}
+
+// Single-band lambda correction of n_ch channels (lambda_correction.py:28-73).  chi: [n_ch][Q][W] complex;
+// weights: [Q] int64 multiplicities; target: [n_ch] complex; lambda_out: [n_ch]; chi_out: [n_ch][Q][W].
+int dga_lambda_c128(const void* chi, int n_q, int niw_half, int n_ch, const long long* weights, const void* target,
+                    double beta, double nk_tot, double delta, double eps, int maxiter, double* lambda_out,
+                    int* iters_out, int* status, void* chi_out, cudaStream_t stream) {
+  if (!chi || !weights || !target || !lambda_out || !chi_out || n_q <= 0 || niw_half <= 0 || n_ch <= 0 ||
+      maxiter <= 0) {
+    dga_set_error("dga_lambda_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  lambda_kernel<<<n_ch, 1024, 0, stream>>>((const double2*)chi, n_q, niw_half, weights, (const double2*)target, beta,
+                                           nk_tot, delta, eps, maxiter, lambda_out, iters_out, status,
+                                           (double2*)chi_out);
+  return vstatus("dga_lambda_c128");
+}
+
+int dga_kernel_assembly_c128(const void* chi0_inv, const void* X, const void* uv, const void* chi_phys,
+                             const void* k_dc, int n_orb, int niv_core, int niw_half, int n_q, double beta, void* K,
+                             void* gamma_out, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb;
+  if (!chi0_inv || !X || !uv || !chi_phys || !K || n2 > MAX_N2 || n_orb <= 0) {
+    dga_set_error("dga_kernel_assembly_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const long long total = (long long)n_q * niw_half * 2 * niv_core;
+  int th = 64;
+  while (th > 8 && (size_t)th * 4 * n2 * n2 * sizeof(double2) > 96 * 1024) th >>= 1;
+  const size_t smem = (size_t)th * 4 * n2 * n2 * sizeof(double2);
+  cudaFuncSetAttribute(kernel_assembly_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel_assembly_kernel<<<(int)((total + th - 1) / th), th, smem, stream>>>(
+      (const double2*)chi0_inv, (const double2*)X, (const double2*)uv, (const double2*)chi_phys,
+      (const double2*)k_dc, n2, 2 * niv_core, niw_half, n_q, beta, (double2*)K, (double2*)gamma_out);
+  return vstatus("dga_kernel_assembly_c128");
+}
+
+// Bytes of the K1 intermediate of dga_dc_kernel_c128.
+size_t dga_dc_scratch_bytes(int n_orb, int niv_full, int niw_half, int n_q) {
+  return (size_t)n_q * niw_half * 2 * niv_full * n_orb * n_orb * n_orb * n_orb * sizeof(double2);
+}
+
+// K_dc [Q][W][nv][n2][n2] from chi0 [Q][W][nvf][n2][n2], u_perm = compound matrix of U_adcb / beta^2
+// [n2][n2] and F_dc [W][Nf][Nf] (compound row (d,c,nu), column (f,e,nu'), Nf = n2 * nvf).
+int dga_dc_kernel_c128(const void* chi0, const void* u_perm, const void* fdc, int n_orb, int niv_core, int niv_shell,
+                       int niw_half, int n_q, void* k_dc, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv_core, nvf = 2 * (niv_core + niv_shell);
+  if (!chi0 || !u_perm || !fdc || !k_dc || !scratch || n2 > MAX_N2 || n_orb <= 0) {
+    dga_set_error("dga_dc_kernel_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  if (scratch_bytes < dga_dc_scratch_bytes(n_orb, niv_core + niv_shell, niw_half, n_q)) {
+    dga_set_error("dga_dc_kernel_c128: scratch too small");
+    return DGA_ERR_SCRATCH;
+  }
+  const long long n_mats = (long long)n_q * niw_half * nvf;
+  dc_left_kernel<<<(int)((n_mats + 127) / 128), 128, 0, stream>>>((const double2*)chi0, (const double2*)u_perm, n2,
+                                                                  n_mats, (double2*)scratch);
+  if (vstatus("dga_dc_kernel_c128")) return DGA_ERR_LAUNCH;
+  DcGemmArgs a;
+  a.k1 = (const double2*)scratch;
+  a.fdc = (const double2*)fdc;
+  a.out = (double2*)k_dc;
+  a.Q = n_q;
+  a.W = niw_half;
+  a.n2 = n2;
+  a.nvf = nvf;
+  a.nv = nv;
+  a.shell = niv_shell;
+  dim3 grid((n2 * nv + DG_TN - 1) / DG_TN, (n_q * n2 + DG_TM - 1) / DG_TM, niw_half);
+  dc_gemm_kernel<<<grid, 256, 0, stream>>>(a);
+  return vstatus("dga_dc_kernel_c128");
+}
+
+}  // extern "C"

@@ -1,0 +1,326 @@
+"""Device-resident nonlocal ladder-DGA pass on one B200.
+
+One pass replays the hot path of ``nonlocal_sde.calculate_self_energy_q`` (dgamore/nonlocal_sde.py:786-879)
+entirely on the device, with every stage a libdga_b200 kernel enqueued on one CUDA stream:
+
+    G(k) --DFT--> G(R) --bubble--> chi0(q_irr, w, nu) --prep--> chi0^-1, nu sums
+    chi0, F_dc --dc GEMM--> K_dc
+    chi0^-1, Gamma_r(w), U_r + V_r^q --BSE (dens, magn)--> X = sum_nu' chi* / beta
+    X --shell correction--> chi_r(q, w) --lambda (single band)--> chi_r^lambda
+    chi0^-1, X, chi_r --assembly--> K = -K_dc + K_d + 3 K_m
+    K, G(R) --Sigma contraction + inverse DFT--> Sigma(k, nu)
+
+Inputs stay resident between passes (``LadderPass.upload``), so a pass needs only the device-side work;
+``run_e2e`` adds the host->device copy of G(k) and the device->host copy of Sigma.  PyTorch is used for
+device memory and the stream only.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from ._lib import call, lib, ll_array
+
+C128 = torch.complex128
+
+
+def _p(t: torch.Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _s() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def twiddles(nk: tuple, sign: int) -> np.ndarray:
+    """e^{sign 2 pi i m / n} for each axis, concatenated (x, y, z), in FP64."""
+    parts = [np.exp(sign * 2j * np.pi * np.arange(n) / n) for n in nk]
+    return np.concatenate(parts).astype(np.complex128)
+
+
+def compound_orb(x: np.ndarray) -> np.ndarray:
+    """[..., a, b, c, d] -> [..., (a,b), (d,c)] compound orbital matrices."""
+    nb = x.shape[-1]
+    return np.swapaxes(x, -1, -2).reshape(*x.shape[:-4], nb * nb, nb * nb)
+
+
+def u_channel(u: np.ndarray, channel: str) -> np.ndarray:
+    """Local interaction in a spin channel (dgamore/interaction.py:43-65)."""
+    u_adcb = np.einsum("abcd->adcb", u)
+    return 2 * u - u_adcb if channel == "dens" else -u_adcb
+
+
+def v_channel(v: np.ndarray, channel: str) -> np.ndarray:
+    """Non-local interaction in a spin channel (dgamore/interaction.py:160-182)."""
+    return 2 * v if channel == "dens" else 0 * v
+
+
+@dataclass
+class PassShapes:
+    n_orb: int
+    nk: tuple
+    beta: float
+    niw: int
+    niv: int
+    niv_shell: int
+    n_q: int
+    niv_g: int
+
+    @property
+    def n2(self):
+        return self.n_orb * self.n_orb
+
+    @property
+    def W(self):
+        return self.niw + 1
+
+    @property
+    def nv(self):
+        return 2 * self.niv
+
+    @property
+    def nvf(self):
+        return 2 * (self.niv + self.niv_shell)
+
+    @property
+    def N(self):
+        return self.n2 * self.nv
+
+    @property
+    def nk_tot(self):
+        return int(np.prod(self.nk))
+
+    @property
+    def n_solves(self) -> int:
+        """(q, w) ladder solves of one pass: irreducible q x (niw+1) x 2 channels."""
+        return self.n_q * self.W * 2
+
+
+class LadderPass:
+    """Resident inputs, work buffers and the kernel sequence of one nonlocal pass."""
+
+    def __init__(self, inp: dict, device: str = "cuda", do_lambda: bool | None = None, sigma_chunks: int | None = None,
+                 keep_intermediates: bool = True):
+        lib()  # fail loudly before anything else if the CUDA library is missing
+        self.dev = torch.device(device)
+        g_k = np.asarray(inp["g_k"])
+        u = np.asarray(inp["u"], dtype=np.complex128)
+        n_orb = u.shape[0]
+        nk = tuple(int(x) for x in inp["nk"])
+        self.sh = PassShapes(
+            n_orb=n_orb, nk=nk, beta=float(inp["beta"]), niw=int(inp["niw"]), niv=int(inp["niv_core"]),
+            niv_shell=int(inp["niv_shell"]), n_q=len(inp["irrk_ind"]), niv_g=g_k.shape[-1] // 2,
+        )
+        sh = self.sh
+        if sh.niv_g < sh.niv + sh.niv_shell + sh.niw:
+            raise ValueError("G(k) must hold at least niv_full + niw fermionic frequencies")
+        self.do_lambda = (n_orb == 1) if do_lambda is None else bool(do_lambda)
+        if self.do_lambda and n_orb != 1:
+            raise NotImplementedError("the lambda-correction is single-band only (dgamore/DGAmore.py:501-508)")
+        self.keep = keep_intermediates
+        dev = self.dev
+        beta = sh.beta
+        # ---------------- host-side preparation (once per request) ----------------
+        irr = np.asarray(inp["irrk_ind"])
+        q_list = np.array(np.unravel_index(irr, nk)).T.astype(np.int32)
+        self.q_irr = torch.from_numpy(np.ascontiguousarray(q_list)).to(dev)
+        self.irrk_inv = torch.from_numpy(np.asarray(inp["irrk_inv"], dtype=np.int32)).to(dev)
+        self.irrk_count = torch.from_numpy(np.asarray(inp["irrk_count"], dtype=np.int64)).to(dev)
+        self.tw_fwd = torch.from_numpy(twiddles(nk, -1)).to(dev)
+        self.tw_inv = torch.from_numpy(twiddles(nk, +1)).to(dev)
+        v_irr = np.asarray(inp["v_q_irr"], dtype=np.complex128)
+        uv = np.stack([compound_orb(v_channel(v_irr, ch) + u_channel(u, ch)[None]) for ch in ("dens", "magn")])
+        self.uv = torch.from_numpy(np.ascontiguousarray(uv)).to(dev)
+        u_perm = np.einsum("abcd->adcb", u) * (1.0 / beta**2)
+        self.u_perm = torch.from_numpy(np.ascontiguousarray(compound_orb(u_perm))).to(dev)
+        self.inv_beta2 = 1.0 / beta**2
+        self.targets = torch.tensor(
+            [complex(inp.get("chi_loc_sum_dens", 0)), complex(inp.get("chi_loc_sum_magn", 0))], dtype=C128, device=dev
+        )
+        # Gamma_r (upstream layout) -> column-major compound [ch][W][N][N]
+        n, nv, W, N = sh.n_orb, sh.nv, sh.W, sh.N
+        self.gamma_cm = torch.empty((2, W, N, N), dtype=C128, device=dev)
+        for ich, ch in enumerate(("dens", "magn")):
+            g_ref = torch.from_numpy(np.ascontiguousarray(inp[f"gamma_{ch}"], dtype=np.complex128)).to(dev)
+            src_strides = list(g_ref.stride())
+            dst = self.gamma_cm[ich]
+            # dims (a, b, c, d, w, nu, nu')
+            dst_strides = [n * nv, nv, nv * N, n * nv * N, N * N, 1, N]
+            call("dga_strided_copy_c128", _p(g_ref), _p(dst), 7, ll_array(g_ref.shape), ll_array(src_strides),
+                 ll_array(dst_strides), 1.0, _s())
+        # F_dc (upstream [d,c,e,f,w,nu,nu']) -> row-major compound [W][Nf][Nf]
+        nvf = sh.nvf
+        Nf = sh.n2 * nvf
+        f_ref = torch.from_numpy(np.ascontiguousarray(inp["f_dc"], dtype=np.complex128)).to(dev)
+        self.fdc = torch.empty((W, Nf, Nf), dtype=C128, device=dev)
+        call("dga_strided_copy_c128", _p(f_ref), _p(self.fdc), 7, ll_array(f_ref.shape), ll_array(list(f_ref.stride())),
+             ll_array([n * nvf * Nf, nvf * Nf, nvf, n * nvf, Nf * Nf, Nf, 1]), 1.0, _s())
+        del f_ref
+        # resident G(k) and work list
+        self.g_k = torch.from_numpy(np.ascontiguousarray(g_k, dtype=np.complex128).reshape(sh.nk_tot, n, n, -1)).to(dev)
+        work = [(ch, q, w) for w in range(W) for ch in range(2) for q in range(sh.n_q)]
+        self.work = torch.tensor(work, dtype=torch.int32, device=dev)
+        self.n_items = len(work)
+        # ---------------- work buffers ----------------
+        Q, n2, nk_tot = sh.n_q, sh.n2, sh.nk_tot
+        t_b = 2 * (sh.niv + sh.niv_shell) // 2 * 2 + sh.niw  # slots [-niv_full - niw, niv_full)
+        self.t_bubble = nvf + sh.niw
+        self.g_r_bubble = torch.empty((self.t_bubble, n, n, nk_tot), dtype=C128, device=dev)
+        self.t_sigma = sh.niv + 2 * sh.niw
+        self.g_r_sigma = torch.empty((self.t_sigma, n, n, nk_tot), dtype=C128, device=dev)
+        self.chi0 = torch.empty((Q, W, nvf, n2, n2), dtype=C128, device=dev)
+        self.chi0_inv = torch.empty((Q, W, nv, n2, n2), dtype=C128, device=dev)
+        self.full_sum = torch.empty((Q, W, n2, n2), dtype=C128, device=dev)
+        self.core_sum = torch.empty((Q, W, n2, n2), dtype=C128, device=dev)
+        self.k_dc = torch.empty((Q, W, nv, n2, n2), dtype=C128, device=dev)
+        self.dc_scratch = torch.empty(
+            int(lib().dga_dc_scratch_bytes(n, sh.niv + sh.niv_shell, W, Q)) // 16 + 1, dtype=C128, device=dev
+        )
+        self.X = torch.empty((2, Q, W, N, n2), dtype=C128, device=dev)
+        self.bse_status = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
+        self.bse_scratch_bytes = int(lib().dga_bse_scratch_bytes(N, n2, self.n_items))
+        self.bse_scratch = torch.empty(self.bse_scratch_bytes // 16 + 1, dtype=C128, device=dev)
+        self.chi_phys = torch.empty((2, Q, W, n2, n2), dtype=C128, device=dev)
+        self.chi_lam = torch.empty((2, Q, W, n2, n2), dtype=C128, device=dev)
+        self.lambdas = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.lambda_iters = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(4, dtype=torch.int32, device=dev)
+        self.K = torch.empty((Q, W, nv, n2, n2), dtype=C128, device=dev)
+        self.gamma3 = torch.empty((2, Q, W, nv, n2, n2), dtype=C128, device=dev) if keep_intermediates else None
+        if sigma_chunks is None:
+            # enough (nu, i, j, w-chunk) CTAs to fill 148 SMs twice
+            base = sh.niv * n2
+            sigma_chunks = max(1, min(2 * sh.niw + 1, -(-296 // base)))
+        self.sigma_chunks = sigma_chunks
+        self.sigma_scratch_bytes = int(lib().dga_sigma_scratch_bytes(n, sh.niv, nk_tot, sigma_chunks))
+        self.sigma_scratch = torch.empty(self.sigma_scratch_bytes // 16 + 1, dtype=C128, device=dev)
+        self.sigma = torch.empty((nk_tot, n, n, 2 * sh.niv), dtype=C128, device=dev)
+        self.g_k_host = torch.from_numpy(np.ascontiguousarray(g_k, dtype=np.complex128).reshape(sh.nk_tot, n, n, -1)).pin_memory()
+        self.sigma_host = torch.empty(self.sigma.shape, dtype=C128).pin_memory()
+
+    # ------------------------------------------------------------------------------------------
+    def _g_transform(self, out: torch.Tensor, nu_first: int, n_slots: int):
+        """out[t][a][b][R] = sum_k G(k)[a][b][nu_first + t] e^{-ikR} (forward transform, n_point_base.py:509-529)."""
+        sh = self.sh
+        n, nvg2 = sh.n_orb, 2 * sh.niv_g
+        base = self.g_k[..., sh.niv_g + nu_first :]
+        nx, ny, nz = sh.nk
+        call("dga_dft_planes_c128", _p(base), 1, nvg2, n * n * nvg2, _p(out), n * n * sh.nk_tot, sh.nk_tot, 1,
+             n * n, n_slots * n * n, nx, ny, nz, _p(self.tw_fwd), 1.0, _s())
+
+    def bubble(self):
+        sh = self.sh
+        n, n2, W, nvf = sh.n_orb, sh.n2, sh.W, sh.nvf
+        self._g_transform(self.g_r_bubble, -(nvf // 2) - sh.niw, self.t_bubble)
+        strides = [W * nvf * n2 * n2, nvf * n2 * n2, n2 * n2, n * n2, n2, 1, n]  # q w nu a b c d
+        nx, ny, nz = sh.nk
+        call("dga_bubble_c128", _p(self.g_r_bubble), n, nvf // 2, sh.niw, nx, ny, nz, _p(self.q_irr), sh.n_q,
+             _p(self.tw_inv), sh.beta, _p(self.chi0), ll_array(strides), _s())
+
+    def chi0_prep(self):
+        sh = self.sh
+        call("dga_chi0_prep_c128", _p(self.chi0), sh.n_orb, sh.niv, sh.niv_shell, sh.W, sh.n_q, sh.beta,
+             _p(self.chi0_inv), _p(self.full_sum), _p(self.core_sum), _p(self.status), _s())
+
+    def dc_kernel(self):
+        sh = self.sh
+        call("dga_dc_kernel_c128", _p(self.chi0), _p(self.u_perm), _p(self.fdc), sh.n_orb, sh.niv, sh.niv_shell, sh.W,
+             sh.n_q, _p(self.k_dc), _p(self.dc_scratch), self.dc_scratch.numel() * 16, _s())
+
+    def bse(self):
+        sh = self.sh
+        call("dga_bse_solve_sum_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2, _p(self.gamma_cm),
+             _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, _p(self.X), _p(self.bse_status),
+             _p(self.bse_scratch), self.bse_scratch.numel() * 16, _s())
+
+    def chi_phys_stage(self):
+        sh = self.sh
+        call("dga_chi_phys_c128", _p(self.X), _p(self.uv), _p(self.full_sum), _p(self.core_sum), sh.n_orb, sh.niv,
+             sh.W, sh.n_q, 2, sh.beta, _p(self.chi_phys), _p(self.status), _s())
+
+    def lambda_stage(self):
+        sh = self.sh
+        if not self.do_lambda:
+            return self.chi_phys
+        call("dga_lambda_c128", _p(self.chi_phys), sh.n_q, sh.W, 2, _p(self.irrk_count), _p(self.targets), sh.beta,
+             float(sh.nk_tot), 0.1, 1e-7, 1000, _p(self.lambdas), _p(self.lambda_iters), _p(self.status[1:]),
+             _p(self.chi_lam), _s())
+        return self.chi_lam
+
+    def kernel_stage(self, chi_r: torch.Tensor):
+        sh = self.sh
+        call("dga_kernel_assembly_c128", _p(self.chi0_inv), _p(self.X), _p(self.uv), _p(chi_r), _p(self.k_dc),
+             sh.n_orb, sh.niv, sh.W, sh.n_q, sh.beta, _p(self.K),
+             _p(self.gamma3) if self.gamma3 is not None else ctypes.c_void_p(0), _s())
+
+    def sigma_stage(self):
+        sh = self.sh
+        self._g_transform(self.g_r_sigma, -sh.niw, self.t_sigma)
+        nx, ny, nz = sh.nk
+        call("dga_sigma_c128", _p(self.K), _p(self.g_r_sigma), sh.n_orb, sh.niv, sh.niw, sh.n_q, nx, ny, nz,
+             _p(self.irrk_inv), _p(self.tw_inv), sh.beta, self.sigma_chunks, _p(self.sigma), _p(self.sigma_scratch),
+             self.sigma_scratch.numel() * 16, _s())
+
+    def run(self):
+        """One device pass over the resident inputs (no host transfers, no synchronisation)."""
+        self.status.zero_()
+        self.bubble()
+        self.dc_kernel()
+        self.chi0_prep()
+        self.bse()
+        self.chi_phys_stage()
+        chi_r = self.lambda_stage()
+        self.kernel_stage(chi_r)
+        self.sigma_stage()
+        return self.sigma
+
+    def run_e2e(self) -> np.ndarray:
+        """Host G(k) in, host Sigma(k, nu) out: H2D copy, one pass, D2H copy (synchronises)."""
+        self.g_k.copy_(self.g_k_host, non_blocking=True)
+        self.run()
+        self.sigma_host.copy_(self.sigma, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.sigma_host.numpy()
+
+    @property
+    def h2d_bytes(self) -> int:
+        return self.g_k_host.numel() * 16
+
+    @property
+    def d2h_bytes(self) -> int:
+        return self.sigma_host.numel() * 16
+
+    # ------------------------------------------------------------------------------------------
+    # conversions of device intermediates to the upstream layouts (for tests)
+    # ------------------------------------------------------------------------------------------
+    def chi0_ref_layout(self) -> np.ndarray:
+        """[Q][W][nvf][(a,b)][(d,c)] -> [q,a,b,c,d,w,nu]."""
+        sh = self.sh
+        n = sh.n_orb
+        x = self.chi0.cpu().numpy().reshape(sh.n_q, sh.W, sh.nvf, n, n, n, n)  # q w v a b d c
+        return x.transpose(0, 3, 4, 6, 5, 1, 2)
+
+    def orbmat_ref_layout(self, t: torch.Tensor) -> np.ndarray:
+        """[Q][W][nv][(a,b)][(d,c)] -> [q,a,b,c,d,w,nu]."""
+        sh = self.sh
+        n = sh.n_orb
+        x = t.cpu().numpy().reshape(t.shape[0], t.shape[1], t.shape[2], n, n, n, n)
+        return x.transpose(0, 3, 4, 6, 5, 1, 2)
+
+    def x_ref_layout(self, ch: int) -> np.ndarray:
+        """X[ch][Q][W][(o1,o2,nu)][(o4,o3)] -> [q,o1,o2,o3,o4,w,nu]."""
+        sh = self.sh
+        n = sh.n_orb
+        x = self.X[ch].cpu().numpy().reshape(sh.n_q, sh.W, n, n, sh.nv, n, n)  # q w o1 o2 nu o4 o3
+        return x.transpose(0, 2, 3, 6, 5, 1, 4)
+
+    def chi_phys_ref_layout(self, t: torch.Tensor, ch: int) -> np.ndarray:
+        """[2][Q][W][(a,b)][(d,c)] -> [q,a,b,c,d,w]."""
+        sh = self.sh
+        n = sh.n_orb
+        x = t[ch].cpu().numpy().reshape(sh.n_q, sh.W, n, n, n, n)
+        return x.transpose(0, 2, 3, 5, 4, 1)

@@ -13,9 +13,10 @@ model, deterministically from a seed:
   compound orbital basis + a seeded complex Gaussian perturbation of relative size 1e-3, symmetrised under
   (nu <-> nu', orbitals abcd -> cdab) as ``symmetrize_v_vp`` (dgamore/local_four_point.py:588-597) and under the
   w=0 conjugation rule F(-w) = conj(flip F(w)) (dgamore/local_n_point.py:218-220);
-* local susceptibility chi_r,loc = (chi0_loc^-1 + Gamma_r / beta^2)^-1 (the local BSE of
-  dgamore/local_sde.py:40-51 read backwards), giving the lambda-correction targets and the local full vertex
-  F_magn = beta^2 (chi0^-1 - chi0^-1 chi_m chi0^-1) used by the double-counting kernel.
+* local susceptibility in the same asymptotic form the nonlocal pass uses: chi*_loc = (chi0_loc^-1 +
+  (Gamma_r - U_r)/beta^2)^-1 and chi_r,loc(w) = [(sum chi*_loc / beta^2)^-1 + U_r]^-1 (dgamore/nonlocal_sde.py:
+  85-96 and 167-182 without momentum), giving the lambda-correction targets sum_w chi_r,loc / beta, and the local
+  vertex F_magn = beta^2 (chi0^-1 - chi0^-1 chi*_m chi0^-1) used by the double-counting kernel.
 
 Array layouts are the upstream ones (see ``oracle/ladder.py``); everything is complex128.
 """
@@ -79,7 +80,7 @@ CONFIGS = {
     "c4_bilayer": DgaConfig("c4_bilayer", 2, (48, 48, 1), 15.0, 30, 30, 0, u=6.0, t=(1.0, 1.0), t_perp=0.8, n=1.8, seed=4),
     "c4_single": DgaConfig("c4_single", 1, (32, 32, 1), 12.5, 50, 50, 0, u=8.0, t=(1.0,), tp=-0.25, n=0.85, seed=5),
     # small cases for parity tests
-    "t1": DgaConfig("t1", 1, (4, 4, 1), 12.5, 4, 4, 2, u=8.0, t=(1.0,), tp=-0.25, v_nn=0.3, n=0.85, seed=11),
+    "t1": DgaConfig("t1", 1, (4, 4, 1), 12.5, 4, 4, 2, u=5.0, t=(1.0,), tp=-0.25, v_nn=0.3, n=0.85, seed=11),
     "t1b": DgaConfig("t1b", 1, (8, 8, 1), 10.0, 6, 6, 0, u=4.0, t=(1.0,), tp=-0.2, n=0.9, seed=12),
     "t2": DgaConfig("t2", 2, (4, 4, 1), 15.0, 2, 3, 1, u=6.0, t=(1.0, 1.0), t_perp=0.8, v_nn=0.2, n=1.8, seed=13),
     "t3": DgaConfig("t3", 3, (4, 4, 1), 20.0, 2, 2, 0, u=2.3, j=0.4, t=(0.5, 0.5, 0.1), n=1.0, seed=14),
@@ -178,9 +179,9 @@ def find_mu(cfg: DgaConfig, ek: np.ndarray) -> float:
     """Bisection of the filling in mu."""
     lo, hi = -4 * cfg.u - 10, 4 * cfg.u + 10
     fn = lambda m, nv: hubbard_i_sigma(cfg, m, nv)
-    for _ in range(50):
+    for _ in range(40):
         mid = 0.5 * (lo + hi)
-        if filling(ek, fn, mid, cfg.beta, 200) < cfg.n:
+        if filling(ek, fn, mid, cfg.beta, 64) < cfg.n:
             lo = mid
         else:
             hi = mid
@@ -247,10 +248,10 @@ def local_bubble(g_loc: np.ndarray, niw: int, niv: int, beta: float) -> np.ndarr
     return out
 
 
-def local_chi_and_f(chi0_loc: np.ndarray, gamma: np.ndarray, beta: float):
-    """Local generalized chi_r = (chi0^-1 + Gamma/beta^2)^-1 and F_r = beta^2 (chi0^-1 - chi0^-1 chi_r chi0^-1).
+def local_chi_and_f(chi0_loc: np.ndarray, gamma: np.ndarray, beta: float, u_r: np.ndarray):
+    """Local auxiliary chi* = (chi0^-1 + (Gamma - U_r)/beta^2)^-1, physical chi and F = beta^2 (chi0^-1 - chi0^-1 chi* chi0^-1).
 
-    Returns (chi_r_phys [a,b,c,d,w] = sum_{nu nu'} chi_r / beta^2, F_r [a,b,c,d,w,nu,nu']).
+    Returns (chi_r_phys [a,b,c,d,w] = [(sum_{nu nu'} chi*/beta^2)^-1 + U_r]^-1, F_r [a,b,c,d,w,nu,nu']).
     """
     nb = chi0_loc.shape[0]
     w_dim, nv = chi0_loc.shape[4], chi0_loc.shape[5]
@@ -263,11 +264,13 @@ def local_chi_and_f(chi0_loc: np.ndarray, gamma: np.ndarray, beta: float):
         c0_full = c0[..., :, None] * eye_v  # [a,b,c,d,nu,nu']
         c0m = c0_full.transpose(0, 1, 4, 3, 2, 5).reshape(n, n)
         c0inv = np.linalg.inv(c0m)
-        gm = gamma[..., iw, :, :].transpose(0, 1, 4, 3, 2, 5).reshape(n, n)
+        gm = (gamma[..., iw, :, :] - u_r[..., None, None]).transpose(0, 1, 4, 3, 2, 5).reshape(n, n)
         chi = np.linalg.inv(c0inv + gm / beta**2)
         fm = beta**2 * (c0inv - c0inv @ chi @ c0inv)
-        chi6 = chi.reshape(nb, nb, nv, nb, nb, nv)
-        chi_phys[..., iw] = chi6.sum(axis=(2, 5)).transpose(0, 1, 3, 2) / beta**2
+        aux = chi.reshape(nb, nb, nv, nb, nb, nv).sum(axis=(2, 5)) / beta**2  # [o1,o2,o4,o3]
+        um = np.swapaxes(u_r, 2, 3).reshape(nb * nb, nb * nb)
+        phys = np.linalg.inv(np.linalg.inv(aux.reshape(nb * nb, nb * nb)) + um)
+        chi_phys[..., iw] = phys.reshape(nb, nb, nb, nb).transpose(0, 1, 3, 2)
         f[..., iw, :, :] = fm.reshape(nb, nb, nv, nb, nb, nv).transpose(0, 1, 4, 3, 2, 5)
     return chi_phys, f
 
@@ -325,12 +328,12 @@ def make_inputs(cfg: DgaConfig | str) -> dict:
     for ch in ("dens", "magn"):
         gamma = gamma_model(cfg, u, ch, rng, cfg.niv)
         out[f"gamma_{ch}"] = gamma
-        chi_phys, _ = local_chi_and_f(chi0_loc_core, gamma, cfg.beta)
+        chi_phys, _ = local_chi_and_f(chi0_loc_core, gamma, cfg.beta, u_channel(u, ch))
         full = np.concatenate([np.conj(np.flip(chi_phys[..., 1:], axis=-1)), chi_phys], axis=-1)
         out[f"chi_loc_sum_{ch}"] = complex(full.sum() / cfg.beta)
         if ch == "magn":
             g_pad = pad_with_u(gamma, u_channel(u, ch), cfg.niv_full)
-            _, f_magn = local_chi_and_f(chi0_loc_full, g_pad, cfg.beta)
+            _, f_magn = local_chi_and_f(chi0_loc_full, g_pad, cfg.beta, u_channel(u, ch))
             out["f_magn_loc"] = f_magn
             out["f_dc"] = 2 * np.einsum("abcd...->cbad...", f_magn)
     return out

@@ -1,0 +1,129 @@
+/*
+ * dga_b200.h -- C ABI of the B200 ladder-DGA hot path (libdga_b200.so).
+ *
+ * Every entry point is extern "C", takes plain device pointers, sizes and a cudaStream_t, enqueues its
+ * kernels on that stream without synchronising, allocates nothing (callers pass scratch buffers sized by the
+ * *_scratch_bytes queries) and returns 0 on success or a DGA_ERR_* code, with a message available from
+ * dga_last_error_string().  Complex arrays are interleaved (re, im) doubles, the memory layout of numpy
+ * complex128.  Per-item status words report singular pivots, non-finite results and non-convergence.
+ *
+ * Layout vocabulary (n = orbitals, n2 = n*n, nv = 2*niv core, nvf = 2*(niv+niv_shell), W = niw+1 bosonic
+ * frequencies w >= 0, Q = irreducible q points, Nk = momentum grid points, N = n2*nv compound size):
+ *   compound orbital matrix  [(o1,o2),(o4,o3)]: row p = o1*n+o2, column s = o4*n+o3
+ *   compound BSE matrix      row (o1,o2,nu) = p*nv+nu, column (o4,o3,nu') = s*nv+nu'
+ *
+ * Each declaration names the upstream (Julpe/DGAmore, Python) function whose body it replaces.
+ */
+#ifndef DGA_B200_H
+#define DGA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* dga_stream_t; /* cudaStream_t */
+
+#define DGA_OK 0
+#define DGA_ERR_ARG 1
+#define DGA_ERR_SCRATCH 2
+#define DGA_ERR_LAUNCH 3
+#define DGA_ERR_CUDA 4
+
+#define DGA_ITEM_OK 0
+#define DGA_ITEM_SINGULAR 1
+#define DGA_ITEM_NONFINITE 2
+#define DGA_ITEM_NOCONVERGE 4
+
+/* Library version (major*10000 + minor*100 + patch) and the last error message of the calling thread. */
+int dga_version(void);
+const char* dga_last_error_string(void);
+
+/* Generic strided complex copy dst[idx . dst_stride] = scale * src[idx . src_stride] over `shape`
+ * (up to 8 dims, strides in complex elements).  Layout conversions at the boundary
+ * (FourPoint.to_compound_indices / to_full_indices, dgamore/four_point.py:166-293). */
+int dga_strided_copy_c128(const void* src, void* dst, int ndim, const long long* shape, const long long* src_stride,
+                          const long long* dst_stride, double scale, dga_stream_t stream);
+
+/* Batched separable DFT of momentum planes; replaces IAmNonLocal.fft / ifft (dgamore/n_point_base.py:509-551).
+ * Element (plane p = p_hi*n_lo + p_lo, point R) at p_hi*s_hi + p_lo*s_lo + R*s_r; tw = nx+ny+nz twiddles
+ * e^{s 2 pi i m/n} (sign folded in by the caller); output multiplied by `scale`. */
+int dga_dft_planes_c128(const void* in, long long in_s_hi, long long in_s_lo, long long in_s_r, void* out,
+                        long long out_s_hi, long long out_s_lo, long long out_s_r, int n_lo, int n_planes, int nx,
+                        int ny, int nz, const void* tw, double scale, dga_stream_t stream);
+
+/* Bare bubble chi0[q_irr,a,b,c,d,w>=0,nu] = -beta/Nk IFFT_R[G_ad(R,nu) G_cb(-R,nu-w)], filtered at 1e-12;
+ * replaces BubbleGenerator.create_generalized_chi0_q_fft_cpu/_gpu/_auto (dgamore/bubble_gen.py:33-144).
+ * g_r: [2niv+niw][n][n][Nk] transforms of G(k) for nu in [-niv-niw, niv); q_irr: [n_qirr][3];
+ * out addressed by 7 element strides (q, w, nu, a, b, c, d). */
+int dga_bubble_c128(const void* g_r, int n_orb, int niv, int niw, int nx, int ny, int nz, const int* q_irr,
+                    int n_qirr, const void* tw, double beta, void* out, const long long* out_strides,
+                    dga_stream_t stream);
+
+/* chi0^-1 per (q, w, nu_core) and the nu sums (1/beta^2) sum chi0 over the full and core boxes; replaces
+ * FourPoint.invert(copy=False) for one nu dimension (dgamore/four_point.py:601-613) and
+ * nonlocal_sde.py:824-835.  chi0: [Q][W][nvf][n2][n2] -> chi0_inv [Q][W][nv][n2][n2], sums [Q][W][n2][n2]. */
+int dga_chi0_prep_c128(const void* chi0, int n_orb, int niv_core, int niv_shell, int niw_half, int n_q, double beta,
+                       void* chi0_inv, void* full_sum, void* core_sum, int* status, dga_stream_t stream);
+
+/* Scratch bytes of dga_bse_solve_sum_c128 / dga_invert_sum_dense_c128 for n_items items of size N. */
+size_t dga_bse_scratch_bytes(int N, int n2, int n_items);
+
+/* Ladder BSE in FP64: X[ch][q][w][(o1,o2,nu)][(o4,o3)] = sum_nu' [chi0^-1 + (Gamma_r - U_r - V_r^q)/beta^2]^-1 / beta
+ * for each work item (ch, q, w); replaces nonlocal_sde.create_auxiliary_chi_r_q_sum_v1/_v3
+ * (dgamore/nonlocal_sde.py:85-156) with FourPoint.invert_and_sum_over_last_vn(_v2) (four_point.py:620-684).
+ * gamma_cm: [n_ch][W][N][N] column-major compound Gamma_r; chi0_inv: [Q][W][nv][n2][n2]; uv: [n_ch][Q][n2][n2]
+ * (U_r + V_r^q); work: [n_items][3] ints (ch, q, w); out: [n_ch][Q][W][N][n2]; status: [n_items]. */
+int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                           const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work, int n_items,
+                           void* out, int* status, void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
+/* Generic FourPoint.invert_and_sum_over_last_vn (dgamore/four_point.py:620-642) on an explicit matrix in the
+ * FourPoint layout [q][o1][o2][o3][o4][w][nu][nu']; out: [Q][W][N][n2]. */
+int dga_invert_sum_dense_c128(int n_orb, int niv, int niw_half, int n_q, double beta, const void* mat, const int* work,
+                              int n_items, void* out, int* status, void* scratch, size_t scratch_bytes,
+                              dga_stream_t stream);
+
+/* Physical susceptibility with the shell correction; replaces
+ * nonlocal_sde.create_generalized_chi_q_with_shell_correction (dgamore/nonlocal_sde.py:167-182) with the nu sum
+ * of nonlocal_sde.py:298.  X from dga_bse_solve_sum_c128; out: [n_ch][Q][W][n2][n2]. */
+int dga_chi_phys_c128(const void* X, const void* uv, const void* full_sum, const void* core_sum, int n_orb,
+                      int niv_core, int niw_half, int n_q, int n_ch, double beta, void* out, int* status,
+                      dga_stream_t stream);
+
+/* Single-band lambda correction (FP64 Newton with delta halving); replaces lambda_correction.find_lambda and
+ * perform_single_lambda_correction (dgamore/lambda_correction.py:28-73).  chi: [n_ch][Q][W]; weights: [Q]
+ * multiplicities (irrk_count); target: [n_ch] complex; outputs lambda [n_ch], iterations, corrected chi. */
+int dga_lambda_c128(const void* chi, int n_q, int niw_half, int n_ch, const long long* weights, const void* target,
+                    double beta, double nk_tot, double delta, double eps, int maxiter, double* lambda_out,
+                    int* iters_out, int* status, void* chi_out, dga_stream_t stream);
+
+/* Three-leg vertex and SDE kernel: gamma_r = beta chi0^-1 X (nonlocal_sde.create_vrg_r_q, :159-164) and
+ * K = -K_dc + K_dens + 3 K_magn with K_r = U_r (gamma - gamma U_r chi_r [- 2/3 1]) (calculate_kernel_r_q,
+ * :201-215, summed as in :820-853).  K: [Q][W][nv][n2][n2]; gamma_out optional [2][Q][W][nv][n2][n2]. */
+int dga_kernel_assembly_c128(const void* chi0_inv, const void* X, const void* uv, const void* chi_phys,
+                             const void* k_dc, int n_orb, int niv_core, int niw_half, int n_q, double beta, void* K,
+                             void* gamma_out, dga_stream_t stream);
+
+/* Double-counting kernel; replaces nonlocal_sde.calculate_sigma_dc_kernel (dgamore/nonlocal_sde.py:185-198).
+ * chi0: [Q][W][nvf][n2][n2]; u_perm: compound U_adcb / beta^2 [n2][n2]; fdc: [W][Nf][Nf] row-major compound
+ * F_dc = 2 F_magn,loc permuted cbad; k_dc: [Q][W][nv][n2][n2]. */
+size_t dga_dc_scratch_bytes(int n_orb, int niv_full, int niw_half, int n_q);
+int dga_dc_kernel_c128(const void* chi0, const void* u_perm, const void* fdc, int n_orb, int niv_core, int niv_shell,
+                       int niw_half, int n_q, void* k_dc, void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
+/* Schwinger-Dyson contraction through real space plus the inverse transform and the full-nu completion;
+ * replaces nonlocal_sde.calculate_sigma_from_kernel_fft_cpu/_gpu/_auto (dgamore/nonlocal_sde.py:544-674) and the
+ * caller's ifft().to_full_niv_range() (:876-879).  kern: [Q][W][nv][n2][n2]; g_r: [niv+2niw][n][n][Nk];
+ * irrk_inv: [Nk]; out: [Nk][n][n][2niv]. */
+size_t dga_sigma_scratch_bytes(int n_orb, int niv, int nk, int n_chunks);
+int dga_sigma_c128(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, int nx, int ny, int nz,
+                   const int* irrk_inv, const void* tw_inv, double beta, int n_chunks, void* out, void* scratch,
+                   size_t scratch_bytes, dga_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGA_B200_H */
