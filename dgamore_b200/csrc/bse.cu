@@ -562,3 +562,106 @@ int dga_invert_sum_dense_c128(int n_orb, int niv, int niw_half, int n_q, double 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Allocation-free variant of dga_bse_solve_sum_c128.
+//
+// Some callers of this library cannot call cudaMalloc: a host program that binds only this C ABI and has no
+// device allocator of its own, or a steady-state serving loop that must never trigger cudaMalloc's implicit
+// device-wide synchronisation.  For them the per-CTA working matrices live in the fixed array below, which is
+// part of this library's device image: every GPU that loads the library holds these 64 MiB until the process
+// exits.  In host code `g_bse_noalloc_scratch` is only a host-side stand-in for the array, not a device
+// address, so the device address is looked up once per device with cudaGetSymbolAddress and cached.
+// ------------------------------------------------------------------------------------------------
+
+#include <mutex>
+
+#define DGA_BSE_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define DGA_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) double2 g_bse_noalloc_scratch[DGA_BSE_NOALLOC_SCRATCH_BYTES / sizeof(double2)];
+
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_ptr[DGA_NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up on the first call per device).
+static int noalloc_scratch_ptr(void** out) {
+  int dev = -1;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess || dev < 0 || dev >= DGA_NOALLOC_MAX_DEVICES) {
+    dga_set_error("dga_bse_solve_sum_noalloc_c128: no usable current device (%s)", cudaGetErrorString(err));
+    return DGA_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    err = cudaGetSymbolAddress(&p, g_bse_noalloc_scratch);
+    if (err != cudaSuccess || !p) {
+      dga_set_error("dga_bse_solve_sum_noalloc_c128: cudaGetSymbolAddress failed: %s", cudaGetErrorString(err));
+      return DGA_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return DGA_OK;
+}
+
+extern "C" {
+
+// Same result as dga_bse_solve_sum_c128 without a caller scratch buffer.  At most
+// DGA_BSE_NOALLOC_SCRATCH_BYTES (64 MiB) of working matrices are used: as many CTAs run as there are
+// (N*N + N*n2)*16-byte slots in it (at least one), so a compound size N above about 2040 is rejected.
+// The first call on a device looks up the array's device address (this can load the module); make that first
+// call before any stream capture.  Calls share the array, so calls that overlap on the GPU (different streams
+// or threads without ordering between them) race; calls on one stream are ordered and safe.  Each item
+// rewrites its slot completely before reading it, so nothing has to be cleared between calls.
+int dga_bse_solve_sum_noalloc_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta,
+                                   double inv_beta2, const void* gamma_cm, const void* chi0_inv, const void* uv,
+                                   const int* work, int n_items, void* out, int* status, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0) {
+    dga_set_error("dga_bse_solve_sum_noalloc_c128: invalid sizes (n_orb=%d niv=%d niw_half=%d n_q=%d n_ch=%d "
+                  "items=%d)", n_orb, niv, niw_half, n_q, n_ch, n_items);
+    return DGA_ERR_ARG;
+  }
+  const size_t slot = (size_t)N * N + (size_t)N * n2;
+  const size_t capacity_slots = DGA_BSE_NOALLOC_SCRATCH_BYTES / (slot * sizeof(double2));
+  if (N > BSE_MAX_N || capacity_slots < 1) {
+    dga_set_error("dga_bse_solve_sum_noalloc_c128: compound size N=%d needs %zu bytes per matrix, more than the "
+                  "fixed %llu-byte scratch; use dga_bse_solve_sum_c128 with a caller buffer", N,
+                  slot * sizeof(double2), (unsigned long long)DGA_BSE_NOALLOC_SCRATCH_BYTES);
+    return DGA_ERR_SCRATCH;
+  }
+  if (!gamma_cm || !chi0_inv || !uv || !work || !out) {
+    dga_set_error("dga_bse_solve_sum_noalloc_c128: null pointer argument");
+    return DGA_ERR_ARG;
+  }
+  void* scratch = nullptr;
+  int rc = noalloc_scratch_ptr(&scratch);
+  if (rc != DGA_OK) return rc;
+  const size_t smem = bse_smem_bytes(N);
+  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<StructuredSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  int grid = bse_grid(n_items, smem);
+  if ((size_t)grid > capacity_slots) grid = (int)capacity_slots;
+  StructuredSource src;
+  src.gamma_cm = (const double2*)gamma_cm;
+  src.chi0_inv = (const double2*)chi0_inv;
+  src.uv = (const double2*)uv;
+  src.n2 = n2;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  src.inv_beta2 = inv_beta2;
+  bse_solve_sum_fp64_kernel<StructuredSource><<<grid, BSE_THREADS, smem, stream>>>(
+      src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, (double2*)out, status,
+      (double2*)scratch, slot);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_bse_solve_sum_noalloc_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"

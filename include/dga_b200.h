@@ -79,6 +79,20 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
                            const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work, int n_items,
                            void* out, int* status, void* scratch, size_t scratch_bytes, dga_stream_t stream);
 
+/* Allocation-free variant of dga_bse_solve_sum_c128 (no counterpart in the upstream, which has no device
+ * code): for callers that cannot call cudaMalloc -- a host that binds only this C ABI and has no device
+ * allocator, or a steady-state loop that must not trigger cudaMalloc's device-wide synchronisation.  The
+ * working matrices live in a fixed DGA_BSE_NOALLOC_SCRATCH_BYTES (64 MiB) array inside the library, held by
+ * every GPU that loads the library until exit; compound sizes N whose N*N + N*n2 complex slot does not fit
+ * (N above about 2040) are rejected with DGA_ERR_SCRATCH.  The first call on a device looks up the array's
+ * device address (it can load the module): make it before any stream capture.  Calls share the array, so
+ * calls that overlap on the GPU race; calls ordered on one stream are safe.  Nothing needs clearing between
+ * calls (every item rewrites its slot before reading it). */
+#define DGA_BSE_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int dga_bse_solve_sum_noalloc_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta,
+                                   double inv_beta2, const void* gamma_cm, const void* chi0_inv, const void* uv,
+                                   const int* work, int n_items, void* out, int* status, dga_stream_t stream);
+
 /* Generic FourPoint.invert_and_sum_over_last_vn (dgamore/four_point.py:620-642) on an explicit matrix in the
  * FourPoint layout [q][o1][o2][o3][o4][w][nu][nu']; out: [Q][W][N][n2]. */
 int dga_invert_sum_dense_c128(int n_orb, int niv, int niw_half, int n_q, double beta, const void* mat, const int* work,
