@@ -46,10 +46,9 @@ struct StructuredSource {
   double inv_beta2;  // 1 / beta**2 computed on the host exactly as the upstream does
 
   // Element (i, j) in FP64, with the upstream's order of operations: (chi0inv_diag + Gamma*ib2) + (-(uv*ib2)).
-  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j) const {
+  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j, int pr, int vr, int pc,
+                                             int vc) const {
     const double2 g = gamma_cm[((size_t)(ch * W + w) * N + j) * N + i];
-    const int pr = i / nv, vr = i - pr * nv;
-    const int pc = j / nv, vc = j - pc * nv;
     const double2 u = uv[((size_t)ch * Q + q) * n2 * n2 + pr * n2 + pc];
     double re = __dmul_rn(g.x, inv_beta2);
     double im = __dmul_rn(g.y, inv_beta2);
@@ -70,9 +69,8 @@ struct DenseSource {
   const double2* mat;  // [Q][n][n][n][n][W][nv][nv]
   int nb, nv, W, Q;
 
-  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j) const {
-    const int pr = i / nv, vr = i - pr * nv;
-    const int pc = j / nv, vc = j - pc * nv;
+  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j, int pr, int vr, int pc,
+                                             int vc) const {
     const int o1 = pr / nb, o2 = pr - o1 * nb;
     const int o4 = pc / nb, o3 = pc - o4 * nb;
     size_t idx = ((((size_t)q * nb + o1) * nb + o2) * nb + o3) * nb + o4;
@@ -136,14 +134,32 @@ __device__ int block_argmax(R v, int idx, R* s_val, int* s_idx) {
 // ----------------------------------------------------------------------------------------------
 template <typename C>
 struct BseSmem {
-  C Ls[BSE_NB][BSE_TILE];  // L21 tile (k, row)
-  C Us[BSE_NB][BSE_TILE];  // U12 tile (k, col)
+  C Ls[BSE_NB][BSE_TILE];  // L21 tile (k, row); also the staging block of the triangular solves
+  C Us[BSE_NB][BSE_TILE];  // U12 tile (k, col); also the A12 chunk of the U12 solve
   C L11[BSE_NB][BSE_NB + 1];
+  C L11i[BSE_NB][BSE_NB + 1];  // inverse of the unit lower triangle of L11
   C row[BSE_NB];
   double red_val[32];
   int red_idx[32];
   int flag;
 };
+
+// X = L^-1 for the unit lower triangular nb x nb block in sm.L11 (column c of X by thread c of warp 0):
+// X[r][c] = -sum_{k=c}^{r-1} L[r][k] X[k][c] for r > c, X[c][c] = 1.
+template <typename C>
+__device__ void unit_lower_inverse(BseSmem<C>& sm, int nb) {
+  using R = decltype(C::x);
+  const int c = threadIdx.x;
+  if (c < nb) {
+    for (int r = 0; r < c; ++r) sm.L11i[r][c] = cmake<C>(R(0), R(0));
+    sm.L11i[c][c] = cmake<C>(R(1), R(0));
+    for (int r = c + 1; r < nb; ++r) {
+      C acc = cmake<C>(R(0), R(0));
+      for (int k = c; k < r; ++k) cfms(acc, sm.L11[r][k], sm.L11i[k][c]);
+      sm.L11i[r][c] = acc;
+    }
+  }
+}
 
 // ----------------------------------------------------------------------------------------------
 // LU with partial pivoting of the N x N column-major matrix A (leading dimension ld) in place.
@@ -170,13 +186,12 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
           bidx = i;
         }
       }
-      // reduce in double precision storage (R may be float)
       int p;
       {
-        double dv = (double)best;
+        double dv = (double)best;  // reduce in double precision storage (R may be float)
         p = block_argmax<double>(dv, bidx, sm.red_val, sm.red_idx);
       }
-      if (p >= N) p = j;  // empty range cannot happen (j < N), kept for safety
+      if (p >= N) p = j;  // cannot happen for j < N; keeps the index in range regardless
       if (tid == 0) piv[j] = p;
       if (p != j) {
         for (int c = tid; c < nb; c += T) {
@@ -191,29 +206,37 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
       const bool zero = (d.x == R(0) && d.y == R(0));
       if (zero) singular = true;
       const C rinv = zero ? cmake<C>(R(0), R(0)) : crecip(d);
-      for (int c = tid; c < nb - jj - 1; c += T) sm.row[c] = A[(size_t)(j + 1 + c) * ld + j];
-      __syncthreads();
       const int ncols = nb - jj - 1;
+      for (int c = tid; c < ncols; c += T) sm.row[c] = A[(size_t)(j + 1 + c) * ld + j];
+      __syncthreads();
       for (int i = j + 1 + tid; i < N; i += T) {
         C l = A[(size_t)j * ld + i];
         if (!zero) l = cmul(l, rinv);
         A[(size_t)j * ld + i] = l;
-        for (int c = 0; c < ncols; ++c) {
-          C* a = A + (size_t)(j + 1 + c) * ld + i;
-          C v = *a;
-          cfms(v, l, sm.row[c]);
-          *a = v;
+        // batched loads: 8 independent loads in flight before the updates
+        for (int c0 = 0; c0 < ncols; c0 += 8) {
+          C v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (c0 + u < ncols) v[u] = A[(size_t)(j + 1 + c0 + u) * ld + i];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (c0 + u < ncols) {
+              cfms(v[u], l, sm.row[c0 + u]);
+              A[(size_t)(j + 1 + c0 + u) * ld + i] = v[u];
+            }
         }
       }
       __syncthreads();
     }
-    // ---- L11 to shared memory ----
+    // ---- L11 and its inverse in shared memory ----
     for (int e = tid; e < nb * nb; e += T) {
       const int r = e % nb, c = e / nb;
       sm.L11[r][c] = A[(size_t)(k0 + c) * ld + k0 + r];
     }
     __syncthreads();
-    // ---- row interchanges on the other columns + U12 = L11^-1 A12 ----
+    unit_lower_inverse(sm, nb);
+    // ---- row interchanges on the columns outside the panel ----
     const int k1 = k0 + nb;
     for (int c = tid; c < N; c += T) {
       if (c >= k0 && c < k1) continue;
@@ -226,25 +249,39 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
           col[p] = t;
         }
       }
-      if (c >= k1) {
-        C x[BSE_NB];
-#pragma unroll
-        for (int r = 0; r < BSE_NB; ++r)
-          if (r < nb) x[r] = col[k0 + r];
-#pragma unroll
-        for (int r = 0; r < BSE_NB; ++r) {
-          if (r < nb) {
-#pragma unroll
-            for (int rr = r + 1; rr < BSE_NB; ++rr)
-              if (rr < nb) cfms(x[rr], sm.L11[rr][r], x[r]);
-          }
-        }
-#pragma unroll
-        for (int r = 0; r < BSE_NB; ++r)
-          if (r < nb) col[k0 + r] = x[r];
-      }
     }
     __syncthreads();
+    // ---- U12 = L11^-1 A12, in chunks of 64 columns staged through shared memory ----
+    for (int c0 = k1; c0 < N; c0 += BSE_TILE) {
+      const int cw = min(BSE_TILE, N - c0);
+      for (int e = tid; e < nb * cw; e += T) {
+        const int c = e / nb, k = e % nb;
+        sm.Us[k][c] = A[(size_t)(c0 + c) * ld + k0 + k];
+      }
+      __syncthreads();
+      {
+        const int c = tid % BSE_TILE, g = tid / BSE_TILE;  // 4 groups of 8 rows
+        if (c < cw) {
+          C out[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) out[u] = cmake<C>(R(0), R(0));
+          for (int k = 0; k < nb; ++k) {
+            const C a = sm.Us[k][c];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int r = g * 8 + u;
+              if (r < nb && k <= r) cfma(out[u], sm.L11i[r][k], a);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int r = g * 8 + u;
+            if (r < nb) A[(size_t)(c0 + c) * ld + k0 + r] = out[u];
+          }
+        }
+      }
+      __syncthreads();
+    }
     // ---- trailing update A22 -= L21 U12 ----
     const int nt = N - k1;
     if (nt > 0) {
@@ -253,6 +290,17 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
       for (int tile = 0; tile < tiles * tiles; ++tile) {
         const int tr0 = k1 + (tile % tiles) * BSE_TILE;
         const int tc0 = k1 + (tile / tiles) * BSE_TILE;
+        // C tile into the accumulators first: its loads overlap the shared-memory staging below
+        C acc[4][4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int c = tc0 + tx + 16 * b;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const int r = tr0 + ty + 16 * a;
+            acc[a][b] = (c < N && r < N) ? A[(size_t)c * ld + r] : cmake<C>(R(0), R(0));
+          }
+        }
         for (int e = tid; e < nb * BSE_TILE; e += T) {
           const int k = e / BSE_TILE, r = e % BSE_TILE;
           sm.Ls[k][r] = (tr0 + r < N) ? A[(size_t)(k0 + k) * ld + tr0 + r] : cmake<C>(R(0), R(0));
@@ -262,11 +310,6 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
           sm.Us[k][c] = (tc0 + c < N) ? A[(size_t)(tc0 + c) * ld + k0 + k] : cmake<C>(R(0), R(0));
         }
         __syncthreads();
-        C acc[4][4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = cmake<C>(R(0), R(0));
         for (int k = 0; k < nb; ++k) {
           C lv[4], uv[4];
 #pragma unroll
@@ -276,7 +319,7 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
 #pragma unroll
           for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) cfma(acc[a][b], lv[a], uv[b]);
+            for (int b = 0; b < 4; ++b) cfms(acc[a][b], lv[a], uv[b]);
         }
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
@@ -286,7 +329,7 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
               const int r = tr0 + ty + 16 * a;
-              if (r < N) col[r] = csub(col[r], acc[a][b]);
+              if (r < N) col[r] = acc[a][b];
             }
           }
         }
@@ -299,13 +342,17 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
 
 // ----------------------------------------------------------------------------------------------
 // Solve (L U) Y = B in place for the n_rhs columns of Y (column-major, leading dimension N), with the LU
-// factors of lu_factor (unit lower L below the diagonal, U on and above).  Blocked by 32 rows.
+// factors of lu_factor (unit lower L below the diagonal, U on and above).  Blocked by 32 rows: the diagonal
+// block is solved by one warp per right-hand side (lane = row, the solved value broadcast by shuffle), the
+// rest of the rows are updated from the block copy in shared memory.
 // ----------------------------------------------------------------------------------------------
 template <typename C, typename CY>
 __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __restrict__ Y, int n_rhs,
                                  BseSmem<C>& sm) {
   using RY = decltype(CY::x);
   const int tid = threadIdx.x, T = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
+  CY* yb = reinterpret_cast<CY*>(&sm.Ls[0][0]);  // [n_rhs][32] solved block
   // forward: L z = b
   for (int b0 = 0; b0 < N; b0 += BSE_NB) {
     const int bn = min(BSE_NB, N - b0);
@@ -314,28 +361,32 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
       sm.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
     }
     __syncthreads();
-    for (int s = tid; s < n_rhs; s += T) {
-      CY* y = Y + (size_t)s * N + b0;
+    for (int s = warp; s < n_rhs; s += nwarps) {
+      CY y = lane < bn ? Y[(size_t)s * N + b0 + lane] : cmake<CY>(RY(0), RY(0));
       for (int r = 0; r < bn; ++r) {
-        const CY yr = y[r];
-        for (int rr = r + 1; rr < bn; ++rr) {
-          const C l = sm.L11[rr][r];
-          CY lw = cmake<CY>((RY)l.x, (RY)l.y);
-          cfms(y[rr], lw, yr);
+        CY yr;
+        yr.x = __shfl_sync(0xffffffffu, y.x, r);
+        yr.y = __shfl_sync(0xffffffffu, y.y, r);
+        if (lane > r && lane < bn) {
+          const C l = sm.L11[lane][r];
+          cfms(y, cmake<CY>((RY)l.x, (RY)l.y), yr);
         }
+      }
+      if (lane < bn) {
+        Y[(size_t)s * N + b0 + lane] = y;
+        yb[s * 32 + lane] = y;
       }
     }
     __syncthreads();
     const int rows = N - b0 - bn;
     for (int e = tid; e < rows * n_rhs; e += T) {
       const int i = b0 + bn + e % rows, s = e / rows;
-      CY* y = Y + (size_t)s * N;
-      CY acc = y[i];
+      CY acc = Y[(size_t)s * N + i];
       for (int r = 0; r < bn; ++r) {
         const C l = A[(size_t)(b0 + r) * ld + i];
-        cfms(acc, cmake<CY>((RY)l.x, (RY)l.y), y[b0 + r]);
+        cfms(acc, cmake<CY>((RY)l.x, (RY)l.y), yb[s * 32 + r]);
       }
-      y[i] = acc;
+      Y[(size_t)s * N + i] = acc;
     }
     __syncthreads();
   }
@@ -349,28 +400,35 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
       sm.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
     }
     __syncthreads();
-    for (int s = tid; s < n_rhs; s += T) {
-      CY* y = Y + (size_t)s * N + b0;
+    for (int s = warp; s < n_rhs; s += nwarps) {
+      CY y = lane < bn ? Y[(size_t)s * N + b0 + lane] : cmake<CY>(RY(0), RY(0));
       for (int r = bn - 1; r >= 0; --r) {
-        const C u = sm.L11[r][r];
-        CY yr = cdiv(y[r], cmake<CY>((RY)u.x, (RY)u.y));
-        y[r] = yr;
-        for (int rr = 0; rr < r; ++rr) {
-          const C l = sm.L11[rr][r];
-          cfms(y[rr], cmake<CY>((RY)l.x, (RY)l.y), yr);
+        if (lane == r) {
+          const C u = sm.L11[r][r];
+          y = cdiv(y, cmake<CY>((RY)u.x, (RY)u.y));
         }
+        CY yr;
+        yr.x = __shfl_sync(0xffffffffu, y.x, r);
+        yr.y = __shfl_sync(0xffffffffu, y.y, r);
+        if (lane < r) {
+          const C u = sm.L11[lane][r];
+          cfms(y, cmake<CY>((RY)u.x, (RY)u.y), yr);
+        }
+      }
+      if (lane < bn) {
+        Y[(size_t)s * N + b0 + lane] = y;
+        yb[s * 32 + lane] = y;
       }
     }
     __syncthreads();
     for (int e = tid; e < b0 * n_rhs; e += T) {
       const int i = e % b0, s = e / b0;
-      CY* y = Y + (size_t)s * N;
-      CY acc = y[i];
+      CY acc = Y[(size_t)s * N + i];
       for (int r = 0; r < bn; ++r) {
         const C u = A[(size_t)(b0 + r) * ld + i];
-        cfms(acc, cmake<CY>((RY)u.x, (RY)u.y), y[b0 + r]);
+        cfms(acc, cmake<CY>((RY)u.x, (RY)u.y), yb[s * 32 + r]);
       }
-      y[i] = acc;
+      Y[(size_t)s * N + i] = acc;
     }
     __syncthreads();
   }
@@ -421,9 +479,25 @@ __global__ void __launch_bounds__(BSE_THREADS, 2)
 
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const WorkItem wi = work[item];
-    for (size_t e = tid; e < (size_t)N * N; e += T) {
-      const int i = (int)(e % N), j = (int)(e / N);
-      A[e] = src.element(wi.ch, wi.q, wi.w, N, i, j);
+    // form A column by column; each thread keeps the (pair, nu) split of its rows in registers
+    {
+      constexpr int MAXR = BSE_MAX_N / BSE_THREADS;
+      int pr[MAXR], vr[MAXR];
+#pragma unroll
+      for (int m = 0; m < MAXR; ++m) {
+        const int i = tid + m * T;
+        pr[m] = i / nv;
+        vr[m] = i - pr[m] * nv;
+      }
+      for (int j = 0; j < N; ++j) {
+        const int pc = j / nv, vc = j - pc * nv;
+        double2* col = A + (size_t)j * N;
+#pragma unroll
+        for (int m = 0; m < MAXR; ++m) {
+          const int i = tid + m * T;
+          if (i < N) col[i] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr[m], vr[m], pc, vc);
+        }
+      }
     }
     __syncthreads();
     const bool singular = lu_factor<double2>(A, N, N, piv, sm);
