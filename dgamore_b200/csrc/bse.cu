@@ -28,9 +28,10 @@
 
 namespace dga {
 
-constexpr int BSE_THREADS = 256;
-constexpr int BSE_NB = 32;    // panel width
-constexpr int BSE_TILE = 64;  // trailing-update tile edge
+constexpr int BSE_THREADS = 128;
+constexpr int BSE_NB = 32;  // panel width (also the row-block of the triangular solves)
+constexpr int BSE_TM = 32;  // trailing-update row tile
+constexpr int BSE_TN = 64;  // trailing-update column strip
 constexpr int BSE_MAX_N = 2048;
 
 // ----------------------------------------------------------------------------------------------
@@ -130,33 +131,41 @@ __device__ int block_argmax(R v, int idx, R* s_val, int* s_idx) {
 }
 
 // ----------------------------------------------------------------------------------------------
-// Shared-memory layout of one CTA
+// Shared-memory layout of one CTA: the GEMM tiles and the panel/triangular-solve buffers are never live at
+// the same time, so they share storage.
 // ----------------------------------------------------------------------------------------------
 template <typename C>
 struct BseSmem {
-  C Ls[BSE_NB][BSE_TILE];  // L21 tile (k, row); also the staging block of the triangular solves
-  C Us[BSE_NB][BSE_TILE];  // U12 tile (k, col); also the A12 chunk of the U12 solve
-  C L11[BSE_NB][BSE_NB + 1];
-  C L11i[BSE_NB][BSE_NB + 1];  // inverse of the unit lower triangle of L11
+  union {
+    struct {
+      C Ls[BSE_NB][BSE_TM];      // L21 row tile (k, row)
+      C Us[BSE_TN][BSE_NB + 1];  // U12 column strip (col, k), padded
+    } g;
+    struct {
+      C L11[BSE_NB][BSE_NB + 1];
+      C L11i[BSE_NB][BSE_NB + 1];  // inverse of the unit lower triangle of L11
+      C A12[BSE_NB][BSE_NB + 1];   // A12 chunk of the U12 solve (col, k); solved block of the RHS solves
+    } t;
+  } u;
   C row[BSE_NB];
   double red_val[32];
   int red_idx[32];
   int flag;
 };
 
-// X = L^-1 for the unit lower triangular nb x nb block in sm.L11 (column c of X by thread c of warp 0):
+// X = L^-1 for the unit lower triangular nb x nb block in L11 (column c of X by thread c):
 // X[r][c] = -sum_{k=c}^{r-1} L[r][k] X[k][c] for r > c, X[c][c] = 1.
 template <typename C>
 __device__ void unit_lower_inverse(BseSmem<C>& sm, int nb) {
   using R = decltype(C::x);
   const int c = threadIdx.x;
   if (c < nb) {
-    for (int r = 0; r < c; ++r) sm.L11i[r][c] = cmake<C>(R(0), R(0));
-    sm.L11i[c][c] = cmake<C>(R(1), R(0));
+    for (int r = 0; r < c; ++r) sm.u.t.L11i[r][c] = cmake<C>(R(0), R(0));
+    sm.u.t.L11i[c][c] = cmake<C>(R(1), R(0));
     for (int r = c + 1; r < nb; ++r) {
       C acc = cmake<C>(R(0), R(0));
-      for (int k = c; k < r; ++k) cfms(acc, sm.L11[r][k], sm.L11i[k][c]);
-      sm.L11i[r][c] = acc;
+      for (int k = c; k < r; ++k) cfms(acc, sm.u.t.L11[r][k], sm.u.t.L11i[k][c]);
+      sm.u.t.L11i[r][c] = acc;
     }
   }
 }
@@ -174,18 +183,18 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
   for (int k0 = 0; k0 < N; k0 += BSE_NB) {
     const int nb = min(BSE_NB, N - k0);
     // ---- panel factorisation (columns k0 .. k0+nb-1) ----
+    // pivot candidates of the first panel column; later columns get theirs from the previous update
+    R best = R(-1);
+    int bidx = 0x7fffffff;
+    for (int i = k0 + tid; i < N; i += T) {
+      R v = cabs1(A[(size_t)k0 * ld + i]);
+      if (v > best) {
+        best = v;
+        bidx = i;
+      }
+    }
     for (int jj = 0; jj < nb; ++jj) {
       const int j = k0 + jj;
-      const C* colj = A + (size_t)j * ld;
-      R best = R(-1);
-      int bidx = 0x7fffffff;
-      for (int i = j + tid; i < N; i += T) {
-        R v = cabs1(colj[i]);
-        if (v > best) {
-          best = v;
-          bidx = i;
-        }
-      }
       int p;
       {
         double dv = (double)best;  // reduce in double precision storage (R may be float)
@@ -209,6 +218,8 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
       const int ncols = nb - jj - 1;
       for (int c = tid; c < ncols; c += T) sm.row[c] = A[(size_t)(j + 1 + c) * ld + j];
       __syncthreads();
+      best = R(-1);
+      bidx = 0x7fffffff;
       for (int i = j + 1 + tid; i < N; i += T) {
         C l = A[(size_t)j * ld + i];
         if (!zero) l = cmul(l, rinv);
@@ -225,6 +236,13 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
               cfms(v[u], l, sm.row[c0 + u]);
               A[(size_t)(j + 1 + c0 + u) * ld + i] = v[u];
             }
+          if (c0 == 0) {  // column j+1 just updated: its pivot candidate (look-ahead)
+            const R a = cabs1(v[0]);
+            if (a > best) {
+              best = a;
+              bidx = i;
+            }
+          }
         }
       }
       __syncthreads();
@@ -232,108 +250,137 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
     // ---- L11 and its inverse in shared memory ----
     for (int e = tid; e < nb * nb; e += T) {
       const int r = e % nb, c = e / nb;
-      sm.L11[r][c] = A[(size_t)(k0 + c) * ld + k0 + r];
+      sm.u.t.L11[r][c] = A[(size_t)(k0 + c) * ld + k0 + r];
     }
     __syncthreads();
     unit_lower_inverse(sm, nb);
     // ---- row interchanges on the columns outside the panel ----
+    // When every pivot row lies below the panel and no two coincide, the interchanges are independent pairs
+    // and are applied in parallel over (interchange, column); otherwise they run in order per column.
     const int k1 = k0 + nb;
-    for (int c = tid; c < N; c += T) {
-      if (c >= k0 && c < k1) continue;
-      C* col = A + (size_t)c * ld;
-      for (int jj = 0; jj < nb; ++jj) {
+    if (tid < 32) {
+      bool ok = true;
+      if (tid < nb) {
+        const int p = piv[k0 + tid];
+        if (p != k0 + tid) {
+          if (p < k1) ok = false;
+          for (int o = 0; o < nb; ++o)
+            if (o != tid && piv[k0 + o] == p) ok = false;
+        }
+      }
+      const unsigned all_ok = __all_sync(0xffffffffu, ok);
+      if (tid == 0) sm.flag = all_ok ? 1 : 0;
+    }
+    __syncthreads();
+    if (sm.flag) {
+      const int ncol = N - nb;
+      for (int e = tid; e < nb * ncol; e += T) {
+        const int jj = e / ncol;
+        int c = e - jj * ncol;
+        c = c < k0 ? c : c + nb;  // skip the panel columns
         const int p = piv[k0 + jj];
         if (p != k0 + jj) {
+          C* col = A + (size_t)c * ld;
           C t = col[k0 + jj];
           col[k0 + jj] = col[p];
           col[p] = t;
         }
       }
+    } else {
+      for (int c = tid; c < N; c += T) {
+        if (c >= k0 && c < k1) continue;
+        C* col = A + (size_t)c * ld;
+        for (int jj = 0; jj < nb; ++jj) {
+          const int p = piv[k0 + jj];
+          if (p != k0 + jj) {
+            C t = col[k0 + jj];
+            col[k0 + jj] = col[p];
+            col[p] = t;
+          }
+        }
+      }
     }
     __syncthreads();
-    // ---- U12 = L11^-1 A12, in chunks of 64 columns staged through shared memory ----
-    for (int c0 = k1; c0 < N; c0 += BSE_TILE) {
-      const int cw = min(BSE_TILE, N - c0);
+    // ---- U12 = L11^-1 A12, in chunks of 32 columns staged through shared memory ----
+    for (int c0 = k1; c0 < N; c0 += BSE_NB) {
+      const int cw = min(BSE_NB, N - c0);
       for (int e = tid; e < nb * cw; e += T) {
         const int c = e / nb, k = e % nb;
-        sm.Us[k][c] = A[(size_t)(c0 + c) * ld + k0 + k];
+        sm.u.t.A12[c][k] = A[(size_t)(c0 + c) * ld + k0 + k];
       }
       __syncthreads();
-      {
-        const int c = tid % BSE_TILE, g = tid / BSE_TILE;  // 4 groups of 8 rows
-        if (c < cw) {
-          C out[8];
+      for (int e = tid; e < cw * (BSE_NB / 8); e += T) {
+        const int c = e % cw, g = e / cw;  // 8-row groups
+        C out[8];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) out[u] = cmake<C>(R(0), R(0));
-          for (int k = 0; k < nb; ++k) {
-            const C a = sm.Us[k][c];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              const int r = g * 8 + u;
-              if (r < nb && k <= r) cfma(out[u], sm.L11i[r][k], a);
-            }
-          }
+        for (int u = 0; u < 8; ++u) out[u] = cmake<C>(R(0), R(0));
+        for (int k = 0; k < nb; ++k) {
+          const C a = sm.u.t.A12[c][k];
 #pragma unroll
           for (int u = 0; u < 8; ++u) {
             const int r = g * 8 + u;
-            if (r < nb) A[(size_t)(c0 + c) * ld + k0 + r] = out[u];
+            if (r < nb && k <= r) cfma(out[u], sm.u.t.L11i[r][k], a);
           }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = g * 8 + u;
+          if (r < nb) A[(size_t)(c0 + c) * ld + k0 + r] = out[u];
         }
       }
       __syncthreads();
     }
-    // ---- trailing update A22 -= L21 U12 ----
+    // ---- trailing update A22 -= L21 U12: column strips of BSE_TN, row tiles of BSE_TM ----
     const int nt = N - k1;
     if (nt > 0) {
-      const int tiles = (nt + BSE_TILE - 1) / BSE_TILE;
-      const int ty = tid & 15, tx = tid >> 4;
-      for (int tile = 0; tile < tiles * tiles; ++tile) {
-        const int tr0 = k1 + (tile % tiles) * BSE_TILE;
-        const int tc0 = k1 + (tile / tiles) * BSE_TILE;
-        // C tile into the accumulators first: its loads overlap the shared-memory staging below
-        C acc[4][4];
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int c = tc0 + tx + 16 * b;
-#pragma unroll
-          for (int a = 0; a < 4; ++a) {
-            const int r = tr0 + ty + 16 * a;
-            acc[a][b] = (c < N && r < N) ? A[(size_t)c * ld + r] : cmake<C>(R(0), R(0));
-          }
-        }
-        for (int e = tid; e < nb * BSE_TILE; e += T) {
-          const int k = e / BSE_TILE, r = e % BSE_TILE;
-          sm.Ls[k][r] = (tr0 + r < N) ? A[(size_t)(k0 + k) * ld + tr0 + r] : cmake<C>(R(0), R(0));
-        }
-        for (int e = tid; e < nb * BSE_TILE; e += T) {
+      const int ty = tid % (BSE_TM / 4), tx = tid / (BSE_TM / 4);  // 8 x 16 thread grid, 4x4 outputs each
+      for (int cs = k1; cs < N; cs += BSE_TN) {
+        for (int e = tid; e < nb * BSE_TN; e += T) {
           const int c = e / nb, k = e % nb;
-          sm.Us[k][c] = (tc0 + c < N) ? A[(size_t)(tc0 + c) * ld + k0 + k] : cmake<C>(R(0), R(0));
+          sm.u.g.Us[c][k] = (cs + c < N) ? A[(size_t)(cs + c) * ld + k0 + k] : cmake<C>(R(0), R(0));
         }
-        __syncthreads();
-        for (int k = 0; k < nb; ++k) {
-          C lv[4], uv[4];
+        for (int rt = k1; rt < N; rt += BSE_TM) {
+          C acc[4][4];
 #pragma unroll
-          for (int a = 0; a < 4; ++a) lv[a] = sm.Ls[k][ty + 16 * a];
-#pragma unroll
-          for (int b = 0; b < 4; ++b) uv[b] = sm.Us[k][tx + 16 * b];
-#pragma unroll
-          for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) cfms(acc[a][b], lv[a], uv[b]);
-        }
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int c = tc0 + tx + 16 * b;
-          if (c < N) {
-            C* col = A + (size_t)c * ld;
+          for (int b = 0; b < 4; ++b) {
+            const int c = cs + tx + 16 * b;
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-              const int r = tr0 + ty + 16 * a;
-              if (r < N) col[r] = acc[a][b];
+              const int r = rt + ty + 8 * a;
+              acc[a][b] = (c < N && r < N) ? A[(size_t)c * ld + r] : cmake<C>(R(0), R(0));
             }
           }
+          for (int e = tid; e < nb * BSE_TM; e += T) {
+            const int k = e / BSE_TM, r = e % BSE_TM;
+            sm.u.g.Ls[k][r] = (rt + r < N) ? A[(size_t)(k0 + k) * ld + rt + r] : cmake<C>(R(0), R(0));
+          }
+          __syncthreads();
+#pragma unroll 4
+          for (int k = 0; k < nb; ++k) {
+            C lv[4], uv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) lv[a] = sm.u.g.Ls[k][ty + 8 * a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) uv[b] = sm.u.g.Us[tx + 16 * b][k];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+              for (int b = 0; b < 4; ++b) cfms(acc[a][b], lv[a], uv[b]);
+          }
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int c = cs + tx + 16 * b;
+            if (c < N) {
+              C* col = A + (size_t)c * ld;
+#pragma unroll
+              for (int a = 0; a < 4; ++a) {
+                const int r = rt + ty + 8 * a;
+                if (r < N) col[r] = acc[a][b];
+              }
+            }
+          }
+          __syncthreads();
         }
-        __syncthreads();
       }
     }
   }
@@ -352,13 +399,13 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
   using RY = decltype(CY::x);
   const int tid = threadIdx.x, T = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
-  CY* yb = reinterpret_cast<CY*>(&sm.Ls[0][0]);  // [n_rhs][32] solved block
+  CY* yb = reinterpret_cast<CY*>(&sm.u.t.A12[0][0]);  // [n_rhs][32] solved block
   // forward: L z = b
   for (int b0 = 0; b0 < N; b0 += BSE_NB) {
     const int bn = min(BSE_NB, N - b0);
     for (int e = tid; e < bn * bn; e += T) {
       const int r = e % bn, c = e / bn;
-      sm.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
+      sm.u.t.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
     }
     __syncthreads();
     for (int s = warp; s < n_rhs; s += nwarps) {
@@ -368,7 +415,7 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
         yr.x = __shfl_sync(0xffffffffu, y.x, r);
         yr.y = __shfl_sync(0xffffffffu, y.y, r);
         if (lane > r && lane < bn) {
-          const C l = sm.L11[lane][r];
+          const C l = sm.u.t.L11[lane][r];
           cfms(y, cmake<CY>((RY)l.x, (RY)l.y), yr);
         }
       }
@@ -382,6 +429,7 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
     for (int e = tid; e < rows * n_rhs; e += T) {
       const int i = b0 + bn + e % rows, s = e / rows;
       CY acc = Y[(size_t)s * N + i];
+#pragma unroll 8
       for (int r = 0; r < bn; ++r) {
         const C l = A[(size_t)(b0 + r) * ld + i];
         cfms(acc, cmake<CY>((RY)l.x, (RY)l.y), yb[s * 32 + r]);
@@ -397,21 +445,21 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
     const int bn = min(BSE_NB, N - b0);
     for (int e = tid; e < bn * bn; e += T) {
       const int r = e % bn, c = e / bn;
-      sm.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
+      sm.u.t.L11[r][c] = A[(size_t)(b0 + c) * ld + b0 + r];
     }
     __syncthreads();
     for (int s = warp; s < n_rhs; s += nwarps) {
       CY y = lane < bn ? Y[(size_t)s * N + b0 + lane] : cmake<CY>(RY(0), RY(0));
       for (int r = bn - 1; r >= 0; --r) {
         if (lane == r) {
-          const C u = sm.L11[r][r];
+          const C u = sm.u.t.L11[r][r];
           y = cdiv(y, cmake<CY>((RY)u.x, (RY)u.y));
         }
         CY yr;
         yr.x = __shfl_sync(0xffffffffu, y.x, r);
         yr.y = __shfl_sync(0xffffffffu, y.y, r);
         if (lane < r) {
-          const C u = sm.L11[lane][r];
+          const C u = sm.u.t.L11[lane][r];
           cfms(y, cmake<CY>((RY)u.x, (RY)u.y), yr);
         }
       }
@@ -424,6 +472,7 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
     for (int e = tid; e < b0 * n_rhs; e += T) {
       const int i = e % b0, s = e / b0;
       CY acc = Y[(size_t)s * N + i];
+#pragma unroll 8
       for (int r = 0; r < bn; ++r) {
         const C u = A[(size_t)(b0 + r) * ld + i];
         cfms(acc, cmake<CY>((RY)u.x, (RY)u.y), yb[s * 32 + r]);
@@ -465,7 +514,7 @@ __device__ void permuted_selector(CY* __restrict__ Y, int N, int nv, int n_rhs, 
 // FP64 kernel: one CTA per work item, persistent over the list.
 // ----------------------------------------------------------------------------------------------
 template <typename Source>
-__global__ void __launch_bounds__(BSE_THREADS, 2)
+__global__ void __launch_bounds__(BSE_THREADS, 3)
     bse_solve_sum_fp64_kernel(Source src, const WorkItem* __restrict__ work, int n_items, int N, int n2,
                               int nv, int W, int Q, double beta, double2* __restrict__ out,
                               int* __restrict__ status, double2* __restrict__ scratch, size_t slot_elems) {
@@ -479,23 +528,26 @@ __global__ void __launch_bounds__(BSE_THREADS, 2)
 
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const WorkItem wi = work[item];
-    // form A column by column; each thread keeps the (pair, nu) split of its rows in registers
+    // form A column by column; the (pair, nu) split of a thread's rows advances by T = q_T nv + r_T per step
     {
-      constexpr int MAXR = BSE_MAX_N / BSE_THREADS;
-      int pr[MAXR], vr[MAXR];
-#pragma unroll
-      for (int m = 0; m < MAXR; ++m) {
-        const int i = tid + m * T;
-        pr[m] = i / nv;
-        vr[m] = i - pr[m] * nv;
-      }
+      const int pr0 = tid / nv, vr0 = tid - pr0 * nv;
+      const int qT = T / nv, rT = T - qT * nv;
+      int pc = 0, vc = 0;
       for (int j = 0; j < N; ++j) {
-        const int pc = j / nv, vc = j - pc * nv;
         double2* col = A + (size_t)j * N;
-#pragma unroll
-        for (int m = 0; m < MAXR; ++m) {
-          const int i = tid + m * T;
-          if (i < N) col[i] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr[m], vr[m], pc, vc);
+        int pr = pr0, vr = vr0;
+        for (int i = tid; i < N; i += T) {
+          col[i] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
+          pr += qT;
+          vr += rT;
+          if (vr >= nv) {
+            vr -= nv;
+            ++pr;
+          }
+        }
+        if (++vc == nv) {
+          vc = 0;
+          ++pc;
         }
       }
     }
