@@ -70,6 +70,8 @@ class ClockSampler:
             self._stop.wait(0.2)
 
     def __enter__(self):
+        if self.index < 0:
+            return self
         self._thread = threading.Thread(target=self._run, daemon=True)
         self._thread.start()
         return self
@@ -136,13 +138,16 @@ def barrier(world: int):
         dist.barrier()
 
 
-def fp64_peak_tflops() -> float:
-    """cuBLAS DGEMM 8192^3 best of 5 on this GPU (the FP64 denominator; MEASURED_PEAKS.json holds bf16 only)."""
+def gemm_peak_tflops(dtype_name: str = "float64") -> float:
+    """cuBLAS GEMM 8192^3 best of 5 on this GPU in FP64 or FP32 without TF32 (the FP64 / FP32 denominators;
+    MEASURED_PEAKS.json holds only the bf16 and HBM peaks)."""
     import torch
 
+    torch.backends.cuda.matmul.allow_tf32 = False
+    dtype = getattr(torch, dtype_name)
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
     for _ in range(2):
         torch.matmul(a, b)
     best = 1e9
@@ -232,16 +237,10 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line))
 
 
-def run_ours(args, rank: int, world: int, local: int):
+def time_pass(lp, args, world: int, local: int, sample_clocks: bool):
+    """Warm-up, then K timed device passes (CUDA events on the launching stream, max over ranks)."""
     import torch
 
-    from dgamore_b200 import synthetic
-    from dgamore_b200.pipeline import LadderPass
-
-    cfg = synthetic.CONFIGS[args.config]
-    inp = synthetic.make_inputs(cfg)
-    lp = LadderPass(inp, keep_intermediates=False)
-    sh = lp.sh
     stream = torch.cuda.current_stream()
 
     # warm-up
@@ -249,13 +248,15 @@ def run_ours(args, rank: int, world: int, local: int):
         lp.run()
     torch.cuda.synchronize()
     status = int(lp.bse_status.abs().sum().item()) + int(lp.status.abs().sum().item())
+    sh = lp.sh
 
     # timed region: device-resident inputs, K passes; the BSE launch is timed separately on the same stream
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier(world)
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    clocks = ClockSampler(local if sample_clocks else -1)
+    with clocks:
         start.record(stream)
         for k in range(args.steps):
             lp.status.zero_()
@@ -277,7 +278,33 @@ def run_ours(args, rank: int, world: int, local: int):
     t = max_over_ranks(t_local, world)
     bse_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
     value = world * sh.n_solves * args.steps / t
-    kernels_per_pass = 14 if lp.do_lambda else 13
+    return {"t": t, "value": value, "bse_ms": bse_ms, "status": status, "clocks": clocks}
+
+
+def run_ours(args, rank: int, world: int, local: int):
+    import torch
+
+    from dgamore_b200 import synthetic
+    from dgamore_b200.pipeline import LadderPass
+
+    cfg = synthetic.CONFIGS[args.config]
+    inp = synthetic.make_inputs(cfg)
+    stream = torch.cuda.current_stream()
+
+    # FP64 drop-in form first: the reference point of the mixed form and of its Sigma error
+    lp64 = LadderPass(inp, keep_intermediates=False, precision="fp64")
+    r64 = time_pass(lp64, args, world, local, sample_clocks=False)
+    sigma64 = lp64.sigma.clone()
+    del lp64
+    torch.cuda.empty_cache()
+
+    lp = LadderPass(inp, keep_intermediates=False, precision=args.precision)
+    sh = lp.sh
+    res = time_pass(lp, args, world, local, sample_clocks=True)
+    t, value, bse_ms, status, clocks = res["t"], res["value"], res["bse_ms"], res["status"], res["clocks"]
+    sig_err = float((lp.sigma - sigma64).abs().max().item() / sigma64.abs().max().item())
+    iters = lp.bse_iters.cpu().numpy() if args.precision == "mixed" else None
+    kernels_per_pass = (14 if lp.do_lambda else 13) + (1 if args.precision == "mixed" else 0)
 
     # end-to-end through the public API: host G(k) -> device pass -> host Sigma
     for _ in range(1):
@@ -292,8 +319,9 @@ def run_ours(args, rank: int, world: int, local: int):
     t_e2e = max_over_ranks(e_s.elapsed_time(e_e) / 1e3, world)
     e2e_value = world * sh.n_solves * args.steps / t_e2e
 
-    peaks = measured_peaks()
-    fp64_peak = fp64_peak_tflops() if rank == 0 else None
+    fp64_peak = gemm_peak_tflops("float64") if rank == 0 else None
+    fp32_peak = gemm_peak_tflops("float32") if rank == 0 else None
+    peak = fp32_peak if args.precision == "mixed" else fp64_peak
     flops_launch = sh.n_solves * f_solve(sh.N, sh.n2)
     achieved = flops_launch / (bse_ms / 1e3) / 1e12
     line = {
@@ -307,12 +335,12 @@ def run_ours(args, rank: int, world: int, local: int):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "complex128",
+        "dtype": "complex64 LU + complex128 refinement" if args.precision == "mixed" else "complex128",
         "data": "synthetic (seeded model inputs with the configuration's shapes; see dgamore_b200/synthetic.py)",
         "config": {
             "workload": f"{args.config}: {cfg.n_bands}-orbital {cfg.nk[0]}x{cfg.nk[1]} square lattice, "
             f"niv=niw={cfg.niv}, N={sh.N}, {sh.n_q} irreducible q, {sh.n_solves} solves per pass",
-            "precision": "fp64 drop-in",
+            "precision": "mixed (FP32 LU, FP64 refinement)" if args.precision == "mixed" else "fp64 drop-in",
             "step": "one full nonlocal pass (bubble, dc kernel, chi0^-1, BSE dens+magn, chi_phys, lambda, kernel, Sigma)",
             "l2": "inputs larger than L2 (Gamma_r alone is %.0f MB)" % (lp.gamma_cm.numel() * 16 / 1e6),
             "parallelism": f"{world} independent replica(s)",
@@ -324,14 +352,25 @@ def run_ours(args, rank: int, world: int, local: int):
             "h2d_bytes_per_step": lp.h2d_bytes,
             "d2h_bytes_per_step": lp.d2h_bytes,
         },
+        "fp64_dropin": {
+            "value": r64["value"],
+            "ms_per_step": 1e3 * r64["t"] / args.steps,
+            "bse_ms_per_launch": r64["bse_ms"],
+            "bse_tflops": flops_launch / (r64["bse_ms"] / 1e3) / 1e12,
+            "bse_frac_of_fp64_peak": (flops_launch / (r64["bse_ms"] / 1e3) / 1e12 / fp64_peak) if fp64_peak else None,
+        },
+        "mixed_vs_fp64": value / r64["value"],
+        "sigma_rel_err_vs_fp64": sig_err,
+        "refinement_iters": None if iters is None else {"mean": float(iters.mean()), "max": int(iters.max())},
         "roofline": {
             "bound": "tensor",
-            "kernel": "bse_solve_sum_fp64_kernel",
+            "kernel": "bse_solve_sum_mixed_kernel" if args.precision == "mixed" else "bse_solve_sum_fp64_kernel",
             "achieved": achieved,
-            "peak": fp64_peak,
+            "peak": peak,
             "unit": "TFLOP/s",
-            "frac": (achieved / fp64_peak) if fp64_peak else None,
-            "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has bf16 and HBM only)",
+            "frac": (achieved / peak) if peak else None,
+            "peak_source": ("FP32 cuBLAS SGEMM (no TF32) 8192^3" if args.precision == "mixed" else "FP64 cuBLAS DGEMM 8192^3")
+            + " measured in this run (MEASURED_PEAKS.json has bf16 and HBM only)",
             "flops_per_launch": flops_launch,
             "bse_ms_per_launch": bse_ms,
             "traffic": None,
@@ -350,6 +389,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c3")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-items", type=int, default=4)
     ap.add_argument("--ref-items", type=int, default=3)

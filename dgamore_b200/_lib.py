@@ -29,6 +29,9 @@ SIGNATURES = {
     "dga_bse_solve_sum_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, VP, PI, VP, SZ, VP]),
     "dga_invert_sum_dense_c128": (I, [I, I, I, I, D, VP, PI, I, VP, PI, VP, SZ, VP]),
     "dga_bse_solve_sum_noalloc_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, VP, PI, VP]),
+    "dga_bse_mixed_scratch_bytes": (SZ, [I, I, I]),
+    "dga_bse_solve_sum_mixed_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, I, D, VP, PI, PI, VP, SZ, VP]),
+    "dga_bse_resolve_fp64_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, VP, PI, I, VP, SZ, VP]),
     "dga_chi_phys_c128": (I, [VP, VP, VP, VP, I, I, I, I, I, D, VP, PI, VP]),
     "dga_lambda_c128": (I, [VP, I, I, I, PI, VP, D, D, D, D, I, PD, PI, PI, VP, VP]),
     "dga_kernel_assembly_c128": (I, [VP, VP, VP, VP, VP, I, I, I, I, D, VP, VP, VP]),

@@ -33,6 +33,7 @@ constexpr int BSE_NB = 32;  // panel width (also the row-block of the triangular
 constexpr int BSE_TM = 32;  // trailing-update row tile
 constexpr int BSE_TN = 64;  // trailing-update column strip
 constexpr int BSE_MAX_N = 2048;
+constexpr int MAX_RHS = 16;  // n2 <= 16 (up to 4 orbitals)
 
 // ----------------------------------------------------------------------------------------------
 // Matrix sources: how A(i, j) of a work item is formed
@@ -393,9 +394,9 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
 // block is solved by one warp per right-hand side (lane = row, the solved value broadcast by shuffle), the
 // rest of the rows are updated from the block copy in shared memory.
 // ----------------------------------------------------------------------------------------------
-template <typename C, typename CY>
-__device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __restrict__ Y, int n_rhs,
-                                 BseSmem<C>& sm) {
+template <typename C, typename CY, int NR>
+__device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __restrict__ Y, BseSmem<C>& sm) {
+  constexpr int n_rhs = NR;
   using RY = decltype(CY::x);
   const int tid = threadIdx.x, T = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
@@ -425,16 +426,19 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
       }
     }
     __syncthreads();
-    const int rows = N - b0 - bn;
-    for (int e = tid; e < rows * n_rhs; e += T) {
-      const int i = b0 + bn + e % rows, s = e / rows;
-      CY acc = Y[(size_t)s * N + i];
-#pragma unroll 8
+    // rows below the block: one thread per row, every right-hand side at once (each L element read once)
+    for (int i = b0 + bn + tid; i < N; i += T) {
+      CY acc[NR];
+#pragma unroll
+      for (int s = 0; s < NR; ++s) acc[s] = Y[(size_t)s * N + i];
       for (int r = 0; r < bn; ++r) {
         const C l = A[(size_t)(b0 + r) * ld + i];
-        cfms(acc, cmake<CY>((RY)l.x, (RY)l.y), yb[s * 32 + r]);
+        const CY lw = cmake<CY>((RY)l.x, (RY)l.y);
+#pragma unroll
+        for (int s = 0; s < NR; ++s) cfms(acc[s], lw, yb[s * 32 + r]);
       }
-      Y[(size_t)s * N + i] = acc;
+#pragma unroll
+      for (int s = 0; s < NR; ++s) Y[(size_t)s * N + i] = acc[s];
     }
     __syncthreads();
   }
@@ -469,15 +473,19 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
       }
     }
     __syncthreads();
-    for (int e = tid; e < b0 * n_rhs; e += T) {
-      const int i = e % b0, s = e / b0;
-      CY acc = Y[(size_t)s * N + i];
-#pragma unroll 8
+    // rows above the block: one thread per row, every right-hand side at once (each U element read once)
+    for (int i = tid; i < b0; i += T) {
+      CY acc[NR];
+#pragma unroll
+      for (int s = 0; s < NR; ++s) acc[s] = Y[(size_t)s * N + i];
       for (int r = 0; r < bn; ++r) {
         const C u = A[(size_t)(b0 + r) * ld + i];
-        cfms(acc, cmake<CY>((RY)u.x, (RY)u.y), yb[s * 32 + r]);
+        const CY uw = cmake<CY>((RY)u.x, (RY)u.y);
+#pragma unroll
+        for (int s = 0; s < NR; ++s) cfms(acc[s], uw, yb[s * 32 + r]);
       }
-      Y[(size_t)s * N + i] = acc;
+#pragma unroll
+      for (int s = 0; s < NR; ++s) Y[(size_t)s * N + i] = acc[s];
     }
     __syncthreads();
   }
@@ -513,11 +521,12 @@ __device__ void permuted_selector(CY* __restrict__ Y, int N, int nv, int n_rhs, 
 // ----------------------------------------------------------------------------------------------
 // FP64 kernel: one CTA per work item, persistent over the list.
 // ----------------------------------------------------------------------------------------------
-template <typename Source>
+template <typename Source, int NR>
 __global__ void __launch_bounds__(BSE_THREADS, 3)
     bse_solve_sum_fp64_kernel(Source src, const WorkItem* __restrict__ work, int n_items, int N, int n2,
                               int nv, int W, int Q, double beta, double2* __restrict__ out,
-                              int* __restrict__ status, double2* __restrict__ scratch, size_t slot_elems) {
+                              int* __restrict__ status, double2* __restrict__ scratch, size_t slot_elems,
+                              int redo_only) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BseSmem<double2>& sm = *reinterpret_cast<BseSmem<double2>*>(smem_raw);
   int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<double2>));
@@ -527,6 +536,8 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   const int tid = threadIdx.x, T = blockDim.x;
 
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    // re-solve mode: only the items whose status says the mixed solve did not converge or was not finite
+    if (redo_only && (status[item] & (DGA_ITEM_NOCONVERGE | DGA_ITEM_NONFINITE)) == 0) continue;
     const WorkItem wi = work[item];
     // form A column by column; the (pair, nu) split of a thread's rows advances by T = q_T nv + r_T per step
     {
@@ -553,8 +564,8 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
     }
     __syncthreads();
     const bool singular = lu_factor<double2>(A, N, N, piv, sm);
-    permuted_selector<double2>(Y, N, nv, n2, piv, perm);
-    lu_solve_inplace<double2, double2>(A, N, N, Y, n2, sm);
+    permuted_selector<double2>(Y, N, nv, NR, piv, perm);
+    lu_solve_inplace<double2, double2, NR>(A, N, N, Y, sm);
     // write X[(ch, q, w)][i][s] = Y[i][s] / beta and check finiteness
     if (tid == 0) sm.flag = 0;
     __syncthreads();
@@ -575,22 +586,242 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   }
 }
 
+
+// ----------------------------------------------------------------------------------------------
+// Mixed form: FP32 LU (same core, float2 storage, FP32 trailing updates) and FP64 iterative refinement.
+//
+//   Y0 = (LU)^-1 P S with the FP32 factors and FP64 accumulation of the triangular solves;
+//   repeat: r = S - A Y with A formed on the fly in FP64 from Gamma_r, chi0^-1 and U_r + V_r^q,
+//           d = (LU)^-1 P r,  Y += d,  until max|d| <= tol max|Y| or max_iter corrections.
+//
+// FP64 is used only for A in the residual, the residual accumulation and Y.  Items that do not reach the
+// tolerance are flagged DGA_ITEM_NOCONVERGE (the host re-solves them with the FP64 kernel).
+// ----------------------------------------------------------------------------------------------
+
+// r[s][i] = S[perm[i]][s] - (A Y)[perm[i]][s]: the residual of original row perm[i], stored at position i
+// (so the correction solve needs no separate permutation).  colsum: shared [n2][n2]; ys: shared [32][n2]
+// staging of Y rows, so the Gamma stream is the only global traffic of the inner loop.
+template <int NR>
+__device__ void structured_residual_permuted(const StructuredSource& src, int ch, int q, int w, int N, int nv,
+                                             const double2* __restrict__ Y, double2* __restrict__ Rp,
+                                             const int* __restrict__ perm, double2* colsum, double2* ys) {
+  constexpr int n2 = NR;
+  const int tid = threadIdx.x, T = blockDim.x;
+  // column sums over nu' of Y for the rank-n2 (U_r + V_r^q) part
+  for (int e = tid; e < n2 * n2; e += T) {
+    const int pc = e / n2, sidx = e - pc * n2;
+    double2 acc = make_double2(0.0, 0.0);
+    const double2* y = Y + (size_t)sidx * N + pc * nv;
+    for (int v = 0; v < nv; ++v) acc = cadd(acc, y[v]);
+    colsum[pc * n2 + sidx] = acc;
+  }
+  __syncthreads();
+  const double2* gam = src.gamma_cm + (size_t)(ch * src.W + w) * N * N;
+  const double2* uvq = src.uv + ((size_t)ch * src.Q + q) * n2 * n2;
+  for (int pos0 = 0; pos0 < N; pos0 += T) {
+    const int pos = pos0 + tid;
+    const bool active = pos < N;
+    const int i = active ? perm[pos] : 0;
+    double2 acc[NR];
+#pragma unroll
+    for (int sidx = 0; sidx < NR; ++sidx) acc[sidx] = make_double2(0.0, 0.0);
+    // Gamma part: sum_j Gamma[i][j] Y[j][s], Y staged 32 rows at a time
+    for (int j0 = 0; j0 < N; j0 += 32) {
+      const int jw = min(32, N - j0);
+      for (int e = tid; e < jw * NR; e += T) {
+        const int jj = e % jw, sidx = e / jw;
+        ys[jj * NR + sidx] = Y[(size_t)sidx * N + j0 + jj];
+      }
+      __syncthreads();
+      if (active) {
+        for (int jj = 0; jj < jw; ++jj) {
+          const double2 g = gam[(size_t)(j0 + jj) * N + i];
+#pragma unroll
+          for (int sidx = 0; sidx < NR; ++sidx) cfma(acc[sidx], g, ys[jj * NR + sidx]);
+        }
+      }
+      __syncthreads();
+    }
+    if (active) {
+      const int pr = i / nv, vr = i - pr * nv;
+      const double2* c0 = src.chi0_inv + (((size_t)q * src.W + w) * nv + vr) * n2 * n2 + pr * n2;
+#pragma unroll
+      for (int sidx = 0; sidx < NR; ++sidx) {
+        double2 a = cscale(acc[sidx], src.inv_beta2);
+        double2 d = make_double2(0.0, 0.0), u = make_double2(0.0, 0.0);
+        for (int pc = 0; pc < n2; ++pc) {
+          cfma(d, c0[pc], Y[(size_t)sidx * N + pc * nv + vr]);
+          cfma(u, uvq[pr * n2 + pc], colsum[pc * n2 + sidx]);
+        }
+        a = cadd(a, d);
+        a = csub(a, cscale(u, src.inv_beta2));
+        const double sel = (pr == sidx) ? 1.0 : 0.0;
+        Rp[(size_t)sidx * N + pos] = make_double2(sel - a.x, -a.y);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    v = lane < nw ? red[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+    if (lane == 0) red[0] = v;
+  }
+  __syncthreads();
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// byte offset of the [n2][n2] column-sum block after the pivot and permutation arrays, 16-byte aligned
+__host__ __device__ inline size_t mixed_colsum_offset(int N) {
+  return (sizeof(BseSmem<float2>) + 2 * sizeof(int) * (size_t)N + 15) & ~(size_t)15;
+}
+
+template <int NR>
+__global__ void __launch_bounds__(BSE_THREADS, 3)
+    bse_solve_sum_mixed_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int n2,
+                               int nv, int W, int Q, double beta, int max_iter, double tol,
+                               double2* __restrict__ out, int* __restrict__ status, int* __restrict__ iters,
+                               unsigned char* __restrict__ scratch, size_t slot_bytes) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BseSmem<float2>& sm = *reinterpret_cast<BseSmem<float2>*>(smem_raw);
+  int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<float2>));
+  int* perm = piv + N;
+  double2* colsum = reinterpret_cast<double2*>(smem_raw + mixed_colsum_offset(N));
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  float2* A = reinterpret_cast<float2*>(slot);
+  double2* Y = reinterpret_cast<double2*>(slot + (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255));
+  double2* Rb = Y + (size_t)N * n2;
+  const int tid = threadIdx.x, T = blockDim.x;
+
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const WorkItem wi = work[item];
+    {
+      const int pr0 = tid / nv, vr0 = tid - pr0 * nv;
+      const int qT = T / nv, rT = T - qT * nv;
+      int pc = 0, vc = 0;
+      for (int j = 0; j < N; ++j) {
+        float2* col = A + (size_t)j * N;
+        int pr = pr0, vr = vr0;
+        for (int i = tid; i < N; i += T) {
+          const double2 a = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
+          col[i] = make_float2((float)a.x, (float)a.y);
+          pr += qT;
+          vr += rT;
+          if (vr >= nv) {
+            vr -= nv;
+            ++pr;
+          }
+        }
+        if (++vc == nv) {
+          vc = 0;
+          ++pc;
+        }
+      }
+    }
+    __syncthreads();
+    const bool singular = lu_factor<float2>(A, N, N, piv, sm);
+    permuted_selector<double2>(Y, N, nv, NR, piv, perm);
+    lu_solve_inplace<float2, double2, NR>(A, N, N, Y, sm);
+    int it = 0;
+    bool converged = false;
+    for (; it < max_iter; ++it) {
+      structured_residual_permuted<NR>(src, wi.ch, wi.q, wi.w, N, nv, Y, Rb, perm, colsum,
+                                       reinterpret_cast<double2*>(&sm.u));
+      lu_solve_inplace<float2, double2, NR>(A, N, N, Rb, sm);
+      double dmax = 0.0, ymax = 0.0;
+      for (int e = tid; e < N * n2; e += T) {
+        const double2 d = Rb[e];
+        const double2 y = cadd(Y[e], d);
+        Y[e] = y;
+        dmax = fmax(dmax, fmax(fabs(d.x), fabs(d.y)));
+        ymax = fmax(ymax, fmax(fabs(y.x), fabs(y.y)));
+      }
+      dmax = block_max(dmax, sm.red_val);
+      ymax = block_max(ymax, sm.red_val);
+      if (!(dmax > tol * ymax)) {  // also stops on NaN, flagged below
+        converged = dmax <= tol * ymax;
+        ++it;
+        break;
+      }
+    }
+    if (tid == 0) sm.flag = 0;
+    __syncthreads();
+    double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * n2;
+    bool bad = false;
+    for (int e = tid; e < N * n2; e += T) {
+      const int i = e / n2, sidx = e % n2;
+      double2 y = Y[(size_t)sidx * N + i];
+      y.x = y.x / beta;
+      y.y = y.y / beta;
+      if (!cfinite(y)) bad = true;
+      o[e] = y;
+    }
+    if (bad) atomicOr(&sm.flag, DGA_ITEM_NONFINITE);
+    __syncthreads();
+    if (tid == 0) {
+      if (status) status[item] = (singular ? DGA_ITEM_SINGULAR : 0) | sm.flag | (converged ? 0 : DGA_ITEM_NOCONVERGE);
+      if (iters) iters[item] = it;
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace dga
 
 using namespace dga;
 
 static size_t bse_smem_bytes(int N) { return sizeof(BseSmem<double2>) + 2 * sizeof(int) * (size_t)N; }
 
-static int bse_grid(int n_items, size_t smem) {
+template <typename K>
+static int grid_for(K kernel, int n_items, size_t smem) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bse_solve_sum_fp64_kernel<StructuredSource>,
-                                                BSE_THREADS, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BSE_THREADS, smem);
   if (per_sm < 1) per_sm = 1;
   int g = sms * per_sm;
   return n_items < g ? n_items : g;
+}
+
+static int bse_grid(int n_items, size_t smem) {
+  return grid_for(bse_solve_sum_fp64_kernel<StructuredSource, 9>, n_items, smem);
+}
+
+static bool supported_rhs(int n2) { return n2 == 1 || n2 == 4 || n2 == 9 || n2 == 16; }
+
+// Launches the FP64 kernel instantiated for n2 right-hand sides (1, 4, 9 or 16 orbital pairs).
+template <typename Source>
+static void launch_fp64(int n2, int grid, size_t smem, cudaStream_t stream, const Source& src, const WorkItem* work,
+                        int n_items, int N, int nv, int W, int Q, double beta, double2* out, int* status,
+                        double2* scratch, size_t slot, int redo) {
+#define DGA_FP64_CASE(NRV)                                                                                        \
+  case NRV:                                                                                                       \
+    cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<Source, NRV>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                         (int)smem);                                                                              \
+    bse_solve_sum_fp64_kernel<Source, NRV><<<grid, BSE_THREADS, smem, stream>>>(                                  \
+        src, work, n_items, N, NRV, nv, W, Q, beta, out, status, scratch, slot, redo);                            \
+    break;
+  switch (n2) {
+    DGA_FP64_CASE(1)
+    DGA_FP64_CASE(4)
+    DGA_FP64_CASE(9)
+    DGA_FP64_CASE(16)
+    default:
+      break;
+  }
+#undef DGA_FP64_CASE
 }
 
 extern "C" {
@@ -600,8 +831,6 @@ extern "C" {
 size_t dga_bse_scratch_bytes(int N, int n2, int n_items) {
   if (N <= 0 || n2 <= 0 || n_items <= 0) return 0;
   const size_t smem = bse_smem_bytes(N);
-  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<StructuredSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
   const int grid = bse_grid(n_items, smem);
   return (size_t)grid * ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
 }
@@ -611,7 +840,7 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
                            int n_items, void* out, int* status, void* scratch, size_t scratch_bytes,
                            cudaStream_t stream) {
   const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
-  if (n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0 || N > BSE_MAX_N) {
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0 || N > BSE_MAX_N) {
     dga_set_error("dga_bse_solve_sum_c128: invalid sizes (n_orb=%d niv=%d niw_half=%d n_q=%d n_ch=%d items=%d)",
                   n_orb, niv, niw_half, n_q, n_ch, n_items);
     return DGA_ERR_ARG;
@@ -621,8 +850,6 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
     return DGA_ERR_ARG;
   }
   const size_t smem = bse_smem_bytes(N);
-  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<StructuredSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
   const int grid = bse_grid(n_items, smem);
   const size_t slot = (size_t)N * N + (size_t)N * n2;
   if (scratch_bytes < (size_t)grid * slot * sizeof(double2)) {
@@ -639,12 +866,51 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
   src.W = niw_half;
   src.Q = n_q;
   src.inv_beta2 = inv_beta2;
-  bse_solve_sum_fp64_kernel<StructuredSource><<<grid, BSE_THREADS, smem, stream>>>(
-      src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, (double2*)out, status,
-      (double2*)scratch, slot);
+  launch_fp64(n2, grid, smem, stream, src, (const WorkItem*)work, n_items, N, nv, niw_half, n_q, beta,
+              (double2*)out, status, (double2*)scratch, slot, 0);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     dga_set_error("dga_bse_solve_sum_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+// FP64 re-solve of the items a mixed launch flagged (status & (NOCONVERGE | NONFINITE)); other items are left
+// untouched.  Same arguments as dga_bse_solve_sum_c128 with `status` read and rewritten for the re-solved items;
+// the scratch may be sized for a smaller grid (grid_limit CTAs).
+int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                              const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work, int n_items,
+                              void* out, int* status, int grid_limit, void* scratch, size_t scratch_bytes,
+                              cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0 || N > BSE_MAX_N ||
+      grid_limit <= 0 || !gamma_cm || !chi0_inv || !uv || !work || !out || !status || !scratch) {
+    dga_set_error("dga_bse_resolve_fp64_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = bse_smem_bytes(N);
+  int grid = bse_grid(n_items, smem);
+  if (grid > grid_limit) grid = grid_limit;
+  const size_t slot = (size_t)N * N + (size_t)N * n2;
+  if (scratch_bytes < (size_t)grid * slot * sizeof(double2)) {
+    dga_set_error("dga_bse_resolve_fp64_c128: scratch too small");
+    return DGA_ERR_SCRATCH;
+  }
+  StructuredSource src;
+  src.gamma_cm = (const double2*)gamma_cm;
+  src.chi0_inv = (const double2*)chi0_inv;
+  src.uv = (const double2*)uv;
+  src.n2 = n2;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  src.inv_beta2 = inv_beta2;
+  launch_fp64(n2, grid, smem, stream, src, (const WorkItem*)work, n_items, N, nv, niw_half, n_q, beta,
+              (double2*)out, status, (double2*)scratch, slot, 1);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_bse_resolve_fp64_c128: launch failed: %s", cudaGetErrorString(err));
     return DGA_ERR_LAUNCH;
   }
   return DGA_OK;
@@ -656,14 +922,12 @@ int dga_invert_sum_dense_c128(int n_orb, int niv, int niw_half, int n_q, double 
                               const int* work, int n_items, void* out, int* status, void* scratch,
                               size_t scratch_bytes, cudaStream_t stream) {
   const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
-  if (n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_items <= 0 || N > BSE_MAX_N || !mat || !work ||
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_items <= 0 || N > BSE_MAX_N || !mat || !work ||
       !out || !scratch) {
     dga_set_error("dga_invert_sum_dense_c128: invalid arguments");
     return DGA_ERR_ARG;
   }
   const size_t smem = bse_smem_bytes(N);
-  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<DenseSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
   const int grid = bse_grid(n_items, smem);
   const size_t slot = (size_t)N * N + (size_t)N * n2;
   if (scratch_bytes < (size_t)grid * slot * sizeof(double2)) {
@@ -676,12 +940,94 @@ int dga_invert_sum_dense_c128(int n_orb, int niv, int niw_half, int n_q, double 
   src.nv = nv;
   src.W = niw_half;
   src.Q = n_q;
-  bse_solve_sum_fp64_kernel<DenseSource><<<grid, BSE_THREADS, smem, stream>>>(
-      src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, (double2*)out, status,
-      (double2*)scratch, slot);
+  launch_fp64(n2, grid, smem, stream, src, (const WorkItem*)work, n_items, N, nv, niw_half, n_q, beta,
+              (double2*)out, status, (double2*)scratch, slot, 0);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     dga_set_error("dga_invert_sum_dense_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"
+
+
+static size_t mixed_smem_bytes(int N, int n2) { return mixed_colsum_offset(N) + (size_t)n2 * n2 * sizeof(double2); }
+
+static size_t mixed_slot_bytes(int N, int n2) {
+  return (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255) + 2 * (size_t)N * n2 * sizeof(double2);
+}
+static int mixed_grid(int n_items, size_t smem) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  (void)sms;
+  return grid_for(bse_solve_sum_mixed_kernel<9>, n_items, smem);
+}
+
+extern "C" {
+
+// Scratch bytes of dga_bse_solve_sum_mixed_c128: one N x N complex64 matrix and two N x n2 complex128
+// blocks per resident CTA.
+size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items) {
+  if (N <= 0 || n2 <= 0 || n_items <= 0) return 0;
+  const size_t smem = mixed_smem_bytes(N, n2);
+  return (size_t)mixed_grid(n_items, smem) * mixed_slot_bytes(N, n2);
+}
+
+// Mixed-precision ladder BSE: same inputs and output as dga_bse_solve_sum_c128; FP32 LU, FP64 residuals and
+// refinement to max|d| <= tol max|Y| within max_iter corrections.  iters: per-item corrections (optional).
+int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                                 const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
+                                 int n_items, int max_iter, double tol, void* out, int* status, int* iters,
+                                 void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0 || N > BSE_MAX_N ||
+      n2 > MAX_RHS || max_iter < 0) {
+    dga_set_error("dga_bse_solve_sum_mixed_c128: invalid sizes (n_orb=%d niv=%d niw_half=%d n_q=%d n_ch=%d items=%d)",
+                  n_orb, niv, niw_half, n_q, n_ch, n_items);
+    return DGA_ERR_ARG;
+  }
+  if (!gamma_cm || !chi0_inv || !uv || !work || !out || !scratch) {
+    dga_set_error("dga_bse_solve_sum_mixed_c128: null pointer argument");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = mixed_smem_bytes(N, n2);
+  const int grid = mixed_grid(n_items, smem);
+  const size_t slot = mixed_slot_bytes(N, n2);
+  if (scratch_bytes < (size_t)grid * slot) {
+    dga_set_error("dga_bse_solve_sum_mixed_c128: scratch too small (%zu < %zu)", scratch_bytes, (size_t)grid * slot);
+    return DGA_ERR_SCRATCH;
+  }
+  StructuredSource src;
+  src.gamma_cm = (const double2*)gamma_cm;
+  src.chi0_inv = (const double2*)chi0_inv;
+  src.uv = (const double2*)uv;
+  src.n2 = n2;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  src.inv_beta2 = inv_beta2;
+#define DGA_MIXED_CASE(NRV)                                                                                       \
+  case NRV:                                                                                                       \
+    cudaFuncSetAttribute(bse_solve_sum_mixed_kernel<NRV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    bse_solve_sum_mixed_kernel<NRV><<<grid, BSE_THREADS, smem, stream>>>(                                          \
+        src, (const WorkItem*)work, n_items, N, NRV, nv, niw_half, n_q, beta, max_iter, tol, (double2*)out, status, \
+        iters, (unsigned char*)scratch, slot);                                                                    \
+    break;
+  switch (n2) {
+    DGA_MIXED_CASE(1)
+    DGA_MIXED_CASE(4)
+    DGA_MIXED_CASE(9)
+    DGA_MIXED_CASE(16)
+    default:
+      break;
+  }
+#undef DGA_MIXED_CASE
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_bse_solve_sum_mixed_c128: launch failed: %s", cudaGetErrorString(err));
     return DGA_ERR_LAUNCH;
   }
   return DGA_OK;
@@ -745,7 +1091,7 @@ int dga_bse_solve_sum_noalloc_c128(int n_orb, int niv, int niw_half, int n_q, in
                                    double inv_beta2, const void* gamma_cm, const void* chi0_inv, const void* uv,
                                    const int* work, int n_items, void* out, int* status, cudaStream_t stream) {
   const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
-  if (n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0) {
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0) {
     dga_set_error("dga_bse_solve_sum_noalloc_c128: invalid sizes (n_orb=%d niv=%d niw_half=%d n_q=%d n_ch=%d "
                   "items=%d)", n_orb, niv, niw_half, n_q, n_ch, n_items);
     return DGA_ERR_ARG;
@@ -766,8 +1112,6 @@ int dga_bse_solve_sum_noalloc_c128(int n_orb, int niv, int niw_half, int n_q, in
   int rc = noalloc_scratch_ptr(&scratch);
   if (rc != DGA_OK) return rc;
   const size_t smem = bse_smem_bytes(N);
-  cudaFuncSetAttribute(bse_solve_sum_fp64_kernel<StructuredSource>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
   int grid = bse_grid(n_items, smem);
   if ((size_t)grid > capacity_slots) grid = (int)capacity_slots;
   StructuredSource src;
@@ -779,9 +1123,8 @@ int dga_bse_solve_sum_noalloc_c128(int n_orb, int niv, int niw_half, int n_q, in
   src.W = niw_half;
   src.Q = n_q;
   src.inv_beta2 = inv_beta2;
-  bse_solve_sum_fp64_kernel<StructuredSource><<<grid, BSE_THREADS, smem, stream>>>(
-      src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, (double2*)out, status,
-      (double2*)scratch, slot);
+  launch_fp64(n2, grid, smem, stream, src, (const WorkItem*)work, n_items, N, nv, niw_half, n_q, beta,
+              (double2*)out, status, (double2*)scratch, slot, 0);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     dga_set_error("dga_bse_solve_sum_noalloc_c128: launch failed: %s", cudaGetErrorString(err));

@@ -104,7 +104,8 @@ class LadderPass:
     """Resident inputs, work buffers and the kernel sequence of one nonlocal pass."""
 
     def __init__(self, inp: dict, device: str = "cuda", do_lambda: bool | None = None, sigma_chunks: int | None = None,
-                 keep_intermediates: bool = True):
+                 keep_intermediates: bool = True, precision: str = "fp64", refine_tol: float = 1e-10,
+                 refine_max_iter: int = 6, resolve_grid: int = 148):
         lib()  # fail loudly before anything else if the CUDA library is missing
         self.dev = torch.device(device)
         g_k = np.asarray(inp["g_k"])
@@ -122,6 +123,11 @@ class LadderPass:
         if self.do_lambda and n_orb != 1:
             raise NotImplementedError("the lambda-correction is single-band only (dgamore/DGAmore.py:501-508)")
         self.keep = keep_intermediates
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+        self.precision = precision
+        self.refine_tol = float(refine_tol)
+        self.refine_max_iter = int(refine_max_iter)
         dev = self.dev
         beta = sh.beta
         # ---------------- host-side preparation (once per request) ----------------
@@ -182,7 +188,15 @@ class LadderPass:
         )
         self.X = torch.empty((2, Q, W, N, n2), dtype=C128, device=dev)
         self.bse_status = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
-        self.bse_scratch_bytes = int(lib().dga_bse_scratch_bytes(N, n2, self.n_items))
+        if precision == "fp64":
+            self.bse_scratch_bytes = int(lib().dga_bse_scratch_bytes(N, n2, self.n_items))
+        else:
+            # mixed solve + a small FP64 grid for the status-driven re-solve of unconverged items
+            self.resolve_grid = int(resolve_grid)
+            self.mixed_scratch_bytes = int(lib().dga_bse_mixed_scratch_bytes(N, n2, self.n_items))
+            self.bse_scratch_bytes = self.resolve_grid * (N * N + N * n2) * 16
+            self.mixed_scratch = torch.empty(self.mixed_scratch_bytes // 16 + 1, dtype=C128, device=dev)
+            self.bse_iters = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
         self.bse_scratch = torch.empty(self.bse_scratch_bytes // 16 + 1, dtype=C128, device=dev)
         self.chi_phys = torch.empty((2, Q, W, n2, n2), dtype=C128, device=dev)
         self.chi_lam = torch.empty((2, Q, W, n2, n2), dtype=C128, device=dev)
@@ -233,6 +247,15 @@ class LadderPass:
 
     def bse(self):
         sh = self.sh
+        if self.precision == "mixed":
+            call("dga_bse_solve_sum_mixed_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
+                 _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, self.refine_max_iter,
+                 self.refine_tol, _p(self.X), _p(self.bse_status), _p(self.bse_iters), _p(self.mixed_scratch),
+                 self.mixed_scratch.numel() * 16, _s())
+            call("dga_bse_resolve_fp64_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
+                 _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, _p(self.X),
+                 _p(self.bse_status), self.resolve_grid, _p(self.bse_scratch), self.bse_scratch.numel() * 16, _s())
+            return
         call("dga_bse_solve_sum_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2, _p(self.gamma_cm),
              _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, _p(self.X), _p(self.bse_status),
              _p(self.bse_scratch), self.bse_scratch.numel() * 16, _s())

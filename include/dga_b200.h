@@ -79,6 +79,24 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
                            const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work, int n_items,
                            void* out, int* status, void* scratch, size_t scratch_bytes, dga_stream_t stream);
 
+/* Mixed-precision ladder BSE (same inputs and outputs as dga_bse_solve_sum_c128): complex64 LU with FP32
+ * trailing updates, then FP64 iterative refinement -- residuals r = S - A Y with A formed in FP64 from Gamma_r,
+ * chi0^-1 and U_r + V_r^q -- until max|correction| <= tol max|Y| or max_iter corrections; items that do not
+ * converge are flagged DGA_ITEM_NOCONVERGE.  Replaces the same upstream functions as dga_bse_solve_sum_c128.
+ * iters: optional per-item number of corrections. */
+size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items);
+int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                                 const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
+                                 int n_items, int max_iter, double tol, void* out, int* status, int* iters,
+                                 void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
+/* FP64 re-solve of the items a mixed launch flagged (status & (NOCONVERGE | NONFINITE)), leaving the others
+ * untouched; at most grid_limit CTAs (scratch: grid_limit * (N*N + N*n2) complex128). */
+int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                              const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work, int n_items,
+                              void* out, int* status, int grid_limit, void* scratch, size_t scratch_bytes,
+                              dga_stream_t stream);
+
 /* Allocation-free variant of dga_bse_solve_sum_c128 (no counterpart in the upstream, which has no device
  * code): for callers that cannot call cudaMalloc -- a host that binds only this C ABI and has no device
  * allocator, or a steady-state loop that must not trigger cudaMalloc's device-wide synchronisation.  The

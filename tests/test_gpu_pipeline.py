@@ -125,3 +125,30 @@ def test_lambda_without_root_reports_nonconvergence():
     torch.cuda.synchronize()
     assert int(status.item()) & 4
     assert np.isfinite(lam.item())
+
+
+@pytest.fixture(scope="module", params=GOLDEN_CONFIGS)
+def mixed_pass(request):
+    from dgamore_b200.pipeline import LadderPass
+
+    inp, ref = load_golden(request.param)
+    lp = LadderPass(inp, precision="mixed")
+    lp.run()
+    torch.cuda.synchronize()
+    return request.param, inp, ref, lp
+
+
+def test_mixed_bse_matches_fp64_reference(mixed_pass):
+    """Mixed form (FP32 LU + FP64 refinement): every solve converges and matches the upstream FP64 BSE."""
+    name, inp, ref, lp = mixed_pass
+    for ch, chname in ((0, "dens"), (1, "magn")):
+        assert rel_err(lp.x_ref_layout(ch), ref[f"chi_aux_sum_{chname}"]) < 1e-11
+    assert int(lp.bse_status.abs().sum().item()) == 0
+    iters = lp.bse_iters.cpu().numpy()
+    assert iters.max() <= lp.refine_max_iter and iters.min() >= 1
+
+
+def test_mixed_sigma_error_bound(mixed_pass):
+    """Sigma from the mixed pass is within 1e-8 of the FP64 upstream Sigma (the mixed-form bound)."""
+    name, inp, ref, lp = mixed_pass
+    assert rel_err(lp.sigma.cpu().numpy(), ref["sigma"]) < 1e-8
