@@ -84,6 +84,9 @@ CONFIGS = {
     "t1b": DgaConfig("t1b", 1, (8, 8, 1), 10.0, 6, 6, 0, u=4.0, t=(1.0,), tp=-0.2, n=0.9, seed=12),
     "t2": DgaConfig("t2", 2, (4, 4, 1), 15.0, 2, 3, 1, u=6.0, t=(1.0, 1.0), t_perp=0.8, v_nn=0.2, n=1.8, seed=13),
     "t3": DgaConfig("t3", 3, (4, 4, 1), 20.0, 2, 2, 0, u=2.3, j=0.4, t=(0.5, 0.5, 0.1), n=1.0, seed=14),
+    # Eliashberg parity cases (niv_pp = min(niw, niv) // 2 = 3)
+    "t4e": DgaConfig("t4e", 2, (6, 6, 1), 15.0, 6, 6, 0, u=6.0, t=(1.0, 1.0), t_perp=0.8, n=1.8, seed=15),
+    "t5e": DgaConfig("t5e", 1, (8, 8, 1), 10.0, 6, 6, 0, u=4.0, t=(1.0,), tp=-0.2, n=0.9, seed=16),
 }
 
 

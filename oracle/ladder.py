@@ -446,3 +446,123 @@ def sde_pass(inp: dict, do_lambda: bool = True) -> dict:
     k_full = map_to_full_bz(k_total, inp["irrk_inv"])
     out["sigma"] = sigma_from_kernel_fft(k_full, inp["g_k"], tuple(inp["nk"]), beta, niv_core)
     return out
+
+
+# ----------------------------------------------------------------------------------------------
+# (a14, a15) Eliashberg: full vertex, PH -> PP (w = 0), pairing vertex and the pairing-kernel eigen-solve
+# ----------------------------------------------------------------------------------------------
+
+
+def full_vertex_q(chi0_inv_core, gamma, uv_q, vrg_r, chi_phys, beta, niv_pp):
+    """F_r(q,w) = beta^2 (chi0^-1 - chi0^-1 chi* chi0^-1) + U_r g g - U_r chi_r U_r g g, cut to the pp box.
+
+    eliashberg_solver.py:175-204 (create_full_vertex_q_r_v2) with chi* the full auxiliary susceptibility
+    (nonlocal_sde.py:72-82), the products of four_point.py:442-588 and the nu-cut of local_n_point.py:134-154.
+    Inputs as in ``sde_pass``; chi_phys [q,a,b,c,d,w] is the (lambda-corrected) physical susceptibility.
+    Returns [q,a,b,c,d,w,2niv_pp,2niv_pp] (half w range).
+    """
+    chi_star = bse_full_inverse(chi0_inv_core, gamma, uv_q, beta)  # [q,abcd,w,nu,nu']
+    nv = chi0_inv_core.shape[-1]
+    eye = np.eye(nv)
+    d_full = chi0_inv_core[..., :, None] * eye  # [q,abcd,w,nu,nu'] diagonal in nu
+    t = np.einsum("qabcdwv,qdcefwvp->qabefwvp", chi0_inv_core, chi_star, optimize=True)
+    t = np.einsum("qabcdwvp,qdcefwp->qabefwvp", t, chi0_inv_core, optimize=True)
+    f1 = beta**2 * (d_full - t)
+    gg = np.einsum("qabcdwv,qdcefwp->qabefwvp", vrg_r, vrg_r, optimize=True)
+    ugg = np.einsum("qabij,qjiefwvp->qabefwvp", uv_q, gg, optimize=True)
+    uc = np.einsum("qabij,qjiefw->qabefw", uv_q, chi_phys, optimize=True)
+    ucu = np.einsum("qabijw,qjief->qabefw", uc, uv_q, optimize=True)
+    ucugg = np.einsum("qabcdw,qdcefwvp->qabefwvp", ucu, gg, optimize=True)
+    f = f1 + ugg - ucugg
+    return cut_niv(f, niv_pp, 2)
+
+
+def ph_to_pp_w0(f_half, niw, niv_pp):
+    """Full vertex to the modified pp notation at w = 0 (eliashberg_solver.py:44-75).
+
+    f_half: [q,a,b,c,d,w>=0,2niv_pp,2niv_pp] (pp box) -> [q,a,b,c,d,2niv_pp,2niv_pp];
+    F_pp[nu, nu'] = -F_full[w = nu - nu'][nu][-nu'-1] with F(-w) = conj(flip F(w)).
+    """
+    nv = 2 * niv_pp
+    vn = np.arange(-niv_pp, niv_pp)
+    omega = vn[:, None] - vn[None, :]
+    full = to_full_niw_range(f_half[..., : niw + 1, :, :], 3)
+    full = np.flip(full, axis=-1)
+    out = np.zeros(f_half.shape[:-3] + (nv, nv), dtype=np.complex128)
+    for idx, w in enumerate(range(-niw, niw + 1)):
+        mask = omega == w
+        out[..., mask] = -full[..., idx, :, :][..., mask]
+    return out
+
+
+def chi0_pp_full_grid(g_k, niv_pp):
+    """chi0pp[kx,ky,kz,a,b,c,d,nu] decompressed (bubble_gen.py:268-279 then decompress_q_dimension)."""
+    nk = g_k.shape[:3]
+    c = chi0_pp_w0_q(g_k, niv_pp)
+    return c.reshape(*nk, *c.shape[1:])
+
+
+def eliashberg_matvec(gamma_r_signed, gamma_flip, chi0pp, gap, beta, sign):
+    """One application of the linearised gap equation (eliashberg_solver.py:420-428).
+
+    gamma_r_signed: sign * FFT_q Gamma_pp(q) [x,y,z,a,b,c,d,nu,nu']; gamma_flip its flipped form
+    (flip_momentum_axis, flip nu', permute abcd->adcb); chi0pp [x,y,z,a,b,c,d,nu]; gap [x,y,z,a,b,nu].
+    """
+    nk_tot = int(np.prod(gap.shape[:3]))
+    norm = 0.5 / nk_tot / beta
+    gap_gg = np.fft.fftn(np.einsum("xyzabcdv,xyzcdv->xyzabv", chi0pp, gap, optimize=True), axes=(0, 1, 2))
+    gap_gg_flipped = np.roll(np.flip(gap_gg, axis=(0, 1, 2)), shift=1, axis=(0, 1, 2))
+    new = np.einsum("xyzacbdvp,xyzcdp->xyzabv", gamma_r_signed, gap_gg, optimize=True) + sign * np.einsum(
+        "xyzacbdvp,xyzcdp->xyzabv", gamma_flip, gap_gg_flipped, optimize=True
+    )
+    return np.fft.ifftn(norm * new, axes=(0, 1, 2))
+
+
+def eliashberg_operator(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel):
+    """Gamma(R) and its flipped form for the matvec (eliashberg_solver.py:392-400); gamma_pp_irr [q_irr,...]."""
+    sign = 1 if channel == "sing" else -1
+    full = map_to_full_bz(gamma_pp_irr, irrk_inv).reshape(*nk, *gamma_pp_irr.shape[1:])
+    g_r = sign * sp_fft.fftn(full, axes=(0, 1, 2))
+    flip = flip_momentum_axis(g_r)
+    flip = np.flip(flip, axis=-1)
+    flip = np.einsum("xyzabcd...->xyzadcb...", flip)
+    return g_r, flip, sign
+
+
+def eliashberg_eigs(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel, v0, n_eig=4, tol=1e-10):
+    """Leading eigenvalues via ARPACK eigsh(which='LA') as eliashberg_solver.py:430-452."""
+    import scipy.sparse.linalg as spla
+
+    g_r, flip, sign = eliashberg_operator(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel)
+    shape = v0.shape
+
+    def mv(x):
+        return eliashberg_matvec(g_r, flip, chi0pp, x.reshape(shape), beta, sign).ravel()
+
+    dim = int(np.prod(shape))
+    op = spla.LinearOperator((dim, dim), matvec=mv, dtype=np.complex128)
+    vals, vecs = spla.eigsh(op, k=n_eig, tol=tol, v0=v0.ravel(), which="LA", maxiter=10000)
+    order = np.argsort(vals)[::-1]
+    return vals[order], vecs[:, order]
+
+
+def d_wave_gap(nk, n_bands, niv_pp, channel):
+    """Initial gap of symmetry 'd-wave' (eliashberg_solver.py:339-372): -cos kx + cos ky, even (singlet) or odd in nu."""
+    kx = np.linspace(0, 2 * np.pi, nk[0], endpoint=False)
+    ky = np.linspace(0, 2 * np.pi, nk[1], endpoint=False)
+    nv = 2 * niv_pp
+    gap = np.zeros((*nk, n_bands, n_bands, nv), dtype=np.complex128)
+    sym = -np.cos(kx)[:, None, None] + np.cos(ky)[None, :, None]
+    gap[..., niv_pp:] = np.repeat(sym[:, :, :, None, None, None], niv_pp, axis=-1)
+    if channel == "sing":
+        gap[..., :niv_pp] = gap[..., niv_pp:]
+    else:
+        gap[..., :niv_pp] = -gap[..., niv_pp:]
+    return gap
+
+
+def symmetrise_gap(gap, irrk_ind, irrk_inv):
+    """gap[k] = gap[irrk_ind][irrk_inv] (eliashberg_solver.py:408-410)."""
+    nk = gap.shape[:3]
+    flat = gap.reshape(int(np.prod(nk)), *gap.shape[3:])
+    return flat[irrk_ind][irrk_inv].reshape(gap.shape)

@@ -45,6 +45,8 @@ from dgamore.interaction import LocalInteraction, Interaction  # noqa: E402
 from dgamore.local_four_point import LocalFourPoint  # noqa: E402
 from dgamore.n_point_base import SpinChannel  # noqa: E402
 from dgamore.self_energy import SelfEnergy  # noqa: E402
+from dgamore import eliashberg_solver  # noqa: E402
+from dgamore.n_point_base import FrequencyNotation  # noqa: E402
 
 from dgamore_b200 import synthetic  # noqa: E402
 
@@ -116,8 +118,10 @@ def run_reference_pass(name: str) -> dict:
     out["chi0_inv"] = gchi0_q_core_inv.mat.copy()
     gchi0_q_core_sum = 1.0 / beta * gchi0_q_core.sum_over_all_vn(beta)
 
+    keep = {}
     for ch, chan in (("dens", SpinChannel.DENS), ("magn", SpinChannel.MAGN)):
         gamma_r = LocalFourPoint(inp[f"gamma_{ch}"], chan, 1, 2, False, True)
+        keep[ch] = {"gamma": gamma_r}
         # calculate_sigma_kernel_r_q (nonlocal_sde.py:257-336), both BSE variants
         aux = nonlocal_sde.create_auxiliary_chi_r_q_sum_v1(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc)
         aux3 = nonlocal_sde.create_auxiliary_chi_r_q_sum_v3(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc, dist)
@@ -134,6 +138,8 @@ def run_reference_pass(name: str) -> dict:
             chi_phys, lam = lc.perform_single_lambda_correction(chi_phys, inp[f"chi_loc_sum_{ch}"])
             out[f"lambda_{ch}"] = np.float64(lam)
         out[f"chi_phys_{ch}"] = chi_phys.mat.copy()
+        keep[ch]["vrg"] = deepcopy(vrg_q)
+        keep[ch]["chi_phys"] = deepcopy(chi_phys)
         k_r = nonlocal_sde.calculate_kernel_r_q(vrg_q, chi_phys, v_nonloc, u_loc)
         out[f"kernel_{ch}"] = k_r.mat.copy()
         kernel += k_r if ch == "dens" else 3 * k_r
@@ -149,10 +155,52 @@ def run_reference_pass(name: str) -> dict:
     sig_direct = nonlocal_sde.calculate_sigma_from_kernel_cpu(deepcopy(kernel_full), giwk, grid.get_q_list())
     out["sigma_direct"] = sig_direct.compress_q_dimension().mat.copy()
 
+    if name in ELIASHBERG_CONFIGS:
+        out.update(run_reference_eliashberg(cfg, inp, giwk, u_loc, v_nonloc, gchi0_q_core_inv, keep, grid))
+
     save = {k: v for k, v in inp.items() if k not in ("config",)}
     save.update({f"ref_{k}": v for k, v in out.items()})
     save["config_name"] = np.array(name)
     return save
+
+
+ELIASHBERG_CONFIGS = ("t4e", "t5e")
+
+
+def run_reference_eliashberg(cfg, inp, giwk, u_loc, v_nonloc, gchi0_q_core_inv, keep, grid) -> dict:
+    """Full vertex, pp transform, pairing vertices and the Lanczos eigen-solve with the upstream functions
+    (eliashberg_solver.py:175-204, 44-75, 620-628, 376-471), d-wave start, n_eig = 4, tol 1e-12."""
+    config.eliashberg.save_fq = False
+    config.eliashberg.construct_fq_cheap = False
+    config.eliashberg.n_eig = 4
+    config.eliashberg.epsilon = 1e-12
+    config.eliashberg.symmetry = "d-wave"
+    niv_pp = min(cfg.niw // 2, cfg.niv // 2)
+    out = {"niv_pp": np.int64(niv_pp)}
+    f_pp = {}
+    for ch in ("dens", "magn"):
+        mats = []
+        for idx in range(grid.nk_irr):
+            f = eliashberg_solver.create_full_vertex_q_r_v2(
+                u_loc, v_nonloc, keep[ch]["gamma"], gchi0_q_core_inv, keep[ch]["vrg"], keep[ch]["chi_phys"], niv_pp, idx
+            )
+            mats.append(f.mat[0])
+        f_pp[ch] = np.stack(mats)
+        out[f"f_pp_{ch}"] = f_pp[ch]
+    gam = {
+        "sing": 0.5 * f_pp["dens"] - 1.5 * f_pp["magn"],
+        "trip": 0.5 * f_pp["dens"] + 0.5 * f_pp["magn"],
+    }
+    chi0pp = BubbleGenerator.create_generalized_chi0_q_pp_w0(giwk, niv_pp, grid)
+    out["chi0pp"] = chi0pp.mat.copy()
+    for ch, chan in (("sing", SpinChannel.SING), ("trip", SpinChannel.TRIP)):
+        out[f"gamma_pp_{ch}"] = gam[ch]
+        gp = FourPoint(gam[ch], chan, tuple(cfg.nk), 0, 2, False, True, True, FrequencyNotation.PP)
+        c0 = deepcopy(chi0pp)
+        lambdas, gaps = eliashberg_solver.solve_eliashberg_lanczos(gp, c0, (0, 0))
+        out[f"lambdas_{ch}"] = np.asarray(lambdas)
+        out[f"gap_{ch}_0"] = gaps[0].mat.copy()
+    return out
 
 
 def upstream_fixtures() -> dict:
@@ -183,7 +231,7 @@ def bse_kat() -> dict:
 
 
 def main():
-    for name in ("t1", "t1b", "t2", "t3"):
+    for name in ("t1", "t1b", "t2", "t3") + ELIASHBERG_CONFIGS:
         data = run_reference_pass(name)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
         print("wrote", name, sorted(data.keys()))

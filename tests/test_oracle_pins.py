@@ -115,3 +115,27 @@ def test_kgrid_irreducible_sizes():
     assert KGrid((64, 64, 1)).nk_irr == 561
     g = KGrid((48, 48, 1))
     assert g.irrk_count.sum() == 48 * 48
+
+
+@pytest.mark.parametrize("name", ("t4e", "t5e"))
+def test_oracle_eliashberg_matches_upstream_fp64(name):
+    """Full vertex in pp notation, chi0pp and the leading singlet/triplet eigenvalues (eliashberg_solver.py)."""
+    inp, ref = load_golden(name)
+    nb = inp["u"].shape[0]
+    niv_pp = int(ref["niv_pp"])
+    out = L.sde_pass(inp, do_lambda=(nb == 1))
+    fpp = {}
+    for ch in ("dens", "magn"):
+        uv = L.u_as_channel(inp["u"], ch)[None] + L.v_as_channel(inp["v_q_irr"], ch)
+        f = L.full_vertex_q(out["chi0_inv"], inp[f"gamma_{ch}"], uv, out[f"vrg_{ch}"], out[f"chi_phys_{ch}"],
+                            inp["beta"], niv_pp)
+        fpp[ch] = L.ph_to_pp_w0(f, inp["niw"], niv_pp)
+        assert rel_err(fpp[ch], ref[f"f_pp_{ch}"]) < 1e-12
+    gam = {"sing": 0.5 * fpp["dens"] - 1.5 * fpp["magn"], "trip": 0.5 * fpp["dens"] + 0.5 * fpp["magn"]}
+    chi0pp = L.chi0_pp_full_grid(inp["g_k"], niv_pp)
+    assert rel_err(chi0pp.reshape(-1, *chi0pp.shape[3:]), ref["chi0pp"]) < 1e-14
+    for ch in ("sing", "trip"):
+        assert rel_err(gam[ch], ref[f"gamma_pp_{ch}"]) < 1e-12
+        v0 = L.symmetrise_gap(L.d_wave_gap(inp["nk"], nb, niv_pp, ch), inp["irrk_ind"], inp["irrk_inv"])
+        vals, _ = L.eliashberg_eigs(gam[ch], inp["irrk_inv"], inp["nk"], chi0pp, inp["beta"], ch, v0, 4, 1e-12)
+        assert np.max(np.abs(vals - ref[f"lambdas_{ch}"])) < 1e-9 * max(1.0, np.max(np.abs(vals)))
