@@ -39,6 +39,13 @@ SIGNATURES = {
     "dga_dc_kernel_c128": (I, [VP, VP, VP, I, I, I, I, I, VP, VP, SZ, VP]),
     "dga_sigma_scratch_bytes": (SZ, [I, I, I, I]),
     "dga_sigma_c128": (I, [VP, VP, I, I, I, I, I, I, I, PI, VP, D, I, VP, VP, SZ, VP]),
+    "dga_dft_planes_gather_c128": (I, [VP, LL, LL, LL, VP, LL, LL, LL, I, I, I, I, I, VP, D, PI, VP]),
+    "dga_eli_vertex_scratch_bytes": (SZ, [I, I, I, I]),
+    "dga_eli_full_vertex_c128": (I, [I, I, I, I, I, I, D, D, VP, VP, VP, VP, VP, PI, I, VP, PI, VP, SZ, VP]),
+    "dga_eli_pairing_vertex_c128": (I, [VP, I, I, I, I, VP, VP]),
+    "dga_eli_chi0pp_c128": (I, [VP, I, I, I, I, VP, VP]),
+    "dga_eli_matvec_scratch_bytes": (SZ, [I, I, I]),
+    "dga_eli_matvec_c128": (I, [VP, VP, VP, I, I, I, I, I, VP, VP, D, D, VP, VP, SZ, VP]),
 }
 
 

@@ -776,6 +776,143 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   }
 }
 
+
+// ----------------------------------------------------------------------------------------------
+// Eliashberg full vertex in the pp frequency box (one CTA per (channel, q, w) item):
+//   F[(p,nu),(s,nu')] = beta^2 (delta_{nu nu'} c0(nu)[p][s] - sum_{m,m'} c0(nu)[p][m] chi*[(m,nu),(m',nu')] c0(nu')[m'][s])
+//                       + (Z G3(nu) G3(nu'))[p][s],   Z = U_r - U_r chi_r U_r,  c0 = chi0^-1,  G3 = gamma_r
+// for nu, nu' in the box [niv - P, niv + P) (eliashberg_solver.py:175-204).  chi* = A^-1 is never formed: the
+// LU factors of A are solved against the unit vectors of KB box frequencies at a time (NR = KB n2 columns).
+//   g3: [2][Q][W][nv][n2][n2]; chi_phys: [2][Q][W][n2][n2]; out: [2][Q][Wpp][Mb][Mb]
+//   slot: A (N x N) | Y (N x NR) | H (2P x n2 x n2) | Z (n2 x n2), complex128
+// ----------------------------------------------------------------------------------------------
+template <int NR>
+__global__ void __launch_bounds__(BSE_THREADS, 3)
+    eli_full_vertex_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int n2, int nv,
+                           int W, int Q, int P, int Wpp, double beta, const double2* __restrict__ g3,
+                           const double2* __restrict__ chi_phys, double2* __restrict__ out, int* __restrict__ status,
+                           double2* __restrict__ scratch, size_t slot_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BseSmem<double2>& sm = *reinterpret_cast<BseSmem<double2>*>(smem_raw);
+  int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<double2>));
+  int* perm = piv + N;
+  double2* A = scratch + (size_t)blockIdx.x * slot_elems;
+  double2* Y = A + (size_t)N * N;
+  const int nvp = 2 * P, Mb = n2 * nvp, KB = NR / n2, off = nv / 2 - P;
+  double2* H = Y + (size_t)N * NR;
+  double2* Z = H + (size_t)nvp * n2 * n2;
+  const int tid = threadIdx.x, T = blockDim.x;
+  const double beta2 = beta * beta;
+
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const WorkItem wi = work[item];
+    {
+      const int pr0 = tid / nv, vr0 = tid - pr0 * nv;
+      const int qT = T / nv, rT = T - qT * nv;
+      int pc = 0, vc = 0;
+      for (int j = 0; j < N; ++j) {
+        double2* col = A + (size_t)j * N;
+        int pr = pr0, vr = vr0;
+        for (int i = tid; i < N; i += T) {
+          col[i] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
+          pr += qT;
+          vr += rT;
+          if (vr >= nv) {
+            vr -= nv;
+            ++pr;
+          }
+        }
+        if (++vc == nv) {
+          vc = 0;
+          ++pc;
+        }
+      }
+    }
+    __syncthreads();
+    const bool singular = lu_factor<double2>(A, N, N, piv, sm);
+    // row permutation of the factorisation
+    for (int i = tid; i < N; i += T) perm[i] = i;
+    __syncthreads();
+    if (tid == 0) {
+      for (int i = 0; i < N; ++i) {
+        const int p = piv[i];
+        if (p != i) {
+          const int t = perm[i];
+          perm[i] = perm[p];
+          perm[p] = t;
+        }
+      }
+    }
+    // Z = U_r - U_r chi_r U_r, then H(nu) = Z G3(nu) for the box frequencies
+    const double2* uvq = src.uv + ((size_t)wi.ch * Q + wi.q) * n2 * n2;
+    const double2* cp = chi_phys + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * n2 * n2;
+    for (int e = tid; e < n2 * n2; e += T) {
+      const int p = e / n2, s = e - p * n2;
+      double2 acc = uvq[e];
+      for (int t = 0; t < n2; ++t) {
+        double2 cu = make_double2(0.0, 0.0);
+        for (int u = 0; u < n2; ++u) cfma(cu, cp[t * n2 + u], uvq[u * n2 + s]);
+        cfms(acc, uvq[p * n2 + t], cu);
+      }
+      Z[e] = acc;
+    }
+    __syncthreads();
+    const double2* g3q = g3 + ((((size_t)wi.ch * Q + wi.q) * W + wi.w) * nv) * n2 * n2;
+    for (int e = tid; e < nvp * n2 * n2; e += T) {
+      const int vb = e / (n2 * n2), ps = e - vb * n2 * n2, p = ps / n2, s = ps - p * n2;
+      const double2* g = g3q + (size_t)(off + vb) * n2 * n2;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int t = 0; t < n2; ++t) cfma(acc, Z[p * n2 + t], g[t * n2 + s]);
+      H[e] = acc;
+    }
+    __syncthreads();
+    double2* o = out + (((size_t)wi.ch * Q + wi.q) * Wpp + wi.w) * (size_t)Mb * Mb;
+    for (int v0 = 0; v0 < nvp; v0 += KB) {
+      // unit vectors of the box columns (m', nu') for nu' in [v0, v0 + KB), permuted by the pivots
+      for (int e = tid; e < N * NR; e += T) {
+        const int i = e % N, sidx = e / N;
+        const int kk = sidx / n2, mp = sidx - kk * n2;
+        const int vb = v0 + kk;
+        const int j = mp * nv + off + vb;
+        Y[(size_t)sidx * N + i] = make_double2((vb < nvp && perm[i] == j) ? 1.0 : 0.0, 0.0);
+      }
+      __syncthreads();
+      lu_solve_inplace<double2, double2, NR>(A, N, N, Y, sm);
+      // F columns (s, nu') for the KB box frequencies of this chunk, rows (p, nu) of the box
+      for (int e = tid; e < Mb * KB * n2; e += T) {
+        const int sidx = e % n2;
+        const int kk = (e / n2) % KB;
+        const int row = e / (n2 * KB);
+        const int vbp = v0 + kk;
+        if (vbp >= nvp) continue;
+        const int p = row / nvp, vb = row - p * nvp;
+        const int vr = off + vb, vc = off + vbp;
+        const double2* c0r = src.chi0_inv + (((size_t)wi.q * W + wi.w) * nv + vr) * n2 * n2;
+        const double2* c0c = src.chi0_inv + (((size_t)wi.q * W + wi.w) * nv + vc) * n2 * n2;
+        // t = sum_{m,m'} c0r[p][m] chi*[(m,vr),(m',vc)] c0c[m'][s]
+        double2 t = make_double2(0.0, 0.0);
+        for (int m = 0; m < n2; ++m) {
+          double2 inner = make_double2(0.0, 0.0);
+          for (int mp = 0; mp < n2; ++mp) cfma(inner, Y[(size_t)(kk * n2 + mp) * N + m * nv + vr], c0c[mp * n2 + sidx]);
+          cfma(t, c0r[p * n2 + m], inner);
+        }
+        double2 f1 = make_double2(-t.x, -t.y);
+        if (vb == vbp) f1 = cadd(f1, c0r[p * n2 + sidx]);
+        f1 = cscale(f1, beta2);
+        // (Z G3(nu)) G3(nu')
+        const double2* hrow = H + (size_t)vb * n2 * n2 + p * n2;
+        const double2* gcol = g3q + (size_t)vc * n2 * n2;
+        double2 f2 = make_double2(0.0, 0.0);
+        for (int u = 0; u < n2; ++u) cfma(f2, hrow[u], gcol[u * n2 + sidx]);
+        o[(size_t)row * Mb + sidx * nvp + vbp] = cadd(f1, f2);
+      }
+      __syncthreads();
+    }
+    if (tid == 0 && status) status[item] = singular ? DGA_ITEM_SINGULAR : 0;
+    __syncthreads();
+  }
+}
+
 }  // namespace dga
 
 using namespace dga;
@@ -1028,6 +1165,78 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     dga_set_error("dga_bse_solve_sum_mixed_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"
+
+
+// ------------------------------------------------------------------------------------------------
+// Eliashberg full vertex (host side)
+// ------------------------------------------------------------------------------------------------
+static int eli_rhs(int n2) { return n2 == 9 ? 9 : 16; }
+
+static size_t eli_slot_elems(int N, int n2, int P) {
+  return (size_t)N * N + (size_t)N * eli_rhs(n2) + (size_t)2 * P * n2 * n2 + (size_t)n2 * n2;
+}
+
+extern "C" {
+
+// Scratch bytes of dga_eli_full_vertex_c128 for n_items items.
+size_t dga_eli_vertex_scratch_bytes(int n_orb, int niv, int niv_pp, int n_items) {
+  const int n2 = n_orb * n_orb, N = n2 * 2 * niv;
+  if (!supported_rhs(n2) || n_items <= 0) return 0;
+  const size_t smem = bse_smem_bytes(N);
+  const int grid = grid_for(eli_full_vertex_kernel<16>, n_items, smem);
+  return (size_t)grid * eli_slot_elems(N, n2, niv_pp) * sizeof(double2);
+}
+
+// Full ladder vertex of both channels in the pp box (eliashberg_solver.py:175-204) for the work items
+// (ch, q, w) with w < w_pp; inputs as dga_bse_solve_sum_c128 plus gamma_r (g3 [2][Q][W][nv][n2][n2]) and the
+// physical susceptibility (chi_phys [2][Q][W][n2][n2]); out: [2][Q][w_pp][Mb][Mb], Mb = n2 * 2 niv_pp.
+int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_pp, int w_pp, double beta,
+                             double inv_beta2, const void* gamma_cm, const void* chi0_inv, const void* uv,
+                             const void* g3, const void* chi_phys, const int* work, int n_items, void* out,
+                             int* status, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || niv_pp <= 0 || niv_pp > niv ||
+      w_pp <= 0 || w_pp > niw_half || n_items <= 0 || N > BSE_MAX_N || !gamma_cm || !chi0_inv || !uv || !g3 ||
+      !chi_phys || !work || !out || !scratch) {
+    dga_set_error("dga_eli_full_vertex_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = bse_smem_bytes(N);
+  const int NR = eli_rhs(n2);
+  int grid = NR == 9 ? grid_for(eli_full_vertex_kernel<9>, n_items, smem)
+                     : grid_for(eli_full_vertex_kernel<16>, n_items, smem);
+  const size_t slot = eli_slot_elems(N, n2, niv_pp);
+  if (scratch_bytes < (size_t)grid * slot * sizeof(double2)) {
+    dga_set_error("dga_eli_full_vertex_c128: scratch too small");
+    return DGA_ERR_SCRATCH;
+  }
+  StructuredSource src;
+  src.gamma_cm = (const double2*)gamma_cm;
+  src.chi0_inv = (const double2*)chi0_inv;
+  src.uv = (const double2*)uv;
+  src.n2 = n2;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  src.inv_beta2 = inv_beta2;
+  if (NR == 9) {
+    eli_full_vertex_kernel<9><<<grid, BSE_THREADS, smem, stream>>>(
+        src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, niv_pp, w_pp, beta, (const double2*)g3,
+        (const double2*)chi_phys, (double2*)out, status, (double2*)scratch, slot);
+  } else {
+    eli_full_vertex_kernel<16><<<grid, BSE_THREADS, smem, stream>>>(
+        src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, niv_pp, w_pp, beta, (const double2*)g3,
+        (const double2*)chi_phys, (double2*)out, status, (double2*)scratch, slot);
+  }
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_eli_full_vertex_c128: launch failed: %s", cudaGetErrorString(err));
     return DGA_ERR_LAUNCH;
   }
   return DGA_OK;

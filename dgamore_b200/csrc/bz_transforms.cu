@@ -99,7 +99,8 @@ struct PlaneAddr {
 __global__ void __launch_bounds__(BZ_THREADS) dft_planes_kernel(const double2* __restrict__ in, PlaneAddr ia,
                                                                  double2* __restrict__ out, PlaneAddr oa,
                                                                  int n_planes, Grid3 g,
-                                                                 const double2* __restrict__ tw, double scale) {
+                                                                 const double2* __restrict__ tw, double scale,
+                                                                 const int* __restrict__ gather) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* a = reinterpret_cast<double2*>(smem_raw);
   double2* b = a + g.nk;
@@ -107,7 +108,7 @@ __global__ void __launch_bounds__(BZ_THREADS) dft_planes_kernel(const double2* _
   load_twiddles(s_tw, tw, g);
   for (int p = blockIdx.x; p < n_planes; p += gridDim.x) {
     __syncthreads();
-    for (int r = threadIdx.x; r < g.nk; r += blockDim.x) a[r] = in[ia.at(p, r)];
+    for (int r = threadIdx.x; r < g.nk; r += blockDim.x) a[r] = in[ia.at(p, gather ? gather[r] : r)];
     __syncthreads();
     plane_dft(a, b, s_tw, g);
     for (int r = threadIdx.x; r < g.nk; r += blockDim.x) {
@@ -358,8 +359,28 @@ int dga_dft_planes_c128(const void* in, long long in_s_hi, long long in_s_lo, lo
   const size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2);
   cudaFuncSetAttribute(dft_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dft_planes_kernel<<<grid_cap(n_planes), BZ_THREADS, smem, stream>>>((const double2*)in, ia, (double2*)out, oa,
-                                                                      n_planes, g, (const double2*)tw, scale);
+                                                                      n_planes, g, (const double2*)tw, scale, nullptr);
   return launch_status("dga_dft_planes_c128");
+}
+
+// Same as dga_dft_planes_c128 with the input point of output R read from gather[R] (an IBZ -> FBZ expansion
+// by the inverse irreducible map, n_point_base.py:489-494, folded into the transform's load).
+int dga_dft_planes_gather_c128(const void* in, long long in_s_hi, long long in_s_lo, long long in_s_r, void* out,
+                               long long out_s_hi, long long out_s_lo, long long out_s_r, int n_lo, int n_planes,
+                               int nx, int ny, int nz, const void* tw, double scale, const int* gather,
+                               cudaStream_t stream) {
+  if (check_grid(nx, ny, nz, "dga_dft_planes_gather_c128")) return DGA_ERR_ARG;
+  if (!in || !out || !tw || !gather || n_planes <= 0 || n_lo <= 0) {
+    dga_set_error("dga_dft_planes_gather_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  Grid3 g{nx, ny, nz, nx * ny * nz};
+  PlaneAddr ia{in_s_hi, in_s_lo, in_s_r, n_lo}, oa{out_s_hi, out_s_lo, out_s_r, n_lo};
+  const size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2);
+  cudaFuncSetAttribute(dft_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dft_planes_kernel<<<grid_cap(n_planes), BZ_THREADS, smem, stream>>>((const double2*)in, ia, (double2*)out, oa,
+                                                                      n_planes, g, (const double2*)tw, scale, gather);
+  return launch_status("dga_dft_planes_gather_c128");
 }
 
 // Fused bubble.  g_r: [2 niv + niw][n][n][Nk] forward transforms of G(k) for nu indices [-niv-niw, niv);
@@ -428,7 +449,8 @@ int dga_sigma_c128(const void* kern, const void* g_r, int n_orb, int niv, int ni
   cudaFuncSetAttribute(dft_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   PlaneAddr pa{(long long)g.nk, 0, 1, 1};
   dft_planes_kernel<<<grid_cap(niv * n2), BZ_THREADS, smem, stream>>>(sig, pa, part, pa, niv * n2, g,
-                                                                      (const double2*)tw_inv, 1.0 / (double)g.nk);
+                                                                      (const double2*)tw_inv, 1.0 / (double)g.nk,
+                                                                      nullptr);
   if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
   sigma_full_nu_kernel<<<grid_cap((n_out + 255) / 256), 256, 0, stream>>>(part, n_orb, niv, g.nk, (double2*)out);
   return launch_status("dga_sigma_c128");

@@ -132,6 +132,7 @@ class LadderPass:
         beta = sh.beta
         # ---------------- host-side preparation (once per request) ----------------
         irr = np.asarray(inp["irrk_ind"])
+        self.irrk_ind_host = irr
         q_list = np.array(np.unravel_index(irr, nk)).T.astype(np.int32)
         self.q_irr = torch.from_numpy(np.ascontiguousarray(q_list)).to(dev)
         self.irrk_inv = torch.from_numpy(np.asarray(inp["irrk_inv"], dtype=np.int32)).to(dev)

@@ -154,6 +154,43 @@ int dga_sigma_c128(const void* kern, const void* g_r, int n_orb, int niv, int ni
                    const int* irrk_inv, const void* tw_inv, double beta, int n_chunks, void* out, void* scratch,
                    size_t scratch_bytes, dga_stream_t stream);
 
+/* dga_dft_planes_c128 with the input point of output R read from gather[R]: the IBZ -> FBZ expansion
+ * (IAmNonLocal._map_to_full_bz, dgamore/n_point_base.py:489-494) folded into the transform's load. */
+int dga_dft_planes_gather_c128(const void* in, long long in_s_hi, long long in_s_lo, long long in_s_r, void* out,
+                               long long out_s_hi, long long out_s_lo, long long out_s_r, int n_lo, int n_planes,
+                               int nx, int ny, int nz, const void* tw, double scale, const int* gather,
+                               dga_stream_t stream);
+
+/* Eliashberg full vertex F_r(q, w) of both channels in the pp frequency box (P = niv_pp, Mb = n2*2P) for the
+ * work items (ch, q, w < w_pp); replaces eliashberg_solver.create_full_vertex_q_r(_v2)
+ * (dgamore/eliashberg_solver.py:78-298) up to the frequency transform.  Inputs as dga_bse_solve_sum_c128 plus
+ * g3 = gamma_r [2][Q][W][nv][n2][n2] and chi_phys [2][Q][W][n2][n2] (lambda-corrected); out [2][Q][w_pp][Mb][Mb],
+ * row (p=(a,b), nu), column (s=(d,c), nu'). */
+size_t dga_eli_vertex_scratch_bytes(int n_orb, int niv, int niv_pp, int n_items);
+int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_pp, int w_pp, double beta,
+                             double inv_beta2, const void* gamma_cm, const void* chi0_inv, const void* uv,
+                             const void* g3, const void* chi_phys, const int* work, int n_items, void* out,
+                             int* status, void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
+/* PH -> PP (w = 0) transform, singlet/triplet combination and gap-equation layout; replaces
+ * _transform_vertex_frequencies_w0 and the Gamma_sing/trip sums (dgamore/eliashberg_solver.py:44-75, 620-628).
+ * fph: [2][Q][w_pp][Mb][Mb] from dga_eli_full_vertex_c128; out [2 (sing, trip)][Q][Mb][Mb] with
+ * Mat[(a,b,nu)][(c,d,nu')] = Gamma[a,c,b,d](nu,nu'). */
+int dga_eli_pairing_vertex_c128(const void* fph, int n_orb, int niv_pp, int n_q, int w_pp, void* out,
+                                dga_stream_t stream);
+
+/* chi0pp[Nk][2P][(a,b)][(c,d)] = G_ad(k,nu) conj(G_cb(k,nu)); replaces
+ * BubbleGenerator.create_generalized_chi0_q_pp_w0 (dgamore/bubble_gen.py:268-279). */
+int dga_eli_chi0pp_c128(const void* g_k, int n_orb, int niv_g, int niv_pp, int nk, void* out, dga_stream_t stream);
+
+/* One application of the linearised gap equation, the matvec of solve_eliashberg_lanczos
+ * (dgamore/eliashberg_solver.py:420-428): mat [Nk][M][M] = sign * FFT_q of the pairing vertex (full BZ),
+ * chi0pp from dga_eli_chi0pp_c128, gap / gap_out [Nk][n2][2P]; sign = +1 singlet, -1 triplet. */
+size_t dga_eli_matvec_scratch_bytes(int n_orb, int niv_pp, int nk);
+int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, int n_orb, int niv_pp, int nx, int ny,
+                        int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign, void* gap_out,
+                        void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
