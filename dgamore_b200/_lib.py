@@ -46,7 +46,26 @@ SIGNATURES = {
     "dga_eli_chi0pp_c128": (I, [VP, I, I, I, I, VP, VP]),
     "dga_eli_matvec_scratch_bytes": (SZ, [I, I, I]),
     "dga_eli_matvec_c128": (I, [VP, VP, VP, I, I, I, I, I, VP, VP, D, D, VP, VP, SZ, VP]),
+    "dga_bse_batch_scratch_bytes": (SZ, [VP, I, I, I]),
+    "dga_bse_solve_sum_batch_c128": (I, [VP, VP, I, PI, I, I, I, D, PI, PI, VP, SZ, VP]),
 }
+
+
+class BseProblem(_c.Structure):
+    """``dga_bse_problem`` of include/dga_b200.h (one request of a heterogeneous BSE batch)."""
+
+    _fields_ = [
+        ("gamma_cm", VP),
+        ("chi0_inv", VP),
+        ("uv", VP),
+        ("out", VP),
+        ("n_orb", I),
+        ("niv", I),
+        ("niw_half", I),
+        ("n_q", I),
+        ("beta", D),
+        ("inv_beta2", D),
+    ]
 
 
 class DgaError(RuntimeError):

@@ -519,8 +519,61 @@ __device__ void permuted_selector(CY* __restrict__ Y, int N, int nv, int n_rhs, 
 }
 
 // ----------------------------------------------------------------------------------------------
-// FP64 kernel: one CTA per work item, persistent over the list.
+// One work item in FP64: form A, LU, selector solve, X = Y / beta into out (rows (p,nu), n2 columns).
+// Returns the item's status bits.  All threads of the CTA call it.
 // ----------------------------------------------------------------------------------------------
+template <typename Source, int NR>
+__device__ int solve_item_fp64(const Source& src, const WorkItem& wi, int N, int nv, double beta,
+                               double2* __restrict__ o, double2* __restrict__ A, double2* __restrict__ Y,
+                               BseSmem<double2>& sm, int* piv, int* perm) {
+  const int tid = threadIdx.x, T = blockDim.x;
+  // form A column by column; the (pair, nu) split of a thread's rows advances by T = q_T nv + r_T per step
+  {
+    const int pr0 = tid / nv, vr0 = tid - pr0 * nv;
+    const int qT = T / nv, rT = T - qT * nv;
+    int pc = 0, vc = 0;
+    for (int j = 0; j < N; ++j) {
+      double2* col = A + (size_t)j * N;
+      int pr = pr0, vr = vr0;
+      for (int i = tid; i < N; i += T) {
+        col[i] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
+        pr += qT;
+        vr += rT;
+        if (vr >= nv) {
+          vr -= nv;
+          ++pr;
+        }
+      }
+      if (++vc == nv) {
+        vc = 0;
+        ++pc;
+      }
+    }
+  }
+  __syncthreads();
+  const bool singular = lu_factor<double2>(A, N, N, piv, sm);
+  permuted_selector<double2>(Y, N, nv, NR, piv, perm);
+  lu_solve_inplace<double2, double2, NR>(A, N, N, Y, sm);
+  // X[i][s] = Y[i][s] / beta, finiteness check
+  if (tid == 0) sm.flag = 0;
+  __syncthreads();
+  bool bad = false;
+  for (int e = tid; e < N * NR; e += T) {
+    const int i = e / NR, s = e % NR;
+    double2 y = Y[(size_t)s * N + i];
+    y.x = y.x / beta;
+    y.y = y.y / beta;
+    if (!cfinite(y)) bad = true;
+    o[e] = y;
+  }
+  if (bad) atomicOr(&sm.flag, DGA_ITEM_NONFINITE);
+  __syncthreads();
+  const int st = (singular ? DGA_ITEM_SINGULAR : 0) | sm.flag;
+  __syncthreads();
+  return st;
+}
+
+// FP64 kernel: one CTA per work item, persistent over the list.
 template <typename Source, int NR>
 __global__ void __launch_bounds__(BSE_THREADS, 3)
     bse_solve_sum_fp64_kernel(Source src, const WorkItem* __restrict__ work, int n_items, int N, int n2,
@@ -533,59 +586,15 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   int* perm = piv + N;
   double2* A = scratch + (size_t)blockIdx.x * slot_elems;
   double2* Y = A + (size_t)N * N;
-  const int tid = threadIdx.x, T = blockDim.x;
-
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     // re-solve mode: only the items whose status says the mixed solve did not converge or was not finite
     if (redo_only && (status[item] & (DGA_ITEM_NOCONVERGE | DGA_ITEM_NONFINITE)) == 0) continue;
     const WorkItem wi = work[item];
-    // form A column by column; the (pair, nu) split of a thread's rows advances by T = q_T nv + r_T per step
-    {
-      const int pr0 = tid / nv, vr0 = tid - pr0 * nv;
-      const int qT = T / nv, rT = T - qT * nv;
-      int pc = 0, vc = 0;
-      for (int j = 0; j < N; ++j) {
-        double2* col = A + (size_t)j * N;
-        int pr = pr0, vr = vr0;
-        for (int i = tid; i < N; i += T) {
-          col[i] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
-          pr += qT;
-          vr += rT;
-          if (vr >= nv) {
-            vr -= nv;
-            ++pr;
-          }
-        }
-        if (++vc == nv) {
-          vc = 0;
-          ++pc;
-        }
-      }
-    }
-    __syncthreads();
-    const bool singular = lu_factor<double2>(A, N, N, piv, sm);
-    permuted_selector<double2>(Y, N, nv, NR, piv, perm);
-    lu_solve_inplace<double2, double2, NR>(A, N, N, Y, sm);
-    // write X[(ch, q, w)][i][s] = Y[i][s] / beta and check finiteness
-    if (tid == 0) sm.flag = 0;
-    __syncthreads();
     double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * n2;
-    bool bad = false;
-    for (int e = tid; e < N * n2; e += T) {
-      const int i = e / n2, s = e % n2;
-      double2 y = Y[(size_t)s * N + i];
-      y.x = y.x / beta;
-      y.y = y.y / beta;
-      if (!cfinite(y)) bad = true;
-      o[e] = y;
-    }
-    if (bad) atomicOr(&sm.flag, DGA_ITEM_NONFINITE);
-    __syncthreads();
-    if (tid == 0 && status) status[item] = (singular ? DGA_ITEM_SINGULAR : 0) | sm.flag;
-    __syncthreads();
+    const int st = solve_item_fp64<Source, NR>(src, wi, N, nv, beta, o, A, Y, sm, piv, perm);
+    if (threadIdx.x == 0 && status) status[item] = st;
   }
 }
-
 
 // ----------------------------------------------------------------------------------------------
 // Mixed form: FP32 LU (same core, float2 storage, FP32 trailing updates) and FP64 iterative refinement.
@@ -686,6 +695,81 @@ __host__ __device__ inline size_t mixed_colsum_offset(int N) {
   return (sizeof(BseSmem<float2>) + 2 * sizeof(int) * (size_t)N + 15) & ~(size_t)15;
 }
 
+// One work item in the mixed form (FP32 LU, FP64 refinement).  Returns the status bits; *iters = corrections.
+template <int NR>
+__device__ int solve_item_mixed(const StructuredSource& src, const WorkItem& wi, int N, int nv, double beta,
+                                int max_iter, double tol, double2* __restrict__ o, float2* __restrict__ A,
+                                double2* __restrict__ Y, double2* __restrict__ Rb, BseSmem<float2>& sm, int* piv,
+                                int* perm, double2* colsum, int* iters) {
+  const int tid = threadIdx.x, T = blockDim.x;
+  {
+    const int pr0 = tid / nv, vr0 = tid - pr0 * nv;
+    const int qT = T / nv, rT = T - qT * nv;
+    int pc = 0, vc = 0;
+    for (int j = 0; j < N; ++j) {
+      float2* col = A + (size_t)j * N;
+      int pr = pr0, vr = vr0;
+      for (int i = tid; i < N; i += T) {
+        const double2 a = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
+        col[i] = make_float2((float)a.x, (float)a.y);
+        pr += qT;
+        vr += rT;
+        if (vr >= nv) {
+          vr -= nv;
+          ++pr;
+        }
+      }
+      if (++vc == nv) {
+        vc = 0;
+        ++pc;
+      }
+    }
+  }
+  __syncthreads();
+  const bool singular = lu_factor<float2>(A, N, N, piv, sm);
+  permuted_selector<double2>(Y, N, nv, NR, piv, perm);
+  lu_solve_inplace<float2, double2, NR>(A, N, N, Y, sm);
+  int it = 0;
+  bool converged = false;
+  for (; it < max_iter; ++it) {
+    structured_residual_permuted<NR>(src, wi.ch, wi.q, wi.w, N, nv, Y, Rb, perm, colsum,
+                                     reinterpret_cast<double2*>(&sm.u));
+    lu_solve_inplace<float2, double2, NR>(A, N, N, Rb, sm);
+    double dmax = 0.0, ymax = 0.0;
+    for (int e = tid; e < N * NR; e += T) {
+      const double2 d = Rb[e];
+      const double2 y = cadd(Y[e], d);
+      Y[e] = y;
+      dmax = fmax(dmax, fmax(fabs(d.x), fabs(d.y)));
+      ymax = fmax(ymax, fmax(fabs(y.x), fabs(y.y)));
+    }
+    dmax = block_max(dmax, sm.red_val);
+    ymax = block_max(ymax, sm.red_val);
+    if (!(dmax > tol * ymax)) {  // also stops on NaN, flagged below
+      converged = dmax <= tol * ymax;
+      ++it;
+      break;
+    }
+  }
+  if (tid == 0) sm.flag = 0;
+  __syncthreads();
+  bool bad = false;
+  for (int e = tid; e < N * NR; e += T) {
+    const int i = e / NR, sidx = e % NR;
+    double2 y = Y[(size_t)sidx * N + i];
+    y.x = y.x / beta;
+    y.y = y.y / beta;
+    if (!cfinite(y)) bad = true;
+    o[e] = y;
+  }
+  if (bad) atomicOr(&sm.flag, DGA_ITEM_NONFINITE);
+  __syncthreads();
+  const int st = (singular ? DGA_ITEM_SINGULAR : 0) | sm.flag | (converged ? 0 : DGA_ITEM_NOCONVERGE);
+  *iters = it;
+  __syncthreads();
+  return st;
+}
+
 template <int NR>
 __global__ void __launch_bounds__(BSE_THREADS, 3)
     bse_solve_sum_mixed_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int n2,
@@ -701,81 +785,89 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   float2* A = reinterpret_cast<float2*>(slot);
   double2* Y = reinterpret_cast<double2*>(slot + (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255));
   double2* Rb = Y + (size_t)N * n2;
-  const int tid = threadIdx.x, T = blockDim.x;
-
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const WorkItem wi = work[item];
-    {
-      const int pr0 = tid / nv, vr0 = tid - pr0 * nv;
-      const int qT = T / nv, rT = T - qT * nv;
-      int pc = 0, vc = 0;
-      for (int j = 0; j < N; ++j) {
-        float2* col = A + (size_t)j * N;
-        int pr = pr0, vr = vr0;
-        for (int i = tid; i < N; i += T) {
-          const double2 a = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
-          col[i] = make_float2((float)a.x, (float)a.y);
-          pr += qT;
-          vr += rT;
-          if (vr >= nv) {
-            vr -= nv;
-            ++pr;
-          }
-        }
-        if (++vc == nv) {
-          vc = 0;
-          ++pc;
-        }
-      }
-    }
-    __syncthreads();
-    const bool singular = lu_factor<float2>(A, N, N, piv, sm);
-    permuted_selector<double2>(Y, N, nv, NR, piv, perm);
-    lu_solve_inplace<float2, double2, NR>(A, N, N, Y, sm);
-    int it = 0;
-    bool converged = false;
-    for (; it < max_iter; ++it) {
-      structured_residual_permuted<NR>(src, wi.ch, wi.q, wi.w, N, nv, Y, Rb, perm, colsum,
-                                       reinterpret_cast<double2*>(&sm.u));
-      lu_solve_inplace<float2, double2, NR>(A, N, N, Rb, sm);
-      double dmax = 0.0, ymax = 0.0;
-      for (int e = tid; e < N * n2; e += T) {
-        const double2 d = Rb[e];
-        const double2 y = cadd(Y[e], d);
-        Y[e] = y;
-        dmax = fmax(dmax, fmax(fabs(d.x), fabs(d.y)));
-        ymax = fmax(ymax, fmax(fabs(y.x), fabs(y.y)));
-      }
-      dmax = block_max(dmax, sm.red_val);
-      ymax = block_max(ymax, sm.red_val);
-      if (!(dmax > tol * ymax)) {  // also stops on NaN, flagged below
-        converged = dmax <= tol * ymax;
-        ++it;
-        break;
-      }
-    }
-    if (tid == 0) sm.flag = 0;
-    __syncthreads();
     double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * n2;
-    bool bad = false;
-    for (int e = tid; e < N * n2; e += T) {
-      const int i = e / n2, sidx = e % n2;
-      double2 y = Y[(size_t)sidx * N + i];
-      y.x = y.x / beta;
-      y.y = y.y / beta;
-      if (!cfinite(y)) bad = true;
-      o[e] = y;
-    }
-    if (bad) atomicOr(&sm.flag, DGA_ITEM_NONFINITE);
-    __syncthreads();
-    if (tid == 0) {
-      if (status) status[item] = (singular ? DGA_ITEM_SINGULAR : 0) | sm.flag | (converged ? 0 : DGA_ITEM_NOCONVERGE);
+    int it = 0;
+    const int st = solve_item_mixed<NR>(src, wi, N, nv, beta, max_iter, tol, o, A, Y, Rb, sm, piv, perm, colsum,
+                                        &it);
+    if (threadIdx.x == 0) {
+      if (status) status[item] = st;
       if (iters) iters[item] = it;
     }
-    __syncthreads();
   }
 }
 
+// ----------------------------------------------------------------------------------------------
+// Heterogeneous batch: one persistent launch over the work items of several problems (requests) whose
+// sizes differ (niv, niw, number of q points, beta, inputs) but which share the number of orbitals, so that
+// the RHS count NR = n_orb^2 is a compile-time constant of the launch.  Each item names its problem, whose
+// descriptor carries the sizes, the resident inputs and the output.  The per-item body is the same as the
+// single-problem kernels.
+// ----------------------------------------------------------------------------------------------
+struct MultiItem {
+  int prob, ch, q, w;
+};
+
+template <bool MIXED, int NR>
+__global__ void __launch_bounds__(BSE_THREADS, 3)
+    bse_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work, int n_items,
+                     int n_max, int max_iter, double tol, int* __restrict__ status, int* __restrict__ iters,
+                     unsigned char* __restrict__ scratch, size_t slot_bytes, int redo_only) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (redo_only && (status[item] & (DGA_ITEM_NOCONVERGE | DGA_ITEM_NONFINITE)) == 0) continue;
+    const MultiItem mi = work[item];
+    const dga_bse_problem d = probs[mi.prob];
+    struct {
+      StructuredSource src;
+      int N, n2, nv, W, Q;
+      double beta;
+      double2* out;
+    } pb;
+    pb.n2 = d.n_orb * d.n_orb;
+    pb.nv = 2 * d.niv;
+    pb.N = pb.n2 * pb.nv;
+    pb.W = d.niw_half;
+    pb.Q = d.n_q;
+    pb.beta = d.beta;
+    pb.out = (double2*)d.out;
+    pb.src.gamma_cm = (const double2*)d.gamma_cm;
+    pb.src.chi0_inv = (const double2*)d.chi0_inv;
+    pb.src.uv = (const double2*)d.uv;
+    pb.src.n2 = pb.n2;
+    pb.src.nv = pb.nv;
+    pb.src.W = pb.W;
+    pb.src.Q = pb.Q;
+    pb.src.inv_beta2 = d.inv_beta2;
+    const WorkItem wi{mi.ch, mi.q, mi.w};
+    double2* o = pb.out + (((size_t)wi.ch * pb.Q + wi.q) * pb.W + wi.w) * (size_t)pb.N * pb.n2;
+    int st = 0, it = 0;
+    if (MIXED) {
+      BseSmem<float2>& sm = *reinterpret_cast<BseSmem<float2>*>(smem_raw);
+      int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<float2>));
+      int* perm = piv + n_max;
+      double2* colsum = reinterpret_cast<double2*>(smem_raw + mixed_colsum_offset(n_max));
+      float2* A = reinterpret_cast<float2*>(slot);
+      double2* Y = reinterpret_cast<double2*>(slot + (((size_t)pb.N * pb.N * sizeof(float2) + 255) & ~(size_t)255));
+      double2* Rb = Y + (size_t)pb.N * pb.n2;
+      st = solve_item_mixed<NR>(pb.src, wi, pb.N, pb.nv, pb.beta, max_iter, tol, o, A, Y, Rb, sm, piv, perm, colsum, &it);
+    } else {
+      BseSmem<double2>& sm = *reinterpret_cast<BseSmem<double2>*>(smem_raw);
+      int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<double2>));
+      int* perm = piv + n_max;
+      double2* A = reinterpret_cast<double2*>(slot);
+      double2* Y = A + (size_t)pb.N * pb.N;
+      st = solve_item_fp64<StructuredSource, NR>(pb.src, wi, pb.N, pb.nv, pb.beta, o, A, Y, sm, piv, perm);
+    }
+    __syncthreads();  // every thread has read status[item] before it is rewritten
+    if (threadIdx.x == 0) {
+      status[item] = st;
+      if (iters && !redo_only) iters[item] = it;
+    }
+  }
+}
 
 // ----------------------------------------------------------------------------------------------
 // Eliashberg full vertex in the pp frequency box (one CTA per (channel, q, w) item):
@@ -1237,6 +1329,120 @@ int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     dga_set_error("dga_eli_full_vertex_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"
+
+
+// ------------------------------------------------------------------------------------------------
+// Heterogeneous batch (host side)
+// ------------------------------------------------------------------------------------------------
+static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot) {
+  *n_max = 0;
+  *slot = 0;
+  if (n_prob <= 0) return false;
+  for (int p = 0; p < n_prob; ++p) {
+    const int n2 = probs[p].n_orb * probs[p].n_orb, N = n2 * 2 * probs[p].niv;
+    if (probs[p].n_orb != probs[0].n_orb || !supported_rhs(n2) || probs[p].niv <= 0 || N > BSE_MAX_N) return false;
+    if (N > *n_max) *n_max = N;
+    const size_t sl = mixed ? mixed_slot_bytes(N, n2) : ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
+    if (sl > *slot) *slot = sl;
+  }
+  *slot = (*slot + 255) & ~(size_t)255;
+  return true;
+}
+
+static size_t batch_smem(int n_max, int n2, int mixed) {
+  return mixed ? mixed_smem_bytes(n_max, n2) : bse_smem_bytes(n_max);
+}
+
+template <bool MIXED, int NR>
+static int batch_grid(int n_items, size_t smem) {
+  return grid_for(bse_multi_kernel<MIXED, NR>, n_items, smem);
+}
+
+static int batch_grid_any(int mixed, int n2, int n_items, size_t smem) {
+#define DGA_BATCH_GRID(R) \
+  if (n2 == R) return mixed ? batch_grid<true, R>(n_items, smem) : batch_grid<false, R>(n_items, smem);
+  DGA_BATCH_GRID(1)
+  DGA_BATCH_GRID(4)
+  DGA_BATCH_GRID(9)
+  DGA_BATCH_GRID(16)
+#undef DGA_BATCH_GRID
+  return 0;
+}
+
+extern "C" {
+
+// Scratch bytes of dga_bse_solve_sum_batch_c128 (probs is a HOST array here); 0 for an invalid batch.
+size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int n_items, int mode) {
+  int n_max = 0;
+  size_t slot = 0;
+  const int mixed = mode == 1;
+  if (!probs || n_items <= 0 || mode < 0 || mode > 2 || !batch_dims(probs, n_prob, mixed, &n_max, &slot)) return 0;
+  const int n2 = probs[0].n_orb * probs[0].n_orb;
+  return (size_t)batch_grid_any(mixed, n2, n_items, batch_smem(n_max, n2, mixed)) * slot;
+}
+
+// One persistent launch over the (problem, ch, q, w) items of several problems of the same orbital count whose
+// frequency boxes, q sets, beta and inputs differ.
+//   probs_host: the descriptors (read on the host for the launch geometry); probs_dev: the same array in device
+//   memory (read by the kernel); work: [n_items][4] ints (problem, channel, q, w) in device memory; mode: 0 =
+//   FP64 LU, 1 = FP32 LU + FP64 refinement (max_iter, tol), 2 = FP64 re-solve of the items whose status holds
+//   NOCONVERGE or NONFINITE; status / iters: [n_items] (iters may be null).  The grid is the smaller of the
+//   resident CTAs, n_items and scratch_bytes / slot: a smaller scratch buffer caps the launch's HBM footprint.
+int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* probs_dev, int n_prob, const int* work,
+                                 int n_items, int mode, int max_iter, double tol, int* status, int* iters,
+                                 void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  int n_max = 0;
+  size_t slot = 0;
+  const int mixed = mode == 1;
+  if (!probs_host || !probs_dev || !work || !scratch || !status || n_items <= 0 || max_iter < 0 || mode < 0 ||
+      mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot)) {
+    dga_set_error("dga_bse_solve_sum_batch_c128: invalid arguments (problems must share n_orb in {1,2,3,4})");
+    return DGA_ERR_ARG;
+  }
+  for (int p = 0; p < n_prob; ++p) {
+    const dga_bse_problem& d = probs_host[p];
+    if (!d.gamma_cm || !d.chi0_inv || !d.uv || !d.out || d.niw_half <= 0 || d.n_q <= 0) {
+      dga_set_error("dga_bse_solve_sum_batch_c128: problem %d has a null pointer or empty size", p);
+      return DGA_ERR_ARG;
+    }
+  }
+  const int n2 = probs_host[0].n_orb * probs_host[0].n_orb;
+  const size_t smem = batch_smem(n_max, n2, mixed);
+  int grid = batch_grid_any(mixed, n2, n_items, smem);
+  if (scratch_bytes < slot) {
+    dga_set_error("dga_bse_solve_sum_batch_c128: scratch too small (%zu < one slot of %zu)", scratch_bytes, slot);
+    return DGA_ERR_SCRATCH;
+  }
+  if ((size_t)grid > scratch_bytes / slot) grid = (int)(scratch_bytes / slot);
+  const int redo = mode == 2;
+  const dga_bse_problem* pd = (const dga_bse_problem*)probs_dev;
+  const MultiItem* wk = (const MultiItem*)work;
+  unsigned char* sc = (unsigned char*)scratch;
+#define DGA_BATCH_CASE(R)                                                                                          \
+  case R:                                                                                                          \
+    if (mixed)                                                                                                     \
+      bse_multi_kernel<true, R><<<grid, BSE_THREADS, smem, stream>>>(pd, wk, n_items, n_max, max_iter, tol, status, \
+                                                                     iters, sc, slot, 0);                         \
+    else                                                                                                           \
+      bse_multi_kernel<false, R><<<grid, BSE_THREADS, smem, stream>>>(pd, wk, n_items, n_max, max_iter, tol,       \
+                                                                      status, iters, sc, slot, redo);             \
+    break;
+  switch (n2) {
+    DGA_BATCH_CASE(1)
+    DGA_BATCH_CASE(4)
+    DGA_BATCH_CASE(9)
+    DGA_BATCH_CASE(16)
+  }
+#undef DGA_BATCH_CASE
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_bse_solve_sum_batch_c128: launch failed: %s", cudaGetErrorString(err));
     return DGA_ERR_LAUNCH;
   }
   return DGA_OK;

@@ -20,6 +20,16 @@
 #define DGA_ITEM_NONFINITE 2   // NaN or Inf in the result
 #define DGA_ITEM_NOCONVERGE 4  // iterative refinement did not reach its tolerance
 
+// One problem (request) of a heterogeneous BSE batch; the layout is part of the C ABI (include/dga_b200.h).
+typedef struct {
+  const void* gamma_cm;  // [2][W][N][N] column-major compound Gamma_r
+  const void* chi0_inv;  // [Q][W][nv][n2][n2]
+  const void* uv;        // [2][Q][n2][n2]
+  void* out;             // [2][Q][W][N][n2]
+  int n_orb, niv, niw_half, n_q;
+  double beta, inv_beta2;
+} dga_bse_problem;
+
 namespace dga {
 
 template <typename R>

@@ -19,7 +19,6 @@
 namespace dga {
 
 constexpr int ELI_THREADS = 128;
-constexpr int ELI_NB = 32;
 
 }  // namespace dga
 

@@ -99,24 +99,80 @@ class PassShapes:
         """(q, w) ladder solves of one pass: irreducible q x (niw+1) x 2 channels."""
         return self.n_q * self.W * 2
 
+    @classmethod
+    def from_inputs(cls, inp: dict) -> "PassShapes":
+        u = np.asarray(inp["u"])
+        g_k = inp["g_k"]
+        return cls(
+            n_orb=u.shape[0], nk=tuple(int(x) for x in inp["nk"]), beta=float(inp["beta"]), niw=int(inp["niw"]),
+            niv=int(inp["niv_core"]), niv_shell=int(inp["niv_shell"]), n_q=len(inp["irrk_ind"]),
+            niv_g=np.shape(g_k)[-1] // 2,
+        )
+
+
+_ALLOC_GRAIN = 512  # the caching allocator's block granularity
+
+
+def _blk(nbytes: int) -> int:
+    return -(-int(nbytes) // _ALLOC_GRAIN) * _ALLOC_GRAIN
+
+
+def sigma_chunks_for(sh: PassShapes) -> int:
+    """(nu, i, j, w-chunk) CTAs of the Sigma contraction: enough to fill 148 SMs twice."""
+    base = sh.niv * sh.n2
+    return max(1, min(2 * sh.niw + 1, -(-296 // base)))
+
+
+def estimate_device_bytes(sh: PassShapes, precision: str = "fp64", keep_intermediates: bool = True,
+                          own_bse_scratch: bool = False) -> int:
+    """HBM held by a LadderPass of these shapes (resident inputs + work buffers), computed without a GPU.
+
+    Mirrors the allocations of ``LadderPass.__init__``; with ``own_bse_scratch`` False (the serving path) the
+    BSE scratch is not counted because the batch launch brings its own."""
+    c = 16
+    n, n2, W, Q, nv, nvf, N, nk = sh.n_orb, sh.n2, sh.W, sh.n_q, sh.nv, sh.nvf, sh.N, sh.nk_tot
+    Nf = n2 * nvf
+    n_items = 2 * Q * W
+    tw = sum(sh.nk) * c
+    chunks = sigma_chunks_for(sh)
+    sizes = [
+        Q * 3 * 4, nk * 4, Q * 8, tw, tw,                      # q_irr, irrk_inv, irrk_count, twiddles
+        2 * Q * n2 * n2 * c, n2 * n2 * c, 2 * c,               # uv, u_perm, targets
+        2 * W * N * N * c, W * Nf * Nf * c,                    # gamma_cm, F_dc
+        nk * n * n * 2 * sh.niv_g * c, n_items * 3 * 4,        # G(k), work
+        (nvf + sh.niw) * n * n * nk * c, (sh.niv + 2 * sh.niw) * n * n * nk * c,  # G(R) slots
+        Q * W * nvf * n2 * n2 * c, Q * W * nv * n2 * n2 * c,   # chi0, chi0^-1
+        Q * W * n2 * n2 * c, Q * W * n2 * n2 * c,              # nu sums
+        Q * W * nv * n2 * n2 * c,                              # K_dc
+        (Q * W * 2 * (nvf // 2) * n2 * n2 * c) // c * c + c,  # dc scratch
+        2 * Q * W * N * n2 * c, n_items * 4, n_items * 4,      # X, status, iters
+        2 * Q * W * n2 * n2 * c, 2 * Q * W * n2 * n2 * c,      # chi_phys, chi_lam
+        2 * 8, 2 * 4, 4 * 4,                                   # lambdas, iterations, status
+        Q * W * nv * n2 * n2 * c,                              # K
+        (chunks * sh.niv * n2 * nk * c * 2) // c * c + c,      # Sigma scratch
+        nk * n * n * 2 * sh.niv * c,                           # Sigma
+    ]
+    if keep_intermediates:
+        sizes.append(2 * Q * W * nv * n2 * n2 * c)
+    if own_bse_scratch:
+        raise ValueError("the BSE scratch of a standalone pass depends on the GPU's occupancy; count it separately")
+    return sum(_blk(x) for x in sizes)
+
 
 class LadderPass:
     """Resident inputs, work buffers and the kernel sequence of one nonlocal pass."""
 
     def __init__(self, inp: dict, device: str = "cuda", do_lambda: bool | None = None, sigma_chunks: int | None = None,
                  keep_intermediates: bool = True, precision: str = "fp64", refine_tol: float = 1e-10,
-                 refine_max_iter: int = 6, resolve_grid: int = 148):
+                 refine_max_iter: int = 6, resolve_grid: int = 148, own_bse_scratch: bool = True):
         lib()  # fail loudly before anything else if the CUDA library is missing
         self.dev = torch.device(device)
         g_k = np.asarray(inp["g_k"])
         u = np.asarray(inp["u"], dtype=np.complex128)
         n_orb = u.shape[0]
-        nk = tuple(int(x) for x in inp["nk"])
-        self.sh = PassShapes(
-            n_orb=n_orb, nk=nk, beta=float(inp["beta"]), niw=int(inp["niw"]), niv=int(inp["niv_core"]),
-            niv_shell=int(inp["niv_shell"]), n_q=len(inp["irrk_ind"]), niv_g=g_k.shape[-1] // 2,
-        )
+        self.sh = PassShapes.from_inputs(inp)
         sh = self.sh
+        nk = sh.nk
         if sh.niv_g < sh.niv + sh.niv_shell + sh.niw:
             raise ValueError("G(k) must hold at least niv_full + niw fermionic frequencies")
         self.do_lambda = (n_orb == 1) if do_lambda is None else bool(do_lambda)
@@ -174,7 +230,6 @@ class LadderPass:
         self.n_items = len(work)
         # ---------------- work buffers ----------------
         Q, n2, nk_tot = sh.n_q, sh.n2, sh.nk_tot
-        t_b = 2 * (sh.niv + sh.niv_shell) // 2 * 2 + sh.niw  # slots [-niv_full - niw, niv_full)
         self.t_bubble = nvf + sh.niw
         self.g_r_bubble = torch.empty((self.t_bubble, n, n, nk_tot), dtype=C128, device=dev)
         self.t_sigma = sh.niv + 2 * sh.niw
@@ -189,7 +244,11 @@ class LadderPass:
         )
         self.X = torch.empty((2, Q, W, N, n2), dtype=C128, device=dev)
         self.bse_status = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
-        if precision == "fp64":
+        self.own_bse_scratch = bool(own_bse_scratch)
+        if not self.own_bse_scratch:
+            # the BSE runs in a batch launch (serving.solve_bse_batch) that brings its own scratch
+            self.bse_scratch = self.mixed_scratch = None
+        elif precision == "fp64":
             self.bse_scratch_bytes = int(lib().dga_bse_scratch_bytes(N, n2, self.n_items))
         else:
             # mixed solve + a small FP64 grid for the status-driven re-solve of unconverged items
@@ -197,8 +256,9 @@ class LadderPass:
             self.mixed_scratch_bytes = int(lib().dga_bse_mixed_scratch_bytes(N, n2, self.n_items))
             self.bse_scratch_bytes = self.resolve_grid * (N * N + N * n2) * 16
             self.mixed_scratch = torch.empty(self.mixed_scratch_bytes // 16 + 1, dtype=C128, device=dev)
-            self.bse_iters = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
-        self.bse_scratch = torch.empty(self.bse_scratch_bytes // 16 + 1, dtype=C128, device=dev)
+        if self.own_bse_scratch:
+            self.bse_scratch = torch.empty(self.bse_scratch_bytes // 16 + 1, dtype=C128, device=dev)
+        self.bse_iters = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
         self.chi_phys = torch.empty((2, Q, W, n2, n2), dtype=C128, device=dev)
         self.chi_lam = torch.empty((2, Q, W, n2, n2), dtype=C128, device=dev)
         self.lambdas = torch.zeros(2, dtype=torch.float64, device=dev)
@@ -207,9 +267,7 @@ class LadderPass:
         self.K = torch.empty((Q, W, nv, n2, n2), dtype=C128, device=dev)
         self.gamma3 = torch.empty((2, Q, W, nv, n2, n2), dtype=C128, device=dev) if keep_intermediates else None
         if sigma_chunks is None:
-            # enough (nu, i, j, w-chunk) CTAs to fill 148 SMs twice
-            base = sh.niv * n2
-            sigma_chunks = max(1, min(2 * sh.niw + 1, -(-296 // base)))
+            sigma_chunks = sigma_chunks_for(sh)
         self.sigma_chunks = sigma_chunks
         self.sigma_scratch_bytes = int(lib().dga_sigma_scratch_bytes(n, sh.niv, nk_tot, sigma_chunks))
         self.sigma_scratch = torch.empty(self.sigma_scratch_bytes // 16 + 1, dtype=C128, device=dev)
@@ -248,6 +306,8 @@ class LadderPass:
 
     def bse(self):
         sh = self.sh
+        if not self.own_bse_scratch:
+            raise RuntimeError("this pass was built without BSE scratch: run its BSE through serving.solve_bse_batch")
         if self.precision == "mixed":
             call("dga_bse_solve_sum_mixed_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
                  _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, self.refine_max_iter,
@@ -289,18 +349,26 @@ class LadderPass:
              _p(self.irrk_inv), _p(self.tw_inv), sh.beta, self.sigma_chunks, _p(self.sigma), _p(self.sigma_scratch),
              self.sigma_scratch.numel() * 16, _s())
 
-    def run(self):
-        """One device pass over the resident inputs (no host transfers, no synchronisation)."""
+    def pre_bse(self):
+        """Stages before the BSE: G(R), bubble, double-counting kernel, chi0^-1 and the nu sums."""
         self.status.zero_()
         self.bubble()
         self.dc_kernel()
         self.chi0_prep()
-        self.bse()
+
+    def post_bse(self):
+        """Stages after the BSE: chi_r with shell correction, lambda, kernel assembly, Sigma."""
         self.chi_phys_stage()
         chi_r = self.lambda_stage()
         self.kernel_stage(chi_r)
         self.sigma_stage()
         return self.sigma
+
+    def run(self):
+        """One device pass over the resident inputs (no host transfers, no synchronisation)."""
+        self.pre_bse()
+        self.bse()
+        return self.post_bse()
 
     def run_e2e(self) -> np.ndarray:
         """Host G(k) in, host Sigma(k, nu) out: H2D copy, one pass, D2H copy (synchronises)."""
@@ -309,6 +377,11 @@ class LadderPass:
         self.sigma_host.copy_(self.sigma, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return self.sigma_host.numpy()
+
+    def device_bytes(self) -> int:
+        """HBM held by this pass's device tensors, in caching-allocator blocks."""
+        return sum(_blk(t.numel() * t.element_size()) for t in vars(self).values()
+                   if isinstance(t, torch.Tensor) and t.is_cuda)
 
     @property
     def h2d_bytes(self) -> int:

@@ -1,0 +1,52 @@
+"""Small profiling case of the ladder pass: a configuration's orbitals and fermionic box (so the BSE matrices
+have the full compound size N) on a reduced momentum grid and bosonic box, so that one BSE launch is a single
+wave of CTAs and an ncu capture of it holds about a gigabyte of device memory.
+
+    python -m dgamore_b200.profile_case --config c3 --nk 4 --niw 10 --passes 1 [--precision mixed]
+
+Runs the passes and prints one JSON line with the shapes, the number of BSE items and the kernels launched.
+"""
+
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+
+import torch
+
+from . import synthetic
+from .pipeline import LadderPass
+
+
+def reduced_config(name: str, nk: int, niw: int) -> synthetic.DgaConfig:
+    cfg = synthetic.CONFIGS[name]
+    return dataclasses.replace(cfg, name=f"{name}_nk{nk}_niw{niw}", nk=(nk, nk, 1), niw=niw)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", default="c3")
+    ap.add_argument("--nk", type=int, default=4)
+    ap.add_argument("--niw", type=int, default=10)
+    ap.add_argument("--passes", type=int, default=1)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    args = ap.parse_args(argv)
+    cfg = reduced_config(args.config, args.nk, args.niw)
+    inp = synthetic.make_inputs(cfg)
+    lp = LadderPass(inp, keep_intermediates=False, precision=args.precision)
+    for _ in range(args.passes):
+        lp.run()
+    torch.cuda.synchronize()
+    status = int(lp.bse_status.abs().sum()) + int(lp.status.abs().sum())
+    print(json.dumps({
+        "case": cfg.name, "n_orb": lp.sh.n_orb, "N": lp.sh.N, "n_q": lp.sh.n_q, "bse_items": lp.n_items,
+        "passes": args.passes, "precision": args.precision, "status": status,
+        "device_bytes": lp.device_bytes() + (lp.bse_scratch.numel() * 16 if lp.bse_scratch is not None else 0),
+    }))
+    if status:
+        raise SystemExit(f"non-zero status {status}")
+
+
+if __name__ == "__main__":
+    main()

@@ -97,6 +97,30 @@ int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_c
                               void* out, int* status, int grid_limit, void* scratch, size_t scratch_bytes,
                               dga_stream_t stream);
 
+/* One request of a heterogeneous BSE batch: the inputs and output of one dga_bse_solve_sum_c128 problem
+ * (both channels; layouts as there) with its own frequency box, q set and beta. */
+typedef struct {
+  const void* gamma_cm; /* [2][W][N][N] column-major compound Gamma_r */
+  const void* chi0_inv; /* [Q][W][nv][n2][n2] */
+  const void* uv;       /* [2][Q][n2][n2] */
+  void* out;            /* [2][Q][W][N][n2] */
+  int n_orb, niv, niw_half, n_q;
+  double beta, inv_beta2;
+} dga_bse_problem;
+
+/* Ladder BSE of several requests in ONE persistent launch (the serving path's continuous batch; the upstream
+ * runs one create_auxiliary_chi_r_q_sum call per request, dgamore/nonlocal_sde.py:85-156).  Requests may differ
+ * in niv, niw, Q, beta and inputs but share n_orb (1..4).  probs_host: the descriptors on the host (launch
+ * geometry); probs_dev: the same array copied to device memory; work: [n_items][4] ints (request, ch, q, w);
+ * mode 0 runs the FP64 LU of dga_bse_solve_sum_c128, mode 1 the FP32 LU + FP64 refinement of
+ * dga_bse_solve_sum_mixed_c128 (max_iter, tol), mode 2 the FP64 re-solve of the items a mode-1 launch flagged;
+ * each item's result is bitwise the single-request result.  The launch uses at most scratch_bytes / slot CTAs
+ * (a smaller scratch caps its footprint); dga_bse_batch_scratch_bytes gives the size for a full grid. */
+size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs_host, int n_prob, int n_items, int mode);
+int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* probs_dev, int n_prob,
+                                 const int* work, int n_items, int mode, int max_iter, double tol, int* status,
+                                 int* iters, void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
 /* Allocation-free variant of dga_bse_solve_sum_c128 (no counterpart in the upstream, which has no device
  * code): for callers that cannot call cudaMalloc -- a host that binds only this C ABI and has no device
  * allocator, or a steady-state loop that must not trigger cudaMalloc's device-wide synchronisation.  The

@@ -48,3 +48,25 @@ def test_argument_errors_are_reported_without_launching():
     assert b"invalid" in lib.dga_last_error_string()
     with pytest.raises(_lib.DgaError):
         _lib.call("dga_strided_copy_c128", None, None, 0, None, None, None, 1.0, None)
+
+
+def test_batch_descriptor_matches_the_c_struct():
+    # dga_bse_problem: four pointers, four ints, two doubles, no padding on LP64
+    assert ctypes.sizeof(_lib.BseProblem) == 64
+    assert _lib.BseProblem.beta.offset == 48 and _lib.BseProblem.n_q.offset == 44
+
+
+def test_batch_rejects_mixed_orbital_counts_without_launching():
+    lib = _lib.lib()
+    arr = (_lib.BseProblem * 2)(
+        _lib.BseProblem(n_orb=1, niv=4, niw_half=3, n_q=2, beta=1.0),
+        _lib.BseProblem(n_orb=2, niv=4, niw_half=3, n_q=2, beta=1.0),
+    )
+    assert lib.dga_bse_batch_scratch_bytes(arr, 2, 10, 0) == 0
+    rc = lib.dga_bse_solve_sum_batch_c128(arr, None, 2, None, 10, 0, 0, 0.0, None, None, None, 0, None)
+    assert rc == 1 and b"n_orb" in lib.dga_last_error_string()
+    one = (_lib.BseProblem * 1)(_lib.BseProblem(n_orb=1, niv=4, niw_half=3, n_q=2, beta=1.0))
+    # null input pointers are caught before any CUDA call; an unknown mode too
+    rc = lib.dga_bse_solve_sum_batch_c128(one, 1, 1, 1, 10, 0, 0, 0.0, 1, None, 1, 1 << 30, None)
+    assert rc == 1 and b"null pointer" in lib.dga_last_error_string()
+    assert lib.dga_bse_solve_sum_batch_c128(one, 1, 1, 1, 10, 3, 0, 0.0, 1, None, 1, 1 << 30, None) == 1
