@@ -22,12 +22,15 @@
 //
 // The same LU core serves the FP64 drop-in (R = double) and the mixed form (R = float for the
 // factorisation, FP64 residuals and refinement; see bse_mixed below).
-#include "dga_common.cuh"
+#include "bse_core.cuh"
 
 #include <stdio.h>
 
 namespace dga {
 
+#ifndef DGA_MIXED_MIN_BLOCKS
+#define DGA_MIXED_MIN_BLOCKS 3  // resident CTAs per SM the mixed-precision kernels are compiled for
+#endif
 constexpr int BSE_THREADS = 128;
 constexpr int BSE_NB = 32;  // panel width (also the row-block of the triangular solves)
 constexpr int BSE_TM = 32;  // trailing-update row tile
@@ -36,66 +39,8 @@ constexpr int BSE_MAX_N = 2048;
 constexpr int MAX_RHS = 16;  // n2 <= 16 (up to 4 orbitals)
 
 // ----------------------------------------------------------------------------------------------
-// Matrix sources: how A(i, j) of a work item is formed
-// ----------------------------------------------------------------------------------------------
-
-// A formed from the resident ladder inputs (structured form of nonlocal_sde.py:85-96).
-struct StructuredSource {
-  const double2* gamma_cm;  // [n_ch][W][N][N]: column-major compound Gamma_r(w): element (i,j) at j*N + i
-  const double2* chi0_inv;  // [Q][W][nv][n2][n2]: chi0^-1 orbital matrices, row (o1,o2), column (o4,o3)
-  const double2* uv;        // [n_ch][Q][n2][n2]: U_r + V_r^q, row (o1,o2), column (o4,o3)
-  int n2, nv, W, Q;
-  double inv_beta2;  // 1 / beta**2 computed on the host exactly as the upstream does
-
-  // Element (i, j) in FP64, with the upstream's order of operations: (chi0inv_diag + Gamma*ib2) + (-(uv*ib2)).
-  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j, int pr, int vr, int pc,
-                                             int vc) const {
-    const double2 g = gamma_cm[((size_t)(ch * W + w) * N + j) * N + i];
-    const double2 u = uv[((size_t)ch * Q + q) * n2 * n2 + pr * n2 + pc];
-    double re = __dmul_rn(g.x, inv_beta2);
-    double im = __dmul_rn(g.y, inv_beta2);
-    if (vr == vc) {
-      const double2 c = chi0_inv[(((size_t)q * W + w) * nv + vr) * n2 * n2 + pr * n2 + pc];
-      re = __dadd_rn(c.x, re);
-      im = __dadd_rn(c.y, im);
-    }
-    re = __dadd_rn(re, -__dmul_rn(u.x, inv_beta2));
-    im = __dadd_rn(im, -__dmul_rn(u.y, inv_beta2));
-    return make_double2(re, im);
-  }
-};
-
-// A given explicitly in the upstream FourPoint layout [q][o1][o2][o3][o4][w][nu][nu'] (the generic
-// FourPoint.invert_and_sum_over_last_vn, four_point.py:620-642).
-struct DenseSource {
-  const double2* mat;  // [Q][n][n][n][n][W][nv][nv]
-  int nb, nv, W, Q;
-
-  __device__ __forceinline__ double2 element(int ch, int q, int w, int N, int i, int j, int pr, int vr, int pc,
-                                             int vc) const {
-    const int o1 = pr / nb, o2 = pr - o1 * nb;
-    const int o4 = pc / nb, o3 = pc - o4 * nb;
-    size_t idx = ((((size_t)q * nb + o1) * nb + o2) * nb + o3) * nb + o4;
-    idx = ((idx * W + w) * nv + vr) * nv + vc;
-    return mat[idx];
-  }
-};
-
-struct WorkItem {
-  int ch, q, w;
-};
-
-// ----------------------------------------------------------------------------------------------
 // Block-wide arg-max of the pivot measure: larger value wins, ties go to the smaller row index.
 // ----------------------------------------------------------------------------------------------
-template <typename R>
-__device__ __forceinline__ void argmax_merge(R& v, int& idx, R ov, int oidx) {
-  if (ov > v || (ov == v && oidx < idx)) {
-    v = ov;
-    idx = oidx;
-  }
-}
-
 template <typename R>
 __device__ int block_argmax(R v, int idx, R* s_val, int* s_idx) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -601,94 +546,12 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
 //
 //   Y0 = (LU)^-1 P S with the FP32 factors and FP64 accumulation of the triangular solves;
 //   repeat: r = S - A Y with A formed on the fly in FP64 from Gamma_r, chi0^-1 and U_r + V_r^q,
-//           d = (LU)^-1 P r,  Y += d,  until max|d| <= tol max|Y| or max_iter corrections.
+//           d = (LU)^-1 P r,  Y += d,  until the correction, or the error left after it as estimated from the
+//           observed contraction, is below tol max|Y| (refine_converged), or max_iter corrections.
 //
 // FP64 is used only for A in the residual, the residual accumulation and Y.  Items that do not reach the
 // tolerance are flagged DGA_ITEM_NOCONVERGE (the host re-solves them with the FP64 kernel).
 // ----------------------------------------------------------------------------------------------
-
-// r[s][i] = S[perm[i]][s] - (A Y)[perm[i]][s]: the residual of original row perm[i], stored at position i
-// (so the correction solve needs no separate permutation).  colsum: shared [n2][n2]; ys: shared [32][n2]
-// staging of Y rows, so the Gamma stream is the only global traffic of the inner loop.
-template <int NR>
-__device__ void structured_residual_permuted(const StructuredSource& src, int ch, int q, int w, int N, int nv,
-                                             const double2* __restrict__ Y, double2* __restrict__ Rp,
-                                             const int* __restrict__ perm, double2* colsum, double2* ys) {
-  constexpr int n2 = NR;
-  const int tid = threadIdx.x, T = blockDim.x;
-  // column sums over nu' of Y for the rank-n2 (U_r + V_r^q) part
-  for (int e = tid; e < n2 * n2; e += T) {
-    const int pc = e / n2, sidx = e - pc * n2;
-    double2 acc = make_double2(0.0, 0.0);
-    const double2* y = Y + (size_t)sidx * N + pc * nv;
-    for (int v = 0; v < nv; ++v) acc = cadd(acc, y[v]);
-    colsum[pc * n2 + sidx] = acc;
-  }
-  __syncthreads();
-  const double2* gam = src.gamma_cm + (size_t)(ch * src.W + w) * N * N;
-  const double2* uvq = src.uv + ((size_t)ch * src.Q + q) * n2 * n2;
-  for (int pos0 = 0; pos0 < N; pos0 += T) {
-    const int pos = pos0 + tid;
-    const bool active = pos < N;
-    const int i = active ? perm[pos] : 0;
-    double2 acc[NR];
-#pragma unroll
-    for (int sidx = 0; sidx < NR; ++sidx) acc[sidx] = make_double2(0.0, 0.0);
-    // Gamma part: sum_j Gamma[i][j] Y[j][s], Y staged 32 rows at a time
-    for (int j0 = 0; j0 < N; j0 += 32) {
-      const int jw = min(32, N - j0);
-      for (int e = tid; e < jw * NR; e += T) {
-        const int jj = e % jw, sidx = e / jw;
-        ys[jj * NR + sidx] = Y[(size_t)sidx * N + j0 + jj];
-      }
-      __syncthreads();
-      if (active) {
-        for (int jj = 0; jj < jw; ++jj) {
-          const double2 g = gam[(size_t)(j0 + jj) * N + i];
-#pragma unroll
-          for (int sidx = 0; sidx < NR; ++sidx) cfma(acc[sidx], g, ys[jj * NR + sidx]);
-        }
-      }
-      __syncthreads();
-    }
-    if (active) {
-      const int pr = i / nv, vr = i - pr * nv;
-      const double2* c0 = src.chi0_inv + (((size_t)q * src.W + w) * nv + vr) * n2 * n2 + pr * n2;
-#pragma unroll
-      for (int sidx = 0; sidx < NR; ++sidx) {
-        double2 a = cscale(acc[sidx], src.inv_beta2);
-        double2 d = make_double2(0.0, 0.0), u = make_double2(0.0, 0.0);
-        for (int pc = 0; pc < n2; ++pc) {
-          cfma(d, c0[pc], Y[(size_t)sidx * N + pc * nv + vr]);
-          cfma(u, uvq[pr * n2 + pc], colsum[pc * n2 + sidx]);
-        }
-        a = cadd(a, d);
-        a = csub(a, cscale(u, src.inv_beta2));
-        const double sel = (pr == sidx) ? 1.0 : 0.0;
-        Rp[(size_t)sidx * N + pos] = make_double2(sel - a.x, -a.y);
-      }
-    }
-  }
-  __syncthreads();
-}
-
-__device__ double block_max(double v, double* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = blockDim.x >> 5;
-    v = lane < nw ? red[lane] : 0.0;
-    for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-    if (lane == 0) red[0] = v;
-  }
-  __syncthreads();
-  const double r = red[0];
-  __syncthreads();
-  return r;
-}
 
 // byte offset of the [n2][n2] column-sum block after the pivot and permutation arrays, 16-byte aligned
 __host__ __device__ inline size_t mixed_colsum_offset(int N) {
@@ -729,6 +592,9 @@ __device__ int solve_item_mixed(const StructuredSource& src, const WorkItem& wi,
   const bool singular = lu_factor<float2>(A, N, N, piv, sm);
   permuted_selector<double2>(Y, N, nv, NR, piv, perm);
   lu_solve_inplace<float2, double2, NR>(A, N, N, Y, sm);
+  double prev = 0.0;
+  for (int e = tid; e < N * NR; e += T) prev = fmax(prev, fmax(fabs(Y[e].x), fabs(Y[e].y)));
+  prev = block_max(prev, sm.red_val);
   int it = 0;
   bool converged = false;
   for (; it < max_iter; ++it) {
@@ -745,11 +611,12 @@ __device__ int solve_item_mixed(const StructuredSource& src, const WorkItem& wi,
     }
     dmax = block_max(dmax, sm.red_val);
     ymax = block_max(ymax, sm.red_val);
-    if (!(dmax > tol * ymax)) {  // also stops on NaN, flagged below
-      converged = dmax <= tol * ymax;
+    if (isnan(dmax) || refine_converged(dmax, ymax, prev, tol)) {  // NaN is flagged below
+      converged = !isnan(dmax);
       ++it;
       break;
     }
+    prev = dmax;
   }
   if (tid == 0) sm.flag = 0;
   __syncthreads();
@@ -771,7 +638,7 @@ __device__ int solve_item_mixed(const StructuredSource& src, const WorkItem& wi,
 }
 
 template <int NR>
-__global__ void __launch_bounds__(BSE_THREADS, 3)
+__global__ void __launch_bounds__(BSE_THREADS, DGA_MIXED_MIN_BLOCKS)
     bse_solve_sum_mixed_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int n2,
                                int nv, int W, int Q, double beta, int max_iter, double tol,
                                double2* __restrict__ out, int* __restrict__ status, int* __restrict__ iters,
@@ -805,12 +672,8 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
 // descriptor carries the sizes, the resident inputs and the output.  The per-item body is the same as the
 // single-problem kernels.
 // ----------------------------------------------------------------------------------------------
-struct MultiItem {
-  int prob, ch, q, w;
-};
-
 template <bool MIXED, int NR>
-__global__ void __launch_bounds__(BSE_THREADS, 3)
+__global__ void __launch_bounds__(BSE_THREADS, MIXED ? DGA_MIXED_MIN_BLOCKS : 3)
     bse_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work, int n_items,
                      int n_max, int max_iter, double tol, int* __restrict__ status, int* __restrict__ iters,
                      unsigned char* __restrict__ scratch, size_t slot_bytes, int redo_only) {
@@ -1201,12 +1064,13 @@ extern "C" {
 // blocks per resident CTA.
 size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items) {
   if (N <= 0 || n2 <= 0 || n_items <= 0) return 0;
+  if (dga_panel_supported(N, n2)) return (size_t)dga_panel_grid(n2, N, n_items) * dga_panel_slot_bytes(N, n2);
   const size_t smem = mixed_smem_bytes(N, n2);
   return (size_t)mixed_grid(n_items, smem) * mixed_slot_bytes(N, n2);
 }
 
 // Mixed-precision ladder BSE: same inputs and output as dga_bse_solve_sum_c128; FP32 LU, FP64 residuals and
-// refinement to max|d| <= tol max|Y| within max_iter corrections.  iters: per-item corrections (optional).
+// refinement to tol (refine_converged) within max_iter corrections.  iters: per-item corrections (optional).
 int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
                                  const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
                                  int n_items, int max_iter, double tol, void* out, int* status, int* iters,
@@ -1222,9 +1086,10 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
     dga_set_error("dga_bse_solve_sum_mixed_c128: null pointer argument");
     return DGA_ERR_ARG;
   }
+  const bool panel = dga_panel_supported(N, n2);
   const size_t smem = mixed_smem_bytes(N, n2);
-  const int grid = mixed_grid(n_items, smem);
-  const size_t slot = mixed_slot_bytes(N, n2);
+  const int grid = panel ? dga_panel_grid(n2, N, n_items) : mixed_grid(n_items, smem);
+  const size_t slot = panel ? dga_panel_slot_bytes(N, n2) : mixed_slot_bytes(N, n2);
   if (scratch_bytes < (size_t)grid * slot) {
     dga_set_error("dga_bse_solve_sum_mixed_c128: scratch too small (%zu < %zu)", scratch_bytes, (size_t)grid * slot);
     return DGA_ERR_SCRATCH;
@@ -1238,6 +1103,17 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
   src.W = niw_half;
   src.Q = n_q;
   src.inv_beta2 = inv_beta2;
+  if (panel) {
+    // N fits the shared-memory panel: one 512-thread CTA per SM (bse_panel.cu)
+    cudaError_t err = dga_panel_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta,
+                                       max_iter, tol, (double2*)out, status, iters, (unsigned char*)scratch, slot,
+                                       stream);
+    if (err != cudaSuccess) {
+      dga_set_error("dga_bse_solve_sum_mixed_c128: launch failed: %s", cudaGetErrorString(err));
+      return DGA_ERR_LAUNCH;
+    }
+    return DGA_OK;
+  }
 #define DGA_MIXED_CASE(NRV)                                                                                       \
   case NRV:                                                                                                       \
     cudaFuncSetAttribute(bse_solve_sum_mixed_kernel<NRV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
@@ -1340,15 +1216,24 @@ int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_
 // ------------------------------------------------------------------------------------------------
 // Heterogeneous batch (host side)
 // ------------------------------------------------------------------------------------------------
-static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot) {
+static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot,
+                       bool* panel) {
   *n_max = 0;
   *slot = 0;
+  *panel = false;
   if (n_prob <= 0) return false;
   for (int p = 0; p < n_prob; ++p) {
     const int n2 = probs[p].n_orb * probs[p].n_orb, N = n2 * 2 * probs[p].niv;
     if (probs[p].n_orb != probs[0].n_orb || !supported_rhs(n2) || probs[p].niv <= 0 || N > BSE_MAX_N) return false;
     if (N > *n_max) *n_max = N;
-    const size_t sl = mixed ? mixed_slot_bytes(N, n2) : ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
+  }
+  const int n2 = probs[0].n_orb * probs[0].n_orb;
+  *panel = mixed && dga_panel_supported(*n_max, n2);
+  for (int p = 0; p < n_prob; ++p) {
+    const int N = n2 * 2 * probs[p].niv;
+    const size_t sl = *panel ? dga_panel_slot_bytes(N, n2)
+                      : mixed ? mixed_slot_bytes(N, n2)
+                              : ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
     if (sl > *slot) *slot = sl;
   }
   *slot = (*slot + 255) & ~(size_t)255;
@@ -1381,9 +1266,12 @@ extern "C" {
 size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int n_items, int mode) {
   int n_max = 0;
   size_t slot = 0;
+  bool panel = false;
   const int mixed = mode == 1;
-  if (!probs || n_items <= 0 || mode < 0 || mode > 2 || !batch_dims(probs, n_prob, mixed, &n_max, &slot)) return 0;
+  if (!probs || n_items <= 0 || mode < 0 || mode > 2 || !batch_dims(probs, n_prob, mixed, &n_max, &slot, &panel))
+    return 0;
   const int n2 = probs[0].n_orb * probs[0].n_orb;
+  if (panel) return (size_t)dga_panel_batch_grid(n2, n_max, n_items) * slot;
   return (size_t)batch_grid_any(mixed, n2, n_items, batch_smem(n_max, n2, mixed)) * slot;
 }
 
@@ -1399,9 +1287,10 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
                                  void* scratch, size_t scratch_bytes, cudaStream_t stream) {
   int n_max = 0;
   size_t slot = 0;
+  bool panel = false;
   const int mixed = mode == 1;
   if (!probs_host || !probs_dev || !work || !scratch || !status || n_items <= 0 || max_iter < 0 || mode < 0 ||
-      mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot)) {
+      mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot, &panel)) {
     dga_set_error("dga_bse_solve_sum_batch_c128: invalid arguments (problems must share n_orb in {1,2,3,4})");
     return DGA_ERR_ARG;
   }
@@ -1414,7 +1303,7 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   }
   const int n2 = probs_host[0].n_orb * probs_host[0].n_orb;
   const size_t smem = batch_smem(n_max, n2, mixed);
-  int grid = batch_grid_any(mixed, n2, n_items, smem);
+  int grid = panel ? dga_panel_batch_grid(n2, n_max, n_items) : batch_grid_any(mixed, n2, n_items, smem);
   if (scratch_bytes < slot) {
     dga_set_error("dga_bse_solve_sum_batch_c128: scratch too small (%zu < one slot of %zu)", scratch_bytes, slot);
     return DGA_ERR_SCRATCH;
@@ -1424,6 +1313,15 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   const dga_bse_problem* pd = (const dga_bse_problem*)probs_dev;
   const MultiItem* wk = (const MultiItem*)work;
   unsigned char* sc = (unsigned char*)scratch;
+  if (panel) {
+    cudaError_t err = dga_panel_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
+                                             stream);
+    if (err != cudaSuccess) {
+      dga_set_error("dga_bse_solve_sum_batch_c128: launch failed: %s", cudaGetErrorString(err));
+      return DGA_ERR_LAUNCH;
+    }
+    return DGA_OK;
+  }
 #define DGA_BATCH_CASE(R)                                                                                          \
   case R:                                                                                                          \
     if (mixed)                                                                                                     \

@@ -1,0 +1,721 @@
+// Mixed-precision ladder BSE with the LU panel in shared memory.
+//
+// Same result as the mixed form of bse.cu (complex64 LU, FP64 iterative refinement of
+// X = sum_nu' A^-1 / beta, dgamore/four_point.py:620-684), organised so that no phase of the factorisation
+// waits on global memory column by column.  One 512-thread CTA per SM owns one (channel, q, w) item at a time:
+//
+//   1. A is formed in FP64 from Gamma_r, chi0^-1 and U_r + V_r^q (StructuredSource::element) and stored as
+//      complex64, column-major, in the CTA's scratch slot;
+//   2. right-looking LU with partial pivoting (LAPACK pivot measure |re|+|im|, first-index ties), 32-column
+//      panels.  The m x 32 panel is loaded into shared memory and factored there: each warp owns a contiguous
+//      block of rows, two barriers per column, and every warp computes the next column's pivot candidate
+//      while it applies the current column's rank-1 update.  The factored panel is written back and stays in
+//      shared memory as the L21 operand of the trailing update.  The panel's row interchanges are applied to
+//      the columns on its right while U12 = L11^-1 A12 is formed, one 64-column strip at a time (the rows the
+//      interchanges touch are read once, then written once), and each strip's 128 x 64 tiles of the trailing
+//      matrix are updated in FP32 with L21 and U12 from shared memory.  The interchanges are never applied to
+//      the columns left of the panel: the forward substitution applies each panel's interchanges to the
+//      right-hand sides before that panel's elimination, which is the same product P_k, L_k^-1 as LAPACK's.
+//   3. The n2 selector right-hand sides are solved in FP32 with the right-hand sides held in shared memory;
+//      the FP64 refinement loop r = S - A Y (A formed on the fly in FP64), d = (LU)^-1 r, Y += d stops when
+//      the correction, or the error left after it as estimated from the observed contraction, is below
+//      tol max|Y| (refine_converged).  Items that do not converge, or whose result is not finite, are flagged.
+//
+// Shared memory holds the m x 32 complex64 panel (256 B per row), so N is limited to about 790 (the 227 KB
+// opt-in limit); larger items use the 128-thread kernel of bse.cu.
+#include "bse_core.cuh"
+
+namespace dga {
+
+constexpr int PT = 512;       // threads per CTA
+constexpr int PW = PT / 32;   // warps
+constexpr int PNB = 32;       // panel width
+constexpr int PTM = 128;      // trailing tile rows
+constexpr int PTN = 64;       // trailing strip columns
+constexpr int P_MAX_SMEM = 232448;  // 227 KB opt-in shared memory per block on sm_100
+
+// ----------------------------------------------------------------------------------------------
+// Shared-memory layout (ldp = leading dimension of the panel = the largest N the launch serves)
+// ----------------------------------------------------------------------------------------------
+// The panel region also holds the solve's right-hand sides (up to 16 x ldp complex64) followed by the residual's
+// staging ([32][16] and [16][16] complex128), so small ldp need more than the panel itself.
+__host__ __device__ inline size_t panel_region_bytes(int ldp) {
+  const size_t panel = (size_t)ldp * PNB * sizeof(float2);
+  const size_t solve = (size_t)16 * ldp * sizeof(float2) + 32 + (32 * 16 + 16 * 16) * sizeof(double2);
+  return ((panel > solve ? panel : solve) + 15) & ~(size_t)15;
+}
+constexpr size_t P_FIXED = 16 * sizeof(double)                 // redd
+                           + PNB * (PNB + 1) * sizeof(float2)  // L11i
+                           + PNB * PTN * sizeof(float2)        // Us
+                           + 16 * sizeof(float) + 16 * sizeof(int)  // red_val, red_idx
+                           + 64 * sizeof(int) * 2              // s_row, s_cont
+                           + 4 * sizeof(int);                  // misc
+__host__ __device__ inline size_t panel_smem_bytes(int ldp) { return panel_region_bytes(ldp) + P_FIXED + sizeof(int) * (size_t)ldp; }
+
+struct PanelSmem {
+  float2* P;     // [PNB][ldp] panel, column-major (also the solve and residual staging area)
+  double* redd;  // [16]
+  float2* L11i;  // [PNB][PNB+1] inverse of the unit lower triangle of L11
+  float2* Us;    // [PNB][PTN] U12 strip
+  float* red_val;
+  int* red_idx;
+  int* s_row;   // [64] rows touched by the panel's interchanges: slots 0..31 the panel rows, 32.. the others
+  int* s_cont;  // [64] old row whose content ends up in s_row[slot]
+  int* misc;    // [0] number of rows below the panel that receive another row
+  int* piv;     // [ldp] row interchanged with row j
+  int ldp;
+
+  __device__ PanelSmem(unsigned char* base, int ldp_) : ldp(ldp_) {
+    unsigned char* p = base;
+    P = reinterpret_cast<float2*>(p);
+    p += panel_region_bytes(ldp);
+    redd = reinterpret_cast<double*>(p);
+    p += 16 * sizeof(double);
+    L11i = reinterpret_cast<float2*>(p);
+    p += PNB * (PNB + 1) * sizeof(float2);
+    Us = reinterpret_cast<float2*>(p);
+    p += PNB * PTN * sizeof(float2);
+    red_val = reinterpret_cast<float*>(p);
+    p += 16 * sizeof(float);
+    red_idx = reinterpret_cast<int*>(p);
+    p += 16 * sizeof(int);
+    s_row = reinterpret_cast<int*>(p);
+    p += 64 * sizeof(int);
+    s_cont = reinterpret_cast<int*>(p);
+    p += 64 * sizeof(int);
+    misc = reinterpret_cast<int*>(p);
+    p += 4 * sizeof(int);
+    piv = reinterpret_cast<int*>(p);
+  }
+};
+
+__device__ __forceinline__ void warp_argmax(float& v, int& idx) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const float ov = __shfl_down_sync(0xffffffffu, v, off);
+    const int oi = __shfl_down_sync(0xffffffffu, idx, off);
+    argmax_merge(v, idx, ov, oi);
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Factor the m x nb panel in shared memory (column-major, leading dimension ldp) with partial pivoting.
+// Rows are local to the panel (row r = global row k0 + r); piv[k0 + j] receives the global pivot row.
+// Returns true if an exact zero pivot was met (the column is then left unscaled, as LAPACK's zgetf2 does).
+// ----------------------------------------------------------------------------------------------
+__device__ bool panel_factor(PanelSmem& s, int m, int nb, int k0) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float2* P = s.P;
+  const int ldp = s.ldp;
+  const int rpw = (m + PW - 1) / PW;
+  const int r0 = warp * rpw, r1 = min(m, r0 + rpw);
+  bool singular = false;
+  {
+    float best = -1.f;
+    int bidx = 0x7fffffff;
+    for (int r = r0 + lane; r < r1; r += 32) {
+      const float v = cabs1(P[r]);
+      if (v > best) {
+        best = v;
+        bidx = r;
+      }
+    }
+    warp_argmax(best, bidx);
+    if (lane == 0) {
+      s.red_val[warp] = best;
+      s.red_idx[warp] = bidx;
+    }
+  }
+  for (int jj = 0; jj < nb; ++jj) {
+    __syncthreads();  // this column's candidates are in place; the previous update is complete
+    float bv = s.red_val[0];
+    int p = s.red_idx[0];
+#pragma unroll
+    for (int w = 1; w < PW; ++w) argmax_merge(bv, p, s.red_val[w], s.red_idx[w]);
+    if (p < jj || p >= m) p = jj;  // cannot happen (row jj itself is a candidate); keeps p in range
+    if (tid == 0) s.piv[k0 + jj] = k0 + p;
+    if (p != jj && tid < nb) {
+      float2* col = P + (size_t)tid * ldp;
+      const float2 t = col[jj];
+      col[jj] = col[p];
+      col[p] = t;
+    }
+    __syncthreads();  // pivot row in place
+    const float2 d = P[(size_t)jj * ldp + jj];
+    const bool zero = (d.x == 0.f && d.y == 0.f);
+    singular |= zero;
+    const float2 rinv = zero ? make_float2(0.f, 0.f) : crecip(d);
+    const int c1 = jj + 1;
+    float best = -1.f;
+    int bidx = 0x7fffffff;
+    for (int r = max(r0, c1) + lane; r < r1; r += 32) {
+      float2 l = P[(size_t)jj * ldp + r];
+      if (!zero) l = cmul(l, rinv);
+      P[(size_t)jj * ldp + r] = l;
+      if (c1 < nb) {
+        float2 v = P[(size_t)c1 * ldp + r];
+        cfms(v, l, P[(size_t)c1 * ldp + jj]);
+        P[(size_t)c1 * ldp + r] = v;
+        const float a = cabs1(v);
+        if (a > best) {
+          best = a;
+          bidx = r;
+        }
+        for (int c = c1 + 1; c < nb; ++c) {
+          float2 x = P[(size_t)c * ldp + r];
+          cfms(x, l, P[(size_t)c * ldp + jj]);
+          P[(size_t)c * ldp + r] = x;
+        }
+      }
+    }
+    warp_argmax(best, bidx);
+    if (lane == 0) {
+      s.red_val[warp] = best;
+      s.red_idx[warp] = bidx;
+    }
+  }
+  __syncthreads();
+  return singular;
+}
+
+// X = L11^-1 for the unit lower nb x nb block at the top of the panel: warp per column, lane = row.
+__device__ void panel_unit_lower_inverse(PanelSmem& s, int nb) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = warp; c < PNB; c += PW) {
+    float2 x = make_float2(lane == c ? 1.f : 0.f, 0.f);
+    for (int k = c; k < nb - 1; ++k) {
+      const float xk_re = __shfl_sync(0xffffffffu, x.x, k);
+      const float xk_im = __shfl_sync(0xffffffffu, x.y, k);
+      if (lane > k && lane < nb) cfms(x, s.P[(size_t)k * s.ldp + lane], make_float2(xk_re, xk_im));
+    }
+    if (lane >= nb || lane < c) x = make_float2(0.f, 0.f);
+    s.L11i[lane * (PNB + 1) + c] = x;
+  }
+}
+
+// Net effect of the panel's interchanges on the rows they touch (one warp): after the sequential swaps
+// (k0+t <-> piv[k0+t]) row s_row[slot] holds the old content of row s_cont[slot].
+__device__ void panel_interchange_map(PanelSmem& s, int k0, int nb) {
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x >= 32) return;
+  s.s_row[lane] = k0 + lane;
+  s.s_cont[lane] = k0 + lane;
+  int n_tgt = 0;
+  __syncwarp();
+  for (int t = 0; t < nb; ++t) {
+    const int p = s.piv[k0 + t];
+    if (p == k0 + t) continue;
+    int slot;
+    if (p < k0 + nb) {
+      slot = p - k0;
+    } else {
+      const unsigned hit = __ballot_sync(0xffffffffu, lane < n_tgt && s.s_row[32 + lane] == p);
+      if (hit) {
+        slot = 32 + __ffs(hit) - 1;
+      } else {
+        slot = 32 + n_tgt;
+        if (lane == 0) {
+          s.s_row[slot] = p;
+          s.s_cont[slot] = p;
+        }
+        ++n_tgt;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const int tmp = s.s_cont[t];
+      s.s_cont[t] = s.s_cont[slot];
+      s.s_cont[slot] = tmp;
+    }
+    __syncwarp();
+  }
+  if (lane == 0) s.misc[0] = n_tgt;
+}
+
+// ----------------------------------------------------------------------------------------------
+// LU of the N x N complex64 column-major matrix A (leading dimension N) in place.
+// ----------------------------------------------------------------------------------------------
+__device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s) {
+  const int tid = threadIdx.x;
+  bool singular = false;
+  for (int k0 = 0; k0 < N; k0 += PNB) {
+    const int nb = min(PNB, N - k0), m = N - k0, k1 = k0 + nb;
+    // ---- load and factor the panel (8 loads per thread in flight) ----
+    for (int e0 = 0; e0 < m * nb; e0 += 8 * PT) {
+      float2 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * PT + tid;
+        if (e < m * nb) {
+          const int c = e / m, r = e - c * m;
+          v[u] = A[(size_t)(k0 + c) * N + k0 + r];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * PT + tid;
+        if (e < m * nb) {
+          const int c = e / m, r = e - c * m;
+          s.P[(size_t)c * s.ldp + r] = v[u];
+        }
+      }
+    }
+    __syncthreads();
+    singular |= panel_factor(s, m, nb, k0);
+    for (int e = tid; e < m * nb; e += PT) {
+      const int c = e / m, r = e - c * m;
+      A[(size_t)(k0 + c) * N + k0 + r] = s.P[(size_t)c * s.ldp + r];
+    }
+    if (k1 >= N) break;
+    panel_unit_lower_inverse(s, nb);
+    panel_interchange_map(s, k0, nb);
+    __syncthreads();
+    const int n_tgt = s.misc[0];
+    // ---- per 64-column strip: interchanges + U12, then the strip's trailing tiles ----
+    for (int cs = k1; cs < N; cs += PTN) {
+      const int cw = min(PTN, N - cs);
+      {
+        // warp w handles columns w, w + 16, w + 32, w + 48 of the strip; lane = row of the U block (reads of the
+        // touched rows are coalesced along the column).  Every old value is read, and U12 computed, before the
+        // barrier; the writes follow it.
+        const int lane = tid & 31, warp = tid >> 5;
+        float2 u[PTN / PW], tv[PTN / PW];
+        const int src_row = s.s_cont[lane];
+        const int tgt_src = lane < n_tgt ? s.s_cont[32 + lane] : 0;
+        float2 av[PTN / PW];
+#pragma unroll
+        for (int q = 0; q < PTN / PW; ++q) {
+          const int c = warp + PW * q;
+          const float2* colp = A + (size_t)(cs + c) * N;
+          av[q] = (c < cw && lane < nb) ? colp[src_row] : make_float2(0.f, 0.f);
+          tv[q] = (c < cw && lane < n_tgt) ? colp[tgt_src] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int q = 0; q < PTN / PW; ++q) {
+          float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int k = 0; k < PNB; ++k) {
+            const float re = __shfl_sync(0xffffffffu, av[q].x, k), im = __shfl_sync(0xffffffffu, av[q].y, k);
+            cfma(acc, s.L11i[lane * (PNB + 1) + k], make_float2(re, im));
+          }
+          u[q] = acc;
+        }
+        __syncthreads();  // every old value of the touched rows is read before any is overwritten
+        const int tgt_row = lane < n_tgt ? s.s_row[32 + lane] : 0;
+#pragma unroll
+        for (int q = 0; q < PTN / PW; ++q) {
+          const int c = warp + PW * q;
+          float2* colw = A + (size_t)(cs + c) * N;
+          const bool act = c < cw && lane < nb;
+          if (act) colw[k0 + lane] = u[q];
+          s.Us[lane * PTN + c] = act ? u[q] : make_float2(0.f, 0.f);
+          if (c < cw && lane < n_tgt) colw[tgt_row] = tv[q];
+        }
+      }
+      __syncthreads();
+      // trailing tiles of the strip, 128 x 64: thread (ty, tx) owns rows rt + 2ty + {0,1} + {0,64} and columns
+      // cs + 2tx + {0,1} + {0,32} (row pairs and column pairs move as one 16-byte access; N is even), with the
+      // real and imaginary parts in separate scalar accumulators.
+      const int ty = tid & 31, tx = tid >> 5;
+      const float2* up = s.Us + 2 * tx;
+      for (int rt = k1; rt < N; rt += PTM) {
+        float cr[16], ci[16];  // index (column j of 4) * 4 + (row i of 4)
+        const int rbase = rt + 2 * ty;
+        const bool full = rt + PTM <= N && cs + PTN <= N;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int c = cs + 2 * tx + (j & 1) + 32 * (j >> 1);
+#pragma unroll
+          for (int ap = 0; ap < 2; ++ap) {
+            const int r = rbase + 64 * ap;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (full || (c < N && r < N)) v = *reinterpret_cast<const float4*>(A + (size_t)c * N + r);
+            cr[j * 4 + 2 * ap] = v.x;
+            ci[j * 4 + 2 * ap] = v.y;
+            cr[j * 4 + 2 * ap + 1] = v.z;
+            ci[j * 4 + 2 * ap + 1] = v.w;
+          }
+        }
+        const bool r0ok = full || rbase < N, r1ok = full || rbase + 64 < N;
+        const float2* lp0 = s.P + (r0ok ? rbase - k0 : 0);
+        const float2* lp1 = s.P + (r1ok ? rbase + 64 - k0 : 0);
+#pragma unroll 4
+        for (int k = 0; k < nb; ++k) {
+          float4 l0 = *reinterpret_cast<const float4*>(lp0 + (size_t)k * s.ldp);
+          float4 l1 = *reinterpret_cast<const float4*>(lp1 + (size_t)k * s.ldp);
+          if (!r0ok) l0 = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (!r1ok) l1 = make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 u0 = *reinterpret_cast<const float4*>(up + k * PTN);
+          const float4 u1 = *reinterpret_cast<const float4*>(up + k * PTN + 32);
+          const float lr[4] = {l0.x, l0.z, l1.x, l1.z}, li[4] = {l0.y, l0.w, l1.y, l1.w};
+          const float ur[4] = {u0.x, u0.z, u1.x, u1.z}, ui[4] = {u0.y, u0.w, u1.y, u1.w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              cr[j * 4 + i] = fmaf(-lr[i], ur[j], cr[j * 4 + i]);
+              cr[j * 4 + i] = fmaf(li[i], ui[j], cr[j * 4 + i]);
+              ci[j * 4 + i] = fmaf(-lr[i], ui[j], ci[j * 4 + i]);
+              ci[j * 4 + i] = fmaf(-li[i], ur[j], ci[j * 4 + i]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int c = cs + 2 * tx + (j & 1) + 32 * (j >> 1);
+#pragma unroll
+          for (int ap = 0; ap < 2; ++ap) {
+            const int r = rbase + 64 * ap;
+            if (full || (c < N && r < N))
+              *reinterpret_cast<float4*>(A + (size_t)c * N + r) =
+                  make_float4(cr[j * 4 + 2 * ap], ci[j * 4 + 2 * ap], cr[j * 4 + 2 * ap + 1], ci[j * 4 + 2 * ap + 1]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  return singular;
+}
+
+// ----------------------------------------------------------------------------------------------
+// In-place solve (L U) y = b for the NR right-hand sides y[s][i] (complex64, shared memory, stride ldy),
+// with the factors of panel_lu and its interchanges piv (applied panel by panel in the forward pass).
+// ----------------------------------------------------------------------------------------------
+template <int NR>
+__device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv, float2* y, int ldy) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // forward: y <- L^-1 P y
+  for (int k0 = 0; k0 < N; k0 += PNB) {
+    const int nb = min(PNB, N - k0), k1 = k0 + nb;
+    if (warp == 0 && lane < NR) {
+      float2* ys = y + (size_t)lane * ldy;
+      for (int t = 0; t < nb; ++t) {
+        const int p = piv[k0 + t];
+        if (p != k0 + t) {
+          const float2 tmp = ys[k0 + t];
+          ys[k0 + t] = ys[p];
+          ys[p] = tmp;
+        }
+      }
+    }
+    __syncthreads();
+    if (warp < NR) {
+      float2* ys = y + (size_t)warp * ldy;
+      float2 yr = lane < nb ? ys[k0 + lane] : make_float2(0.f, 0.f);
+      float2 lrow[PNB];
+#pragma unroll
+      for (int k = 0; k < PNB; ++k)
+        lrow[k] = (lane < nb && k < lane) ? A[(size_t)(k0 + k) * N + k0 + lane] : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < PNB - 1; ++k) {
+        const float re = __shfl_sync(0xffffffffu, yr.x, k), im = __shfl_sync(0xffffffffu, yr.y, k);
+        if (k < lane) cfms(yr, lrow[k], make_float2(re, im));
+      }
+      if (lane < nb) ys[k0 + lane] = yr;
+    }
+    __syncthreads();
+    for (int i = k1 + tid; i < N; i += PT) {
+      float2 acc[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) acc[r] = y[(size_t)r * ldy + i];
+      for (int k = 0; k < nb; k += 16) {  // 16 factor loads in flight
+        float2 l[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) l[u] = (k + u < nb) ? A[(size_t)(k0 + k + u) * N + i] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+          if (k + u < nb) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) cfms(acc[r], l[u], y[(size_t)r * ldy + k0 + k + u]);
+          }
+      }
+#pragma unroll
+      for (int r = 0; r < NR; ++r) y[(size_t)r * ldy + i] = acc[r];
+    }
+    __syncthreads();
+  }
+  // backward: y <- U^-1 y
+  const int nblk = (N + PNB - 1) / PNB;
+  for (int bk = nblk - 1; bk >= 0; --bk) {
+    const int k0 = bk * PNB, nb = min(PNB, N - k0);
+    if (warp < NR) {
+      float2* ys = y + (size_t)warp * ldy;
+      float2 yr = lane < nb ? ys[k0 + lane] : make_float2(0.f, 0.f);
+      float2 urow[PNB];
+#pragma unroll
+      for (int k = 0; k < PNB; ++k)
+        urow[k] = (lane < nb && k >= lane && k < nb) ? A[(size_t)(k0 + k) * N + k0 + lane] : make_float2(1.f, 0.f);
+#pragma unroll
+      for (int k = PNB - 1; k >= 0; --k) {
+        if (k < nb) {
+          if (lane == k) yr = cdiv(yr, urow[k]);
+          const float re = __shfl_sync(0xffffffffu, yr.x, k), im = __shfl_sync(0xffffffffu, yr.y, k);
+          if (lane < k) cfms(yr, urow[k], make_float2(re, im));
+        }
+      }
+      if (lane < nb) ys[k0 + lane] = yr;
+    }
+    __syncthreads();
+    for (int i = tid; i < k0; i += PT) {
+      float2 acc[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) acc[r] = y[(size_t)r * ldy + i];
+      for (int k = 0; k < nb; k += 16) {
+        float2 u[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) u[q] = (k + q < nb) ? A[(size_t)(k0 + k + q) * N + i] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          if (k + q < nb) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) cfms(acc[r], u[q], y[(size_t)r * ldy + k0 + k + q]);
+          }
+      }
+#pragma unroll
+      for (int r = 0; r < NR; ++r) y[(size_t)r * ldy + i] = acc[r];
+    }
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// One work item: form, factor, solve, refine.  Returns the status bits; *iters = number of corrections.
+//   slot: A (N x N complex64) | Y (NR x N complex128) | Rb (NR x N complex128)
+// ----------------------------------------------------------------------------------------------
+__host__ __device__ inline size_t panel_slot_bytes(int N, int n2) {
+  return (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255) + 2 * (size_t)N * n2 * sizeof(double2);
+}
+
+template <int NR>
+__device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi, int N, int nv, double beta,
+                                int max_iter, double tol, double2* __restrict__ o, unsigned char* slot, PanelSmem& s,
+                                int* iters) {
+  const int tid = threadIdx.x;
+  float2* A = reinterpret_cast<float2*>(slot);
+  double2* Y = reinterpret_cast<double2*>(slot + (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255));
+  double2* Rb = Y + (size_t)N * NR;
+  // ---- form A in complex64 (8 independent elements per thread in flight) ----
+  {
+    const long long NN = (long long)N * N;
+    for (long long e0 = 0; e0 < NN; e0 += 8LL * PT) {
+      double2 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const long long e = e0 + (long long)u * PT + tid;
+        if (e < NN) {
+          const int j = (int)(e / N), i = (int)(e - (long long)j * N);
+          const int pr = i / nv, vr = i - pr * nv, pc = j / nv, vc = j - pc * nv;
+          v[u] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const long long e = e0 + (long long)u * PT + tid;
+        if (e < NN) A[e] = make_float2((float)v[u].x, (float)v[u].y);
+      }
+    }
+  }
+  __syncthreads();
+  const bool singular = panel_lu(A, N, s);
+  // ---- initial solve against the selector: S[(p,nu)][s] = delta_{p s} ----
+  const int ldy = N;
+  float2* y = s.P;
+  double2* ys = reinterpret_cast<double2*>(s.P) + (((size_t)NR * N + 1) / 2 + 1);  // after y, 16-byte aligned
+  double2* colsum = ys + 32 * NR;
+  for (int e = tid; e < NR * N; e += PT) {
+    const int r = e / N, i = e - r * N;
+    y[e] = make_float2((i / nv) == r ? 1.f : 0.f, 0.f);
+  }
+  __syncthreads();
+  panel_solve<NR>(A, N, s.piv, y, ldy);
+  double prev = 0.0;
+  for (int e = tid; e < NR * N; e += PT) {
+    Y[e] = make_double2(y[e].x, y[e].y);
+    prev = fmax(prev, (double)fmaxf(fabsf(y[e].x), fabsf(y[e].y)));
+  }
+  prev = block_max(prev, s.redd);
+  int it = 0;
+  bool converged = false;
+  for (; it < max_iter; ++it) {
+    structured_residual_permuted<NR>(src, wi.ch, wi.q, wi.w, N, nv, Y, Rb, nullptr, colsum, ys);
+    for (int e = tid; e < NR * N; e += PT) y[e] = make_float2((float)Rb[e].x, (float)Rb[e].y);
+    __syncthreads();
+    panel_solve<NR>(A, N, s.piv, y, ldy);
+    double dmax = 0.0, ymax = 0.0;
+    for (int e = tid; e < NR * N; e += PT) {
+      const double2 d = make_double2(y[e].x, y[e].y);
+      const double2 v = cadd(Y[e], d);
+      Y[e] = v;
+      dmax = fmax(dmax, fmax(fabs(d.x), fabs(d.y)));
+      ymax = fmax(ymax, fmax(fabs(v.x), fabs(v.y)));
+    }
+    dmax = block_max(dmax, s.redd);
+    ymax = block_max(ymax, s.redd);
+    if (isnan(dmax) || refine_converged(dmax, ymax, prev, tol)) {  // NaN is flagged below
+      converged = !isnan(dmax);
+      ++it;
+      break;
+    }
+    prev = dmax;
+  }
+  if (tid == 0) s.misc[1] = 0;
+  __syncthreads();
+  bool bad = false;
+  for (int e = tid; e < N * NR; e += PT) {
+    const int i = e / NR, r = e - i * NR;
+    double2 v = Y[(size_t)r * N + i];
+    v.x = v.x / beta;
+    v.y = v.y / beta;
+    if (!cfinite(v)) bad = true;
+    o[e] = v;
+  }
+  if (bad) atomicOr(&s.misc[1], DGA_ITEM_NONFINITE);
+  __syncthreads();
+  const int st = (singular ? DGA_ITEM_SINGULAR : 0) | s.misc[1] | (converged ? 0 : DGA_ITEM_NOCONVERGE);
+  *iters = it;
+  __syncthreads();
+  return st;
+}
+
+template <int NR>
+__global__ void __launch_bounds__(PT, 1)
+    bse_panel_mixed_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int nv, int W,
+                           int Q, double beta, int max_iter, double tol, double2* __restrict__ out,
+                           int* __restrict__ status, int* __restrict__ iters, unsigned char* __restrict__ scratch,
+                           size_t slot_bytes) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PanelSmem s(smem_raw, N);
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const WorkItem wi = work[item];
+    double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * NR;
+    int it = 0;
+    const int st = solve_item_panel<NR>(src, wi, N, nv, beta, max_iter, tol, o, slot, s, &it);
+    if (threadIdx.x == 0) {
+      if (status) status[item] = st;
+      if (iters) iters[item] = it;
+    }
+  }
+}
+
+// Heterogeneous batch (requests of one orbital count): see bse_multi_kernel in bse.cu.
+template <int NR>
+__global__ void __launch_bounds__(PT, 1)
+    bse_panel_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work,
+                           int n_items, int n_max, int max_iter, double tol, int* __restrict__ status,
+                           int* __restrict__ iters, unsigned char* __restrict__ scratch, size_t slot_bytes) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PanelSmem s(smem_raw, n_max);
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const MultiItem mi = work[item];
+    const dga_bse_problem d = probs[mi.prob];
+    StructuredSource src;
+    src.gamma_cm = (const double2*)d.gamma_cm;
+    src.chi0_inv = (const double2*)d.chi0_inv;
+    src.uv = (const double2*)d.uv;
+    src.n2 = NR;
+    src.nv = 2 * d.niv;
+    src.W = d.niw_half;
+    src.Q = d.n_q;
+    src.inv_beta2 = d.inv_beta2;
+    const int N = NR * src.nv;
+    const WorkItem wi{mi.ch, mi.q, mi.w};
+    double2* o = (double2*)d.out + (((size_t)wi.ch * src.Q + wi.q) * src.W + wi.w) * (size_t)N * NR;
+    int it = 0;
+    const int st = solve_item_panel<NR>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, &it);
+    if (threadIdx.x == 0) {
+      status[item] = st;
+      if (iters) iters[item] = it;
+    }
+  }
+}
+
+}  // namespace dga
+
+using namespace dga;
+
+// ----------------------------------------------------------------------------------------------
+// Host side (called from bse.cu)
+// ----------------------------------------------------------------------------------------------
+bool dga_panel_supported(int N, int n2) {
+#ifdef DGA_DISABLE_PANEL
+  return false;
+#else
+  return (n2 == 1 || n2 == 4 || n2 == 9 || n2 == 16) && N > 0 && panel_smem_bytes(N) <= (size_t)P_MAX_SMEM;
+#endif
+}
+
+size_t dga_panel_slot_bytes(int N, int n2) { return (panel_slot_bytes(N, n2) + 255) & ~(size_t)255; }
+
+template <typename K>
+static int panel_grid_for(K kernel, int n_items, size_t smem) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PT, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int g = sms * per_sm;
+  return n_items < g ? n_items : g;
+}
+
+int dga_panel_grid(int n2, int N, int n_items) {
+  const size_t smem = panel_smem_bytes(N);
+  switch (n2) {
+    case 1: return panel_grid_for(bse_panel_mixed_kernel<1>, n_items, smem);
+    case 4: return panel_grid_for(bse_panel_mixed_kernel<4>, n_items, smem);
+    case 9: return panel_grid_for(bse_panel_mixed_kernel<9>, n_items, smem);
+    default: return panel_grid_for(bse_panel_mixed_kernel<16>, n_items, smem);
+  }
+}
+
+int dga_panel_batch_grid(int n2, int n_max, int n_items) {
+  const size_t smem = panel_smem_bytes(n_max);
+  switch (n2) {
+    case 1: return panel_grid_for(bse_panel_multi_kernel<1>, n_items, smem);
+    case 4: return panel_grid_for(bse_panel_multi_kernel<4>, n_items, smem);
+    case 9: return panel_grid_for(bse_panel_multi_kernel<9>, n_items, smem);
+    default: return panel_grid_for(bse_panel_multi_kernel<16>, n_items, smem);
+  }
+}
+
+cudaError_t dga_panel_launch(int grid, const StructuredSource& src, const WorkItem* work, int n_items, int N, int n2,
+                             int nv, int W, int Q, double beta, int max_iter, double tol, double2* out, int* status,
+                             int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream) {
+  const size_t smem = panel_smem_bytes(N);
+#define DGA_PANEL_CASE(R)                                                                                        \
+  case R:                                                                                                        \
+    bse_panel_mixed_kernel<R><<<grid, PT, smem, stream>>>(src, work, n_items, N, nv, W, Q, beta, max_iter, tol, \
+                                                          out, status, iters, scratch, slot_bytes);             \
+    break;
+  switch (n2) {
+    DGA_PANEL_CASE(1)
+    DGA_PANEL_CASE(4)
+    DGA_PANEL_CASE(9)
+    DGA_PANEL_CASE(16)
+  }
+#undef DGA_PANEL_CASE
+  return cudaGetLastError();
+}
+
+cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
+                                   int n_max, int max_iter, double tol, int* status, int* iters,
+                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream) {
+  const size_t smem = panel_smem_bytes(n_max);
+#define DGA_PANEL_CASE(R)                                                                                       \
+  case R:                                                                                                       \
+    bse_panel_multi_kernel<R><<<grid, PT, smem, stream>>>(probs, work, n_items, n_max, max_iter, tol, status, \
+                                                          iters, scratch, slot_bytes);                         \
+    break;
+  switch (n2) {
+    DGA_PANEL_CASE(1)
+    DGA_PANEL_CASE(4)
+    DGA_PANEL_CASE(9)
+    DGA_PANEL_CASE(16)
+  }
+#undef DGA_PANEL_CASE
+  return cudaGetLastError();
+}

@@ -81,9 +81,11 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
 
 /* Mixed-precision ladder BSE (same inputs and outputs as dga_bse_solve_sum_c128): complex64 LU with FP32
  * trailing updates, then FP64 iterative refinement -- residuals r = S - A Y with A formed in FP64 from Gamma_r,
- * chi0^-1 and U_r + V_r^q -- until max|correction| <= tol max|Y| or max_iter corrections; items that do not
- * converge are flagged DGA_ITEM_NOCONVERGE.  Replaces the same upstream functions as dga_bse_solve_sum_c128.
- * iters: optional per-item number of corrections. */
+ * chi0^-1 and U_r + V_r^q -- until the correction, or the error left after it estimated from the observed
+ * contraction rho = |d_k|/|d_(k-1)| as |d_k| rho/(1-rho), is at most tol max|Y|, or max_iter corrections; items
+ * that do not converge are flagged DGA_ITEM_NOCONVERGE.  Items with N up to about 790 run the shared-memory-panel
+ * kernel (one 512-thread CTA per SM), larger ones the 128-thread kernel.  Replaces the same upstream functions
+ * as dga_bse_solve_sum_c128.  iters: optional per-item number of corrections. */
 size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items);
 int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
                                  const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
