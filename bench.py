@@ -238,61 +238,97 @@ def run_reference(args, rank: int, world: int):
 
 
 def time_pass(lp, args, world: int, local: int, sample_clocks: bool):
-    """Warm-up, then K timed device passes (CUDA events on the launching stream, max over ranks)."""
+    """Warm-up, then K timed device passes replayed from one CUDA graph (CUDA events on the launching stream,
+    max over ranks); one more eager pass times the BSE launch alone for the roofline."""
     import torch
 
     stream = torch.cuda.current_stream()
-
-    # warm-up
     for _ in range(args.warmup):
         lp.run()
     torch.cuda.synchronize()
     status = int(lp.bse_status.abs().sum().item()) + int(lp.status.abs().sum().item())
     sh = lp.sh
 
-    # timed region: device-resident inputs, K passes; the BSE launch is timed separately on the same stream
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # BSE launch time (eager pass, events around the BSE on the same stream)
+    bse_ms = []
+    for _ in range(2):
+        lp.pre_bse()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        lp.bse()
+        b.record(stream)
+        lp.post_bse()
+        b.synchronize()
+        bse_ms.append(a.elapsed_time(b))
+
+    # timed region: device-resident inputs, K graph replays of the whole pass
+    lp.capture()
+    for _ in range(max(1, args.warmup)):
+        lp.replay()
     barrier(world)
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local if sample_clocks else -1)
     with clocks:
         start.record(stream)
-        for k in range(args.steps):
-            lp.status.zero_()
-            lp.bubble()
-            lp.dc_kernel()
-            lp.chi0_prep()
-            ev[k][0].record(stream)
-            lp.bse()
-            ev[k][1].record(stream)
-            lp.chi_phys_stage()
-            chi_r = lp.lambda_stage()
-            lp.kernel_stage(chi_r)
-            lp.sigma_stage()
+        for _ in range(args.steps):
+            lp.replay()
         end.record(stream)
         end.synchronize()
     torch.cuda.synchronize()
     barrier(world)
-    t_local = start.elapsed_time(end) / 1e3
-    t = max_over_ranks(t_local, world)
-    bse_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    t = max_over_ranks(start.elapsed_time(end) / 1e3, world)
     value = world * sh.n_solves * args.steps / t
-    return {"t": t, "value": value, "bse_ms": bse_ms, "status": status, "clocks": clocks}
+    return {"t": t, "value": value, "bse_ms": float(min(bse_ms)), "status": status, "clocks": clocks}
+
+
+# DRAM bytes per BSE item of each kernel, from `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` of a
+# single-wave launch of the same kernel on the 3-orbital case with the full N = 720 (4x4 grid, niw = 10,
+# 132 items); traffic grows in proportion to the items, so a full launch's traffic is items x this.
+DRAM_BYTES_PER_ITEM = {
+    "bse_solve_sum_fp64_kernel": 22.89e9 / 132,
+    "bse_panel_mixed_kernel": (5.670e9 + 4.917e9) / 132,
+    "bse_solve_sum_mixed_kernel": 11.79e9 / 132,
+}
+
+
+def kernel_name(lp) -> str:
+    if lp.precision == "fp64":
+        return "bse_solve_sum_fp64_kernel"
+    kernel = lp.tuning.kernel if lp.tuning is not None else 0
+    if kernel == 2:
+        return "bse_solve_sum_mixed_kernel"
+    return "bse_panel_mixed_kernel"
+
+
+def serving_leg(precision: str, n_requests: int) -> dict:
+    """Continuous-batching server on a seeded Poisson mix of requests (1-3 orbitals, several grids and boxes,
+    beta ~ U[5,30], U ~ U[2,10]): p50 / p99 latency from arrival to Sigma on the host."""
+    from dgamore_b200.serving import LadderServer, serving_workload
+
+    reqs = serving_workload(n_requests, rate_per_s=20.0, seed=5, precision=precision)
+    srv = LadderServer(hbm_budget=40 << 30, scratch_bytes=2 << 30, items_per_request=256)
+    stats = srv.serve(reqs, realtime=True)
+    out = stats.summary()
+    out["bse_status_nonzero"] = int(sum(int(np.abs(r.bse_status).sum()) for r in stats.completed))
+    return out
 
 
 def run_ours(args, rank: int, world: int, local: int):
     import torch
 
-    from dgamore_b200 import synthetic
+    from dgamore_b200 import autotune, synthetic
     from dgamore_b200.pipeline import LadderPass
 
     cfg = synthetic.CONFIGS[args.config]
     inp = synthetic.make_inputs(cfg)
     stream = torch.cuda.current_stream()
+    cache = os.path.join(HERE, "_build", "tuning.json") if args.tune_cache else None
 
     # FP64 drop-in form first: the reference point of the mixed form and of its Sigma error
     lp64 = LadderPass(inp, keep_intermediates=False, precision="fp64")
+    lp64.pre_bse()
+    tune64 = autotune.tune_bse(lp64, cache_path=cache)
     r64 = time_pass(lp64, args, world, local, sample_clocks=False)
     sigma64 = lp64.sigma.clone()
     del lp64
@@ -300,15 +336,17 @@ def run_ours(args, rank: int, world: int, local: int):
 
     lp = LadderPass(inp, keep_intermediates=False, precision=args.precision)
     sh = lp.sh
+    lp.pre_bse()
+    tune = autotune.tune_bse(lp, cache_path=cache)
     res = time_pass(lp, args, world, local, sample_clocks=True)
     t, value, bse_ms, status, clocks = res["t"], res["value"], res["bse_ms"], res["status"], res["clocks"]
     sig_err = float((lp.sigma - sigma64).abs().max().item() / sigma64.abs().max().item())
     iters = lp.bse_iters.cpu().numpy() if args.precision == "mixed" else None
+    kname = kernel_name(lp)
     kernels_per_pass = (14 if lp.do_lambda else 13) + (1 if args.precision == "mixed" else 0)
 
-    # end-to-end through the public API: host G(k) -> device pass -> host Sigma
-    for _ in range(1):
-        lp.run_e2e()
+    # end to end through the public API: host G(k) -> device pass (graph replay) -> host Sigma
+    lp.run_e2e()
     barrier(world)
     e_s, e_e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_s.record(stream)
@@ -318,12 +356,19 @@ def run_ours(args, rank: int, world: int, local: int):
     e_e.synchronize()
     t_e2e = max_over_ranks(e_s.elapsed_time(e_e) / 1e3, world)
     e2e_value = world * sh.n_solves * args.steps / t_e2e
+    del lp
+    torch.cuda.empty_cache()
 
     fp64_peak = gemm_peak_tflops("float64") if rank == 0 else None
     fp32_peak = gemm_peak_tflops("float32") if rank == 0 else None
     peak = fp32_peak if args.precision == "mixed" else fp64_peak
     flops_launch = sh.n_solves * f_solve(sh.N, sh.n2)
     achieved = flops_launch / (bse_ms / 1e3) / 1e12
+    per_item = DRAM_BYTES_PER_ITEM.get(kname)
+    serving = {}
+    if args.serve_requests > 0 and rank == 0:
+        for prec in ("fp64", "mixed"):
+            serving[prec] = serving_leg(prec, args.serve_requests)
     line = {
         "metric": "(q,w) ladder solves/s",
         "value": value,
@@ -341,16 +386,18 @@ def run_ours(args, rank: int, world: int, local: int):
             "workload": f"{args.config}: {cfg.n_bands}-orbital {cfg.nk[0]}x{cfg.nk[1]} square lattice, "
             f"niv=niw={cfg.niv}, N={sh.N}, {sh.n_q} irreducible q, {sh.n_solves} solves per pass",
             "precision": "mixed (FP32 LU, FP64 refinement)" if args.precision == "mixed" else "fp64 drop-in",
-            "step": "one full nonlocal pass (bubble, dc kernel, chi0^-1, BSE dens+magn, chi_phys, lambda, kernel, Sigma)",
-            "l2": "inputs larger than L2 (Gamma_r alone is %.0f MB)" % (lp.gamma_cm.numel() * 16 / 1e6),
+            "step": "one full nonlocal pass (bubble, dc kernel, chi0^-1, BSE dens+magn, chi_phys, lambda, kernel, "
+            "Sigma) replayed from one CUDA graph",
+            "l2": "inputs larger than L2 (Gamma_r alone is %.0f MB)" % (2 * sh.W * sh.N * sh.N * 16 / 1e6),
             "parallelism": f"{world} independent replica(s)",
+            "bse_launch": {"kernel": kname, "tuning": list(tune.choice), "tuning_times_ms": tune.times_ms},
         },
         "gpu_launches": kernels_per_pass * args.steps,
         "e2e": {
             "value": e2e_value,
             "unit": "(q,w) ladder solves/s",
-            "h2d_bytes_per_step": lp.h2d_bytes,
-            "d2h_bytes_per_step": lp.d2h_bytes,
+            "h2d_bytes_per_step": inp["g_k"].size * 16,
+            "d2h_bytes_per_step": sh.nk_tot * sh.n2 * 2 * sh.niv * 16,
         },
         "fp64_dropin": {
             "value": r64["value"],
@@ -358,13 +405,14 @@ def run_ours(args, rank: int, world: int, local: int):
             "bse_ms_per_launch": r64["bse_ms"],
             "bse_tflops": flops_launch / (r64["bse_ms"] / 1e3) / 1e12,
             "bse_frac_of_fp64_peak": (flops_launch / (r64["bse_ms"] / 1e3) / 1e12 / fp64_peak) if fp64_peak else None,
+            "tuning": list(tune64.choice),
         },
         "mixed_vs_fp64": value / r64["value"],
         "sigma_rel_err_vs_fp64": sig_err,
         "refinement_iters": None if iters is None else {"mean": float(iters.mean()), "max": int(iters.max())},
         "roofline": {
             "bound": "tensor",
-            "kernel": "bse_solve_sum_mixed_kernel" if args.precision == "mixed" else "bse_solve_sum_fp64_kernel",
+            "kernel": kname,
             "achieved": achieved,
             "peak": peak,
             "unit": "TFLOP/s",
@@ -373,10 +421,13 @@ def run_ours(args, rank: int, world: int, local: int):
             + " measured in this run (MEASURED_PEAKS.json has bf16 and HBM only)",
             "flops_per_launch": flops_launch,
             "bse_ms_per_launch": bse_ms,
-            "traffic": None,
+            "traffic": None if per_item is None else per_item * sh.n_solves,
+            "traffic_note": "ncu DRAM bytes per item of a 132-item launch of the same kernel, times the items",
+            "algorithmic_bytes": 2 * sh.W * sh.N * sh.N * 16 + sh.n_solves * (sh.nv * sh.n2 * sh.n2 + sh.N * sh.n2) * 16,
         },
         "bse_status_nonzero": status,
         "clocks": clocks.summary(),
+        "serving": serving,
     }
     if rank == 0:
         line["cpu_baseline"] = cpu_baseline_sample(inp, args.cpu_items)
@@ -393,6 +444,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-items", type=int, default=4)
     ap.add_argument("--ref-items", type=int, default=3)
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--tune-cache", action="store_true", help="keep autotuner choices in _build/tuning.json")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     try:

@@ -48,7 +48,15 @@ SIGNATURES = {
     "dga_eli_matvec_c128": (I, [VP, VP, VP, I, I, I, I, I, VP, VP, D, D, VP, VP, SZ, VP]),
     "dga_bse_batch_scratch_bytes": (SZ, [VP, I, I, I]),
     "dga_bse_solve_sum_batch_c128": (I, [VP, VP, I, PI, I, I, I, D, PI, PI, VP, SZ, VP]),
+    "dga_bse_tuned_scratch_bytes": (SZ, [I, I, I, I, VP]),
+    "dga_bse_solve_sum_tuned_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, I, I, D, VP, PI, PI, VP, VP, SZ, VP]),
 }
+
+
+class BseTuning(_c.Structure):
+    """``dga_bse_tuning`` of include/dga_b200.h (kernel choice and CTAs per SM of the BSE solvers)."""
+
+    _fields_ = [("kernel", I), ("ctas_per_sm", I)]
 
 
 class BseProblem(_c.Structure):

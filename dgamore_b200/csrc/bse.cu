@@ -1349,6 +1349,130 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------------
+// Tuned entry: the same solves with an explicit kernel choice and CTAs per SM (the autotuner's knobs)
+// ------------------------------------------------------------------------------------------------
+static int sm_count() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+// 1 = panel kernel, 2 = 128-thread kernel, -1 = the requested kernel cannot run this size
+static int tuned_kernel(int mixed, int N, int n2, const dga_bse_tuning* t) {
+  const int k = t ? t->kernel : 0;
+  if (k < 0 || k > 2) return -1;
+  if (!mixed) return k == 1 ? -1 : 2;
+  if (k == 0) return dga_panel_supported(N, n2) ? 1 : 2;
+  if (k == 1 && !dga_panel_supported(N, n2)) return -1;
+  return k;
+}
+
+static int tuned_grid(int kernel, int mixed, int N, int n2, int n_items, const dga_bse_tuning* t, size_t* slot,
+                      size_t* smem) {
+  if (kernel == 1) {
+    *slot = dga_panel_slot_bytes(N, n2);
+    *smem = 0;
+    return dga_panel_grid(n2, N, n_items);
+  }
+  int grid;
+  if (mixed) {
+    *smem = mixed_smem_bytes(N, n2);
+    *slot = mixed_slot_bytes(N, n2);
+    grid = mixed_grid(n_items, *smem);
+  } else {
+    *smem = bse_smem_bytes(N);
+    *slot = ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
+    grid = bse_grid(n_items, *smem);
+  }
+  const int cps = t ? t->ctas_per_sm : 0;
+  if (cps > 0) {
+    const int cap = sm_count() * cps;
+    if (grid > cap) grid = cap;
+  }
+  return grid;
+}
+
+extern "C" {
+
+size_t dga_bse_tuned_scratch_bytes(int N, int n2, int n_items, int mixed, const dga_bse_tuning* t) {
+  if (N <= 0 || !supported_rhs(n2) || n_items <= 0 || N > BSE_MAX_N) return 0;
+  const int kernel = tuned_kernel(mixed, N, n2, t);
+  if (kernel < 0) return 0;
+  size_t slot = 0, smem = 0;
+  return (size_t)tuned_grid(kernel, mixed, N, n2, n_items, t, &slot, &smem) * slot;
+}
+
+int dga_bse_solve_sum_tuned_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                                 const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
+                                 int n_items, int mixed, int max_iter, double tol, void* out, int* status, int* iters,
+                                 const dga_bse_tuning* t, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch <= 0 || n_items <= 0 ||
+      N > BSE_MAX_N || max_iter < 0 || (mixed != 0 && mixed != 1)) {
+    dga_set_error("dga_bse_solve_sum_tuned_c128: invalid sizes (n_orb=%d niv=%d niw_half=%d n_q=%d items=%d)", n_orb,
+                  niv, niw_half, n_q, n_items);
+    return DGA_ERR_ARG;
+  }
+  if (!gamma_cm || !chi0_inv || !uv || !work || !out || !scratch || (mixed && !status)) {
+    dga_set_error("dga_bse_solve_sum_tuned_c128: null pointer argument");
+    return DGA_ERR_ARG;
+  }
+  const int kernel = tuned_kernel(mixed, N, n2, t);
+  if (kernel < 0) {
+    dga_set_error("dga_bse_solve_sum_tuned_c128: kernel %d cannot run N=%d in this precision", t ? t->kernel : 0, N);
+    return DGA_ERR_ARG;
+  }
+  size_t slot = 0, smem = 0;
+  const int grid = tuned_grid(kernel, mixed, N, n2, n_items, t, &slot, &smem);
+  if (scratch_bytes < (size_t)grid * slot) {
+    dga_set_error("dga_bse_solve_sum_tuned_c128: scratch too small (%zu < %zu)", scratch_bytes, (size_t)grid * slot);
+    return DGA_ERR_SCRATCH;
+  }
+  StructuredSource src;
+  src.gamma_cm = (const double2*)gamma_cm;
+  src.chi0_inv = (const double2*)chi0_inv;
+  src.uv = (const double2*)uv;
+  src.n2 = n2;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  src.inv_beta2 = inv_beta2;
+  cudaError_t err;
+  if (kernel == 1) {
+    err = dga_panel_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, max_iter, tol,
+                           (double2*)out, status, iters, (unsigned char*)scratch, slot, stream);
+  } else if (mixed) {
+#define DGA_TUNED_MIXED_CASE(NRV)                                                                                    \
+  case NRV:                                                                                                          \
+    cudaFuncSetAttribute(bse_solve_sum_mixed_kernel<NRV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+    bse_solve_sum_mixed_kernel<NRV><<<grid, BSE_THREADS, smem, stream>>>(                                            \
+        src, (const WorkItem*)work, n_items, N, NRV, nv, niw_half, n_q, beta, max_iter, tol, (double2*)out, status,  \
+        iters, (unsigned char*)scratch, slot);                                                                       \
+    break;
+    switch (n2) {
+      DGA_TUNED_MIXED_CASE(1)
+      DGA_TUNED_MIXED_CASE(4)
+      DGA_TUNED_MIXED_CASE(9)
+      DGA_TUNED_MIXED_CASE(16)
+    }
+#undef DGA_TUNED_MIXED_CASE
+    err = cudaGetLastError();
+  } else {
+    launch_fp64(n2, grid, smem, stream, src, (const WorkItem*)work, n_items, N, nv, niw_half, n_q, beta,
+                (double2*)out, status, (double2*)scratch, slot / sizeof(double2), 0);
+    err = cudaGetLastError();
+  }
+  if (err != cudaSuccess) {
+    dga_set_error("dga_bse_solve_sum_tuned_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
 // Allocation-free variant of dga_bse_solve_sum_c128.
 //
 // Some callers of this library cannot call cudaMalloc: a host program that binds only this C ABI and has no

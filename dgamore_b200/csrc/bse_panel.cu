@@ -33,6 +33,10 @@ constexpr int PNB = 32;       // panel width
 constexpr int PTM = 128;      // trailing tile rows
 constexpr int PTN = 64;       // trailing strip columns
 constexpr int P_MAX_SMEM = 232448;  // 227 KB opt-in shared memory per block on sm_100
+#ifndef DGA_PANEL_TILE_UNROLL
+#define DGA_PANEL_TILE_UNROLL 8
+#endif
+constexpr int P_TILE_UNROLL = DGA_PANEL_TILE_UNROLL;  // unroll of the trailing tiles' k loop
 
 // ----------------------------------------------------------------------------------------------
 // Shared-memory layout (ldp = leading dimension of the panel = the largest N the launch serves)
@@ -339,7 +343,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s) {
         const bool r0ok = full || rbase < N, r1ok = full || rbase + 64 < N;
         const float2* lp0 = s.P + (r0ok ? rbase - k0 : 0);
         const float2* lp1 = s.P + (r1ok ? rbase + 64 - k0 : 0);
-#pragma unroll 4
+#pragma unroll P_TILE_UNROLL
         for (int k = 0; k < nb; ++k) {
           float4 l0 = *reinterpret_cast<const float4*>(lp0 + (size_t)k * s.ldp);
           float4 l1 = *reinterpret_cast<const float4*>(lp1 + (size_t)k * s.ldp);

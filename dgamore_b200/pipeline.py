@@ -245,6 +245,7 @@ class LadderPass:
         self.X = torch.empty((2, Q, W, N, n2), dtype=C128, device=dev)
         self.bse_status = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
         self.own_bse_scratch = bool(own_bse_scratch)
+        self.tuning = None
         if not self.own_bse_scratch:
             # the BSE runs in a batch launch (serving.solve_bse_batch) that brings its own scratch
             self.bse_scratch = self.mixed_scratch = None
@@ -304,10 +305,42 @@ class LadderPass:
         call("dga_dc_kernel_c128", _p(self.chi0), _p(self.u_perm), _p(self.fdc), sh.n_orb, sh.niv, sh.niv_shell, sh.W,
              sh.n_q, _p(self.k_dc), _p(self.dc_scratch), self.dc_scratch.numel() * 16, _s())
 
+    def set_tuning(self, choice) -> None:
+        """Uses the launch choice (kernel, ctas_per_sm) of dga_bse_tuning for this pass's BSE (see autotune.py)."""
+        from ._lib import BseTuning
+
+        t = BseTuning(kernel=int(choice[0]), ctas_per_sm=int(choice[1]))
+        sh = self.sh
+        mixed = 1 if self.precision == "mixed" else 0
+        nbytes = int(lib().dga_bse_tuned_scratch_bytes(sh.N, sh.n2, self.n_items, mixed, ctypes.byref(t)))
+        if nbytes == 0:
+            raise ValueError(f"tuning {tuple(choice)} cannot run N={sh.N} in {self.precision}")
+        self.tuning = t
+        self.mixed_scratch = None
+        if mixed:
+            self.tuned_scratch = torch.empty(nbytes // 16 + 1, dtype=C128, device=self.dev)
+        else:
+            # the FP64 form reuses its own scratch when it is large enough
+            if self.bse_scratch is None or self.bse_scratch.numel() * 16 < nbytes:
+                self.bse_scratch = torch.empty(nbytes // 16 + 1, dtype=C128, device=self.dev)
+            self.tuned_scratch = self.bse_scratch
+
     def bse(self):
         sh = self.sh
         if not self.own_bse_scratch:
             raise RuntimeError("this pass was built without BSE scratch: run its BSE through serving.solve_bse_batch")
+        if self.tuning is not None:
+            mixed = 1 if self.precision == "mixed" else 0
+            call("dga_bse_solve_sum_tuned_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
+                 _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, mixed,
+                 self.refine_max_iter, self.refine_tol, _p(self.X), _p(self.bse_status), _p(self.bse_iters),
+                 ctypes.byref(self.tuning), _p(self.tuned_scratch), self.tuned_scratch.numel() * 16, _s())
+            if mixed:
+                call("dga_bse_resolve_fp64_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
+                     _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, _p(self.X),
+                     _p(self.bse_status), self.resolve_grid, _p(self.bse_scratch), self.bse_scratch.numel() * 16,
+                     _s())
+            return
         if self.precision == "mixed":
             call("dga_bse_solve_sum_mixed_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
                  _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, self.refine_max_iter,
@@ -370,10 +403,31 @@ class LadderPass:
         self.bse()
         return self.post_bse()
 
+    def capture(self) -> "torch.cuda.CUDAGraph":
+        """Captures one device pass into a CUDA graph (``replay`` then re-runs all its kernels with one launch).
+
+        Runs the pass once eagerly first, so that kernel attributes and module loading happen outside the
+        capture.  The graph reads and writes this pass's own buffers: refresh ``g_k`` in place between replays."""
+        self.run()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            self.run()
+        torch.cuda.synchronize()
+        self.graph = g
+        return g
+
+    def replay(self) -> torch.Tensor:
+        self.graph.replay()
+        return self.sigma
+
     def run_e2e(self) -> np.ndarray:
         """Host G(k) in, host Sigma(k, nu) out: H2D copy, one pass, D2H copy (synchronises)."""
         self.g_k.copy_(self.g_k_host, non_blocking=True)
-        self.run()
+        if getattr(self, "graph", None) is not None:
+            self.graph.replay()
+        else:
+            self.run()
         self.sigma_host.copy_(self.sigma, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return self.sigma_host.numpy()

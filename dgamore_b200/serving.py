@@ -323,3 +323,30 @@ def poisson_arrivals(n: int, rate_per_s: float, seed: int = 0) -> np.ndarray:
     gaps = rng.exponential(1.0 / rate_per_s, size=n)
     gaps[0] = 0.0
     return np.cumsum(gaps)
+
+
+# (n_orb, nk, niv = niw) shapes of the serving mix: orbitals 1-3, small and mid momentum grids and boxes
+SERVE_SHAPES = ((1, 16, 10), (1, 16, 20), (2, 8, 10), (2, 16, 10), (3, 8, 8), (3, 8, 12))
+
+
+def serving_workload(n_requests: int = 24, rate_per_s: float = 20.0, seed: int = 5, precision: str = "fp64",
+                     shapes=SERVE_SHAPES) -> list[Request]:
+    """Seeded serving mix: each request draws a shape (orbitals, grid, frequency box), a temperature
+    beta ~ U[5, 30] and an interaction U ~ U[2, 10] and gets its own synthetic inputs; arrivals are Poisson."""
+    import dataclasses
+
+    from . import synthetic
+
+    rng = np.random.default_rng(seed)
+    arrivals = poisson_arrivals(n_requests, rate_per_s, seed=seed)
+    reqs = []
+    for i in range(n_requests):
+        n_orb, nk, niv = shapes[int(rng.integers(len(shapes)))]
+        beta = float(rng.uniform(5.0, 30.0))
+        u = float(rng.uniform(2.0, 10.0))
+        base = {1: "c1", 2: "c4_bilayer", 3: "c3"}[n_orb]
+        cfg = dataclasses.replace(synthetic.CONFIGS[base], name=f"serve{i}", nk=(nk, nk, 1), niw=niv, niv=niv,
+                                  niv_shell=0, beta=beta, u=u, seed=1000 + i)
+        reqs.append(Request(synthetic.make_inputs(cfg), arrival=float(arrivals[i]), precision=precision))
+    return reqs
+

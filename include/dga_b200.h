@@ -99,6 +99,25 @@ int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_c
                               void* out, int* status, int grid_limit, void* scratch, size_t scratch_bytes,
                               dga_stream_t stream);
 
+/* Launch choices of the BSE solvers, the search space of the autotuner (dgamore_b200/autotune.py); no
+ * counterpart in the upstream.  kernel: 0 = default (mixed form: the shared-memory-panel kernel when N fits,
+ * else the 128-thread kernel; FP64: the 128-thread kernel), 1 = shared-memory-panel kernel (mixed form only,
+ * N up to about 790), 2 = 128-thread kernel; ctas_per_sm: CTAs per SM of the 128-thread kernel (0 = all that
+ * fit).  Both choices change the speed only: every choice computes the same solves. */
+typedef struct {
+  int kernel;
+  int ctas_per_sm;
+} dga_bse_tuning;
+
+/* dga_bse_solve_sum_c128 (mixed = 0) or dga_bse_solve_sum_mixed_c128 (mixed = 1) with an explicit tuning;
+ * status is required in the mixed form.  Scratch: dga_bse_tuned_scratch_bytes (0 if the tuning cannot run). */
+size_t dga_bse_tuned_scratch_bytes(int N, int n2, int n_items, int mixed, const dga_bse_tuning* tuning);
+int dga_bse_solve_sum_tuned_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                                 const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
+                                 int n_items, int mixed, int max_iter, double tol, void* out, int* status, int* iters,
+                                 const dga_bse_tuning* tuning, void* scratch, size_t scratch_bytes,
+                                 dga_stream_t stream);
+
 /* One request of a heterogeneous BSE batch: the inputs and output of one dga_bse_solve_sum_c128 problem
  * (both channels; layouts as there) with its own frequency box, q set and beta. */
 typedef struct {

@@ -1,0 +1,75 @@
+"""The BSE launch choices of the autotuner compute the same solves, and the tuner installs a working choice.
+
+FP64: every choice of the 128-thread kernel (any CTAs per SM) gives bitwise the default X.  Mixed: every
+kernel choice converges and matches the upstream FP64 BSE to 1e-11 relative.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = ("t1b", "t3", "t4e")
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_choices_are_bitwise_equal(name):
+    from dgamore_b200.autotune import CANDIDATES
+    from dgamore_b200.pipeline import LadderPass
+
+    inp, _ = load_golden(name)
+    lp = LadderPass(inp, keep_intermediates=False)
+    lp.pre_bse()
+    lp.bse()
+    torch.cuda.synchronize()
+    x0 = lp.X.cpu().numpy()
+    for choice in CANDIDATES["fp64"]:
+        lp.set_tuning(choice)
+        lp.X.zero_()
+        lp.bse()
+        torch.cuda.synchronize()
+        assert np.array_equal(lp.X.cpu().numpy(), x0), choice
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_choices_match_upstream(name):
+    from dgamore_b200.autotune import CANDIDATES, scratch_bytes
+    from dgamore_b200.pipeline import LadderPass
+
+    inp, ref = load_golden(name)
+    lp = LadderPass(inp, keep_intermediates=False, precision="mixed")
+    lp.pre_bse()
+    for choice in CANDIDATES["mixed"]:
+        if scratch_bytes(lp, lp.n_items, 1, choice) == 0:
+            continue
+        lp.set_tuning(choice)
+        lp.X.zero_()
+        lp.bse()
+        torch.cuda.synchronize()
+        assert int(lp.bse_status.abs().sum()) == 0, choice
+        for ch, chname in ((0, "dens"), (1, "magn")):
+            assert rel_err(lp.x_ref_layout(ch), ref[f"chi_aux_sum_{chname}"]) < 1e-11, (choice, chname)
+
+
+def test_tuner_picks_and_caches_a_choice(tmp_path):
+    from dgamore_b200 import autotune
+    from dgamore_b200.pipeline import LadderPass
+
+    inp, ref = load_golden("t1b")
+    path = str(tmp_path / "tuning.json")
+    lp = LadderPass(inp, keep_intermediates=False, precision="mixed")
+    lp.pre_bse()
+    res = autotune.tune_bse(lp, cache_path=path, force=True)
+    assert res.choice in [tuple(c) for c in autotune.CANDIDATES["mixed"]]
+    assert res.times_ms
+    lp.run()
+    torch.cuda.synchronize()
+    assert rel_err(lp.sigma.cpu().numpy(), ref["sigma"]) < 1e-8
+    # a second pass of the same shape takes the cached choice without timing
+    lp2 = LadderPass(inp, keep_intermediates=False, precision="mixed")
+    lp2.pre_bse()
+    res2 = autotune.tune_bse(lp2, cache_path=path)
+    assert res2.choice == res.choice and not res2.times_ms

@@ -70,3 +70,15 @@ def test_batch_rejects_mixed_orbital_counts_without_launching():
     rc = lib.dga_bse_solve_sum_batch_c128(one, 1, 1, 1, 10, 0, 0, 0.0, 1, None, 1, 1 << 30, None)
     assert rc == 1 and b"null pointer" in lib.dga_last_error_string()
     assert lib.dga_bse_solve_sum_batch_c128(one, 1, 1, 1, 10, 3, 0, 0.0, 1, None, 1, 1 << 30, None) == 1
+
+
+def test_tuning_struct_and_rejected_choices_without_gpu():
+    assert ctypes.sizeof(_lib.BseTuning) == 8
+    lib = _lib.lib()
+    bad = _lib.BseTuning(kernel=5, ctas_per_sm=0)
+    assert lib.dga_bse_tuned_scratch_bytes(720, 9, 100, 1, ctypes.byref(bad)) == 0
+    panel_fp64 = _lib.BseTuning(kernel=1, ctas_per_sm=0)  # the panel kernel is mixed-precision only
+    assert lib.dga_bse_tuned_scratch_bytes(720, 9, 100, 0, ctypes.byref(panel_fp64)) == 0
+    rc = lib.dga_bse_solve_sum_tuned_c128(3, 40, 41, 153, 2, 20.0, 1 / 400, None, None, None, None, 10, 1, 4, 1e-10,
+                                          None, None, None, ctypes.byref(bad), None, 0, None)
+    assert rc == 1
