@@ -585,3 +585,65 @@ int dga_dc_kernel_c128(const void* chi0, const void* u_perm, const void* fdc, in
 }
 
 }  // extern "C"
+
+// Hartree and Fock terms (nonlocal_sde.get_hartree_fock, dgamore/nonlocal_sde.py:31-69), one thread per (k, a, b):
+//   fock[k][a][b] = -1/Nq sum_q sum_cd (U + V_q)[a][b][c][d] occ_k[k+q][d][c]  (k + q wrapped per axis)
+//   hartree[a][b] = 2 sum_cd (U + V_(q=0))[a][b][c][d] occ[d][c]               (threads of k = 0)
+//   u: [n^4]; v_q: [Nq][n^4] over the full grid in row-major (qx, qy, qz) order; occ: [n][n]; occ_k: [Nk][n][n]
+//   sigma (optional): [Nk][n][n][nv2]; hartree + fock is added to every frequency (nonlocal_sde.py:884)
+__global__ void hartree_fock_kernel(const double2* __restrict__ u, const double2* __restrict__ v_q,
+                                    const double2* __restrict__ occ, const double2* __restrict__ occ_k, int n,
+                                    int nx, int ny, int nz, double2* __restrict__ hartree,
+                                    double2* __restrict__ fock, double2* __restrict__ sigma, int nv2) {
+  const int n2 = n * n, nk = nx * ny * nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nk * n2) return;
+  const int k = t / n2, ab = t - k * n2;
+  const int kx = k / (ny * nz), ky = (k / nz) % ny, kz = k % nz;
+  const double2* uab = u + (size_t)ab * n2;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int qx = 0; qx < nx; ++qx) {
+    const int sx = (kx + qx) % nx;
+    for (int qy = 0; qy < ny; ++qy) {
+      const int sy = (ky + qy) % ny;
+      for (int qz = 0; qz < nz; ++qz) {
+        const int sz = (kz + qz) % nz;
+        const int q = (qx * ny + qy) * nz + qz, kq = (sx * ny + sy) * nz + sz;
+        const double2* vab = v_q + ((size_t)q * n2 + ab) * n2;
+        const double2* o = occ_k + (size_t)kq * n2;
+        for (int c = 0; c < n; ++c)
+          for (int d = 0; d < n; ++d) cfma(acc, cadd(uab[c * n + d], vab[c * n + d]), o[d * n + c]);
+      }
+    }
+  }
+  const double2 f = cscale(acc, -1.0 / nk);
+  fock[(size_t)k * n2 + ab] = f;
+  double2 h = make_double2(0.0, 0.0);
+  const double2* v0 = v_q + (size_t)ab * n2;
+  for (int c = 0; c < n; ++c)
+    for (int d = 0; d < n; ++d) cfma(h, cadd(uab[c * n + d], v0[c * n + d]), occ[d * n + c]);
+  h = cscale(h, 2.0);
+  if (k == 0) hartree[ab] = h;
+  if (sigma) {
+    double2* sg = sigma + ((size_t)k * n2 + ab) * nv2;
+    const double2 hf = cadd(h, f);
+    for (int v = 0; v < nv2; ++v) sg[v] = cadd(sg[v], hf);
+  }
+}
+
+extern "C" int dga_hartree_fock_c128(const void* u, const void* v_q, const void* occ, const void* occ_k, int n_orb,
+                                     int nx, int ny, int nz, void* hartree, void* fock, void* sigma, int nv2,
+                                     cudaStream_t stream) {
+  if (!u || !v_q || !occ || !occ_k || !hartree || !fock || n_orb <= 0 || n_orb > 4 || nx <= 0 || ny <= 0 ||
+      nz <= 0 || (long long)nx * ny * nz > (1LL << 24) || (sigma && nv2 <= 0)) {
+    dga_set_error("dga_hartree_fock_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const int total = nx * ny * nz * n_orb * n_orb;
+  hartree_fock_kernel<<<(total + 127) / 128, 128, 0, stream>>>((const double2*)u, (const double2*)v_q,
+                                                                (const double2*)occ, (const double2*)occ_k, n_orb,
+                                                                nx, ny, nz, (double2*)hartree, (double2*)fock,
+                                                                (double2*)sigma, nv2);
+  return vstatus("dga_hartree_fock_c128");
+}
+

@@ -382,6 +382,26 @@ class LadderPass:
              _p(self.irrk_inv), _p(self.tw_inv), sh.beta, self.sigma_chunks, _p(self.sigma), _p(self.sigma_scratch),
              self.sigma_scratch.numel() * 16, _s())
 
+    def set_occupations(self, occ: np.ndarray, occ_k: np.ndarray, v_q_full: np.ndarray, u: np.ndarray) -> None:
+        """Adds the Hartree-Fock term to Sigma at the end of every pass (nonlocal_sde.py:782-784, 884), from
+        config.sys.occ [n][n], config.sys.occ_k [kx,ky,kz,n,n], V(q) over the full grid [Nq][n][n][n][n] and U."""
+        dev, sh = self.dev, self.sh
+        up = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128)).to(dev)
+        self.hf_u = up(u)
+        self.hf_v = up(np.asarray(v_q_full).reshape(sh.nk_tot, -1))
+        self.hf_occ = up(occ)
+        self.hf_occ_k = up(np.asarray(occ_k).reshape(sh.nk_tot, sh.n_orb, sh.n_orb))
+        self.hartree = torch.empty((sh.n_orb, sh.n_orb), dtype=C128, device=dev)
+        self.fock = torch.empty((sh.nk_tot, sh.n_orb, sh.n_orb), dtype=C128, device=dev)
+
+    def hartree_fock_stage(self):
+        if getattr(self, "hf_occ", None) is None:
+            return
+        sh = self.sh
+        nx, ny, nz = sh.nk
+        call("dga_hartree_fock_c128", _p(self.hf_u), _p(self.hf_v), _p(self.hf_occ), _p(self.hf_occ_k), sh.n_orb,
+             nx, ny, nz, _p(self.hartree), _p(self.fock), _p(self.sigma), 2 * sh.niv, _s())
+
     def pre_bse(self):
         """Stages before the BSE: G(R), bubble, double-counting kernel, chi0^-1 and the nu sums."""
         self.status.zero_()
@@ -395,6 +415,7 @@ class LadderPass:
         chi_r = self.lambda_stage()
         self.kernel_stage(chi_r)
         self.sigma_stage()
+        self.hartree_fock_stage()
         return self.sigma
 
     def run(self):

@@ -340,3 +340,24 @@ def make_inputs(cfg: DgaConfig | str) -> dict:
             out["f_magn_loc"] = f_magn
             out["f_dc"] = 2 * np.einsum("abcd...->cbad...", f_magn)
     return out
+
+
+def make_occupations(cfg: DgaConfig | str, seed_offset: int = 7919) -> tuple[np.ndarray, np.ndarray]:
+    """Seeded occupation matrices for the Hartree-Fock term: occ_k [kx, ky, kz, n, n] Hermitian with eigenvalues
+    in (0, 1) (a smooth band-like k dependence plus a small seeded perturbation) and occ = its k average, the
+    shapes of config.sys.occ_k / config.sys.occ (dgamore/greens_function.py:212-240)."""
+    if isinstance(cfg, str):
+        cfg = CONFIGS[cfg]
+    rng = np.random.default_rng(cfg.seed + seed_offset)
+    nb = cfg.n_bands
+    kx = 2 * np.pi * np.arange(cfg.nk[0]) / cfg.nk[0]
+    ky = 2 * np.pi * np.arange(cfg.nk[1]) / cfg.nk[1]
+    kz = 2 * np.pi * np.arange(cfg.nk[2]) / cfg.nk[2]
+    ek = np.cos(kx)[:, None, None] + np.cos(ky)[None, :, None] + 0.5 * np.cos(kz)[None, None, :]
+    occ_k = np.zeros((*cfg.nk, nb, nb), dtype=np.complex128)
+    for a in range(nb):
+        occ_k[..., a, a] = 0.5 - 0.2 * ek * (1.0 + 0.1 * a)
+    pert = 0.02 * (rng.standard_normal((*cfg.nk, nb, nb)) + 1j * rng.standard_normal((*cfg.nk, nb, nb)))
+    occ_k += 0.5 * (pert + np.conj(np.swapaxes(pert, -1, -2)))
+    occ = occ_k.mean(axis=(0, 1, 2))
+    return occ, occ_k

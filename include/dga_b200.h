@@ -169,6 +169,15 @@ int dga_chi_phys_c128(const void* X, const void* uv, const void* full_sum, const
                       int niv_core, int niw_half, int n_q, int n_ch, double beta, void* out, int* status,
                       dga_stream_t stream);
 
+/* Hartree and Fock terms; replaces nonlocal_sde.get_hartree_fock (dgamore/nonlocal_sde.py:31-69) on the full,
+ * ordered q list of one rank.  u: [n][n][n][n] local U; v_q: [Nq][n][n][n][n] V(q) over the full grid in
+ * row-major (qx, qy, qz) order (Nq = Nk = nx*ny*nz); occ: [n][n] (config.sys.occ); occ_k: [Nk][n][n]
+ * (config.sys.occ_k).  hartree: [n][n] = 2 sum_cd (U+V_(q=0))_abcd occ_dc; fock: [Nk][n][n] =
+ * -1/Nq sum_q sum_cd (U+V_q)_abcd occ_k(k+q)_dc.  sigma (optional, [Nk][n][n][nv2]): hartree + fock is added
+ * to every frequency, as calculate_self_energy_q does before returning (nonlocal_sde.py:884). */
+int dga_hartree_fock_c128(const void* u, const void* v_q, const void* occ, const void* occ_k, int n_orb, int nx,
+                          int ny, int nz, void* hartree, void* fock, void* sigma, int nv2, dga_stream_t stream);
+
 /* Single-band lambda correction (FP64 Newton with delta halving); replaces lambda_correction.find_lambda and
  * perform_single_lambda_correction (dgamore/lambda_correction.py:28-73).  chi: [n_ch][Q][W]; weights: [Q]
  * multiplicities (irrk_count); target: [n_ch] complex; outputs lambda [n_ch], iterations, corrected chi. */

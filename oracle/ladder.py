@@ -403,6 +403,31 @@ def sigma_from_kernel_direct(kernel_full: np.ndarray, g_k: np.ndarray, nk: tuple
 # ----------------------------------------------------------------------------------------------
 
 
+def hartree_fock(u: np.ndarray, v_full: np.ndarray, occ: np.ndarray, occ_k: np.ndarray):
+    """Hartree and Fock terms (nonlocal_sde.get_hartree_fock, dgamore/nonlocal_sde.py:31-69) with the full,
+    ordered q list of one rank:
+
+        hartree[a,b] = 2 sum_cd (U + V_(q=0))[a,b,c,d] occ[d,c]                        (nonlocal_sde.py:45)
+        fock[k,a,b]  = -1/Nq sum_q sum_cd (U + V_q)[a,b,c,d] occ_k[k+q][d,c]          (nonlocal_sde.py:52-68)
+
+    (the upstream pairs the permuted interaction uq[:, a, d, c, b] = (U + V_q)[a, b, c, d] with
+    np.roll(occ_k, -q), i.e. occ_k at k + q).  v_full: [kx, ky, kz, a, b, c, d]; occ_k: [kx, ky, kz, n, n].
+    Returns hartree [1, n, n, 1] and fock [Nk, n, n, 1] as the upstream does."""
+    nk = occ_k.shape[:3]
+    nb = occ.shape[0]
+    hartree = 2.0 * np.einsum("abcd,dc->ab", u + v_full[0, 0, 0], occ)
+    nk_tot = int(np.prod(nk))
+    fock = np.zeros((nk_tot, nb, nb), dtype=np.result_type(v_full, occ_k))
+    for qx in range(nk[0]):
+        for qy in range(nk[1]):
+            for qz in range(nk[2]):
+                w = u + v_full[qx, qy, qz]
+                occ_shift = np.roll(occ_k, (-qx, -qy, -qz), axis=(0, 1, 2)).reshape(nk_tot, nb, nb)
+                fock += np.einsum("abcd,kdc->kab", w, occ_shift)
+    fock *= -1.0 / nk_tot
+    return hartree[None, ..., None], fock[..., None]
+
+
 def sde_pass(inp: dict, do_lambda: bool = True) -> dict:
     """One pass of the hot path of nonlocal_sde.calculate_self_energy_q (nonlocal_sde.py:786-879).
 

@@ -230,7 +230,40 @@ def bse_kat() -> dict:
     return {"beta": beta, "v1": v1, "v2": v2}
 
 
+HF_CONFIGS = ("t1", "t2", "t3")
+
+
+def hf_fixtures() -> dict:
+    """nonlocal_sde.get_hartree_fock (nonlocal_sde.py:31-69) on the configurations' interactions and seeded
+    occupations, with the full ordered q list of a single rank."""
+    out = {}
+    for name in HF_CONFIGS:
+        cfg = synthetic.CONFIGS[name]
+        inp = synthetic.make_inputs(cfg)
+        _setup_config(cfg, inp)
+        occ, occ_k = synthetic.make_occupations(cfg)
+        config.sys.occ = occ
+        config.sys.occ_k = occ_k
+        u_loc = LocalInteraction(inp["u"])
+        v_full = Interaction(inp["v_q_full"].reshape(*cfg.nk, *inp["v_q_full"].shape[1:]), SpinChannel.NONE,
+                             tuple(cfg.nk))
+        hartree, fock = nonlocal_sde.get_hartree_fock(u_loc, v_full, config.lattice.q_grid.get_q_list())
+        out[f"{name}_u"] = inp["u"]
+        out[f"{name}_v_q_full"] = inp["v_q_full"]
+        out[f"{name}_nk"] = np.array(cfg.nk)
+        out[f"{name}_occ"] = occ
+        out[f"{name}_occ_k"] = occ_k
+        out[f"{name}_hartree"] = hartree
+        out[f"{name}_fock"] = fock
+    return out
+
+
 def main():
+    if "--only-hf" in sys.argv:
+        np.savez_compressed(os.path.join(HERE, "hartree_fock.npz"), **hf_fixtures())
+        print("wrote hartree_fock.npz")
+        return
+    np.savez_compressed(os.path.join(HERE, "hartree_fock.npz"), **hf_fixtures())
     for name in ("t1", "t1b", "t2", "t3") + ELIASHBERG_CONFIGS:
         data = run_reference_pass(name)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)

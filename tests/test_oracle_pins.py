@@ -1,9 +1,11 @@
 """Pins the CPU oracle to the upstream code: its own fixtures and its outputs on seeded synthetic inputs."""
 
+import os
+
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CONFIGS, load_golden, rel_err
+from conftest import GOLDEN, GOLDEN_CONFIGS, load_golden, rel_err
 from oracle import ladder as L
 from dgamore_b200.kgrid import KGrid
 
@@ -139,3 +141,14 @@ def test_oracle_eliashberg_matches_upstream_fp64(name):
         v0 = L.symmetrise_gap(L.d_wave_gap(inp["nk"], nb, niv_pp, ch), inp["irrk_ind"], inp["irrk_inv"])
         vals, _ = L.eliashberg_eigs(gam[ch], inp["irrk_inv"], inp["nk"], chi0pp, inp["beta"], ch, v0, 4, 1e-12)
         assert np.max(np.abs(vals - ref[f"lambdas_{ch}"])) < 1e-9 * max(1.0, np.max(np.abs(vals)))
+
+
+@pytest.mark.parametrize("name", ("t1", "t2", "t3"))
+def test_hartree_fock_oracle_matches_upstream(name):
+    """nonlocal_sde.get_hartree_fock run here (tests/golden/make_golden.py) vs the oracle restatement."""
+    d = np.load(os.path.join(GOLDEN, "hartree_fock.npz"))
+    nk = tuple(int(x) for x in d[f"{name}_nk"])
+    v = d[f"{name}_v_q_full"].reshape(*nk, *d[f"{name}_v_q_full"].shape[1:])
+    h, f = L.hartree_fock(d[f"{name}_u"], v, d[f"{name}_occ"], d[f"{name}_occ_k"])
+    assert rel_err(h, d[f"{name}_hartree"]) < 1e-14
+    assert rel_err(f, d[f"{name}_fock"]) < 1e-14
