@@ -333,7 +333,15 @@ def make_inputs(cfg: DgaConfig | str) -> dict:
         out[f"gamma_{ch}"] = gamma
         chi_phys, _ = local_chi_and_f(chi0_loc_core, gamma, cfg.beta, u_channel(u, ch))
         full = np.concatenate([np.conj(np.flip(chi_phys[..., 1:], axis=-1)), chi_phys], axis=-1)
-        out[f"chi_loc_sum_{ch}"] = complex(full.sum() / cfg.beta)
+        target = complex(full.sum() / cfg.beta)
+        if target.real <= 0.0 and cfg.n_bands == 1:
+            # (single band: the only case with a lambda-correction) the model vertex drove the local ladder past its instability (a negative local susceptibility
+            # sum, which a DMFT susceptibility never has and for which the lambda equation has no root): use
+            # the local bubble's sum instead, the susceptibility of the non-interacting local problem
+            c0 = chi0_loc_core.sum(axis=-1) / cfg.beta**2  # [a,b,c,d,w]
+            c0_full = np.concatenate([np.conj(np.flip(c0[..., 1:], axis=-1)), c0], axis=-1)
+            target = complex(c0_full.sum() / cfg.beta)
+        out[f"chi_loc_sum_{ch}"] = target
         if ch == "magn":
             g_pad = pad_with_u(gamma, u_channel(u, ch), cfg.niv_full)
             _, f_magn = local_chi_and_f(chi0_loc_full, g_pad, cfg.beta, u_channel(u, ch))
