@@ -22,9 +22,10 @@ from ._lib import BseTuning, call, lib
 
 C128 = torch.complex128
 
-# (kernel, ctas_per_sm): kernel 1 = shared-memory panel (mixed only), 2 = 128-thread kernel
+# (kernel, ctas_per_sm): kernel 1 = shared-memory panel (mixed only), 2 = 128-thread kernel, 3 = shared-memory
+# panel with tensor-core trailing tiles (mixed only)
 CANDIDATES = {
-    "mixed": [(1, 0), (2, 0), (2, 2), (2, 1)],
+    "mixed": [(3, 0), (1, 0), (2, 0), (2, 2), (2, 1)],
     "fp64": [(2, 0), (2, 2), (2, 1)],
 }
 
@@ -120,10 +121,13 @@ def tune_bse(lp, precision: str | None = None, sample_items: int | None = None, 
             b.record(stream)
             b.synchronize()
             best = min(best, a.elapsed_time(b))
-        if int(status.abs().sum()) == 0 or mixed:  # unconverged mixed items are re-solved in FP64 later
-            times[c] = best
+        clean = int(status.abs().sum()) == 0
+        times[c] = (best, clean)
     del scratch
-    choice = min(times, key=times.get)
+    # the fastest candidate whose sampled items all came back clean (a flagged item costs an FP64 re-solve)
+    ok = {c: t for c, (t, clean) in times.items() if clean} or {c: t for c, (t, _) in times.items()}
+    choice = min(ok, key=ok.get)
+    times = {c: t for c, (t, _) in times.items()}
     _CACHE[key] = choice
     save_cache(cache_path)
     lp.set_tuning(choice)

@@ -1358,22 +1358,24 @@ static int sm_count() {
   return sms;
 }
 
-// 1 = panel kernel, 2 = 128-thread kernel, -1 = the requested kernel cannot run this size
+// 1 = panel kernel, 2 = 128-thread kernel, 3 = panel kernel with tensor-core trailing tiles,
+// -1 = the requested kernel cannot run this size
 static int tuned_kernel(int mixed, int N, int n2, const dga_bse_tuning* t) {
   const int k = t ? t->kernel : 0;
-  if (k < 0 || k > 2) return -1;
-  if (!mixed) return k == 1 ? -1 : 2;
+  if (k < 0 || k > 3) return -1;
+  if (!mixed) return (k == 1 || k == 3) ? -1 : 2;
   if (k == 0) return dga_panel_supported(N, n2) ? 1 : 2;
   if (k == 1 && !dga_panel_supported(N, n2)) return -1;
+  if (k == 3 && !dga_panel_supported(N, n2, true)) return -1;
   return k;
 }
 
 static int tuned_grid(int kernel, int mixed, int N, int n2, int n_items, const dga_bse_tuning* t, size_t* slot,
                       size_t* smem) {
-  if (kernel == 1) {
+  if (kernel == 1 || kernel == 3) {
     *slot = dga_panel_slot_bytes(N, n2);
     *smem = 0;
-    return dga_panel_grid(n2, N, n_items);
+    return dga_panel_grid(n2, N, n_items, kernel == 3);
   }
   int grid;
   if (mixed) {
@@ -1439,9 +1441,9 @@ int dga_bse_solve_sum_tuned_c128(int n_orb, int niv, int niw_half, int n_q, int 
   src.Q = n_q;
   src.inv_beta2 = inv_beta2;
   cudaError_t err;
-  if (kernel == 1) {
+  if (kernel == 1 || kernel == 3) {
     err = dga_panel_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, max_iter, tol,
-                           (double2*)out, status, iters, (unsigned char*)scratch, slot, stream);
+                           (double2*)out, status, iters, (unsigned char*)scratch, slot, stream, kernel == 3);
   } else if (mixed) {
 #define DGA_TUNED_MIXED_CASE(NRV)                                                                                    \
   case NRV:                                                                                                          \

@@ -24,6 +24,7 @@
 // Shared memory holds the m x 32 complex64 panel (256 B per row), so N is limited to about 790 (the 227 KB
 // opt-in limit); larger items use the 128-thread kernel of bse.cu.
 #include "bse_core.cuh"
+#include "tc_tile.cuh"
 
 namespace dga {
 
@@ -43,18 +44,24 @@ constexpr int P_TILE_UNROLL = DGA_PANEL_TILE_UNROLL;  // unroll of the trailing 
 // ----------------------------------------------------------------------------------------------
 // The panel region also holds the solve's right-hand sides (up to 16 x ldp complex64) followed by the residual's
 // staging ([32][16] and [16][16] complex128), so small ldp need more than the panel itself.
-__host__ __device__ inline size_t panel_region_bytes(int ldp) {
+// With the tensor-core trailing update (tc) the region also holds the four 32 KB TF32 operand buffers of a tile.
+__host__ __device__ inline size_t panel_region_bytes(int ldp, bool tc = false) {
   const size_t panel = (size_t)ldp * PNB * sizeof(float2);
   const size_t solve = (size_t)16 * ldp * sizeof(float2) + 32 + (32 * 16 + 16 * 16) * sizeof(double2);
-  return ((panel > solve ? panel : solve) + 15) & ~(size_t)15;
+  size_t r = panel > solve ? panel : solve;
+  if (tc && r < 4 * (size_t)TC_OPERAND_FLOATS * sizeof(float)) r = 4 * (size_t)TC_OPERAND_FLOATS * sizeof(float);
+  return (r + 127) & ~(size_t)127;
 }
 constexpr size_t P_FIXED = 16 * sizeof(double)                 // redd
                            + PNB * (PNB + 1) * sizeof(float2)  // L11i
                            + PNB * PTN * sizeof(float2)        // Us
                            + 16 * sizeof(float) + 16 * sizeof(int)  // red_val, red_idx
                            + 64 * sizeof(int) * 2              // s_row, s_cont
-                           + 4 * sizeof(int);                  // misc
-__host__ __device__ inline size_t panel_smem_bytes(int ldp) { return panel_region_bytes(ldp) + P_FIXED + sizeof(int) * (size_t)ldp; }
+                           + 4 * sizeof(int)                   // misc
+                           + 16;                               // TMEM address + completion barrier
+__host__ __device__ inline size_t panel_smem_bytes(int ldp, bool tc = false) {
+  return panel_region_bytes(ldp, tc) + P_FIXED + sizeof(int) * (size_t)ldp;
+}
 
 struct PanelSmem {
   float2* P;     // [PNB][ldp] panel, column-major (also the solve and residual staging area)
@@ -65,16 +72,22 @@ struct PanelSmem {
   int* red_idx;
   int* s_row;   // [64] rows touched by the panel's interchanges: slots 0..31 the panel rows, 32.. the others
   int* s_cont;  // [64] old row whose content ends up in s_row[slot]
-  int* misc;    // [0] number of rows below the panel that receive another row
+  int* misc;    // [0] rows below the panel that receive another row, [1] status bits, [2] tensor-core wait failure
+  uint64_t* bar;    // completion barrier of the tensor-core tile
+  uint32_t* tslot;  // TMEM address of the tile accumulator
   int* piv;     // [ldp] row interchanged with row j
   int ldp;
 
-  __device__ PanelSmem(unsigned char* base, int ldp_) : ldp(ldp_) {
+  __device__ PanelSmem(unsigned char* base, int ldp_, bool tc) : ldp(ldp_) {
     unsigned char* p = base;
     P = reinterpret_cast<float2*>(p);
-    p += panel_region_bytes(ldp);
+    p += panel_region_bytes(ldp, tc);
     redd = reinterpret_cast<double*>(p);
     p += 16 * sizeof(double);
+    bar = reinterpret_cast<uint64_t*>(p);
+    p += 8;
+    tslot = reinterpret_cast<uint32_t*>(p);
+    p += 8;
     L11i = reinterpret_cast<float2*>(p);
     p += PNB * (PNB + 1) * sizeof(float2);
     Us = reinterpret_cast<float2*>(p);
@@ -239,7 +252,10 @@ __device__ void panel_interchange_map(PanelSmem& s, int k0, int nb) {
 // ----------------------------------------------------------------------------------------------
 // LU of the N x N complex64 column-major matrix A (leading dimension N) in place.
 // ----------------------------------------------------------------------------------------------
-__device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s) {
+// TC = true: the trailing tiles run on the tensor cores (tc_tile.cuh); L21 is then read back from global memory
+// (the panel region holds the tile operands), and parity tracks the phase of the tile completion barrier.
+template <bool TC>
+__device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& parity) {
   const int tid = threadIdx.x;
   bool singular = false;
   for (int k0 = 0; k0 < N; k0 += PNB) {
@@ -306,72 +322,145 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s) {
         }
         __syncthreads();  // every old value of the touched rows is read before any is overwritten
         const int tgt_row = lane < n_tgt ? s.s_row[32 + lane] : 0;
+        float* b_hi = reinterpret_cast<float*>(s.P) + 2 * TC_OPERAND_FLOATS;
+        float* b_lo = b_hi + TC_OPERAND_FLOATS;
 #pragma unroll
         for (int q = 0; q < PTN / PW; ++q) {
           const int c = warp + PW * q;
           float2* colw = A + (size_t)(cs + c) * N;
           const bool act = c < cw && lane < nb;
           if (act) colw[k0 + lane] = u[q];
-          s.Us[lane * PTN + c] = act ? u[q] : make_float2(0.f, 0.f);
+          const float2 uq = act ? u[q] : make_float2(0.f, 0.f);
+          if (TC) {
+            // B[2k + t][2c + s] of the real product (tc_tile.cuh), k = lane, stored K-major by column 2c + s
+            tc_store_split(b_hi, b_lo, tc_off(2 * c, 2 * lane), uq.x);
+            tc_store_split(b_hi, b_lo, tc_off(2 * c, 2 * lane + 1), -uq.y);
+            tc_store_split(b_hi, b_lo, tc_off(2 * c + 1, 2 * lane), uq.y);
+            tc_store_split(b_hi, b_lo, tc_off(2 * c + 1, 2 * lane + 1), uq.x);
+          } else {
+            s.Us[lane * PTN + c] = uq;
+          }
           if (c < cw && lane < n_tgt) colw[tgt_row] = tv[q];
         }
       }
       __syncthreads();
-      // trailing tiles of the strip, 128 x 64: thread (ty, tx) owns rows rt + 2ty + {0,1} + {0,64} and columns
-      // cs + 2tx + {0,1} + {0,32} (row pairs and column pairs move as one 16-byte access; N is even), with the
-      // real and imaginary parts in separate scalar accumulators.
-      const int ty = tid & 31, tx = tid >> 5;
-      const float2* up = s.Us + 2 * tx;
-      for (int rt = k1; rt < N; rt += PTM) {
-        float cr[16], ci[16];  // index (column j of 4) * 4 + (row i of 4)
-        const int rbase = rt + 2 * ty;
-        const bool full = rt + PTM <= N && cs + PTN <= N;
+      if (TC) {
+        // trailing tiles of the strip on the tensor cores, 128 rows x 64 complex columns per tile
+        float* a_hi = reinterpret_cast<float*>(s.P);
+        float* a_lo = a_hi + TC_OPERAND_FLOATS;
+        const float* b_hi = a_lo + TC_OPERAND_FLOATS;
+        const float* b_lo = b_hi + TC_OPERAND_FLOATS;
+        const int lane = tid & 31, warp = tid >> 5;
+        const uint32_t tbase = *s.tslot;
+        const uint32_t taddr = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + 32 * (warp >> 2);
+        for (int rt = k1; rt < N; rt += TC_M) {
+          {  // L21 rows rt .. rt + 127 (written back with the panel) -> A_hi / A_lo; thread: a row, 4 chunks of 2 k
+            const int row = tid & (TC_M - 1), cg = tid >> 7;
+            const int r = rt + row;
+            const bool rok = r < N;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int c = cs + 2 * tx + (j & 1) + 32 * (j >> 1);
-#pragma unroll
-          for (int ap = 0; ap < 2; ++ap) {
-            const int r = rbase + 64 * ap;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (full || (c < N && r < N)) v = *reinterpret_cast<const float4*>(A + (size_t)c * N + r);
-            cr[j * 4 + 2 * ap] = v.x;
-            ci[j * 4 + 2 * ap] = v.y;
-            cr[j * 4 + 2 * ap + 1] = v.z;
-            ci[j * 4 + 2 * ap + 1] = v.w;
-          }
-        }
-        const bool r0ok = full || rbase < N, r1ok = full || rbase + 64 < N;
-        const float2* lp0 = s.P + (r0ok ? rbase - k0 : 0);
-        const float2* lp1 = s.P + (r1ok ? rbase + 64 - k0 : 0);
-#pragma unroll P_TILE_UNROLL
-        for (int k = 0; k < nb; ++k) {
-          float4 l0 = *reinterpret_cast<const float4*>(lp0 + (size_t)k * s.ldp);
-          float4 l1 = *reinterpret_cast<const float4*>(lp1 + (size_t)k * s.ldp);
-          if (!r0ok) l0 = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (!r1ok) l1 = make_float4(0.f, 0.f, 0.f, 0.f);
-          const float4 u0 = *reinterpret_cast<const float4*>(up + k * PTN);
-          const float4 u1 = *reinterpret_cast<const float4*>(up + k * PTN + 32);
-          const float lr[4] = {l0.x, l0.z, l1.x, l1.z}, li[4] = {l0.y, l0.w, l1.y, l1.w};
-          const float ur[4] = {u0.x, u0.z, u1.x, u1.z}, ui[4] = {u0.y, u0.w, u1.y, u1.w};
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              cr[j * 4 + i] = fmaf(-lr[i], ur[j], cr[j * 4 + i]);
-              cr[j * 4 + i] = fmaf(li[i], ui[j], cr[j * 4 + i]);
-              ci[j * 4 + i] = fmaf(-lr[i], ui[j], ci[j * 4 + i]);
-              ci[j * 4 + i] = fmaf(-li[i], ur[j], ci[j * 4 + i]);
+            for (int j = 0; j < 4; ++j) {
+              const int ch = cg + 4 * j;
+              const float2 x0 = rok ? A[(size_t)(k0 + 2 * ch) * N + r] : make_float2(0.f, 0.f);
+              const float2 x1 = rok ? A[(size_t)(k0 + 2 * ch + 1) * N + r] : make_float2(0.f, 0.f);
+              const float4 h = make_float4(tf32_hi(x0.x), tf32_hi(x0.y), tf32_hi(x1.x), tf32_hi(x1.y));
+              const float4 l = make_float4(x0.x - h.x, x0.y - h.y, x1.x - h.z, x1.y - h.w);
+              *reinterpret_cast<float4*>(a_hi + tc_off(row, 4 * ch)) = h;
+              *reinterpret_cast<float4*>(a_lo + tc_off(row, 4 * ch)) = l;
             }
+          }
+          const int r = rt + 32 * (warp & 3) + lane, cb = cs + 16 * (warp >> 2);
+          float v[32];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = cb + j;
+            const float2 x = (r < N && c < N) ? A[(size_t)c * N + r] : make_float2(0.f, 0.f);
+            v[2 * j] = x.x;
+            v[2 * j + 1] = x.y;
+          }
+          tmem_st32(taddr, v);
+          tmem_wait_st();
+          tc_fence_async_smem();
+          tc_fence_before();
+          __syncthreads();
+          const bool live = s.misc[2] == 0;  // a CTA whose tensor-core wait ever ran out issues no more tiles
+          if (live && tid == 0) {
+            tc_fence_after();
+            tc_issue_tile(tbase, a_hi, a_lo, b_hi, b_lo, s.bar);
+          }
+          const bool ok = live && mbar_wait(s.bar, parity);
+          if (live) parity ^= 1u;
+          tc_fence_after();
+          if (ok) {
+            tmem_ld32(taddr, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int c = cb + j;
+              if (r < N && c < N) A[(size_t)c * N + r] = make_float2(v[2 * j], v[2 * j + 1]);
+            }
+          } else {
+            s.misc[2] = 1;
+          }
+          tc_fence_before();
         }
+      } else {
+      // trailing tiles of the strip, 128 x 64: thread (ty, tx) owns rows rt + 2ty + {0,1} + {0,64} and columns
+        // cs + 2tx + {0,1} + {0,32} (row pairs and column pairs move as one 16-byte access; N is even), with the
+        // real and imaginary parts in separate scalar accumulators.
+        const int ty = tid & 31, tx = tid >> 5;
+        const float2* up = s.Us + 2 * tx;
+        for (int rt = k1; rt < N; rt += PTM) {
+          float cr[16], ci[16];  // index (column j of 4) * 4 + (row i of 4)
+          const int rbase = rt + 2 * ty;
+          const bool full = rt + PTM <= N && cs + PTN <= N;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int c = cs + 2 * tx + (j & 1) + 32 * (j >> 1);
+          for (int j = 0; j < 4; ++j) {
+            const int c = cs + 2 * tx + (j & 1) + 32 * (j >> 1);
 #pragma unroll
-          for (int ap = 0; ap < 2; ++ap) {
-            const int r = rbase + 64 * ap;
-            if (full || (c < N && r < N))
-              *reinterpret_cast<float4*>(A + (size_t)c * N + r) =
-                  make_float4(cr[j * 4 + 2 * ap], ci[j * 4 + 2 * ap], cr[j * 4 + 2 * ap + 1], ci[j * 4 + 2 * ap + 1]);
+            for (int ap = 0; ap < 2; ++ap) {
+              const int r = rbase + 64 * ap;
+              float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+              if (full || (c < N && r < N)) v = *reinterpret_cast<const float4*>(A + (size_t)c * N + r);
+              cr[j * 4 + 2 * ap] = v.x;
+              ci[j * 4 + 2 * ap] = v.y;
+              cr[j * 4 + 2 * ap + 1] = v.z;
+              ci[j * 4 + 2 * ap + 1] = v.w;
+            }
+          }
+          const bool r0ok = full || rbase < N, r1ok = full || rbase + 64 < N;
+          const float2* lp0 = s.P + (r0ok ? rbase - k0 : 0);
+          const float2* lp1 = s.P + (r1ok ? rbase + 64 - k0 : 0);
+#pragma unroll P_TILE_UNROLL
+          for (int k = 0; k < nb; ++k) {
+            float4 l0 = *reinterpret_cast<const float4*>(lp0 + (size_t)k * s.ldp);
+            float4 l1 = *reinterpret_cast<const float4*>(lp1 + (size_t)k * s.ldp);
+            if (!r0ok) l0 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (!r1ok) l1 = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 u0 = *reinterpret_cast<const float4*>(up + k * PTN);
+            const float4 u1 = *reinterpret_cast<const float4*>(up + k * PTN + 32);
+            const float lr[4] = {l0.x, l0.z, l1.x, l1.z}, li[4] = {l0.y, l0.w, l1.y, l1.w};
+            const float ur[4] = {u0.x, u0.z, u1.x, u1.z}, ui[4] = {u0.y, u0.w, u1.y, u1.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+              for (int i = 0; i < 4; ++i) {
+                cr[j * 4 + i] = fmaf(-lr[i], ur[j], cr[j * 4 + i]);
+                cr[j * 4 + i] = fmaf(li[i], ui[j], cr[j * 4 + i]);
+                ci[j * 4 + i] = fmaf(-lr[i], ui[j], ci[j * 4 + i]);
+                ci[j * 4 + i] = fmaf(-li[i], ur[j], ci[j * 4 + i]);
+              }
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int c = cs + 2 * tx + (j & 1) + 32 * (j >> 1);
+#pragma unroll
+            for (int ap = 0; ap < 2; ++ap) {
+              const int r = rbase + 64 * ap;
+              if (full || (c < N && r < N))
+                *reinterpret_cast<float4*>(A + (size_t)c * N + r) =
+                    make_float4(cr[j * 4 + 2 * ap], ci[j * 4 + 2 * ap], cr[j * 4 + 2 * ap + 1], ci[j * 4 + 2 * ap + 1]);
+            }
           }
         }
       }
@@ -491,10 +580,10 @@ __host__ __device__ inline size_t panel_slot_bytes(int N, int n2) {
   return (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255) + 2 * (size_t)N * n2 * sizeof(double2);
 }
 
-template <int NR>
+template <int NR, bool TC>
 __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi, int N, int nv, double beta,
                                 int max_iter, double tol, double2* __restrict__ o, unsigned char* slot, PanelSmem& s,
-                                int* iters) {
+                                int* iters, uint32_t& parity) {
   const int tid = threadIdx.x;
   float2* A = reinterpret_cast<float2*>(slot);
   double2* Y = reinterpret_cast<double2*>(slot + (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255));
@@ -521,7 +610,7 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
     }
   }
   __syncthreads();
-  const bool singular = panel_lu(A, N, s);
+  const bool singular = panel_lu<TC>(A, N, s, parity);
   // ---- initial solve against the selector: S[(p,nu)][s] = delta_{p s} ----
   const int ldy = N;
   float2* y = s.P;
@@ -576,31 +665,60 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
   }
   if (bad) atomicOr(&s.misc[1], DGA_ITEM_NONFINITE);
   __syncthreads();
-  const int st = (singular ? DGA_ITEM_SINGULAR : 0) | s.misc[1] | (converged ? 0 : DGA_ITEM_NOCONVERGE);
+  // a tensor-core wait that ran out leaves the factors incomplete: flag the item for the FP64 re-solve
+  const int st = (singular ? DGA_ITEM_SINGULAR : 0) | s.misc[1] | (converged ? 0 : DGA_ITEM_NOCONVERGE) |
+                 (s.misc[2] ? DGA_ITEM_NONFINITE : 0);
   *iters = it;
   __syncthreads();
   return st;
 }
 
-template <int NR>
+// TMEM for the tensor-core tiles: one warp allocates 128 columns (the 128 x 128 fp32 accumulator) for the CTA's
+// lifetime; the completion barrier is initialised once.  At exit, a CTA whose wait ever ran out waits once more
+// (bounded) for its last tile before the columns are freed.
+template <bool TC>
+__device__ void panel_kernel_begin(PanelSmem& s) {
+  if (threadIdx.x == 0) s.misc[2] = 0;
+  if (TC) {
+    if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, TC_NR);
+    if (threadIdx.x == 0) mbar_init(s.bar);
+    tc_fence_before();
+  }
+  __syncthreads();
+  if (TC) tc_fence_after();
+}
+
+template <bool TC>
+__device__ void panel_kernel_end(PanelSmem& s, uint32_t parity) {
+  if (!TC) return;
+  tc_fence_before();
+  __syncthreads();
+  if (s.misc[2]) mbar_wait(s.bar, parity ^ 1u);
+  if ((threadIdx.x >> 5) == 0) tc_dealloc(*s.tslot, TC_NR);
+}
+
+template <int NR, bool TC>
 __global__ void __launch_bounds__(PT, 1)
     bse_panel_mixed_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int nv, int W,
                            int Q, double beta, int max_iter, double tol, double2* __restrict__ out,
                            int* __restrict__ status, int* __restrict__ iters, unsigned char* __restrict__ scratch,
                            size_t slot_bytes) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  PanelSmem s(smem_raw, N);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PanelSmem s(smem_raw, N, TC);
   unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  uint32_t parity = 0;
+  panel_kernel_begin<TC>(s);
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const WorkItem wi = work[item];
     double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * NR;
     int it = 0;
-    const int st = solve_item_panel<NR>(src, wi, N, nv, beta, max_iter, tol, o, slot, s, &it);
+    const int st = solve_item_panel<NR, TC>(src, wi, N, nv, beta, max_iter, tol, o, slot, s, &it, parity);
     if (threadIdx.x == 0) {
       if (status) status[item] = st;
       if (iters) iters[item] = it;
     }
   }
+  panel_kernel_end<TC>(s, parity);
 }
 
 // Heterogeneous batch (requests of one orbital count): see bse_multi_kernel in bse.cu.
@@ -609,9 +727,11 @@ __global__ void __launch_bounds__(PT, 1)
     bse_panel_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work,
                            int n_items, int n_max, int max_iter, double tol, int* __restrict__ status,
                            int* __restrict__ iters, unsigned char* __restrict__ scratch, size_t slot_bytes) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  PanelSmem s(smem_raw, n_max);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PanelSmem s(smem_raw, n_max, false);
   unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  uint32_t parity = 0;
+  panel_kernel_begin<false>(s);
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const MultiItem mi = work[item];
     const dga_bse_problem d = probs[mi.prob];
@@ -628,7 +748,7 @@ __global__ void __launch_bounds__(PT, 1)
     const WorkItem wi{mi.ch, mi.q, mi.w};
     double2* o = (double2*)d.out + (((size_t)wi.ch * src.Q + wi.q) * src.W + wi.w) * (size_t)N * NR;
     int it = 0;
-    const int st = solve_item_panel<NR>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, &it);
+    const int st = solve_item_panel<NR, false>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, &it, parity);
     if (threadIdx.x == 0) {
       status[item] = st;
       if (iters) iters[item] = it;
@@ -643,11 +763,11 @@ using namespace dga;
 // ----------------------------------------------------------------------------------------------
 // Host side (called from bse.cu)
 // ----------------------------------------------------------------------------------------------
-bool dga_panel_supported(int N, int n2) {
+bool dga_panel_supported(int N, int n2, bool tc) {
 #ifdef DGA_DISABLE_PANEL
   return false;
 #else
-  return (n2 == 1 || n2 == 4 || n2 == 9 || n2 == 16) && N > 0 && panel_smem_bytes(N) <= (size_t)P_MAX_SMEM;
+  return (n2 == 1 || n2 == 4 || n2 == 9 || n2 == 16) && N > 0 && panel_smem_bytes(N, tc) <= (size_t)P_MAX_SMEM;
 #endif
 }
 
@@ -666,18 +786,23 @@ static int panel_grid_for(K kernel, int n_items, size_t smem) {
   return n_items < g ? n_items : g;
 }
 
-int dga_panel_grid(int n2, int N, int n_items) {
-  const size_t smem = panel_smem_bytes(N);
+template <bool TC>
+static int panel_grid_tc(int n2, int N, int n_items) {
+  const size_t smem = panel_smem_bytes(N, TC);
   switch (n2) {
-    case 1: return panel_grid_for(bse_panel_mixed_kernel<1>, n_items, smem);
-    case 4: return panel_grid_for(bse_panel_mixed_kernel<4>, n_items, smem);
-    case 9: return panel_grid_for(bse_panel_mixed_kernel<9>, n_items, smem);
-    default: return panel_grid_for(bse_panel_mixed_kernel<16>, n_items, smem);
+    case 1: return panel_grid_for(bse_panel_mixed_kernel<1, TC>, n_items, smem);
+    case 4: return panel_grid_for(bse_panel_mixed_kernel<4, TC>, n_items, smem);
+    case 9: return panel_grid_for(bse_panel_mixed_kernel<9, TC>, n_items, smem);
+    default: return panel_grid_for(bse_panel_mixed_kernel<16, TC>, n_items, smem);
   }
 }
 
+int dga_panel_grid(int n2, int N, int n_items, bool tc) {
+  return tc ? panel_grid_tc<true>(n2, N, n_items) : panel_grid_tc<false>(n2, N, n_items);
+}
+
 int dga_panel_batch_grid(int n2, int n_max, int n_items) {
-  const size_t smem = panel_smem_bytes(n_max);
+  const size_t smem = panel_smem_bytes(n_max, false);
   switch (n2) {
     case 1: return panel_grid_for(bse_panel_multi_kernel<1>, n_items, smem);
     case 4: return panel_grid_for(bse_panel_multi_kernel<4>, n_items, smem);
@@ -686,14 +811,15 @@ int dga_panel_batch_grid(int n2, int n_max, int n_items) {
   }
 }
 
-cudaError_t dga_panel_launch(int grid, const StructuredSource& src, const WorkItem* work, int n_items, int N, int n2,
-                             int nv, int W, int Q, double beta, int max_iter, double tol, double2* out, int* status,
-                             int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream) {
-  const size_t smem = panel_smem_bytes(N);
-#define DGA_PANEL_CASE(R)                                                                                        \
-  case R:                                                                                                        \
-    bse_panel_mixed_kernel<R><<<grid, PT, smem, stream>>>(src, work, n_items, N, nv, W, Q, beta, max_iter, tol, \
-                                                          out, status, iters, scratch, slot_bytes);             \
+template <bool TC>
+static void panel_launch_tc(int grid, const StructuredSource& src, const WorkItem* work, int n_items, int N, int n2,
+                            int nv, int W, int Q, double beta, int max_iter, double tol, double2* out, int* status,
+                            int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream) {
+  const size_t smem = panel_smem_bytes(N, TC);
+#define DGA_PANEL_CASE(R)                                                                                          \
+  case R:                                                                                                          \
+    bse_panel_mixed_kernel<R, TC><<<grid, PT, smem, stream>>>(src, work, n_items, N, nv, W, Q, beta, max_iter, tol, \
+                                                              out, status, iters, scratch, slot_bytes);           \
     break;
   switch (n2) {
     DGA_PANEL_CASE(1)
@@ -702,13 +828,24 @@ cudaError_t dga_panel_launch(int grid, const StructuredSource& src, const WorkIt
     DGA_PANEL_CASE(16)
   }
 #undef DGA_PANEL_CASE
+}
+
+cudaError_t dga_panel_launch(int grid, const StructuredSource& src, const WorkItem* work, int n_items, int N, int n2,
+                             int nv, int W, int Q, double beta, int max_iter, double tol, double2* out, int* status,
+                             int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc) {
+  if (tc)
+    panel_launch_tc<true>(grid, src, work, n_items, N, n2, nv, W, Q, beta, max_iter, tol, out, status, iters, scratch,
+                          slot_bytes, stream);
+  else
+    panel_launch_tc<false>(grid, src, work, n_items, N, n2, nv, W, Q, beta, max_iter, tol, out, status, iters,
+                           scratch, slot_bytes, stream);
   return cudaGetLastError();
 }
 
 cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
                                    int n_max, int max_iter, double tol, int* status, int* iters,
                                    unsigned char* scratch, size_t slot_bytes, cudaStream_t stream) {
-  const size_t smem = panel_smem_bytes(n_max);
+  const size_t smem = panel_smem_bytes(n_max, false);
 #define DGA_PANEL_CASE(R)                                                                                       \
   case R:                                                                                                       \
     bse_panel_multi_kernel<R><<<grid, PT, smem, stream>>>(probs, work, n_items, n_max, max_iter, tol, status, \

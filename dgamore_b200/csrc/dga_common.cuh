@@ -32,7 +32,8 @@ typedef struct {
 
 // Launch choices of the BSE solvers (the search space of the autotuner); layout is part of the C ABI.
 typedef struct {
-  int kernel;       // 0 = default, 1 = shared-memory-panel kernel (mixed form only), 2 = 128-thread kernel
+  int kernel;       // 0 = default, 1 = shared-memory-panel kernel (mixed form only), 2 = 128-thread kernel,
+                    // 3 = shared-memory-panel kernel with tensor-core (tcgen05) trailing tiles (mixed form only)
   int ctas_per_sm;  // CTAs per SM of the 128-thread kernels (0 = as many as fit)
 } dga_bse_tuning;
 

@@ -102,8 +102,10 @@ int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_c
 /* Launch choices of the BSE solvers, the search space of the autotuner (dgamore_b200/autotune.py); no
  * counterpart in the upstream.  kernel: 0 = default (mixed form: the shared-memory-panel kernel when N fits,
  * else the 128-thread kernel; FP64: the 128-thread kernel), 1 = shared-memory-panel kernel (mixed form only,
- * N up to about 790), 2 = 128-thread kernel; ctas_per_sm: CTAs per SM of the 128-thread kernel (0 = all that
- * fit).  Both choices change the speed only: every choice computes the same solves. */
+ * N up to about 790), 2 = 128-thread kernel, 3 = shared-memory-panel kernel whose trailing tiles run on the
+ * tensor cores (tcgen05.mma kind::tf32 with a three-term split for FP32-level products, accumulators in tensor
+ * memory; mixed form only); ctas_per_sm: CTAs per SM of the 128-thread kernel (0 = all that fit).  The choices
+ * change the speed only: every choice computes the same solves (the mixed ones to the refinement tolerance). */
 typedef struct {
   int kernel;
   int ctas_per_sm;

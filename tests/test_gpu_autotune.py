@@ -1,7 +1,8 @@
 """The BSE launch choices of the autotuner compute the same solves, and the tuner installs a working choice.
 
 FP64: every choice of the 128-thread kernel (any CTAs per SM) gives bitwise the default X.  Mixed: every
-kernel choice converges and matches the upstream FP64 BSE to 1e-11 relative.
+kernel choice (including the tensor-core trailing tiles) converges and, refined to 1e-12, matches the upstream
+FP64 BSE to 1e-11 relative.
 """
 
 import numpy as np
@@ -40,7 +41,8 @@ def test_mixed_choices_match_upstream(name):
     from dgamore_b200.pipeline import LadderPass
 
     inp, ref = load_golden(name)
-    lp = LadderPass(inp, keep_intermediates=False, precision="mixed")
+    # X is checked to 1e-11, so the refinement runs to a tolerance below that
+    lp = LadderPass(inp, keep_intermediates=False, precision="mixed", refine_tol=1e-12)
     lp.pre_bse()
     for choice in CANDIDATES["mixed"]:
         if scratch_bytes(lp, lp.n_items, 1, choice) == 0:
