@@ -44,12 +44,13 @@ constexpr int P_TILE_UNROLL = DGA_PANEL_TILE_UNROLL;  // unroll of the trailing 
 // ----------------------------------------------------------------------------------------------
 // The panel region also holds the solve's right-hand sides (up to 16 x ldp complex64) followed by the residual's
 // staging ([32][16] and [16][16] complex128), so small ldp need more than the panel itself.
-// With the tensor-core trailing update (tc) the region also holds the four 32 KB TF32 operand buffers of a tile.
+// With the tensor-core trailing update (tc) the region also holds the six 32 KB TF32 operand buffers (A_hi, A_lo
+// for two tiles in flight, B_hi, B_lo of the strip).
 __host__ __device__ inline size_t panel_region_bytes(int ldp, bool tc = false) {
   const size_t panel = (size_t)ldp * PNB * sizeof(float2);
   const size_t solve = (size_t)16 * ldp * sizeof(float2) + 32 + (32 * 16 + 16 * 16) * sizeof(double2);
   size_t r = panel > solve ? panel : solve;
-  if (tc && r < 4 * (size_t)TC_OPERAND_FLOATS * sizeof(float)) r = 4 * (size_t)TC_OPERAND_FLOATS * sizeof(float);
+  if (tc && r < 6 * (size_t)TC_OPERAND_FLOATS * sizeof(float)) r = 6 * (size_t)TC_OPERAND_FLOATS * sizeof(float);
   return (r + 127) & ~(size_t)127;
 }
 constexpr size_t P_FIXED = 16 * sizeof(double)                 // redd
@@ -58,7 +59,7 @@ constexpr size_t P_FIXED = 16 * sizeof(double)                 // redd
                            + 16 * sizeof(float) + 16 * sizeof(int)  // red_val, red_idx
                            + 64 * sizeof(int) * 2              // s_row, s_cont
                            + 4 * sizeof(int)                   // misc
-                           + 16;                               // TMEM address + completion barrier
+                           + 32;                               // two completion barriers + TMEM address
 __host__ __device__ inline size_t panel_smem_bytes(int ldp, bool tc = false) {
   return panel_region_bytes(ldp, tc) + P_FIXED + sizeof(int) * (size_t)ldp;
 }
@@ -73,8 +74,8 @@ struct PanelSmem {
   int* s_row;   // [64] rows touched by the panel's interchanges: slots 0..31 the panel rows, 32.. the others
   int* s_cont;  // [64] old row whose content ends up in s_row[slot]
   int* misc;    // [0] rows below the panel that receive another row, [1] status bits, [2] tensor-core wait failure
-  uint64_t* bar;    // completion barrier of the tensor-core tile
-  uint32_t* tslot;  // TMEM address of the tile accumulator
+  uint64_t* bar;    // [2] completion barriers of the two tensor-core tiles in flight
+  uint32_t* tslot;  // TMEM address of the two tile accumulators
   int* piv;     // [ldp] row interchanged with row j
   int ldp;
 
@@ -85,9 +86,9 @@ struct PanelSmem {
     redd = reinterpret_cast<double*>(p);
     p += 16 * sizeof(double);
     bar = reinterpret_cast<uint64_t*>(p);
-    p += 8;
+    p += 16;
     tslot = reinterpret_cast<uint32_t*>(p);
-    p += 8;
+    p += 16;
     L11i = reinterpret_cast<float2*>(p);
     p += PNB * (PNB + 1) * sizeof(float2);
     Us = reinterpret_cast<float2*>(p);
@@ -322,7 +323,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
         }
         __syncthreads();  // every old value of the touched rows is read before any is overwritten
         const int tgt_row = lane < n_tgt ? s.s_row[32 + lane] : 0;
-        float* b_hi = reinterpret_cast<float*>(s.P) + 2 * TC_OPERAND_FLOATS;
+        float* b_hi = reinterpret_cast<float*>(s.P) + 4 * TC_OPERAND_FLOATS;  // after the two tiles' A buffers
         float* b_lo = b_hi + TC_OPERAND_FLOATS;
 #pragma unroll
         for (int q = 0; q < PTN / PW; ++q) {
@@ -345,16 +346,22 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
       }
       __syncthreads();
       if (TC) {
-        // trailing tiles of the strip on the tensor cores, 128 rows x 64 complex columns per tile
-        float* a_hi = reinterpret_cast<float*>(s.P);
-        float* a_lo = a_hi + TC_OPERAND_FLOATS;
-        const float* b_hi = a_lo + TC_OPERAND_FLOATS;
+        // trailing tiles of the strip on the tensor cores, 128 rows x 64 complex columns per tile, two tiles in
+        // flight: while the MMAs of tile i run, the threads stage tile i + 1 (L21 rows into the other A buffers,
+        // C into the other TMEM accumulator), then wait for tile i and write it back.
+        float* const a_base = reinterpret_cast<float*>(s.P);
+        const float* b_hi = a_base + 4 * TC_OPERAND_FLOATS;
         const float* b_lo = b_hi + TC_OPERAND_FLOATS;
         const int lane = tid & 31, warp = tid >> 5;
         const uint32_t tbase = *s.tslot;
         const uint32_t taddr = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + 32 * (warp >> 2);
-        for (int rt = k1; rt < N; rt += TC_M) {
-          {  // L21 rows rt .. rt + 127 (written back with the panel) -> A_hi / A_lo; thread: a row, 4 chunks of 2 k
+        const int ntiles = (N - k1 + TC_M - 1) / TC_M;
+        float v[32];
+        auto stage = [&](int i) {
+          const int rt = k1 + i * TC_M;
+          float* ah = a_base + (i & 1) * 2 * TC_OPERAND_FLOATS;
+          float* al = ah + TC_OPERAND_FLOATS;
+          {  // L21 rows rt .. rt + 127 (written back with the panel): a thread takes a row and 4 chunks of 2 k
             const int row = tid & (TC_M - 1), cg = tid >> 7;
             const int r = rt + row;
             const bool rok = r < N;
@@ -365,12 +372,11 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
               const float2 x1 = rok ? A[(size_t)(k0 + 2 * ch + 1) * N + r] : make_float2(0.f, 0.f);
               const float4 h = make_float4(tf32_hi(x0.x), tf32_hi(x0.y), tf32_hi(x1.x), tf32_hi(x1.y));
               const float4 l = make_float4(x0.x - h.x, x0.y - h.y, x1.x - h.z, x1.y - h.w);
-              *reinterpret_cast<float4*>(a_hi + tc_off(row, 4 * ch)) = h;
-              *reinterpret_cast<float4*>(a_lo + tc_off(row, 4 * ch)) = l;
+              *reinterpret_cast<float4*>(ah + tc_off(row, 4 * ch)) = h;
+              *reinterpret_cast<float4*>(al + tc_off(row, 4 * ch)) = l;
             }
           }
           const int r = rt + 32 * (warp & 3) + lane, cb = cs + 16 * (warp >> 2);
-          float v[32];
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int c = cb + j;
@@ -378,22 +384,28 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
             v[2 * j] = x.x;
             v[2 * j + 1] = x.y;
           }
-          tmem_st32(taddr, v);
+          tmem_st32(taddr + (i & 1) * TC_NR, v);
           tmem_wait_st();
           tc_fence_async_smem();
-          tc_fence_before();
-          __syncthreads();
-          const bool live = s.misc[2] == 0;  // a CTA whose tensor-core wait ever ran out issues no more tiles
+        };
+        bool live = true;
+        auto issue = [&](int i) {  // after a barrier: every operand and accumulator of tile i is in place
+          live = s.misc[2] == 0;   // a CTA whose tensor-core wait ever ran out issues no more tiles
           if (live && tid == 0) {
             tc_fence_after();
-            tc_issue_tile(tbase, a_hi, a_lo, b_hi, b_lo, s.bar);
+            const float* ah = a_base + (i & 1) * 2 * TC_OPERAND_FLOATS;
+            tc_issue_tile(tbase + (i & 1) * TC_NR, ah, ah + TC_OPERAND_FLOATS, b_hi, b_lo, s.bar + (i & 1));
           }
-          const bool ok = live && mbar_wait(s.bar, parity);
-          if (live) parity ^= 1u;
+        };
+        auto finish = [&](int i) {
+          const int bsel = i & 1;
+          const bool ok = live && mbar_wait(s.bar + bsel, (parity >> bsel) & 1u);
+          if (live) parity ^= 1u << bsel;
           tc_fence_after();
           if (ok) {
-            tmem_ld32(taddr, v);
+            tmem_ld32(taddr + bsel * TC_NR, v);
             tmem_wait_ld();
+            const int r = k1 + i * TC_M + 32 * (warp & 3) + lane, cb = cs + 16 * (warp >> 2);
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const int c = cb + j;
@@ -402,8 +414,21 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
           } else {
             s.misc[2] = 1;
           }
-          tc_fence_before();
+        };
+        stage(0);
+        tc_fence_before();
+        __syncthreads();
+        issue(0);
+        for (int i = 0; i < ntiles; ++i) {
+          if (i + 1 < ntiles) stage(i + 1);
+          finish(i);
+          if (i + 1 < ntiles) {
+            tc_fence_before();
+            __syncthreads();
+            issue(i + 1);
+          }
         }
+        tc_fence_before();
       } else {
       // trailing tiles of the strip, 128 x 64: thread (ty, tx) owns rows rt + 2ty + {0,1} + {0,64} and columns
         // cs + 2tx + {0,1} + {0,32} (row pairs and column pairs move as one 16-byte access; N is even), with the
@@ -673,15 +698,18 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
   return st;
 }
 
-// TMEM for the tensor-core tiles: one warp allocates 128 columns (the 128 x 128 fp32 accumulator) for the CTA's
-// lifetime; the completion barrier is initialised once.  At exit, a CTA whose wait ever ran out waits once more
-// (bounded) for its last tile before the columns are freed.
+// TMEM for the tensor-core tiles: one warp allocates 256 columns (two 128 x 128 fp32 accumulators, one per tile in
+// flight) for the CTA's lifetime; the two completion barriers are initialised once.  At exit, a CTA whose wait
+// ever ran out waits once more (bounded) for each tile still in flight before the columns are freed.
 template <bool TC>
 __device__ void panel_kernel_begin(PanelSmem& s) {
   if (threadIdx.x == 0) s.misc[2] = 0;
   if (TC) {
-    if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, TC_NR);
-    if (threadIdx.x == 0) mbar_init(s.bar);
+    if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, 2 * TC_NR);
+    if (threadIdx.x == 0) {
+      mbar_init(s.bar);
+      mbar_init(s.bar + 1);
+    }
     tc_fence_before();
   }
   __syncthreads();
@@ -693,8 +721,11 @@ __device__ void panel_kernel_end(PanelSmem& s, uint32_t parity) {
   if (!TC) return;
   tc_fence_before();
   __syncthreads();
-  if (s.misc[2]) mbar_wait(s.bar, parity ^ 1u);
-  if ((threadIdx.x >> 5) == 0) tc_dealloc(*s.tslot, TC_NR);
+  if (s.misc[2]) {  // a wait ran out: give each tile still in flight one more bounded wait before freeing TMEM
+    mbar_wait(s.bar, (parity & 1u) ^ 1u);
+    mbar_wait(s.bar + 1, ((parity >> 1) & 1u) ^ 1u);
+  }
+  if ((threadIdx.x >> 5) == 0) tc_dealloc(*s.tslot, 2 * TC_NR);
 }
 
 template <int NR, bool TC>
