@@ -323,28 +323,34 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
         }
         __syncthreads();  // every old value of the touched rows is read before any is overwritten
         const int tgt_row = lane < n_tgt ? s.s_row[32 + lane] : 0;
-        float* b_hi = reinterpret_cast<float*>(s.P) + 4 * TC_OPERAND_FLOATS;  // after the two tiles' A buffers
-        float* b_lo = b_hi + TC_OPERAND_FLOATS;
 #pragma unroll
         for (int q = 0; q < PTN / PW; ++q) {
           const int c = warp + PW * q;
           float2* colw = A + (size_t)(cs + c) * N;
           const bool act = c < cw && lane < nb;
           if (act) colw[k0 + lane] = u[q];
-          const float2 uq = act ? u[q] : make_float2(0.f, 0.f);
-          if (TC) {
-            // B[2k + t][2c + s] of the real product (tc_tile.cuh), k = lane, stored K-major by column 2c + s
-            tc_store_split(b_hi, b_lo, tc_off(2 * c, 2 * lane), uq.x);
-            tc_store_split(b_hi, b_lo, tc_off(2 * c, 2 * lane + 1), -uq.y);
-            tc_store_split(b_hi, b_lo, tc_off(2 * c + 1, 2 * lane), uq.y);
-            tc_store_split(b_hi, b_lo, tc_off(2 * c + 1, 2 * lane + 1), uq.x);
-          } else {
-            s.Us[lane * PTN + c] = uq;
-          }
+          s.Us[lane * PTN + c] = act ? u[q] : make_float2(0.f, 0.f);
           if (c < cw && lane < n_tgt) colw[tgt_row] = tv[q];
         }
       }
       __syncthreads();
+      if (TC) {
+        // U12 strip -> the B operand of the real product (tc_tile.cuh), split into TF32 pairs: row 2c + s of B
+        // (K-major) holds, for k = 2j, 2j + 1, the four reals (Re U, -Im U) (s = 0) or (Im U, Re U) (s = 1);
+        // a thread writes one 16-byte chunk, consecutive threads consecutive rows of a core matrix.
+        float* b_hi = reinterpret_cast<float*>(s.P) + 4 * TC_OPERAND_FLOATS;  // after the two tiles' A buffers
+        float* b_lo = b_hi + TC_OPERAND_FLOATS;
+#pragma unroll
+        for (int e = tid; e < TC_NR * (TC_KR / 4); e += PT) {
+          const int row = e & (TC_NR - 1), j = e >> 7;  // B row (2c + s) and 16-byte K chunk (k = 2j, 2j + 1)
+          const int c = row >> 1, sgn = row & 1;
+          const float2 u0 = s.Us[(2 * j) * PTN + c], u1 = s.Us[(2 * j + 1) * PTN + c];
+          const float4 x = sgn ? make_float4(u0.y, u0.x, u1.y, u1.x) : make_float4(u0.x, -u0.y, u1.x, -u1.y);
+          const float4 h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+          *reinterpret_cast<float4*>(b_hi + tc_off(row, 4 * j)) = h;
+          *reinterpret_cast<float4*>(b_lo + tc_off(row, 4 * j)) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+        }
+      }
       if (TC) {
         // trailing tiles of the strip on the tensor cores, 128 rows x 64 complex columns per tile, two tiles in
         // flight: while the MMAs of tile i run, the threads stage tile i + 1 (L21 rows into the other A buffers,
