@@ -619,24 +619,49 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
   float2* A = reinterpret_cast<float2*>(slot);
   double2* Y = reinterpret_cast<double2*>(slot + (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255));
   double2* Rb = Y + (size_t)N * NR;
-  // ---- form A in complex64 (8 independent elements per thread in flight) ----
+  // ---- form A in complex64: thread t owns rows t and t + PT (N <= 2 PT here), 8 columns of loads in flight ----
+  // element (i, j) as StructuredSource::element: (chi0^-1 [block diagonal] + Gamma / beta^2) + (-(U + V) / beta^2)
   {
-    const long long NN = (long long)N * N;
-    for (long long e0 = 0; e0 < NN; e0 += 8LL * PT) {
-      double2 v[8];
+    const double2* gam = src.gamma_cm + ((size_t)(wi.ch * src.W + wi.w) * N) * N;
+    const double2* c0 = src.chi0_inv + ((size_t)wi.q * src.W + wi.w) * nv * NR * NR;
+    const double2* uvq = src.uv + ((size_t)wi.ch * src.Q + wi.q) * NR * NR;
+    const double ib2 = src.inv_beta2;
+    int ri[2], pr[2], vr[2];
+    bool rok[2];
+#pragma unroll
+    for (int a2 = 0; a2 < 2; ++a2) {
+      ri[a2] = tid + a2 * PT;
+      rok[a2] = ri[a2] < N;
+      pr[a2] = rok[a2] ? ri[a2] / nv : 0;
+      vr[a2] = rok[a2] ? ri[a2] - pr[a2] * nv : 0;
+    }
+    for (int j0 = 0; j0 < N; j0 += 8) {
+      double2 g[2][8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2)
+          g[a2][u] = (rok[a2] && j0 + u < N) ? gam[(size_t)(j0 + u) * N + ri[a2]] : make_double2(0.0, 0.0);
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        const long long e = e0 + (long long)u * PT + tid;
-        if (e < NN) {
-          const int j = (int)(e / N), i = (int)(e - (long long)j * N);
-          const int pr = i / nv, vr = i - pr * nv, pc = j / nv, vc = j - pc * nv;
-          v[u] = src.element(wi.ch, wi.q, wi.w, N, i, j, pr, vr, pc, vc);
+        const int j = j0 + u;
+        if (j >= N) break;
+        const int pc = j / nv, vc = j - pc * nv;
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2) {
+          if (!rok[a2]) continue;
+          const double2 uu = uvq[pr[a2] * NR + pc];
+          double re = __dmul_rn(g[a2][u].x, ib2);
+          double im = __dmul_rn(g[a2][u].y, ib2);
+          if (vr[a2] == vc) {
+            const double2 c = c0[(size_t)vr[a2] * NR * NR + pr[a2] * NR + pc];
+            re = __dadd_rn(c.x, re);
+            im = __dadd_rn(c.y, im);
+          }
+          re = __dadd_rn(re, -__dmul_rn(uu.x, ib2));
+          im = __dadd_rn(im, -__dmul_rn(uu.y, ib2));
+          A[(size_t)j * N + ri[a2]] = make_float2((float)re, (float)im);
         }
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const long long e = e0 + (long long)u * PT + tid;
-        if (e < NN) A[e] = make_float2((float)v[u].x, (float)v[u].y);
       }
     }
   }
