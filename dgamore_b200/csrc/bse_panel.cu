@@ -31,6 +31,7 @@ namespace dga {
 constexpr int PT = 512;       // threads per CTA
 constexpr int PW = PT / 32;   // warps
 constexpr int PNB = 32;       // panel width
+constexpr int PSB = 8;        // sub-panel width inside the panel factorisation
 constexpr int PTM = 128;      // trailing tile rows
 constexpr int PTN = 64;       // trailing strip columns
 constexpr int P_MAX_SMEM = 232448;  // 227 KB opt-in shared memory per block on sm_100
@@ -163,14 +164,17 @@ __device__ bool panel_factor(PanelSmem& s, int m, int nb, int k0) {
     const bool zero = (d.x == 0.f && d.y == 0.f);
     singular |= zero;
     const float2 rinv = zero ? make_float2(0.f, 0.f) : crecip(d);
+    // rank-1 update restricted to the current 8-column sub-panel; the columns to its right are brought up to
+    // date by one triangular solve and one rank-8 update when the sub-panel is complete
     const int c1 = jj + 1;
+    const int cend = min(nb, (jj / PSB + 1) * PSB);
     float best = -1.f;
     int bidx = 0x7fffffff;
     for (int r = max(r0, c1) + lane; r < r1; r += 32) {
       float2 l = P[(size_t)jj * ldp + r];
       if (!zero) l = cmul(l, rinv);
       P[(size_t)jj * ldp + r] = l;
-      if (c1 < nb) {
+      if (c1 < cend) {
         float2 v = P[(size_t)c1 * ldp + r];
         cfms(v, l, P[(size_t)c1 * ldp + jj]);
         P[(size_t)c1 * ldp + r] = v;
@@ -179,10 +183,52 @@ __device__ bool panel_factor(PanelSmem& s, int m, int nb, int k0) {
           best = a;
           bidx = r;
         }
-        for (int c = c1 + 1; c < nb; ++c) {
+        for (int c = c1 + 1; c < cend; ++c) {
           float2 x = P[(size_t)c * ldp + r];
           cfms(x, l, P[(size_t)c * ldp + jj]);
           P[(size_t)c * ldp + r] = x;
+        }
+      }
+    }
+    if (c1 == cend && cend < nb) {
+      const int cb = cend - PSB;
+      __syncthreads();  // the sub-panel's multipliers are final
+      // U block rows cb .. cend-1 of the columns to the right: unit lower solve with the sub-panel's L11
+      for (int c = cend + tid; c < nb; c += PT) {
+        float2* col = P + (size_t)c * ldp + cb;
+        float2 x[PSB];
+#pragma unroll
+        for (int k = 0; k < PSB; ++k) x[k] = col[k];
+#pragma unroll
+        for (int k = 1; k < PSB; ++k)
+#pragma unroll
+          for (int q = 0; q < k; ++q) cfms(x[k], P[(size_t)(cb + q) * ldp + cb + k], x[q]);
+#pragma unroll
+        for (int k = 0; k < PSB; ++k) col[k] = x[k];
+      }
+      __syncthreads();
+      // rank-8 update of the rows below, with the next column's pivot candidate
+      for (int r = max(r0, cend) + lane; r < r1; r += 32) {
+        float2 l[PSB];
+#pragma unroll
+        for (int k = 0; k < PSB; ++k) l[k] = P[(size_t)(cb + k) * ldp + r];
+        for (int c = cend; c < nb; ++c) {
+          const float4* u4 = reinterpret_cast<const float4*>(P + (size_t)c * ldp + cb);
+          float2 v = P[(size_t)c * ldp + r];
+#pragma unroll
+          for (int k2 = 0; k2 < PSB / 2; ++k2) {
+            const float4 uu = u4[k2];
+            cfms(v, l[2 * k2], make_float2(uu.x, uu.y));
+            cfms(v, l[2 * k2 + 1], make_float2(uu.z, uu.w));
+          }
+          P[(size_t)c * ldp + r] = v;
+          if (c == cend) {
+            const float a = cabs1(v);
+            if (a > best) {
+              best = a;
+              bidx = r;
+            }
+          }
         }
       }
     }
