@@ -295,9 +295,11 @@ DRAM_BYTES_PER_ITEM = {
 def kernel_name(lp) -> str:
     if lp.precision == "fp64":
         return "bse_solve_sum_fp64_kernel"
-    kernel = lp.tuning.kernel if lp.tuning is not None else 0
+    kernel = lp.tuning.kernel if lp.tuning is not None else (3 if lp.sh.N >= 320 else 2)
     if kernel == 2:
         return "bse_solve_sum_mixed_kernel"
+    if kernel == 3:
+        return "bse_panel_mixed_kernel<TC> (tcgen05 trailing tiles)"
     return "bse_panel_mixed_kernel"
 
 

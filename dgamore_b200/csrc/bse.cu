@@ -1050,6 +1050,16 @@ static size_t mixed_smem_bytes(int N, int n2) { return mixed_colsum_offset(N) + 
 static size_t mixed_slot_bytes(int N, int n2) {
   return (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255) + 2 * (size_t)N * n2 * sizeof(double2);
 }
+// Default launch of the mixed form: below N = 320 the 128-thread kernel keeps several items per SM in flight and
+// wins; above it the shared-memory-panel kernel with tensor-core trailing tiles (3), if its shared memory fits,
+// else the panel kernel with FP32 tiles (1), else the 128-thread kernel (2).
+static int default_mixed_kernel(int N, int n2) {
+  if (N < 320) return 2;
+  if (dga_panel_supported(N, n2, true)) return 3;
+  if (dga_panel_supported(N, n2)) return 1;
+  return 2;
+}
+
 static int mixed_grid(int n_items, size_t smem) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -1064,7 +1074,8 @@ extern "C" {
 // blocks per resident CTA.
 size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items) {
   if (N <= 0 || n2 <= 0 || n_items <= 0) return 0;
-  if (dga_panel_supported(N, n2)) return (size_t)dga_panel_grid(n2, N, n_items) * dga_panel_slot_bytes(N, n2);
+  const int kernel = default_mixed_kernel(N, n2);
+  if (kernel != 2) return (size_t)dga_panel_grid(n2, N, n_items, kernel == 3) * dga_panel_slot_bytes(N, n2);
   const size_t smem = mixed_smem_bytes(N, n2);
   return (size_t)mixed_grid(n_items, smem) * mixed_slot_bytes(N, n2);
 }
@@ -1086,9 +1097,10 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
     dga_set_error("dga_bse_solve_sum_mixed_c128: null pointer argument");
     return DGA_ERR_ARG;
   }
-  const bool panel = dga_panel_supported(N, n2);
+  const int kernel = default_mixed_kernel(N, n2);
+  const bool panel = kernel != 2;
   const size_t smem = mixed_smem_bytes(N, n2);
-  const int grid = panel ? dga_panel_grid(n2, N, n_items) : mixed_grid(n_items, smem);
+  const int grid = panel ? dga_panel_grid(n2, N, n_items, kernel == 3) : mixed_grid(n_items, smem);
   const size_t slot = panel ? dga_panel_slot_bytes(N, n2) : mixed_slot_bytes(N, n2);
   if (scratch_bytes < (size_t)grid * slot) {
     dga_set_error("dga_bse_solve_sum_mixed_c128: scratch too small (%zu < %zu)", scratch_bytes, (size_t)grid * slot);
@@ -1107,7 +1119,7 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
     // N fits the shared-memory panel: one 512-thread CTA per SM (bse_panel.cu)
     cudaError_t err = dga_panel_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta,
                                        max_iter, tol, (double2*)out, status, iters, (unsigned char*)scratch, slot,
-                                       stream);
+                                       stream, kernel == 3);
     if (err != cudaSuccess) {
       dga_set_error("dga_bse_solve_sum_mixed_c128: launch failed: %s", cudaGetErrorString(err));
       return DGA_ERR_LAUNCH;
@@ -1216,22 +1228,29 @@ int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_
 // ------------------------------------------------------------------------------------------------
 // Heterogeneous batch (host side)
 // ------------------------------------------------------------------------------------------------
-static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot,
-                       bool* panel) {
+// Launch geometry of a batch.  In the mixed form every request must have the same default kernel as when it runs
+// alone (default_mixed_kernel), so that a request's results are the same in a batch and alone; *kernel receives
+// it (1, 3: shared-memory panel, 2: 128-thread kernel; always 2 in FP64).  Returns false for an invalid batch.
+static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot, int* kernel) {
   *n_max = 0;
   *slot = 0;
-  *panel = false;
+  *kernel = 2;
   if (n_prob <= 0) return false;
-  for (int p = 0; p < n_prob; ++p) {
-    const int n2 = probs[p].n_orb * probs[p].n_orb, N = n2 * 2 * probs[p].niv;
-    if (probs[p].n_orb != probs[0].n_orb || !supported_rhs(n2) || probs[p].niv <= 0 || N > BSE_MAX_N) return false;
-    if (N > *n_max) *n_max = N;
-  }
   const int n2 = probs[0].n_orb * probs[0].n_orb;
-  *panel = mixed && dga_panel_supported(*n_max, n2);
   for (int p = 0; p < n_prob; ++p) {
     const int N = n2 * 2 * probs[p].niv;
-    const size_t sl = *panel ? dga_panel_slot_bytes(N, n2)
+    if (probs[p].n_orb != probs[0].n_orb || !supported_rhs(n2) || probs[p].niv <= 0 || N > BSE_MAX_N) return false;
+    if (mixed) {
+      const int k = default_mixed_kernel(N, n2);
+      if (p == 0) *kernel = k;
+      if (k != *kernel) return false;
+    }
+    if (N > *n_max) *n_max = N;
+  }
+  const bool panel = *kernel != 2;
+  for (int p = 0; p < n_prob; ++p) {
+    const int N = n2 * 2 * probs[p].niv;
+    const size_t sl = panel ? dga_panel_slot_bytes(N, n2)
                       : mixed ? mixed_slot_bytes(N, n2)
                               : ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
     if (sl > *slot) *slot = sl;
@@ -1264,14 +1283,14 @@ extern "C" {
 
 // Scratch bytes of dga_bse_solve_sum_batch_c128 (probs is a HOST array here); 0 for an invalid batch.
 size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int n_items, int mode) {
-  int n_max = 0;
+  int n_max = 0, kernel = 2;
   size_t slot = 0;
-  bool panel = false;
   const int mixed = mode == 1;
-  if (!probs || n_items <= 0 || mode < 0 || mode > 2 || !batch_dims(probs, n_prob, mixed, &n_max, &slot, &panel))
+  if (!probs || n_items <= 0 || mode < 0 || mode > 2 || !batch_dims(probs, n_prob, mixed, &n_max, &slot, &kernel))
     return 0;
   const int n2 = probs[0].n_orb * probs[0].n_orb;
-  if (panel) return (size_t)dga_panel_batch_grid(n2, n_max, n_items) * slot;
+  const bool panel = kernel != 2;
+  if (panel) return (size_t)dga_panel_batch_grid(n2, n_max, n_items, kernel == 3) * slot;
   return (size_t)batch_grid_any(mixed, n2, n_items, batch_smem(n_max, n2, mixed)) * slot;
 }
 
@@ -1285,13 +1304,13 @@ size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int
 int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* probs_dev, int n_prob, const int* work,
                                  int n_items, int mode, int max_iter, double tol, int* status, int* iters,
                                  void* scratch, size_t scratch_bytes, cudaStream_t stream) {
-  int n_max = 0;
+  int n_max = 0, kernel = 2;
   size_t slot = 0;
-  bool panel = false;
   const int mixed = mode == 1;
   if (!probs_host || !probs_dev || !work || !scratch || !status || n_items <= 0 || max_iter < 0 || mode < 0 ||
-      mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot, &panel)) {
-    dga_set_error("dga_bse_solve_sum_batch_c128: invalid arguments (problems must share n_orb in {1,2,3,4})");
+      mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot, &kernel)) {
+    dga_set_error("dga_bse_solve_sum_batch_c128: invalid arguments (problems must share n_orb in {1,2,3,4}, and in "
+                  "the mixed form all have N below 320 or all from 320 up)");
     return DGA_ERR_ARG;
   }
   for (int p = 0; p < n_prob; ++p) {
@@ -1303,7 +1322,8 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   }
   const int n2 = probs_host[0].n_orb * probs_host[0].n_orb;
   const size_t smem = batch_smem(n_max, n2, mixed);
-  int grid = panel ? dga_panel_batch_grid(n2, n_max, n_items) : batch_grid_any(mixed, n2, n_items, smem);
+  const bool panel = kernel != 2;
+  int grid = panel ? dga_panel_batch_grid(n2, n_max, n_items, kernel == 3) : batch_grid_any(mixed, n2, n_items, smem);
   if (scratch_bytes < slot) {
     dga_set_error("dga_bse_solve_sum_batch_c128: scratch too small (%zu < one slot of %zu)", scratch_bytes, slot);
     return DGA_ERR_SCRATCH;
@@ -1315,7 +1335,7 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   unsigned char* sc = (unsigned char*)scratch;
   if (panel) {
     cudaError_t err = dga_panel_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
-                                             stream);
+                                             stream, kernel == 3);
     if (err != cudaSuccess) {
       dga_set_error("dga_bse_solve_sum_batch_c128: launch failed: %s", cudaGetErrorString(err));
       return DGA_ERR_LAUNCH;
@@ -1364,7 +1384,7 @@ static int tuned_kernel(int mixed, int N, int n2, const dga_bse_tuning* t) {
   const int k = t ? t->kernel : 0;
   if (k < 0 || k > 3) return -1;
   if (!mixed) return (k == 1 || k == 3) ? -1 : 2;
-  if (k == 0) return dga_panel_supported(N, n2) ? 1 : 2;
+  if (k == 0) return default_mixed_kernel(N, n2);
   if (k == 1 && !dga_panel_supported(N, n2)) return -1;
   if (k == 3 && !dga_panel_supported(N, n2, true)) return -1;
   return k;

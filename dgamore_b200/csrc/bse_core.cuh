@@ -181,11 +181,11 @@ __device__ void structured_residual_permuted(const StructuredSource& src, int ch
 bool dga_panel_supported(int N, int n2, bool tc = false);
 size_t dga_panel_slot_bytes(int N, int n2);
 int dga_panel_grid(int n2, int N, int n_items, bool tc = false);
-int dga_panel_batch_grid(int n2, int n_max, int n_items);
+int dga_panel_batch_grid(int n2, int n_max, int n_items, bool tc = false);
 cudaError_t dga_panel_launch(int grid, const dga::StructuredSource& src, const dga::WorkItem* work, int n_items, int N,
                              int n2, int nv, int W, int Q, double beta, int max_iter, double tol, double2* out,
                              int* status, int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
                              bool tc = false);
 cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const dga::MultiItem* work,
                                    int n_items, int n_max, int max_iter, double tol, int* status, int* iters,
-                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream);
+                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc = false);

@@ -830,16 +830,16 @@ __global__ void __launch_bounds__(PT, 1)
 }
 
 // Heterogeneous batch (requests of one orbital count): see bse_multi_kernel in bse.cu.
-template <int NR>
+template <int NR, bool TC>
 __global__ void __launch_bounds__(PT, 1)
     bse_panel_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work,
                            int n_items, int n_max, int max_iter, double tol, int* __restrict__ status,
                            int* __restrict__ iters, unsigned char* __restrict__ scratch, size_t slot_bytes) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  PanelSmem s(smem_raw, n_max, false);
+  PanelSmem s(smem_raw, n_max, TC);
   unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
   uint32_t parity = 0;
-  panel_kernel_begin<false>(s);
+  panel_kernel_begin<TC>(s);
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const MultiItem mi = work[item];
     const dga_bse_problem d = probs[mi.prob];
@@ -856,12 +856,13 @@ __global__ void __launch_bounds__(PT, 1)
     const WorkItem wi{mi.ch, mi.q, mi.w};
     double2* o = (double2*)d.out + (((size_t)wi.ch * src.Q + wi.q) * src.W + wi.w) * (size_t)N * NR;
     int it = 0;
-    const int st = solve_item_panel<NR, false>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, &it, parity);
+    const int st = solve_item_panel<NR, TC>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, &it, parity);
     if (threadIdx.x == 0) {
       status[item] = st;
       if (iters) iters[item] = it;
     }
   }
+  panel_kernel_end<TC>(s, parity);
 }
 
 }  // namespace dga
@@ -909,14 +910,19 @@ int dga_panel_grid(int n2, int N, int n_items, bool tc) {
   return tc ? panel_grid_tc<true>(n2, N, n_items) : panel_grid_tc<false>(n2, N, n_items);
 }
 
-int dga_panel_batch_grid(int n2, int n_max, int n_items) {
-  const size_t smem = panel_smem_bytes(n_max, false);
+template <bool TC>
+static int panel_batch_grid_tc(int n2, int n_max, int n_items) {
+  const size_t smem = panel_smem_bytes(n_max, TC);
   switch (n2) {
-    case 1: return panel_grid_for(bse_panel_multi_kernel<1>, n_items, smem);
-    case 4: return panel_grid_for(bse_panel_multi_kernel<4>, n_items, smem);
-    case 9: return panel_grid_for(bse_panel_multi_kernel<9>, n_items, smem);
-    default: return panel_grid_for(bse_panel_multi_kernel<16>, n_items, smem);
+    case 1: return panel_grid_for(bse_panel_multi_kernel<1, TC>, n_items, smem);
+    case 4: return panel_grid_for(bse_panel_multi_kernel<4, TC>, n_items, smem);
+    case 9: return panel_grid_for(bse_panel_multi_kernel<9, TC>, n_items, smem);
+    default: return panel_grid_for(bse_panel_multi_kernel<16, TC>, n_items, smem);
   }
+}
+
+int dga_panel_batch_grid(int n2, int n_max, int n_items, bool tc) {
+  return tc ? panel_batch_grid_tc<true>(n2, n_max, n_items) : panel_batch_grid_tc<false>(n2, n_max, n_items);
 }
 
 template <bool TC>
@@ -950,14 +956,15 @@ cudaError_t dga_panel_launch(int grid, const StructuredSource& src, const WorkIt
   return cudaGetLastError();
 }
 
-cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
-                                   int n_max, int max_iter, double tol, int* status, int* iters,
-                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream) {
-  const size_t smem = panel_smem_bytes(n_max, false);
-#define DGA_PANEL_CASE(R)                                                                                       \
-  case R:                                                                                                       \
-    bse_panel_multi_kernel<R><<<grid, PT, smem, stream>>>(probs, work, n_items, n_max, max_iter, tol, status, \
-                                                          iters, scratch, slot_bytes);                         \
+template <bool TC>
+static void panel_batch_launch_tc(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
+                                  int n_max, int max_iter, double tol, int* status, int* iters, unsigned char* scratch,
+                                  size_t slot_bytes, cudaStream_t stream) {
+  const size_t smem = panel_smem_bytes(n_max, TC);
+#define DGA_PANEL_CASE(R)                                                                                           \
+  case R:                                                                                                           \
+    bse_panel_multi_kernel<R, TC><<<grid, PT, smem, stream>>>(probs, work, n_items, n_max, max_iter, tol, status, \
+                                                              iters, scratch, slot_bytes);                         \
     break;
   switch (n2) {
     DGA_PANEL_CASE(1)
@@ -966,5 +973,16 @@ cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* prob
     DGA_PANEL_CASE(16)
   }
 #undef DGA_PANEL_CASE
+}
+
+cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
+                                   int n_max, int max_iter, double tol, int* status, int* iters,
+                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc) {
+  if (tc)
+    panel_batch_launch_tc<true>(grid, n2, probs, work, n_items, n_max, max_iter, tol, status, iters, scratch,
+                                slot_bytes, stream);
+  else
+    panel_batch_launch_tc<false>(grid, n2, probs, work, n_items, n_max, max_iter, tol, status, iters, scratch,
+                                 slot_bytes, stream);
   return cudaGetLastError();
 }

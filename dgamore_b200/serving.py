@@ -9,7 +9,8 @@ temperatures, interactions -- on one GPU is done here the way LLM servers batch 
   (``pipeline.estimate_device_bytes``, computed from its shapes before anything is allocated) fit the
   server's budget next to the requests already running; otherwise it waits in FIFO order.
 * **One persistent launch per iteration.**  Every iteration gathers BSE work items (request, channel, q, w)
-  from all running requests of the same orbital count into one ``dga_bse_solve_sum_batch_c128`` launch.
+  from all running requests of the same launch class (orbital count; in the mixed form also the side of
+  ``PANEL_MIN_N`` the compound size is on) into one ``dga_bse_solve_sum_batch_c128`` launch.
   Items are taken round-robin, a bounded number per request per iteration (``items_per_request``), so a
   small request that arrives while a large one runs finishes in a few iterations instead of waiting for
   the large one to drain (the chunked scheduling of long prompts in LLM serving).
@@ -45,6 +46,17 @@ def _stream() -> ctypes.c_void_p:
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+# Compound size from which the mixed form runs the shared-memory-panel kernel when alone (the library's default
+# rule); a batch launch serves requests on one side of it only, so each gets the kernel it gets alone.
+PANEL_MIN_N = 320
+
+
+def launch_class(lp: LadderPass, precision: str) -> tuple:
+    """Requests of one class share a batch launch: orbital count, precision and, in the mixed form, the side of
+    PANEL_MIN_N their compound size is on."""
+    return (lp.sh.n_orb, precision, precision == "mixed" and lp.sh.N >= PANEL_MIN_N)
+
+
 def item_cost(sh: PassShapes) -> float:
     """Relative cost of one BSE item: the LU of an N x N matrix."""
     return float(sh.N) ** 3
@@ -59,7 +71,7 @@ def _descriptor(lp: LadderPass) -> BseProblem:
 
 
 class BseBatch:
-    """One launch over BSE items of several passes of the same orbital count.
+    """One launch over BSE items of several passes of the same launch class (``launch_class``).
 
     ``items`` is a list of (pass, item indices into ``pass.work``).  The launch writes each item's X into its
     own pass and its status word into ``pass.bse_status``; in mixed precision the items whose refinement did
@@ -75,8 +87,8 @@ class BseBatch:
             if id(lp) not in index:
                 index[id(lp)] = len(passes)
                 passes.append(lp)
-        if len({lp.sh.n_orb for lp in passes}) != 1:
-            raise ValueError("a batch launch needs passes of one orbital count; split the batch by n_orb")
+        if len({launch_class(lp, precision) for lp in passes}) != 1:
+            raise ValueError("a batch launch needs passes of one launch class (launch_class); split the batch")
         self.passes = passes
         self.precision = precision
         self.refine_max_iter = int(refine_max_iter)
@@ -130,10 +142,11 @@ class BseBatch:
 
 def solve_bse_batch(passes: list[LadderPass], precision: str = "fp64", scratch: torch.Tensor | None = None,
                     **kw) -> None:
-    """BSE of several whole passes (all their items), one launch per orbital count."""
-    groups: dict[int, list[LadderPass]] = {}
+    """BSE of several whole passes (all their items), one launch per launch class (orbital count, and in the
+    mixed form the side of PANEL_MIN_N)."""
+    groups: dict[tuple, list[LadderPass]] = {}
     for lp in passes:
-        groups.setdefault(lp.sh.n_orb, []).append(lp)
+        groups.setdefault(launch_class(lp, precision), []).append(lp)
     for group in groups.values():
         dev = group[0].dev
         batch = BseBatch([(lp, torch.arange(lp.n_items, device=dev)) for lp in group], precision, **kw)
@@ -267,8 +280,8 @@ class LadderServer:
             left = r.lp.n_items - r.cursor
             take = left if self.items_per_request is None else min(left, self.items_per_request)
             if take > 0:
-                groups.setdefault((r.lp.sh.n_orb, r.req.precision), []).append((r, take))
-        for (_, precision), members in groups.items():
+                groups.setdefault(launch_class(r.lp, r.req.precision), []).append((r, take))
+        for (_, precision, _), members in groups.items():
             items = []
             for r, take in members:
                 items.append((r.lp, torch.arange(r.cursor, r.cursor + take, device=self.dev)))

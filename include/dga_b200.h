@@ -83,9 +83,10 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
  * trailing updates, then FP64 iterative refinement -- residuals r = S - A Y with A formed in FP64 from Gamma_r,
  * chi0^-1 and U_r + V_r^q -- until the correction, or the error left after it estimated from the observed
  * contraction rho = |d_k|/|d_(k-1)| as |d_k| rho/(1-rho), is at most tol max|Y|, or max_iter corrections; items
- * that do not converge are flagged DGA_ITEM_NOCONVERGE.  Items with N up to about 790 run the shared-memory-panel
- * kernel (one 512-thread CTA per SM), larger ones the 128-thread kernel.  Replaces the same upstream functions
- * as dga_bse_solve_sum_c128.  iters: optional per-item number of corrections. */
+ * that do not converge are flagged DGA_ITEM_NOCONVERGE.  Items with 320 <= N <= about 790 run the
+ * shared-memory-panel kernel (one 512-thread CTA per SM) with tensor-core trailing tiles, the others the
+ * 128-thread kernel.  Replaces the same upstream functions as dga_bse_solve_sum_c128.  iters: optional per-item
+ * number of corrections. */
 size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items);
 int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
                                  const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
@@ -100,8 +101,8 @@ int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_c
                               dga_stream_t stream);
 
 /* Launch choices of the BSE solvers, the search space of the autotuner (dgamore_b200/autotune.py); no
- * counterpart in the upstream.  kernel: 0 = default (mixed form: the shared-memory-panel kernel when N fits,
- * else the 128-thread kernel; FP64: the 128-thread kernel), 1 = shared-memory-panel kernel (mixed form only,
+ * counterpart in the upstream.  kernel: 0 = default (mixed form: kernel 3 for 320 <= N when it fits, else the
+ * 128-thread kernel; FP64: the 128-thread kernel), 1 = shared-memory-panel kernel (mixed form only,
  * N up to about 790), 2 = 128-thread kernel, 3 = shared-memory-panel kernel whose trailing tiles run on the
  * tensor cores (tcgen05.mma kind::tf32 with a three-term split for FP32-level products, accumulators in tensor
  * memory; mixed form only); ctas_per_sm: CTAs per SM of the 128-thread kernel (0 = all that fit).  The choices
