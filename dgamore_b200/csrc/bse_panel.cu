@@ -60,7 +60,7 @@ constexpr size_t P_FIXED = 16 * sizeof(double)                 // redd
                            + 16 * sizeof(float) + 16 * sizeof(int)  // red_val, red_idx
                            + 64 * sizeof(int) * 2              // s_row, s_cont
                            + 4 * sizeof(int)                   // misc
-                           + 32;                               // two completion barriers + TMEM address
+                           + 48;                               // tile barriers [2], panel-load barrier, TMEM address
 __host__ __device__ inline size_t panel_smem_bytes(int ldp, bool tc = false) {
   return panel_region_bytes(ldp, tc) + P_FIXED + sizeof(int) * (size_t)ldp;
 }
@@ -76,6 +76,7 @@ struct PanelSmem {
   int* s_cont;  // [64] old row whose content ends up in s_row[slot]
   int* misc;    // [0] rows below the panel that receive another row, [1] status bits, [2] tensor-core wait failure
   uint64_t* bar;    // [2] completion barriers of the two tensor-core tiles in flight
+  uint64_t* pbar;   // completion barrier of the panel's bulk load
   uint32_t* tslot;  // TMEM address of the two tile accumulators
   int* piv;     // [ldp] row interchanged with row j
   int ldp;
@@ -87,6 +88,8 @@ struct PanelSmem {
     redd = reinterpret_cast<double*>(p);
     p += 16 * sizeof(double);
     bar = reinterpret_cast<uint64_t*>(p);
+    p += 16;
+    pbar = reinterpret_cast<uint64_t*>(p);
     p += 16;
     tslot = reinterpret_cast<uint32_t*>(p);
     p += 16;
@@ -307,26 +310,19 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
   bool singular = false;
   for (int k0 = 0; k0 < N; k0 += PNB) {
     const int nb = min(PNB, N - k0), m = N - k0, k1 = k0 + nb;
-    // ---- load and factor the panel (8 loads per thread in flight) ----
-    for (int e0 = 0; e0 < m * nb; e0 += 8 * PT) {
-      float2 v[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int e = e0 + u * PT + tid;
-        if (e < m * nb) {
-          const int c = e / m, r = e - c * m;
-          v[u] = A[(size_t)(k0 + c) * N + k0 + r];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int e = e0 + u * PT + tid;
-        if (e < m * nb) {
-          const int c = e / m, r = e - c * m;
-          s.P[(size_t)c * s.ldp + r] = v[u];
-        }
-      }
+    // ---- load the panel: one bulk copy (TMA engine) per column, global -> shared, completing on the panel
+    // barrier; the fence orders every thread's earlier accesses (its writes of these columns, its reads of the
+    // panel region) before the copies ----
+    fence_proxy_async_all();
+    __syncthreads();
+    if (tid < 32) {
+      if (tid == 0) mbar_expect_tx(s.pbar, (uint32_t)((size_t)m * nb * sizeof(float2)));
+      __syncwarp();
+      for (int c = tid; c < nb; c += 32)
+        bulk_g2s(s.P + (size_t)c * s.ldp, A + (size_t)(k0 + c) * N + k0, (uint32_t)(m * sizeof(float2)), s.pbar);
     }
+    if (!mbar_wait(s.pbar, (parity >> 2) & 1u)) s.misc[2] = 1;  // flags the item; the CTA issues no more tiles
+    parity ^= 4u;
     __syncthreads();
     singular |= panel_factor(s, m, nb, k0);
     for (int e = tid; e < m * nb; e += PT) {
@@ -780,7 +776,10 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
 // ever ran out waits once more (bounded) for each tile still in flight before the columns are freed.
 template <bool TC>
 __device__ void panel_kernel_begin(PanelSmem& s) {
-  if (threadIdx.x == 0) s.misc[2] = 0;
+  if (threadIdx.x == 0) {
+    s.misc[2] = 0;
+    mbar_init(s.pbar);
+  }
   if (TC) {
     if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, 2 * TC_NR);
     if (threadIdx.x == 0) {
@@ -795,6 +794,8 @@ __device__ void panel_kernel_begin(PanelSmem& s) {
 
 template <bool TC>
 __device__ void panel_kernel_end(PanelSmem& s, uint32_t parity) {
+  __syncthreads();
+  if (s.misc[2]) mbar_wait(s.pbar, ((parity >> 2) & 1u) ^ 1u);  // a panel load that ran out may still be landing
   if (!TC) return;
   tc_fence_before();
   __syncthreads();
