@@ -18,7 +18,6 @@
 
 namespace dga {
 
-constexpr int ELI_THREADS = 128;
 
 }  // namespace dga
 
@@ -114,12 +113,16 @@ __global__ void eli_apply_chi0pp_kernel(const double2* __restrict__ chi0pp, cons
 }
 
 // Per R: direct[R][I] = sum_J Mat(R)[I][J] g(R)[J];  flip[R][I] = sum_J Mat(R)[I][J] g~(R)[J] with
-// g~[(c,d),nu'] = g[(d,c), 2P-1-nu'].  One CTA per R, one warp per row, lanes over J.
+// g~[(c,d),nu'] = g[(d,c), 2P-1-nu'].  One CTA per R (grid-stride), each warp two rows at a time with lanes
+// over J and eight 16-byte loads of Mat(R) per lane in flight, so the Gamma(R) stream keeps enough bytes in
+// flight per SM to run at HBM bandwidth.
 //   gR: [Nk][n2][nvp] (forward transform of v), mat: [Nk][M][M]
-__global__ void __launch_bounds__(ELI_THREADS) eli_vertex_apply_kernel(const double2* __restrict__ mat,
-                                                                        const double2* __restrict__ gR, int nb,
-                                                                        int nvp, int nk, double2* __restrict__ direct,
-                                                                        double2* __restrict__ flip) {
+constexpr int ELI_APPLY_THREADS = 256;
+__global__ void __launch_bounds__(ELI_APPLY_THREADS) eli_vertex_apply_kernel(const double2* __restrict__ mat,
+                                                                              const double2* __restrict__ gR, int nb,
+                                                                              int nvp, int nk,
+                                                                              double2* __restrict__ direct,
+                                                                              double2* __restrict__ flip) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n2 = nb * nb, M = n2 * nvp;
   double2* g = reinterpret_cast<double2*>(smem_raw);
@@ -135,23 +138,48 @@ __global__ void __launch_bounds__(ELI_THREADS) eli_vertex_apply_kernel(const dou
     }
     __syncthreads();
     const double2* m = mat + (size_t)R * M * M;
-    for (int I = warp; I < M; I += nw) {
-      double2 a1 = make_double2(0.0, 0.0), a2 = make_double2(0.0, 0.0);
-      const double2* row = m + (size_t)I * M;
-      for (int J = lane; J < M; J += 32) {
-        const double2 x = row[J];
-        cfma(a1, x, g[J]);
-        cfma(a2, x, gt[J]);
+    for (int I0 = 2 * warp; I0 < M; I0 += 2 * nw) {
+      const bool two = I0 + 1 < M;
+      const double2* row0 = m + (size_t)I0 * M;
+      const double2* row1 = row0 + M;
+      double2 a1 = make_double2(0.0, 0.0), a2 = a1, b1 = a1, b2 = a1;
+      for (int J0 = 0; J0 < M; J0 += 128) {
+        double2 x0[4], x1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int J = J0 + 32 * u + lane;
+          x0[u] = J < M ? row0[J] : make_double2(0.0, 0.0);
+          x1[u] = (two && J < M) ? row1[J] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int J = J0 + 32 * u + lane;
+          if (J < M) {
+            const double2 gj = g[J], gtj = gt[J];
+            cfma(a1, x0[u], gj);
+            cfma(a2, x0[u], gtj);
+            cfma(b1, x1[u], gj);
+            cfma(b2, x1[u], gtj);
+          }
+        }
       }
       for (int off = 16; off > 0; off >>= 1) {
         a1.x += __shfl_down_sync(0xffffffffu, a1.x, off);
         a1.y += __shfl_down_sync(0xffffffffu, a1.y, off);
         a2.x += __shfl_down_sync(0xffffffffu, a2.x, off);
         a2.y += __shfl_down_sync(0xffffffffu, a2.y, off);
+        b1.x += __shfl_down_sync(0xffffffffu, b1.x, off);
+        b1.y += __shfl_down_sync(0xffffffffu, b1.y, off);
+        b2.x += __shfl_down_sync(0xffffffffu, b2.x, off);
+        b2.y += __shfl_down_sync(0xffffffffu, b2.y, off);
       }
       if (lane == 0) {
-        direct[(size_t)R * M + I] = a1;
-        flip[(size_t)R * M + I] = a2;
+        direct[(size_t)R * M + I0] = a1;
+        flip[(size_t)R * M + I0] = a2;
+        if (two) {
+          direct[(size_t)R * M + I0 + 1] = b1;
+          flip[(size_t)R * M + I0 + 1] = b2;
+        }
       }
     }
   }
@@ -256,7 +284,7 @@ int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, in
   if (rc) return rc;
   const size_t smem = 2 * (size_t)M * sizeof(double2);
   cudaFuncSetAttribute(eli_vertex_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  eli_vertex_apply_kernel<<<nk < 148 * 8 ? nk : 148 * 8, ELI_THREADS, smem, stream>>>(
+  eli_vertex_apply_kernel<<<nk < 148 * 8 ? nk : 148 * 8, ELI_APPLY_THREADS, smem, stream>>>(
       (const double2*)mat, s1, n_orb, nvp, nk, s2, s3);
   if (eli_status("dga_eli_matvec_c128")) return DGA_ERR_LAUNCH;
   eli_combine_kernel<<<eli_blocks((long long)nk * M), 256, 0, stream>>>(s2, s3, M, nx, ny, nz, sign, s0);
