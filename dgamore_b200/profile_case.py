@@ -5,6 +5,10 @@ wave of CTAs and an ncu capture of it holds about a gigabyte of device memory.
     python -m dgamore_b200.profile_case --config c3 --nk 4 --niw 10 --passes 1 [--precision mixed]
 
 Runs the passes and prints one JSON line with the shapes, the number of BSE items and the kernels launched.
+With ``--eliashberg K`` it then builds the pairing vertices of the same pass (FP64, three-leg vertex kept) and
+applies the singlet gap-equation operator K times:
+
+    python -m dgamore_b200.profile_case --config c4_bilayer --nk 48 --niw 30 --eliashberg 5
 """
 
 from __future__ import annotations
@@ -31,10 +35,11 @@ def main(argv=None):
     ap.add_argument("--niw", type=int, default=10)
     ap.add_argument("--passes", type=int, default=1)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--eliashberg", type=int, default=0, help="gap-equation operator applications after the pass")
     args = ap.parse_args(argv)
     cfg = reduced_config(args.config, args.nk, args.niw)
     inp = synthetic.make_inputs(cfg)
-    lp = LadderPass(inp, keep_intermediates=False, precision=args.precision)
+    lp = LadderPass(inp, keep_intermediates=args.eliashberg > 0, precision=args.precision)
     for _ in range(args.passes):
         lp.run()
     torch.cuda.synchronize()
@@ -46,6 +51,17 @@ def main(argv=None):
     }))
     if status:
         raise SystemExit(f"non-zero status {status}")
+    if args.eliashberg > 0:
+        from .eliashberg_solver import EliashbergSolver
+
+        es = EliashbergSolver(lp)
+        x = torch.ones(es.dim, dtype=torch.complex128, device=lp.dev)
+        out = torch.empty_like(x)
+        for _ in range(args.eliashberg):
+            es.matvec("sing", x, out)
+        torch.cuda.synchronize()
+        print(json.dumps({"eliashberg_M": es.M, "nk": lp.sh.nk_tot, "matvecs": args.eliashberg,
+                          "vertex_status": int(es.vertex_status.abs().sum())}))
 
 
 if __name__ == "__main__":
