@@ -304,8 +304,10 @@ __device__ void panel_interchange_map(PanelSmem& s, int k0, int nb) {
 // ----------------------------------------------------------------------------------------------
 // TC = true: the trailing tiles run on the tensor cores (tc_tile.cuh); L21 is then read back from global memory
 // (the panel region holds the tile operands), and parity tracks the phase of the tile completion barrier.
+// A has NC >= N columns: columns N .. NC-1 are extra right-hand sides, which receive every interchange and
+// trailing update, so that they end as L^-1 P times their start (the forward substitution done in passing).
 template <bool TC>
-__device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& parity) {
+__device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, uint32_t& parity) {
   const int tid = threadIdx.x;
   bool singular = false;
   for (int k0 = 0; k0 < N; k0 += PNB) {
@@ -329,14 +331,14 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
       const int c = e / m, r = e - c * m;
       A[(size_t)(k0 + c) * N + k0 + r] = s.P[(size_t)c * s.ldp + r];
     }
-    if (k1 >= N) break;
+    if (k1 >= NC) break;
     panel_unit_lower_inverse(s, nb);
     panel_interchange_map(s, k0, nb);
     __syncthreads();
     const int n_tgt = s.misc[0];
     // ---- per 64-column strip: interchanges + U12, then the strip's trailing tiles ----
-    for (int cs = k1; cs < N; cs += PTN) {
-      const int cw = min(PTN, N - cs);
+    for (int cs = k1; cs < NC; cs += PTN) {
+      const int cw = min(PTN, NC - cs);
       {
         // warp w handles columns w, w + 16, w + 32, w + 48 of the strip; lane = row of the U block (reads of the
         // touched rows are coalesced along the column).  Every old value is read, and U12 computed, before the
@@ -428,7 +430,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int c = cb + j;
-            const float2 x = (r < N && c < N) ? A[(size_t)c * N + r] : make_float2(0.f, 0.f);
+            const float2 x = (r < N && c < NC) ? A[(size_t)c * N + r] : make_float2(0.f, 0.f);
             v[2 * j] = x.x;
             v[2 * j + 1] = x.y;
           }
@@ -457,16 +459,18 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const int c = cb + j;
-              if (r < N && c < N) A[(size_t)c * N + r] = make_float2(v[2 * j], v[2 * j + 1]);
+              if (r < N && c < NC) A[(size_t)c * N + r] = make_float2(v[2 * j], v[2 * j + 1]);
             }
           } else {
             s.misc[2] = 1;
           }
         };
-        stage(0);
-        tc_fence_before();
-        __syncthreads();
-        issue(0);
+        if (ntiles > 0) {  // the last panel can have columns to its right (the extra ones) but no rows below
+          stage(0);
+          tc_fence_before();
+          __syncthreads();
+          issue(0);
+        }
         for (int i = 0; i < ntiles; ++i) {
           if (i + 1 < ntiles) stage(i + 1);
           finish(i);
@@ -486,7 +490,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
         for (int rt = k1; rt < N; rt += PTM) {
           float cr[16], ci[16];  // index (column j of 4) * 4 + (row i of 4)
           const int rbase = rt + 2 * ty;
-          const bool full = rt + PTM <= N && cs + PTN <= N;
+          const bool full = rt + PTM <= N && cs + PTN <= NC;
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const int c = cs + 2 * tx + (j & 1) + 32 * (j >> 1);
@@ -494,7 +498,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
             for (int ap = 0; ap < 2; ++ap) {
               const int r = rbase + 64 * ap;
               float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-              if (full || (c < N && r < N)) v = *reinterpret_cast<const float4*>(A + (size_t)c * N + r);
+              if (full || (c < NC && r < N)) v = *reinterpret_cast<const float4*>(A + (size_t)c * N + r);
               cr[j * 4 + 2 * ap] = v.x;
               ci[j * 4 + 2 * ap] = v.y;
               cr[j * 4 + 2 * ap + 1] = v.z;
@@ -530,7 +534,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
 #pragma unroll
             for (int ap = 0; ap < 2; ++ap) {
               const int r = rbase + 64 * ap;
-              if (full || (c < N && r < N))
+              if (full || (c < NC && r < N))
                 *reinterpret_cast<float4*>(A + (size_t)c * N + r) =
                     make_float4(cr[j * 4 + 2 * ap], ci[j * 4 + 2 * ap], cr[j * 4 + 2 * ap + 1], ci[j * 4 + 2 * ap + 1]);
             }
@@ -549,10 +553,11 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, PanelSmem& s, uint32_t& 
 // with the factors of panel_lu and its interchanges piv (applied panel by panel in the forward pass).
 // ----------------------------------------------------------------------------------------------
 template <int NR>
-__device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv, float2* y, int ldy) {
+__device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv, float2* y, int ldy,
+                            bool forward = true) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // forward: y <- L^-1 P y
-  for (int k0 = 0; k0 < N; k0 += PNB) {
+  // forward: y <- L^-1 P y (skipped when y already holds L^-1 P b)
+  for (int k0 = 0; forward && k0 < N; k0 += PNB) {
     const int nb = min(PNB, N - k0), k1 = k0 + nb;
     if (warp == 0 && lane < NR) {
       float2* ys = y + (size_t)lane * ldy;
@@ -649,8 +654,12 @@ __device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv,
 // One work item: form, factor, solve, refine.  Returns the status bits; *iters = number of corrections.
 //   slot: A (N x N complex64) | Y (NR x N complex128) | Rb (NR x N complex128)
 // ----------------------------------------------------------------------------------------------
+// slot: A with its n2 selector columns (N x (N + n2) complex64) | Y (n2 x N complex128) | Rb (n2 x N complex128)
+__host__ __device__ inline size_t panel_a_bytes(int N, int n2) {
+  return ((size_t)N * (N + n2) * sizeof(float2) + 255) & ~(size_t)255;
+}
 __host__ __device__ inline size_t panel_slot_bytes(int N, int n2) {
-  return (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255) + 2 * (size_t)N * n2 * sizeof(double2);
+  return panel_a_bytes(N, n2) + 2 * (size_t)N * n2 * sizeof(double2);
 }
 
 template <int NR, bool TC>
@@ -659,7 +668,7 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
                                 int* iters, uint32_t& parity) {
   const int tid = threadIdx.x;
   float2* A = reinterpret_cast<float2*>(slot);
-  double2* Y = reinterpret_cast<double2*>(slot + (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255));
+  double2* Y = reinterpret_cast<double2*>(slot + panel_a_bytes(N, NR));
   double2* Rb = Y + (size_t)N * NR;
   // ---- form A in complex64: thread t owns rows t and t + PT (N <= 2 PT here), 8 columns of loads in flight ----
   // element (i, j) as StructuredSource::element: (chi0^-1 [block diagonal] + Gamma / beta^2) + (-(U + V) / beta^2)
@@ -706,20 +715,23 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
         }
       }
     }
+    // the n2 selector columns S[(p, nu)][s] = delta_ps, factored along with A (panel_lu's extra columns)
+#pragma unroll
+    for (int a2 = 0; a2 < 2; ++a2)
+      if (rok[a2])
+        for (int r = 0; r < NR; ++r) A[(size_t)(N + r) * N + ri[a2]] = make_float2(pr[a2] == r ? 1.f : 0.f, 0.f);
   }
   __syncthreads();
-  const bool singular = panel_lu<TC>(A, N, s, parity);
+  const bool singular = panel_lu<TC>(A, N, N + NR, s, parity);
   // ---- initial solve against the selector: S[(p,nu)][s] = delta_{p s} ----
   const int ldy = N;
   float2* y = s.P;
   double2* ys = reinterpret_cast<double2*>(s.P) + (((size_t)NR * N + 1) / 2 + 1);  // after y, 16-byte aligned
   double2* colsum = ys + 32 * NR;
-  for (int e = tid; e < NR * N; e += PT) {
-    const int r = e / N, i = e - r * N;
-    y[e] = make_float2((i / nv) == r ? 1.f : 0.f, 0.f);
-  }
+  // the selector columns hold L^-1 P S after the factorisation: only the back substitution is left
+  for (int e = tid; e < NR * N; e += PT) y[e] = A[(size_t)N * N + e];
   __syncthreads();
-  panel_solve<NR>(A, N, s.piv, y, ldy);
+  panel_solve<NR>(A, N, s.piv, y, ldy, false);
   double prev = 0.0;
   for (int e = tid; e < NR * N; e += PT) {
     Y[e] = make_double2(y[e].x, y[e].y);
