@@ -150,10 +150,16 @@ __device__ bool panel_factor(PanelSmem& s, int m, int nb, int k0) {
   }
   for (int jj = 0; jj < nb; ++jj) {
     __syncthreads();  // this column's candidates are in place; the previous update is complete
-    float bv = s.red_val[0];
-    int p = s.red_idx[0];
+    // every warp merges the 16 warp candidates with a butterfly (the merge is commutative and associative, so
+    // all lanes of all warps agree on the pivot)
+    float bv = lane < PW ? s.red_val[lane] : -1.f;
+    int p = lane < PW ? s.red_idx[lane] : 0x7fffffff;
 #pragma unroll
-    for (int w = 1; w < PW; ++w) argmax_merge(bv, p, s.red_val[w], s.red_idx[w]);
+    for (int off = 16; off > 0; off >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, p, off);
+      argmax_merge(bv, p, ov, oi);
+    }
     if (p < jj || p >= m) p = jj;  // cannot happen (row jj itself is a candidate); keeps p in range
     if (tid == 0) s.piv[k0 + jj] = k0 + p;
     if (p != jj && tid < nb) {
