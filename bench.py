@@ -269,17 +269,24 @@ def time_pass(lp, args, world: int, local: int, sample_clocks: bool):
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local if sample_clocks else -1)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     with clocks:
         start.record(stream)
-        for _ in range(args.steps):
+        marks[0].record(stream)
+        for k in range(args.steps):
             lp.replay()
+            marks[k + 1].record(stream)
         end.record(stream)
         end.synchronize()
     torch.cuda.synchronize()
     barrier(world)
     t = max_over_ranks(start.elapsed_time(end) / 1e3, world)
     value = world * sh.n_solves * args.steps / t
-    return {"t": t, "value": value, "bse_ms": float(min(bse_ms)), "status": status, "clocks": clocks}
+    per_step = np.array([marks[k].elapsed_time(marks[k + 1]) for k in range(args.steps)])
+    step_ms = {"median": float(np.median(per_step)), "p10": float(np.percentile(per_step, 10)),
+               "p90": float(np.percentile(per_step, 90))}
+    return {"t": t, "value": value, "bse_ms": float(min(bse_ms)), "status": status, "clocks": clocks,
+            "step_ms": step_ms}
 
 
 # DRAM bytes per BSE item of each kernel, from `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` of a
@@ -444,6 +451,7 @@ def run_ours(args, rank: int, world: int, local: int):
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": 1e3 * t / args.steps,
+        "step_ms": res["step_ms"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
