@@ -30,6 +30,7 @@ namespace dga {
 
 constexpr int PT = 512;       // threads per CTA
 constexpr int PW = PT / 32;   // warps
+static_assert(PW <= 32 && (PW & (PW - 1)) == 0, "the pivot butterfly merges PW candidates in log2(PW) steps");
 constexpr int PNB = 32;       // panel width
 constexpr int PSB = 8;        // sub-panel width inside the panel factorisation
 constexpr int PTM = 128;      // trailing tile rows
@@ -150,12 +151,12 @@ __device__ bool panel_factor(PanelSmem& s, int m, int nb, int k0) {
   }
   for (int jj = 0; jj < nb; ++jj) {
     __syncthreads();  // this column's candidates are in place; the previous update is complete
-    // every warp merges the 16 warp candidates with a butterfly (the merge is commutative and associative, so
-    // all lanes of all warps agree on the pivot)
-    float bv = lane < PW ? s.red_val[lane] : -1.f;
-    int p = lane < PW ? s.red_idx[lane] : 0x7fffffff;
+    // every warp merges the 16 warp candidates with a butterfly, lanes l and l + 16 holding the same candidate
+    // (the merge is commutative and associative, so all lanes of all warps agree on the pivot)
+    float bv = s.red_val[lane & (PW - 1)];
+    int p = s.red_idx[lane & (PW - 1)];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
+    for (int off = PW / 2; off > 0; off >>= 1) {
       const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
       const int oi = __shfl_xor_sync(0xffffffffu, p, off);
       argmax_merge(bv, p, ov, oi);
@@ -251,10 +252,16 @@ __device__ bool panel_factor(PanelSmem& s, int m, int nb, int k0) {
   return singular;
 }
 
-// X = L11^-1 for the unit lower nb x nb block at the top of the panel: warp per column, lane = row.
-__device__ void panel_unit_lower_inverse(PanelSmem& s, int nb) {
+// Inverses of the panel's diagonal blocks, lane = row, warp w doing columns w and 31 - w (equal chain lengths):
+// X = L11^-1 (unit lower) into s.L11i for U12 and into linv, and Z = U11^-1 (upper) into uinv (both stored
+// transposed, [column][row], zero outside the triangle and beyond nb) for the triangular solves, whose diagonal
+// steps are then products.
+__device__ void panel_diag_inverses(PanelSmem& s, int nb, float2* __restrict__ linv, float2* __restrict__ uinv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int c = warp; c < PNB; c += PW) {
+  const float2 dinv = lane < nb ? crecip(s.P[(size_t)lane * s.ldp + lane]) : make_float2(0.f, 0.f);
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    const int c = h == 0 ? warp : PNB - 1 - warp;
     float2 x = make_float2(lane == c ? 1.f : 0.f, 0.f);
     for (int k = c; k < nb - 1; ++k) {
       const float xk_re = __shfl_sync(0xffffffffu, x.x, k);
@@ -263,6 +270,16 @@ __device__ void panel_unit_lower_inverse(PanelSmem& s, int nb) {
     }
     if (lane >= nb || lane < c) x = make_float2(0.f, 0.f);
     s.L11i[lane * (PNB + 1) + c] = x;
+    linv[c * PNB + lane] = x;
+    // U11 z = e_c by back substitution, U[r][k] = P[k * ldp + r] for r <= k
+    float2 rhs = make_float2(lane == c ? 1.f : 0.f, 0.f), z = make_float2(0.f, 0.f);
+    for (int k = min(c, nb - 1); k >= 0; --k) {
+      if (lane == k) z = cmul(rhs, dinv);
+      const float zr = __shfl_sync(0xffffffffu, z.x, k), zi = __shfl_sync(0xffffffffu, z.y, k);
+      if (lane < k) cfms(rhs, s.P[(size_t)k * s.ldp + lane], make_float2(zr, zi));
+    }
+    if (lane > c || lane >= nb) z = make_float2(0.f, 0.f);
+    uinv[c * PNB + lane] = z;
   }
 }
 
@@ -312,8 +329,10 @@ __device__ void panel_interchange_map(PanelSmem& s, int k0, int nb) {
 // (the panel region holds the tile operands), and parity tracks the phase of the tile completion barrier.
 // A has NC >= N columns: columns N .. NC-1 are extra right-hand sides, which receive every interchange and
 // trailing update, so that they end as L^-1 P times their start (the forward substitution done in passing).
+// inv: per panel b, L11^-1 at inv + 2048 b and U11^-1 at inv + 2048 b + 1024 (panel_diag_inverses).
 template <bool TC>
-__device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, uint32_t& parity) {
+__device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, uint32_t& parity,
+                         float2* __restrict__ inv) {
   const int tid = threadIdx.x;
   bool singular = false;
   for (int k0 = 0; k0 < N; k0 += PNB) {
@@ -338,7 +357,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
       A[(size_t)(k0 + c) * N + k0 + r] = s.P[(size_t)c * s.ldp + r];
     }
     if (k1 >= NC) break;
-    panel_unit_lower_inverse(s, nb);
+    panel_diag_inverses(s, nb, inv + (size_t)(k0 / PNB) * 2 * PNB * PNB, inv + (size_t)(k0 / PNB) * 2 * PNB * PNB + PNB * PNB);
     panel_interchange_map(s, k0, nb);
     __syncthreads();
     const int n_tgt = s.misc[0];
@@ -558,41 +577,93 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
 // In-place solve (L U) y = b for the NR right-hand sides y[s][i] (complex64, shared memory, stride ldy),
 // with the factors of panel_lu and its interchanges piv (applied panel by panel in the forward pass).
 // ----------------------------------------------------------------------------------------------
+// L2 prefetch of rows [r0, r1) of the factor's columns [c0, c0 + nc) (column-major, leading dimension N), one
+// bulk prefetch per column by the calling warp's lanes.  The range is widened to 16-byte boundaries, which stays
+// inside the item's slot (A starts 256-byte aligned and its selector columns follow column N - 1).
+__device__ __forceinline__ void prefetch_factor_cols(const float2* A, int N, int c0, int nc, int r0, int r1) {
+  const int lane = threadIdx.x & 31;
+  if (r1 <= r0) return;
+  for (int c = lane; c < nc; c += 32) {
+    const float2* col = A + (size_t)(c0 + c) * N;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(col + r0) & ~(uintptr_t)15;
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(col + r1) + 15) & ~(uintptr_t)15;
+    bulk_prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(e - a));
+  }
+}
+
+// Prefetch of step b of a triangular solve: the factor block the step's update reads and its diagonal inverse.
+__device__ __forceinline__ void prefetch_solve_step(const float2* A, int N, const float2* inv, int b, bool forward) {
+  const int nblk = (N + PNB - 1) / PNB;
+  if (b < 0 || b >= nblk) return;
+  const int k0 = b * PNB, nb = min(PNB, N - k0);
+  if (forward) prefetch_factor_cols(A, N, k0, nb, k0 + nb, N);
+  else prefetch_factor_cols(A, N, k0, nb, 0, k0);
+  if ((threadIdx.x & 31) == 0)
+    bulk_prefetch_l2(inv + (size_t)b * 2 * PNB * PNB + (forward ? 0 : PNB * PNB), PNB * PNB * sizeof(float2));
+}
+
+// Triangular solves with the factors in A (column-major, leading dimension N) and the inverses of their diagonal
+// blocks in inv, for NR right-hand sides y[r * ldy + i] in shared memory.  A step of either solve is a product
+// with the block's inverse (warp r for right-hand side r, lane = row) followed by the update of the rows beyond
+// the block (thread per row).  The next step's inverse is staged into sinv (shared, 2 x 32 x 32, double
+// buffered) during the update, and the factor blocks two steps ahead are prefetched into L2.
 template <int NR>
 __device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv, float2* y, int ldy,
-                            bool forward = true) {
+                            const float2* __restrict__ inv, float2* sinv, bool forward = true) {
+  static_assert(PNB * PNB == 2 * PT, "the staging of a block inverse gives every thread two elements");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // forward: y <- L^-1 P y (skipped when y already holds L^-1 P b)
-  for (int k0 = 0; forward && k0 < N; k0 += PNB) {
-    const int nb = min(PNB, N - k0), k1 = k0 + nb;
-    if (warp == 0 && lane < NR) {
-      float2* ys = y + (size_t)lane * ldy;
-      for (int t = 0; t < nb; ++t) {
-        const int p = piv[k0 + t];
-        if (p != k0 + t) {
-          const float2 tmp = ys[k0 + t];
-          ys[k0 + t] = ys[p];
-          ys[p] = tmp;
+  const int nblk = (N + PNB - 1) / PNB;
+  const int nf = forward ? nblk : 0, nsteps = nf + nblk;
+  // step st: forward block st (st < nf), else backward block nblk - 1 - (st - nf)
+  auto step_block = [&](int st) { return st < nf ? st : nblk - 1 - (st - nf); };
+  auto step_inv = [&](int st) { return inv + (size_t)step_block(st) * 2 * PNB * PNB + (st < nf ? 0 : PNB * PNB); };
+  if (warp == PW - 1) {
+    for (int st = 0; st < 2 && st < nsteps; ++st) prefetch_solve_step(A, N, inv, step_block(st), st < nf);
+  }
+  {
+    const float2* src = step_inv(0);
+    sinv[tid] = src[tid];
+    sinv[tid + PT] = src[tid + PT];
+  }
+  __syncthreads();
+  for (int st = 0; st < nsteps; ++st) {
+    const bool fwd = st < nf;
+    const int b = step_block(st), k0 = b * PNB, nb = min(PNB, N - k0);
+    const float2* sv = sinv + (st & 1) * PNB * PNB;
+    if (warp == PW - 1 && st + 2 < nsteps) prefetch_solve_step(A, N, inv, step_block(st + 2), st + 2 < nf);
+    if (fwd) {  // the panel's row interchanges
+      if (warp == 0 && lane < NR) {
+        float2* ys = y + (size_t)lane * ldy;
+        for (int t = 0; t < nb; ++t) {
+          const int p = piv[k0 + t];
+          if (p != k0 + t) {
+            const float2 tmp = ys[k0 + t];
+            ys[k0 + t] = ys[p];
+            ys[p] = tmp;
+          }
         }
       }
+      __syncthreads();
     }
-    __syncthreads();
+    // diagonal block: y_b <- inv_b y_b
     if (warp < NR) {
-      float2* ys = y + (size_t)warp * ldy;
-      float2 yr = lane < nb ? ys[k0 + lane] : make_float2(0.f, 0.f);
-      float2 lrow[PNB];
-#pragma unroll
-      for (int k = 0; k < PNB; ++k)
-        lrow[k] = (lane < nb && k < lane) ? A[(size_t)(k0 + k) * N + k0 + lane] : make_float2(0.f, 0.f);
-#pragma unroll
-      for (int k = 0; k < PNB - 1; ++k) {
-        const float re = __shfl_sync(0xffffffffu, yr.x, k), im = __shfl_sync(0xffffffffu, yr.y, k);
-        if (k < lane) cfms(yr, lrow[k], make_float2(re, im));
-      }
-      if (lane < nb) ys[k0 + lane] = yr;
+      float2* ys = y + (size_t)warp * ldy + k0;
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll 8
+      for (int k = 0; k < nb; ++k) cfma(acc, sv[k * PNB + lane], ys[k]);
+      __syncwarp();
+      if (lane < nb) ys[lane] = acc;
+    }
+    float2 nx0 = make_float2(0.f, 0.f), nx1 = nx0;  // the next step's inverse, stored after the update
+    if (st + 1 < nsteps) {
+      const float2* src = step_inv(st + 1);
+      nx0 = src[tid];
+      nx1 = src[tid + PT];
     }
     __syncthreads();
-    for (int i = k1 + tid; i < N; i += PT) {
+    // update of the rows beyond the block: forward rows [k0 + nb, N), backward rows [0, k0)
+    const int i0 = fwd ? k0 + nb : 0, i1 = fwd ? N : k0;
+    for (int i = i0 + tid; i < i1; i += PT) {
       float2 acc[NR];
 #pragma unroll
       for (int r = 0; r < NR; ++r) acc[r] = y[(size_t)r * ldy + i];
@@ -610,47 +681,10 @@ __device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv,
 #pragma unroll
       for (int r = 0; r < NR; ++r) y[(size_t)r * ldy + i] = acc[r];
     }
-    __syncthreads();
-  }
-  // backward: y <- U^-1 y
-  const int nblk = (N + PNB - 1) / PNB;
-  for (int bk = nblk - 1; bk >= 0; --bk) {
-    const int k0 = bk * PNB, nb = min(PNB, N - k0);
-    if (warp < NR) {
-      float2* ys = y + (size_t)warp * ldy;
-      float2 yr = lane < nb ? ys[k0 + lane] : make_float2(0.f, 0.f);
-      float2 urow[PNB];
-#pragma unroll
-      for (int k = 0; k < PNB; ++k)
-        urow[k] = (lane < nb && k >= lane && k < nb) ? A[(size_t)(k0 + k) * N + k0 + lane] : make_float2(1.f, 0.f);
-#pragma unroll
-      for (int k = PNB - 1; k >= 0; --k) {
-        if (k < nb) {
-          if (lane == k) yr = cdiv(yr, urow[k]);
-          const float re = __shfl_sync(0xffffffffu, yr.x, k), im = __shfl_sync(0xffffffffu, yr.y, k);
-          if (lane < k) cfms(yr, urow[k], make_float2(re, im));
-        }
-      }
-      if (lane < nb) ys[k0 + lane] = yr;
-    }
-    __syncthreads();
-    for (int i = tid; i < k0; i += PT) {
-      float2 acc[NR];
-#pragma unroll
-      for (int r = 0; r < NR; ++r) acc[r] = y[(size_t)r * ldy + i];
-      for (int k = 0; k < nb; k += 16) {
-        float2 u[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) u[q] = (k + q < nb) ? A[(size_t)(k0 + k + q) * N + i] : make_float2(0.f, 0.f);
-#pragma unroll
-        for (int q = 0; q < 16; ++q)
-          if (k + q < nb) {
-#pragma unroll
-            for (int r = 0; r < NR; ++r) cfms(acc[r], u[q], y[(size_t)r * ldy + k0 + k + q]);
-          }
-      }
-#pragma unroll
-      for (int r = 0; r < NR; ++r) y[(size_t)r * ldy + i] = acc[r];
+    if (st + 1 < nsteps) {
+      float2* dst = sinv + ((st + 1) & 1) * PNB * PNB;
+      dst[tid] = nx0;
+      dst[tid + PT] = nx1;
     }
     __syncthreads();
   }
@@ -661,11 +695,13 @@ __device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv,
 //   slot: A (N x N complex64) | Y (NR x N complex128) | Rb (NR x N complex128)
 // ----------------------------------------------------------------------------------------------
 // slot: A with its n2 selector columns (N x (N + n2) complex64) | Y (n2 x N complex128) | Rb (n2 x N complex128)
+//       | inverses of the diagonal blocks (2 x 32 x 32 complex64 per 32-column panel)
 __host__ __device__ inline size_t panel_a_bytes(int N, int n2) {
   return ((size_t)N * (N + n2) * sizeof(float2) + 255) & ~(size_t)255;
 }
 __host__ __device__ inline size_t panel_slot_bytes(int N, int n2) {
-  return panel_a_bytes(N, n2) + 2 * (size_t)N * n2 * sizeof(double2);
+  return panel_a_bytes(N, n2) + 2 * (size_t)N * n2 * sizeof(double2) +
+         (size_t)((N + PNB - 1) / PNB) * 2 * PNB * PNB * sizeof(float2);
 }
 
 template <int NR, bool TC>
@@ -676,6 +712,7 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
   float2* A = reinterpret_cast<float2*>(slot);
   double2* Y = reinterpret_cast<double2*>(slot + panel_a_bytes(N, NR));
   double2* Rb = Y + (size_t)N * NR;
+  float2* inv = reinterpret_cast<float2*>(Rb + (size_t)N * NR);
   // ---- form A in complex64: thread t owns rows t and t + PT (N <= 2 PT here), 8 columns of loads in flight ----
   // element (i, j) as StructuredSource::element: (chi0^-1 [block diagonal] + Gamma / beta^2) + (-(U + V) / beta^2)
   {
@@ -728,7 +765,7 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
         for (int r = 0; r < NR; ++r) A[(size_t)(N + r) * N + ri[a2]] = make_float2(pr[a2] == r ? 1.f : 0.f, 0.f);
   }
   __syncthreads();
-  const bool singular = panel_lu<TC>(A, N, N + NR, s, parity);
+  const bool singular = panel_lu<TC>(A, N, N + NR, s, parity, inv);
   // ---- initial solve against the selector: S[(p,nu)][s] = delta_{p s} ----
   const int ldy = N;
   float2* y = s.P;
@@ -737,7 +774,7 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
   // the selector columns hold L^-1 P S after the factorisation: only the back substitution is left
   for (int e = tid; e < NR * N; e += PT) y[e] = A[(size_t)N * N + e];
   __syncthreads();
-  panel_solve<NR>(A, N, s.piv, y, ldy, false);
+  panel_solve<NR>(A, N, s.piv, y, ldy, inv, s.Us, false);
   double prev = 0.0;
   for (int e = tid; e < NR * N; e += PT) {
     Y[e] = make_double2(y[e].x, y[e].y);
@@ -750,7 +787,7 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
     structured_residual_permuted<NR>(src, wi.ch, wi.q, wi.w, N, nv, Y, Rb, nullptr, colsum, ys);
     for (int e = tid; e < NR * N; e += PT) y[e] = make_float2((float)Rb[e].x, (float)Rb[e].y);
     __syncthreads();
-    panel_solve<NR>(A, N, s.piv, y, ldy);
+    panel_solve<NR>(A, N, s.piv, y, ldy, inv, s.Us);
     double dmax = 0.0, ymax = 0.0;
     for (int e = tid; e < NR * N; e += PT) {
       const double2 d = make_double2(y[e].x, y[e].y);
