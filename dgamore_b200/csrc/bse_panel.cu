@@ -30,7 +30,7 @@ namespace dga {
 
 constexpr int PT = 512;       // threads per CTA
 constexpr int PW = PT / 32;   // warps
-static_assert(PW <= 32 && (PW & (PW - 1)) == 0, "the pivot butterfly merges PW candidates in log2(PW) steps");
+static_assert(PW <= 32 && 32 % PW == 0, "a warp merges the PW warp candidates of the pivot search");
 constexpr int PNB = 32;       // panel width
 constexpr int PSB = 8;        // sub-panel width inside the panel factorisation
 constexpr int PTM = 128;      // trailing tile rows
@@ -112,13 +112,16 @@ struct PanelSmem {
   }
 };
 
+// Warp-wide argmax of the pivot candidates (v, idx), in every lane: the largest v, ties to the smallest idx (the
+// rule of argmax_merge).  Non-negative floats order as their bit patterns, so two integer reductions do it; a
+// negative or NaN v is no candidate.
 __device__ __forceinline__ void warp_argmax(float& v, int& idx) {
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const float ov = __shfl_down_sync(0xffffffffu, v, off);
-    const int oi = __shfl_down_sync(0xffffffffu, idx, off);
-    argmax_merge(v, idx, ov, oi);
-  }
+  const bool ok = v >= 0.f;
+  const unsigned key = ok ? __float_as_uint(v) : 0u;
+  const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+  const unsigned imin = __reduce_min_sync(0xffffffffu, (ok && key == kmax) ? (unsigned)idx : 0x7fffffffu);
+  v = __uint_as_float(kmax);
+  idx = (int)imin;
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -151,16 +154,11 @@ __device__ bool panel_factor(PanelSmem& s, int m, int nb, int k0) {
   }
   for (int jj = 0; jj < nb; ++jj) {
     __syncthreads();  // this column's candidates are in place; the previous update is complete
-    // every warp merges the 16 warp candidates with a butterfly, lanes l and l + 16 holding the same candidate
-    // (the merge is commutative and associative, so all lanes of all warps agree on the pivot)
+    // every warp merges the 16 warp candidates (lanes l and l + 16 holding the same one), so all lanes of all
+    // warps agree on the pivot
     float bv = s.red_val[lane & (PW - 1)];
     int p = s.red_idx[lane & (PW - 1)];
-#pragma unroll
-    for (int off = PW / 2; off > 0; off >>= 1) {
-      const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, p, off);
-      argmax_merge(bv, p, ov, oi);
-    }
+    warp_argmax(bv, p);
     if (p < jj || p >= m) p = jj;  // cannot happen (row jj itself is a candidate); keeps p in range
     if (tid == 0) s.piv[k0 + jj] = k0 + p;
     if (p != jj && tid < nb) {
@@ -329,6 +327,20 @@ __device__ void panel_interchange_map(PanelSmem& s, int k0, int nb) {
 // (the panel region holds the tile operands), and parity tracks the phase of the tile completion barrier.
 // A has NC >= N columns: columns N .. NC-1 are extra right-hand sides, which receive every interchange and
 // trailing update, so that they end as L^-1 P times their start (the forward substitution done in passing).
+// L2 prefetch of rows [r0, r1) of columns [c0, c0 + nc) of the item's matrix (column-major, leading dimension
+// N), one bulk prefetch per column by the calling warp's lanes.  The range is widened to 16-byte boundaries, which stays
+// inside the item's slot (A starts 256-byte aligned and its selector columns follow column N - 1).
+__device__ __forceinline__ void prefetch_factor_cols(const float2* A, int N, int c0, int nc, int r0, int r1) {
+  const int lane = threadIdx.x & 31;
+  if (r1 <= r0) return;
+  for (int c = lane; c < nc; c += 32) {
+    const float2* col = A + (size_t)(c0 + c) * N;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(col + r0) & ~(uintptr_t)15;
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(col + r1) + 15) & ~(uintptr_t)15;
+    bulk_prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(e - a));
+  }
+}
+
 // inv: per panel b, L11^-1 at inv + 2048 b and U11^-1 at inv + 2048 b + 1024 (panel_diag_inverses).
 template <bool TC>
 __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, uint32_t& parity,
@@ -577,19 +589,6 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
 // In-place solve (L U) y = b for the NR right-hand sides y[s][i] (complex64, shared memory, stride ldy),
 // with the factors of panel_lu and its interchanges piv (applied panel by panel in the forward pass).
 // ----------------------------------------------------------------------------------------------
-// L2 prefetch of rows [r0, r1) of the factor's columns [c0, c0 + nc) (column-major, leading dimension N), one
-// bulk prefetch per column by the calling warp's lanes.  The range is widened to 16-byte boundaries, which stays
-// inside the item's slot (A starts 256-byte aligned and its selector columns follow column N - 1).
-__device__ __forceinline__ void prefetch_factor_cols(const float2* A, int N, int c0, int nc, int r0, int r1) {
-  const int lane = threadIdx.x & 31;
-  if (r1 <= r0) return;
-  for (int c = lane; c < nc; c += 32) {
-    const float2* col = A + (size_t)(c0 + c) * N;
-    const uintptr_t a = reinterpret_cast<uintptr_t>(col + r0) & ~(uintptr_t)15;
-    const uintptr_t e = (reinterpret_cast<uintptr_t>(col + r1) + 15) & ~(uintptr_t)15;
-    bulk_prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(e - a));
-  }
-}
 
 // Prefetch of step b of a triangular solve: the factor block the step's update reads and its diagonal inverse.
 __device__ __forceinline__ void prefetch_solve_step(const float2* A, int N, const float2* inv, int b, bool forward) {
