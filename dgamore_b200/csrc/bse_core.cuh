@@ -143,7 +143,7 @@ __device__ void structured_residual_permuted(const StructuredSource& src, int ch
           double2 g[8];
 #pragma unroll
           for (int u = 0; u < 8; ++u)
-            g[u] = (jj0 + u < jw) ? gam[(size_t)(j0 + jj0 + u) * N + i] : make_double2(0.0, 0.0);
+            g[u] = (jj0 + u < jw) ? __ldcg(gam + (size_t)(j0 + jj0 + u) * N + i) : make_double2(0.0, 0.0);
 #pragma unroll
           for (int u = 0; u < 8; ++u)
             if (jj0 + u < jw) {

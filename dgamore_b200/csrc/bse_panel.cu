@@ -389,8 +389,8 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
         for (int q = 0; q < PTN / PW; ++q) {
           const int c = warp + PW * q;
           const float2* colp = A + (size_t)(cs + c) * N;
-          av[q] = (c < cw && lane < nb) ? colp[src_row] : make_float2(0.f, 0.f);
-          tv[q] = (c < cw && lane < n_tgt) ? colp[tgt_src] : make_float2(0.f, 0.f);
+          av[q] = (c < cw && lane < nb) ? __ldcg(colp + src_row) : make_float2(0.f, 0.f);
+          tv[q] = (c < cw && lane < n_tgt) ? __ldcg(colp + tgt_src) : make_float2(0.f, 0.f);
         }
 #pragma unroll
         for (int q = 0; q < PTN / PW; ++q) {
@@ -455,8 +455,8 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               const int ch = cg + 4 * j;
-              const float2 x0 = rok ? A[(size_t)(k0 + 2 * ch) * N + r] : make_float2(0.f, 0.f);
-              const float2 x1 = rok ? A[(size_t)(k0 + 2 * ch + 1) * N + r] : make_float2(0.f, 0.f);
+              const float2 x0 = rok ? __ldcg(A + (size_t)(k0 + 2 * ch) * N + r) : make_float2(0.f, 0.f);
+              const float2 x1 = rok ? __ldcg(A + (size_t)(k0 + 2 * ch + 1) * N + r) : make_float2(0.f, 0.f);
               const float4 h = make_float4(tf32_hi(x0.x), tf32_hi(x0.y), tf32_hi(x1.x), tf32_hi(x1.y));
               const float4 l = make_float4(x0.x - h.x, x0.y - h.y, x1.x - h.z, x1.y - h.w);
               *reinterpret_cast<float4*>(ah + tc_off(row, 4 * ch)) = h;
@@ -467,7 +467,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int c = cb + j;
-            const float2 x = (r < N && c < NC) ? A[(size_t)c * N + r] : make_float2(0.f, 0.f);
+            const float2 x = (r < N && c < NC) ? __ldcg(A + (size_t)c * N + r) : make_float2(0.f, 0.f);
             v[2 * j] = x.x;
             v[2 * j + 1] = x.y;
           }
@@ -669,7 +669,7 @@ __device__ void panel_solve(const float2* __restrict__ A, int N, const int* piv,
       for (int k = 0; k < nb; k += 16) {  // 16 factor loads in flight
         float2 l[16];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) l[u] = (k + u < nb) ? A[(size_t)(k0 + k + u) * N + i] : make_float2(0.f, 0.f);
+        for (int u = 0; u < 16; ++u) l[u] = (k + u < nb) ? __ldcg(A + (size_t)(k0 + k + u) * N + i) : make_float2(0.f, 0.f);
 #pragma unroll
         for (int u = 0; u < 16; ++u)
           if (k + u < nb) {
@@ -734,7 +734,7 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
       for (int u = 0; u < 8; ++u)
 #pragma unroll
         for (int a2 = 0; a2 < 2; ++a2)
-          g[a2][u] = (rok[a2] && j0 + u < N) ? gam[(size_t)(j0 + u) * N + ri[a2]] : make_double2(0.0, 0.0);
+          g[a2][u] = (rok[a2] && j0 + u < N) ? __ldcg(gam + (size_t)(j0 + u) * N + ri[a2]) : make_double2(0.0, 0.0);
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const int j = j0 + u;
