@@ -289,84 +289,120 @@ __global__ void lambda_kernel(const double2* __restrict__ chi, int Q, int W, con
 }
 
 // ------------------------------------------------------------------------------------------------
-// kernel assembly: one thread per (q, w, nu)
+// kernel assembly: one warp per (q, w, nu) matrix; lane l computes the elements l, l + 32, ... of every n2 x n2
+// product, whose left operands sit in the warp's shared scratch (g3, t1, t2: 3 n2^2 complex)
 //   chi0_inv: [Q][W][nv][n2][n2]; X: [2][Q][W][N][n2]; uv: [2][Q][n2][n2]; chi_phys: [2][Q][W][n2][n2]
 //   k_dc: [Q][W][nv][n2][n2] or null;  out K: [Q][W][nv][n2][n2];  gamma_out (optional): [2][Q][W][nv][n2][n2]
 // ------------------------------------------------------------------------------------------------
-__global__ void kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __restrict__ X,
+constexpr int KA_WARPS = 8;                            // matrices per block
+constexpr int KA_EPL = (MAX_N2 * MAX_N2 + 31) / 32;    // elements per lane
+__global__ void __launch_bounds__(32 * KA_WARPS, 2)
+kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __restrict__ X,
                                        const double2* __restrict__ uv, const double2* __restrict__ chi_phys,
                                        const double2* __restrict__ k_dc, int n2, int nv, int W, int Q, double beta,
                                        double2* __restrict__ K, double2* __restrict__ gamma_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nn = n2 * n2;
-  double2* s = reinterpret_cast<double2*>(smem_raw) + (size_t)threadIdx.x * 4 * nn;
-  double2* g3 = s;
-  double2* t1 = s + nn;
-  double2* t2 = s + 2 * nn;
-  double2* acc = s + 3 * nn;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double2* g3 = reinterpret_cast<double2*>(smem_raw) + (size_t)wib * 3 * nn;
+  double2* t1 = g3 + nn;
+  double2* t2 = t1 + nn;
+  const long long t = blockIdx.x * (long long)KA_WARPS + wib;
   const long long total = (long long)Q * W * nv;
-  if (t >= total) return;
+  if (t >= total) return;  // the whole warp; the block has no block-wide barrier
   const int v = (int)(t % nv);
   const long long qw = t / nv;
   const int q = (int)(qw / W);
   const int N = n2 * nv;
   const double2* c0i = chi0_inv + (size_t)t * nn;
-  if (k_dc) {
-    for (int e = 0; e < nn; ++e) {
+  double2 acc[KA_EPL];
+#pragma unroll
+  for (int j = 0; j < KA_EPL; ++j) {
+    const int e = lane + 32 * j;
+    acc[j] = make_double2(0.0, 0.0);
+    if (e < nn && k_dc) {
       const double2 z = k_dc[(size_t)t * nn + e];
-      acc[e] = make_double2(-z.x, -z.y);
+      acc[j] = make_double2(-z.x, -z.y);
     }
-  } else {
-    for (int e = 0; e < nn; ++e) acc[e] = make_double2(0.0, 0.0);
   }
   for (int ch = 0; ch < 2; ++ch) {
     const double2* x = X + ((size_t)ch * Q * W + qw) * N * n2;
-    // gamma = beta * (chi0_inv @ X_nu)
-    for (int p = 0; p < n2; ++p)
-      for (int sidx = 0; sidx < n2; ++sidx) {
-        double2 a = make_double2(0.0, 0.0);
-        for (int m = 0; m < n2; ++m) cfma(a, c0i[p * n2 + m], x[(size_t)(m * nv + v) * n2 + sidx]);
-        g3[p * n2 + sidx] = make_double2(beta * a.x, beta * a.y);
-      }
-    if (gamma_out) {
-      double2* go = gamma_out + ((size_t)ch * Q * W * nv + t) * nn;
-      for (int e = 0; e < nn; ++e) go[e] = g3[e];
-    }
     const double2* u = uv + ((size_t)ch * Q + q) * nn;
     const double2* cp = chi_phys + ((size_t)ch * Q * W + qw) * nn;
-    matmul_n(g3, u, t1, n2);   // gamma @ U_r
-    matmul_n(t1, cp, t2, n2);  // @ chi_r
-    for (int e = 0; e < nn; ++e) t1[e] = csub(g3[e], t2[e]);
-    if (ch == 1)
-      for (int p = 0; p < n2; ++p) t1[p * n2 + p].x += -(2.0 / 3.0);
-    matmul_n(u, t1, t2, n2);  // U_r @ (...)
-    const double f = ch == 0 ? 1.0 : 3.0;
-    for (int e = 0; e < nn; ++e) {
-      acc[e].x += f * t2[e].x;
-      acc[e].y += f * t2[e].y;
+    double2* go = gamma_out ? gamma_out + ((size_t)ch * Q * W * nv + t) * nn : nullptr;
+    // gamma = beta * (chi0_inv @ X_nu)
+#pragma unroll
+    for (int j = 0; j < KA_EPL; ++j) {
+      const int e = lane + 32 * j;
+      if (e >= nn) break;
+      const int p = e / n2, sidx = e - p * n2;
+      double2 a = make_double2(0.0, 0.0);
+      for (int m = 0; m < n2; ++m) cfma(a, c0i[p * n2 + m], x[(size_t)(m * nv + v) * n2 + sidx]);
+      g3[e] = make_double2(beta * a.x, beta * a.y);
+      if (go) go[e] = g3[e];
     }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < KA_EPL; ++j) {  // t1 = gamma @ U_r
+      const int e = lane + 32 * j;
+      if (e >= nn) break;
+      const int p = e / n2, sidx = e - p * n2;
+      double2 a = make_double2(0.0, 0.0);
+      for (int k = 0; k < n2; ++k) cfma(a, g3[p * n2 + k], u[k * n2 + sidx]);
+      t1[e] = a;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < KA_EPL; ++j) {  // t2 = gamma - t1 @ chi_r  (- 2/3 on the diagonal in the magnetic channel)
+      const int e = lane + 32 * j;
+      if (e >= nn) break;
+      const int p = e / n2, sidx = e - p * n2;
+      double2 a = make_double2(0.0, 0.0);
+      for (int k = 0; k < n2; ++k) cfma(a, t1[p * n2 + k], cp[k * n2 + sidx]);
+      double2 r = csub(g3[e], a);
+      if (ch == 1 && p == sidx) r.x += -(2.0 / 3.0);
+      t2[e] = r;
+    }
+    __syncwarp();
+    const double f = ch == 0 ? 1.0 : 3.0;
+#pragma unroll
+    for (int j = 0; j < KA_EPL; ++j) {  // K += f U_r @ t2
+      const int e = lane + 32 * j;
+      if (e >= nn) break;
+      const int p = e / n2, sidx = e - p * n2;
+      double2 a = make_double2(0.0, 0.0);
+      for (int k = 0; k < n2; ++k) cfma(a, u[p * n2 + k], t2[k * n2 + sidx]);
+      acc[j].x += f * a.x;
+      acc[j].y += f * a.y;
+    }
+    __syncwarp();  // g3, t1, t2 are rewritten by the next channel
   }
   double2* o = K + (size_t)t * nn;
-  for (int e = 0; e < nn; ++e) o[e] = acc[e];
+#pragma unroll
+  for (int j = 0; j < KA_EPL; ++j) {
+    const int e = lane + 32 * j;
+    if (e < nn) o[e] = acc[j];
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
-// K1 = (U_adcb / beta^2) @ chi0 for every (q, w, nu_full): one thread per matrix
+// K1 = (U_adcb / beta^2) @ chi0 for every (q, w, nu_full): one warp per matrix
 // ------------------------------------------------------------------------------------------------
 __global__ void dc_left_kernel(const double2* __restrict__ chi0, const double2* __restrict__ u_perm, int n2,
                                long long n_mats, double2* __restrict__ k1) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  // one warp per matrix, lane l computing the elements l, l + 32, ... (coalesced along the matrix)
+  const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (t >= n_mats) return;
   const int nn = n2 * n2;
   const double2* c = chi0 + (size_t)t * nn;
   double2* o = k1 + (size_t)t * nn;
-  for (int i = 0; i < n2; ++i)
-    for (int j = 0; j < n2; ++j) {
-      double2 a = make_double2(0.0, 0.0);
-      for (int k = 0; k < n2; ++k) cfma(a, u_perm[i * n2 + k], c[k * n2 + j]);
-      o[i * n2 + j] = a;
-    }
+  for (int e = lane; e < nn; e += 32) {
+    const int i = e / n2, j = e - i * n2;
+    double2 a = make_double2(0.0, 0.0);
+    for (int k = 0; k < n2; ++k) cfma(a, u_perm[i * n2 + k], c[k * n2 + j]);
+    o[e] = a;
+  }
 }
 
 // Batched complex GEMM C = A @ B over w with two-level row/column addressing:
@@ -537,11 +573,9 @@ int dga_kernel_assembly_c128(const void* chi0_inv, const void* X, const void* uv
     return DGA_ERR_ARG;
   }
   const long long total = (long long)n_q * niw_half * 2 * niv_core;
-  int th = 64;
-  while (th > 8 && (size_t)th * 4 * n2 * n2 * sizeof(double2) > 96 * 1024) th >>= 1;
-  const size_t smem = (size_t)th * 4 * n2 * n2 * sizeof(double2);
+  const size_t smem = (size_t)KA_WARPS * 3 * n2 * n2 * sizeof(double2);
   cudaFuncSetAttribute(kernel_assembly_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kernel_assembly_kernel<<<(int)((total + th - 1) / th), th, smem, stream>>>(
+  kernel_assembly_kernel<<<(int)((total + KA_WARPS - 1) / KA_WARPS), 32 * KA_WARPS, smem, stream>>>(
       (const double2*)chi0_inv, (const double2*)X, (const double2*)uv, (const double2*)chi_phys,
       (const double2*)k_dc, n2, 2 * niv_core, niw_half, n_q, beta, (double2*)K, (double2*)gamma_out);
   return vstatus("dga_kernel_assembly_c128");
@@ -566,7 +600,7 @@ int dga_dc_kernel_c128(const void* chi0, const void* u_perm, const void* fdc, in
     return DGA_ERR_SCRATCH;
   }
   const long long n_mats = (long long)n_q * niw_half * nvf;
-  dc_left_kernel<<<(int)((n_mats + 127) / 128), 128, 0, stream>>>((const double2*)chi0, (const double2*)u_perm, n2,
+  dc_left_kernel<<<(int)((n_mats * 32 + 255) / 256), 256, 0, stream>>>((const double2*)chi0, (const double2*)u_perm, n2,
                                                                   n_mats, (double2*)scratch);
   if (vstatus("dga_dc_kernel_c128")) return DGA_ERR_LAUNCH;
   DcGemmArgs a;
