@@ -295,7 +295,7 @@ def time_pass(lp, args, world: int, local: int, sample_clocks: bool):
 DRAM_BYTES_PER_ITEM = {
     "bse_solve_sum_fp64_kernel": 22.89e9 / 132,
     "bse_panel_mixed_kernel": (5.670e9 + 4.917e9) / 132,
-    "bse_panel_mixed_kernel<TC> (tcgen05 trailing tiles)": (5.938e9 + 4.916e9) / 132,
+    "bse_panel_mixed_kernel<TC> (tcgen05 trailing tiles)": (6.093e9 + 4.978e9) / 132,
     "bse_solve_sum_mixed_kernel": 11.79e9 / 132,
 }
 

@@ -35,6 +35,7 @@ constexpr int PNB = 32;       // panel width
 constexpr int PSB = 8;        // sub-panel width inside the panel factorisation
 constexpr int PTM = 128;      // trailing tile rows
 constexpr int PTN = 64;       // trailing strip columns
+static_assert(4 * PW == PTN, "prefetch_c_tile gives each warp four columns of a strip");
 constexpr int P_MAX_SMEM = 232448;  // 227 KB opt-in shared memory per block on sm_100
 #ifndef DGA_PANEL_TILE_UNROLL
 #define DGA_PANEL_TILE_UNROLL 8
@@ -341,6 +342,13 @@ __device__ __forceinline__ void prefetch_factor_cols(const float2* A, int N, int
   }
 }
 
+// L2 prefetch of rows [r0, min(r0 + nr, N)) of the strip's columns [cs, cs + cw), spread over the CTA's warps
+// (warp w takes columns 4w .. 4w + 3; PW * 4 = PTN covers the strip).
+__device__ __forceinline__ void prefetch_c_tile(const float2* A, int N, int cs, int cw, int r0, int nr) {
+  const int c0 = 4 * (threadIdx.x >> 5);
+  if (c0 < cw) prefetch_factor_cols(A, N, cs + c0, min(4, cw - c0), r0, min(r0 + nr, N));
+}
+
 // inv: per panel b, L11^-1 at inv + 2048 b and U11^-1 at inv + 2048 b + 1024 (panel_diag_inverses).
 template <bool TC>
 __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, uint32_t& parity,
@@ -376,6 +384,9 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
     // ---- per 64-column strip: interchanges + U12, then the strip's trailing tiles ----
     for (int cs = k1; cs < NC; cs += PTN) {
       const int cw = min(PTN, NC - cs);
+      // L2 prefetch of the strip's first two C tiles (warp w: columns 4w .. 4w + 3); the tile loop keeps two
+      // tiles ahead, so the C stream reads from L2 instead of waiting on DRAM
+      if (TC) prefetch_c_tile(A, N, cs, cw, k1, 2 * TC_M);
       {
         // warp w handles columns w, w + 16, w + 32, w + 48 of the strip; lane = row of the U block (reads of the
         // touched rows are coalesced along the column).  Every old value is read, and U12 computed, before the
@@ -509,6 +520,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
           issue(0);
         }
         for (int i = 0; i < ntiles; ++i) {
+          if (i + 2 < ntiles) prefetch_c_tile(A, N, cs, cw, k1 + (i + 2) * TC_M, TC_M);
           if (i + 1 < ntiles) stage(i + 1);
           finish(i);
           if (i + 1 < ntiles) {
