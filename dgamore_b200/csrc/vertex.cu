@@ -130,48 +130,67 @@ __global__ void chi0_sums_kernel(const double2* __restrict__ chi0, int n2, int n
 }
 
 // ------------------------------------------------------------------------------------------------
-// physical susceptibility: one thread per (ch, q, w)
+// physical susceptibility: one warp per (ch, q, w)
 //   X: [n_ch][Q][W][N][n2] with row i = p * nv + nu;  uv: [n_ch][Q][n2][n2];  sums: [Q][W][n2][n2]
 //   out: [n_ch][Q][W][n2][n2]
+// The nu sum reads the item's X block coalesced: lane g * n2 + s (g < G = 32 / n2) sums column s over the rows
+// nu = g, g + G, ..., and the G partial sums of a column are added by shuffles.  The two n2 x n2 inverses run on
+// one lane from the warp's shared-memory copy.
 // ------------------------------------------------------------------------------------------------
-__global__ void chi_phys_kernel(const double2* __restrict__ X, const double2* __restrict__ uv,
-                                const double2* __restrict__ full_sum, const double2* __restrict__ core_sum, int n2,
-                                int nv, int W, int Q, int n_ch, double inv_beta, double2* __restrict__ out,
-                                int* __restrict__ status) {
+constexpr int CP_WARPS = 4;  // items per block
+__global__ void __launch_bounds__(32 * CP_WARPS)
+chi_phys_kernel(const double2* __restrict__ X, const double2* __restrict__ uv, const double2* __restrict__ full_sum,
+                const double2* __restrict__ core_sum, int n2, int nv, int W, int Q, int n_ch, double inv_beta,
+                double2* __restrict__ out, int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* s = reinterpret_cast<double2*>(smem_raw);
   const int nn = n2 * n2;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* mine = reinterpret_cast<double2*>(smem_raw) + (size_t)wib * nn;
+  const long long t = blockIdx.x * (long long)CP_WARPS + wib;
   const long long total = (long long)n_ch * Q * W;
   if (t >= total) return;
   const int w = (int)(t % W);
   const int q = (int)((t / W) % Q);
   const int ch = (int)(t / ((long long)W * Q));
-  double2* mine = s + threadIdx.x;
   const int N = n2 * nv;
   const double2* x = X + (size_t)t * N * n2;
   const size_t qw = (size_t)q * W + w;
-  for (int p = 0; p < n2; ++p)
-    for (int sidx = 0; sidx < n2; ++sidx) {
-      double sr = 0.0, si = 0.0;
-      for (int v = 0; v < nv; ++v) {
-        const double2 y = x[(size_t)(p * nv + v) * n2 + sidx];
+  const int G = 32 / n2, g = lane / n2, sc = lane - g * n2;
+  for (int p = 0; p < n2; ++p) {
+    double sr = 0.0, si = 0.0;
+    if (g < G)
+      for (int v = g; v < nv; v += G) {
+        const double2 y = x[(size_t)(p * nv + v) * n2 + sc];
         sr += y.x;
         si += y.y;
       }
-      // (sum / beta + full) - core
-      const double2 f = full_sum[qw * nn + p * n2 + sidx];
-      const double2 c = core_sum[qw * nn + p * n2 + sidx];
-      const double ar = inv_beta * sr + f.x, ai = inv_beta * si + f.y;
-      mine[(p * n2 + sidx) * blockDim.x] = make_double2(ar - c.x, ai - c.y);
+    for (int h = 1; h < G; ++h) {  // lanes 0 .. n2 - 1 collect the partial sums of lanes sc + h n2
+      const int src = min(lane + h * n2, 31);
+      const double pr = __shfl_sync(0xffffffffu, sr, src), pi = __shfl_sync(0xffffffffu, si, src);
+      if (g == 0) {
+        sr += pr;
+        si += pi;
+      }
     }
-  bool ok = gj_inverse(mine, n2, blockDim.x);
-  const double2* u = uv + ((size_t)ch * Q + q) * nn;
-  for (int e = 0; e < nn; ++e) mine[e * blockDim.x] = cadd(mine[e * blockDim.x], u[e]);
-  ok = gj_inverse(mine, n2, blockDim.x) && ok;
+    if (g == 0) {
+      // (sum / beta + full) - core
+      const double2 f = full_sum[qw * nn + p * n2 + sc];
+      const double2 c = core_sum[qw * nn + p * n2 + sc];
+      const double ar = inv_beta * sr + f.x, ai = inv_beta * si + f.y;
+      mine[p * n2 + sc] = make_double2(ar - c.x, ai - c.y);
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    bool ok = gj_inverse(mine, n2, 1);
+    const double2* u = uv + ((size_t)ch * Q + q) * nn;
+    for (int e = 0; e < nn; ++e) mine[e] = cadd(mine[e], u[e]);
+    ok = gj_inverse(mine, n2, 1) && ok;
+    if (!ok && status) atomicOr(status, DGA_ITEM_SINGULAR);
+  }
+  __syncwarp();
   double2* o = out + (size_t)t * nn;
-  for (int e = 0; e < nn; ++e) o[e] = mine[e * blockDim.x];
-  if (!ok && status) atomicOr(status, DGA_ITEM_SINGULAR);
+  for (int e = lane; e < nn; e += 32) o[e] = mine[e];
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -539,10 +558,8 @@ int dga_chi_phys_c128(const void* X, const void* uv, const void* full_sum, const
     return DGA_ERR_ARG;
   }
   const long long total = (long long)n_ch * n_q * niw_half;
-  const int th = small_threads(n2);
-  const size_t smem = (size_t)th * n2 * n2 * sizeof(double2);
-  cudaFuncSetAttribute(chi_phys_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  chi_phys_kernel<<<(int)((total + th - 1) / th), th, smem, stream>>>(
+  const size_t smem = (size_t)CP_WARPS * n2 * n2 * sizeof(double2);
+  chi_phys_kernel<<<(int)((total + CP_WARPS - 1) / CP_WARPS), 32 * CP_WARPS, smem, stream>>>(
       (const double2*)X, (const double2*)uv, (const double2*)full_sum, (const double2*)core_sum, n2, 2 * niv_core,
       niw_half, n_q, n_ch, 1.0 / beta, (double2*)out, status);
   return vstatus("dga_chi_phys_c128");
