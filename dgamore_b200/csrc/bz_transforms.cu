@@ -37,17 +37,32 @@ __device__ void plane_dft(double2* a, double2* b, const double2* s_tw, const Gri
   const double2* twy = s_tw + g.nx;
   const double2* twz = s_tw + g.nx + g.ny;
   const int nyz = g.ny * g.nz;
-  // x axis: a -> b
-  for (int e = threadIdx.x; e < g.nk; e += T) {
-    const int kx = e / nyz, yz = e - kx * nyz;
-    double2 acc = make_double2(0.0, 0.0);
-    int m = 0;
-    for (int x = 0; x < g.nx; ++x) {
-      cfma(acc, a[x * nyz + yz], twx[m]);
-      m += kx;
-      if (m >= g.nx) m -= g.nx;
+  // x axis: a -> b.  A thread computes the outputs kx = grp + j ngx (j < XR) of one yz column, so each load of a
+  // serves XR products (the twiddle loads are warp broadcasts); every output still sums over x in order.
+  constexpr int XR = 4;
+  const int ngx = (g.nx + XR - 1) / XR;
+  for (int t = threadIdx.x; t < ngx * nyz; t += T) {
+    const int grp = t / nyz, yz = t - grp * nyz;
+    double2 acc[XR];
+    int m[XR], kx[XR];
+#pragma unroll
+    for (int j = 0; j < XR; ++j) {
+      acc[j] = make_double2(0.0, 0.0);
+      m[j] = 0;
+      kx[j] = min(grp + j * ngx, g.nx - 1);  // outputs past nx are computed on a valid index and dropped
     }
-    b[e] = acc;
+    for (int x = 0; x < g.nx; ++x) {
+      const double2 v = a[x * nyz + yz];
+#pragma unroll
+      for (int j = 0; j < XR; ++j) {
+        cfma(acc[j], v, twx[m[j]]);
+        m[j] += kx[j];
+        if (m[j] >= g.nx) m[j] -= g.nx;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < XR; ++j)
+      if (grp + j * ngx < g.nx) b[(grp + j * ngx) * nyz + yz] = acc[j];
   }
   __syncthreads();
   // y axis: b -> a
