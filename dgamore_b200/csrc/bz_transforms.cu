@@ -29,17 +29,13 @@ __device__ __forceinline__ void load_twiddles(double2* s_tw, const double2* tw, 
   for (int i = threadIdx.x; i < g.nx + g.ny + g.nz; i += blockDim.x) s_tw[i] = tw[i];
 }
 
-// out[kx][y][z] = sum_x in[x][y][z] * twx[(kx*x) % nx], then along y, then z (skipped when the axis has
-// length 1).  Result ends in `a` (the input buffer); `b` is work space.  Both buffers hold g.nk points.
-__device__ void plane_dft(double2* a, double2* b, const double2* s_tw, const Grid3 g) {
-  const int T = blockDim.x;
-  const double2* twx = s_tw;
-  const double2* twy = s_tw + g.nx;
-  const double2* twz = s_tw + g.nx + g.ny;
-  const int nyz = g.ny * g.nz;
-  // x axis: a -> b.  A thread computes the outputs kx = grp + j ngx (j < XR) of one yz column, so each load of a
-  // serves XR products (the twiddle loads are warp broadcasts); every output still sums over x in order.
-  constexpr int XR = 4;
+// DFT along x of an nx x (ny nz) plane in shared memory (in -> out, both [x][yz]; twx = the nx twiddles),
+// followed by a barrier.
+constexpr int XR = 4;  // outputs per thread of the blocked axis passes
+__device__ __forceinline__ void dft_axis_x(const double2* in, double2* out, const double2* twx, const Grid3 g) {
+  const int T = blockDim.x, nyz = g.ny * g.nz;
+  // A thread computes the outputs kx = grp + j ngx (j < XR) of one yz column, so each load serves XR
+  // products (the twiddle loads are warp broadcasts); every output still sums over x in order.
   const int ngx = (g.nx + XR - 1) / XR;
   for (int t = threadIdx.x; t < ngx * nyz; t += T) {
     const int grp = t / nyz, yz = t - grp * nyz;
@@ -52,7 +48,7 @@ __device__ void plane_dft(double2* a, double2* b, const double2* s_tw, const Gri
       kx[j] = min(grp + j * ngx, g.nx - 1);  // outputs past nx are computed on a valid index and dropped
     }
     for (int x = 0; x < g.nx; ++x) {
-      const double2 v = a[x * nyz + yz];
+      const double2 v = in[x * nyz + yz];
 #pragma unroll
       for (int j = 0; j < XR; ++j) {
         cfma(acc[j], v, twx[m[j]]);
@@ -62,22 +58,45 @@ __device__ void plane_dft(double2* a, double2* b, const double2* s_tw, const Gri
     }
 #pragma unroll
     for (int j = 0; j < XR; ++j)
-      if (grp + j * ngx < g.nx) b[(grp + j * ngx) * nyz + yz] = acc[j];
+      if (grp + j * ngx < g.nx) out[(grp + j * ngx) * nyz + yz] = acc[j];
   }
   __syncthreads();
-  // y axis: b -> a
-  for (int e = threadIdx.x; e < g.nk; e += T) {
-    const int kx = e / nyz, r = e - kx * nyz;
+}
+
+// out[kx][y][z] = sum_x in[x][y][z] * twx[(kx*x) % nx], then along y, then z (skipped when the axis has
+// length 1).  Result ends in `a` (the input buffer); `b` is work space.  Both buffers hold g.nk points.
+__device__ void plane_dft(double2* a, double2* b, const double2* s_tw, const Grid3 g) {
+  const int T = blockDim.x;
+  const double2* twx = s_tw;
+  const double2* twy = s_tw + g.nx;
+  const double2* twz = s_tw + g.nx + g.ny;
+  const int nyz = g.ny * g.nz;
+  dft_axis_x(a, b, twx, g);  // x axis: a -> b
+  const int ngx = (g.nx + XR - 1) / XR;
+  // y axis: b -> a.  A thread computes the outputs of one (ky, z) for the rows kx = grp + j ngx (j < XR), so each
+  // twiddle load (distinct across the lanes) serves XR products and the row loads are warp broadcasts; every
+  // output still sums over y in order.
+  for (int t = threadIdx.x; t < ngx * nyz; t += T) {
+    const int grp = t / nyz, r = t - grp * nyz;
     const int ky = r / g.nz, z = r - ky * g.nz;
-    const double2* row = b + kx * nyz + z;
-    double2 acc = make_double2(0.0, 0.0);
+    double2 acc[XR];
+    const double2* row[XR];
+#pragma unroll
+    for (int j = 0; j < XR; ++j) {
+      acc[j] = make_double2(0.0, 0.0);
+      row[j] = b + min(grp + j * ngx, g.nx - 1) * nyz + z;  // rows past nx are read on a valid row and dropped
+    }
     int m = 0;
     for (int y = 0; y < g.ny; ++y) {
-      cfma(acc, row[y * g.nz], twy[m]);
+      const double2 w = twy[m];
+#pragma unroll
+      for (int j = 0; j < XR; ++j) cfma(acc[j], row[j][y * g.nz], w);
       m += ky;
       if (m >= g.ny) m -= g.ny;
     }
-    a[e] = acc;
+#pragma unroll
+    for (int j = 0; j < XR; ++j)
+      if (grp + j * ngx < g.nx) a[(grp + j * ngx) * nyz + r] = acc[j];
   }
   __syncthreads();
   if (g.nz > 1) {
@@ -178,22 +197,7 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
         P[r] = cmul(gad[r], gcb[(xm * g.ny + ym) * g.nz + zm]);
       }
       __syncthreads();
-      // x axis in full (P -> T1)
-      {
-        const double2* twx = s_tw;
-        for (int e = threadIdx.x; e < g.nk; e += blockDim.x) {
-          const int kx = e / nyz, yz = e - kx * nyz;
-          double2 acc = make_double2(0.0, 0.0);
-          int m = 0;
-          for (int x = 0; x < g.nx; ++x) {
-            cfma(acc, P[x * nyz + yz], twx[m]);
-            m += kx;
-            if (m >= g.nx) m -= g.nx;
-          }
-          T1[e] = acc;
-        }
-      }
-      __syncthreads();
+      dft_axis_x(P, T1, s_tw, g);  // x axis in full (P -> T1)
       // y and z axes only at the irreducible q points
       const double2* twy = s_tw + g.nx;
       const double2* twz = s_tw + g.nx + g.ny;
