@@ -118,9 +118,11 @@ def _blk(nbytes: int) -> int:
 
 
 def sigma_chunks_for(sh: PassShapes) -> int:
-    """(nu, i, j, w-chunk) CTAs of the Sigma contraction: enough to fill 148 SMs twice."""
+    """(nu, i, j, w-chunk) CTAs of the Sigma contraction: at least four waves of its two resident CTAs per SM on
+    148 SMs (1,184 CTAs), so that the last wave's tail is short (the 3-orbital 32x32 pass has 360 (nu, i, j)
+    units: 4 chunks)."""
     base = sh.niv * sh.n2
-    return max(1, min(2 * sh.niw + 1, -(-296 // base)))
+    return max(1, min(2 * sh.niw + 1, -(-1184 // base)))
 
 
 def estimate_device_bytes(sh: PassShapes, precision: str = "fp64", keep_intermediates: bool = True,
