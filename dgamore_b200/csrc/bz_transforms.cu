@@ -235,8 +235,11 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
 //   kern: [Q][W][nv][n2][n2] irreducible kernel, matrix row (a,i), column (d,j); W = niw+1, nv = 2 niv
 //   g_r:  [T][n][n][Nk] with slot t = nu_index + niw, nu_index in [-niw, niv+niw)
 //   part: [n_chunks][niv][n2][Nk]
+//   MAXR: accumulators per thread (Nk <= MAXR * BZ_THREADS), so small grids hold fewer registers and keep more
+//   CTAs resident
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(BZ_THREADS) sigma_partial_kernel(const double2* __restrict__ kern,
+template <int MAXR>
+__global__ void __launch_bounds__(BZ_THREADS, MAXR <= 4 ? 3 : 1) sigma_partial_kernel(const double2* __restrict__ kern,
                                                                     const double2* __restrict__ g_r, int nb, int niv,
                                                                     int niw, int Q, Grid3 g,
                                                                     const int* __restrict__ irrk_inv,
@@ -253,7 +256,6 @@ __global__ void __launch_bounds__(BZ_THREADS) sigma_partial_kernel(const double2
   const int n2 = nb * nb, nv = 2 * niv, W = niw + 1, nwf = 2 * niw + 1;
   const int per_chunk = (nwf + n_chunks - 1) / n_chunks;
   const int total = niv * n2 * n_chunks;
-  constexpr int MAXR = BZ_MAX_NK / BZ_THREADS;
   for (int blk = blockIdx.x; blk < total; blk += gridDim.x) {
     const int chunk = blk % n_chunks;
     const int ij = (blk / n_chunks) % n2;
@@ -453,11 +455,16 @@ int dga_sigma_c128(const void* kern, const void* g_r, int n_orb, int niv, int ni
   double2* part = (double2*)scratch;
   double2* sig = part + (size_t)n_chunks * niv * n2 * g.nk;
   size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + sizeof(int) * (size_t)g.nk;
-  cudaFuncSetAttribute(sigma_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long work = (long long)niv * n2 * n_chunks;
-  sigma_partial_kernel<<<grid_cap(work), BZ_THREADS, smem, stream>>>(
-      (const double2*)kern, (const double2*)g_r, n_orb, niv, niw, n_q, g, irrk_inv, (const double2*)tw_inv, n_chunks,
-      part);
+  auto partial = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<grid_cap(work), BZ_THREADS, smem, stream>>>((const double2*)kern, (const double2*)g_r, n_orb, niv, niw,
+                                                         n_q, g, irrk_inv, (const double2*)tw_inv, n_chunks, part);
+  };
+  static_assert(16 * BZ_THREADS >= BZ_MAX_NK, "the largest accumulator set covers the largest grid");
+  if (g.nk <= 4 * BZ_THREADS) partial(sigma_partial_kernel<4>);
+  else if (g.nk <= 8 * BZ_THREADS) partial(sigma_partial_kernel<8>);
+  else partial(sigma_partial_kernel<16>);
   if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
   const long long n_out = (long long)niv * n2 * g.nk;
   const double factor = -0.5 / beta / (double)g.nk;
