@@ -138,12 +138,13 @@ def barrier(world: int):
         dist.barrier()
 
 
-def gemm_peak_tflops(dtype_name: str = "float64") -> float:
-    """cuBLAS GEMM 8192^3 best of 5 on this GPU in FP64 or FP32 without TF32 (the FP64 / FP32 denominators;
-    MEASURED_PEAKS.json holds only the bf16 and HBM peaks)."""
+def gemm_peak_tflops(dtype_name: str = "float64", tf32: bool = False) -> float:
+    """cuBLAS GEMM 8192^3 best of 5 on this GPU: FP64 (DMMA), FP32 without TF32 (CUDA cores) or FP32 with TF32
+    allowed (the TF32 tensor-core rate) -- the denominators MEASURED_PEAKS.json does not hold (it has bf16 and
+    HBM only)."""
     import torch
 
-    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = bool(tf32)
     dtype = getattr(torch, dtype_name)
     n = 8192
     a = torch.randn(n, n, dtype=dtype, device="cuda")
@@ -160,6 +161,7 @@ def gemm_peak_tflops(dtype_name: str = "float64") -> float:
         best = min(best, s.elapsed_time(e) / 1e3)
     del a, b
     torch.cuda.empty_cache()
+    torch.backends.cuda.matmul.allow_tf32 = False
     return 2.0 * n**3 / best / 1e12
 
 
@@ -434,10 +436,22 @@ def run_ours(args, rank: int, world: int, local: int):
 
     fp64_peak = gemm_peak_tflops("float64") if rank == 0 else None
     fp32_peak = gemm_peak_tflops("float32") if rank == 0 else None
-    peak = fp32_peak if args.precision == "mixed" else fp64_peak
+    tf32_peak = gemm_peak_tflops("float32", tf32=True) if rank == 0 else None
+    tensor_kernel = args.precision == "mixed" and "TC" in kname or "tcgen05" in kname
+    peak = (tf32_peak if tensor_kernel else fp32_peak) if args.precision == "mixed" else fp64_peak
     flops_launch = sh.n_solves * f_solve(sh.N, sh.n2)
     achieved = flops_launch / (bse_ms / 1e3) / 1e12
     per_item = DRAM_BYTES_PER_ITEM.get(kname)
+    peaks = measured_peaks()
+    algo_bytes = 2 * sh.W * sh.N * sh.N * 16 + sh.n_solves * (sh.nv * sh.n2 * sh.n2 + sh.N * sh.n2) * 16
+    if args.precision == "mixed" and tensor_kernel:
+        peak_source = ("cuBLAS FP32 GEMM 8192^3 with TF32 allowed (the TF32 tensor-core rate), measured in this run; "
+                       "the kernel issues every trailing-update product as three TF32 MMAs (hi*hi + hi*lo + lo*hi), "
+                       "so its tensor pipe does 3x the algorithmic flops of the update")
+    elif args.precision == "mixed":
+        peak_source = "cuBLAS FP32 SGEMM 8192^3 without TF32 (CUDA cores), measured in this run"
+    else:
+        peak_source = "cuBLAS FP64 DGEMM 8192^3, measured in this run"
     serving = {}
     if args.serve_requests > 0 and rank == 0:
         for prec in ("fp64", "mixed"):
@@ -492,13 +506,19 @@ def run_ours(args, rank: int, world: int, local: int):
             "peak": peak,
             "unit": "TFLOP/s",
             "frac": (achieved / peak) if peak else None,
-            "peak_source": ("FP32 cuBLAS SGEMM (no TF32) 8192^3" if args.precision == "mixed" else "FP64 cuBLAS DGEMM 8192^3")
-            + " measured in this run (MEASURED_PEAKS.json has bf16 and HBM only)",
+            "frac_note": "achieved = flops_per_launch / bse_ms_per_launch (algorithmic complex-LU flops, "
+            "8/3 N^3 + 8 n2 N^2 per solve); frac = achieved / peak",
+            "peak_source": peak_source,
+            "peaks_measured_tflops": {"tf32_tensor": tf32_peak, "fp32_cuda_core": fp32_peak, "fp64": fp64_peak,
+                                      "bf16_sustained (MEASURED_PEAKS.json)": peaks.get("bf16_tflops_sustained")},
+            "frac_of_bf16_sustained": (achieved / peaks["bf16_tflops_sustained"])
+            if peaks.get("bf16_tflops_sustained") else None,
             "flops_per_launch": flops_launch,
             "bse_ms_per_launch": bse_ms,
             "traffic": None if per_item is None else per_item * sh.n_solves,
-            "traffic_note": "ncu DRAM bytes per item of a 132-item launch of the same kernel, times the items",
-            "algorithmic_bytes": 2 * sh.W * sh.N * sh.N * 16 + sh.n_solves * (sh.nv * sh.n2 * sh.n2 + sh.N * sh.n2) * 16,
+            "traffic_note": "ncu DRAM bytes per item of a single-wave launch of the same kernel, times the items",
+            "algorithmic_bytes": algo_bytes,
+            "traffic_over_algorithmic": None if per_item is None else per_item * sh.n_solves / algo_bytes,
         },
         "bse_status_nonzero": status,
         "clocks": clocks.summary(),

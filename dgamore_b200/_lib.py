@@ -20,6 +20,7 @@ PD = _c.c_void_p
 # name -> (restype, argtypes); must match include/dga_b200.h
 SIGNATURES = {
     "dga_version": (I, []),
+    "dga_device_sm_count": (I, []),
     "dga_last_error_string": (_c.c_char_p, []),
     "dga_strided_copy_c128": (I, [VP, VP, I, PLL, PLL, PLL, D, VP]),
     "dga_dft_planes_c128": (I, [VP, LL, LL, LL, VP, LL, LL, LL, I, I, I, I, I, VP, D, VP]),
@@ -57,7 +58,7 @@ SIGNATURES = {
 class BseTuning(_c.Structure):
     """``dga_bse_tuning`` of include/dga_b200.h (kernel choice and CTAs per SM of the BSE solvers)."""
 
-    _fields_ = [("kernel", I), ("ctas_per_sm", I)]
+    _fields_ = [("kernel", I), ("ctas_per_sm", I), ("wait_limit", LL)]
 
 
 class BseProblem(_c.Structure):

@@ -47,37 +47,43 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources() + _headers())
 
 
+def _compile_cmd(nvcc: str, src: str, obj: str, ptxas_info: bool) -> list[str]:
+    cmd = [nvcc, *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-fmad=true", "-Xcompiler", "-fPIC", "-c",
+           "-I", os.path.join(os.path.dirname(HERE), "include"), "-o", obj, src]
+    if ptxas_info:
+        cmd.insert(1, "-Xptxas=-v")
+    return cmd
+
+
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    """Compiles every .cu under csrc/ into one shared library next to this file; returns its path."""
+    """Compiles every .cu under csrc/ (one nvcc process per file, in parallel) and links them into one shared
+    library next to this file; returns its path."""
     if not force and up_to_date():
         return LIB_PATH
     nvcc = nvcc_path()
-    cmd = [
-        nvcc,
-        *ARCH_FLAGS,
-        "-O3",
-        "-lineinfo",
-        "-std=c++17",
-        "-fmad=true",
-        "-Xcompiler",
-        "-fPIC",
-        "-shared",
-        "-I",
-        os.path.join(os.path.dirname(HERE), "include"),
-        "-o",
-        LIB_PATH + ".tmp",
-        *sources(),
-        "-lcudart",
-    ]
-    if ptxas_info:
-        cmd.insert(1, "-Xptxas=-v")
-    if verbose:
-        print(" ".join(cmd))
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    obj_dir = os.path.join(os.path.dirname(HERE), "_build", "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    jobs = []
+    for src in sources():
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        cmd = _compile_cmd(nvcc, src, obj, ptxas_info)
+        if verbose:
+            print(" ".join(cmd))
+        jobs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    objs, errors = [], []
+    for src, obj, proc in jobs:
+        out, err = proc.communicate()
+        if proc.returncode != 0:
+            errors.append(f"nvcc failed on {os.path.basename(src)} ({proc.returncode}):\n{out}\n{err}")
+        elif ptxas_info or verbose:
+            sys.stderr.write(err)
+        objs.append(obj)
+    if errors:
+        raise RuntimeError("\n".join(errors))
+    link = [nvcc, *ARCH_FLAGS, "-shared", "-Xcompiler", "-fPIC", "-o", LIB_PATH + ".tmp", *objs, "-lcudart"]
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
-    if ptxas_info or verbose:
-        sys.stderr.write(res.stderr)
+        raise RuntimeError(f"nvcc link failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
     os.replace(LIB_PATH + ".tmp", LIB_PATH)
     return LIB_PATH
 

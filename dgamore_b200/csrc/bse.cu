@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   double2* Y = A + (size_t)N * N;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     // re-solve mode: only the items whose status says the mixed solve did not converge or was not finite
-    if (redo_only && (status[item] & (DGA_ITEM_NOCONVERGE | DGA_ITEM_NONFINITE)) == 0) continue;
+    if (redo_only && (status[item] & DGA_ITEM_REDO) == 0) continue;
     const WorkItem wi = work[item];
     double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * n2;
     const int st = solve_item_fp64<Source, NR>(src, wi, N, nv, beta, o, A, Y, sm, piv, perm);
@@ -680,7 +680,7 @@ __global__ void __launch_bounds__(BSE_THREADS, MIXED ? DGA_MIXED_MIN_BLOCKS : 3)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    if (redo_only && (status[item] & (DGA_ITEM_NOCONVERGE | DGA_ITEM_NONFINITE)) == 0) continue;
+    if (redo_only && (status[item] & DGA_ITEM_REDO) == 0) continue;
     const MultiItem mi = work[item];
     const dga_bse_problem d = probs[mi.prob];
     struct {
@@ -1371,22 +1371,18 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
 // ------------------------------------------------------------------------------------------------
 // Tuned entry: the same solves with an explicit kernel choice and CTAs per SM (the autotuner's knobs)
 // ------------------------------------------------------------------------------------------------
-static int sm_count() {
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return sms;
-}
+static int sm_count() { return device_sm_count(); }
 
 // 1 = panel kernel, 2 = 128-thread kernel, 3 = panel kernel with tensor-core trailing tiles,
 // -1 = the requested kernel cannot run this size
 static int tuned_kernel(int mixed, int N, int n2, const dga_bse_tuning* t) {
   const int k = t ? t->kernel : 0;
-  if (k < 0 || k > 3) return -1;
-  if (!mixed) return (k == 1 || k == 3) ? -1 : 2;
+  if (k < 0 || k > 4) return -1;
+  if (!mixed) return (k == 1 || k == 3 || k == 4) ? -1 : 2;
   if (k == 0) return default_mixed_kernel(N, n2);
   if (k == 1 && !dga_panel_supported(N, n2)) return -1;
   if (k == 3 && !dga_panel_supported(N, n2, true)) return -1;
+  if (k == 4 && !dga_block_supported(N, n2)) return -1;
   return k;
 }
 
@@ -1396,6 +1392,11 @@ static int tuned_grid(int kernel, int mixed, int N, int n2, int n_items, const d
     *slot = dga_panel_slot_bytes(N, n2);
     *smem = 0;
     return dga_panel_grid(n2, N, n_items, kernel == 3);
+  }
+  if (kernel == 4) {
+    *slot = dga_block_slot_bytes(N, n2);
+    *smem = 0;
+    return dga_block_grid(n2, n_items);
   }
   int grid;
   if (mixed) {
@@ -1463,7 +1464,11 @@ int dga_bse_solve_sum_tuned_c128(int n_orb, int niv, int niw_half, int n_q, int 
   cudaError_t err;
   if (kernel == 1 || kernel == 3) {
     err = dga_panel_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, max_iter, tol,
-                           (double2*)out, status, iters, (unsigned char*)scratch, slot, stream, kernel == 3);
+                           (double2*)out, status, iters, (unsigned char*)scratch, slot, stream, kernel == 3,
+                           t ? t->wait_limit : 0);
+  } else if (kernel == 4) {
+    err = dga_block_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, max_iter, tol,
+                           (double2*)out, status, iters, (unsigned char*)scratch, slot, stream, t ? t->wait_limit : 0);
   } else if (mixed) {
 #define DGA_TUNED_MIXED_CASE(NRV)                                                                                    \
   case NRV:                                                                                                          \

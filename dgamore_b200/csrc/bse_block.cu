@@ -1,0 +1,779 @@
+// Mixed-precision ladder BSE, block form: the LU's pivot search restricted to 32 x 32 diagonal blocks, every
+// update on the tensor cores (kernel choice 4 of dga_bse_tuning).
+//
+// Same result as the other mixed kernels: X = sum_nu' A^-1 / beta for each (channel, q, w) work item
+// (dgamore/four_point.py:620-684, reached from nonlocal_sde.py:85-156), with A = chi0^-1 + (Gamma_r - U_r - V_r^q)
+// / beta^2 formed in FP64 (the upstream's order of operations) and stored as complex64, factored with FP32-level
+// products, and refined in FP64 until the correction is below tol max|Y|.
+//
+// Factorisation: block Gaussian elimination on 32 x 32 blocks in Schur-complement form.  Step k:
+//   D_k^-1                  inverse of the current diagonal block, by Gauss-Jordan elimination with partial
+//                           pivoting inside the block (one warp; the row interchanges end up inside D_k^-1);
+//   W_k = D_k^-1 A[k, >k]   the block row, overwritten in place (tensor cores, transposed 128-column tiles);
+//   A[>k, >k] -= A[>k, k] W_k   the trailing update (tensor cores, 128 x 32 tiles); the block column is kept.
+// Then A = L U with L = [I; A_ik D_k^-1] and U = [D_k, A_kj], so the solves are
+//   forward   y_k <- D_k^-1 y_k, then y_i -= A_ik y_k for i > k;
+//   backward  x_k = y_k - sum_{j > k} W_kj x_j.
+// The n2 selector columns ride along as extra columns, so after the factorisation they hold the forward result.
+// Restricting the pivot search to the diagonal block removes the CTA-wide, column-by-column pivot chain; the
+// FP64 refinement restores full accuracy (one correction at the 3-orbital size, as with partial pivoting).  An
+// exactly singular diagonal block, or a refinement that does not converge (small pivots inside a block), flags
+// the item DGA_ITEM_NOCONVERGE for the FP64 re-solve with partial pivoting.
+//
+// Tensor-core products (tcgen05.mma kind::tf32): complex operands as planar (Re, Im) TF32 matrices with the
+// three-term split x = x_hi + x_lo (A B ~ A_lo B_hi + A_hi B_lo + A_hi B_hi, the dropped A_lo B_lo is 2^-22
+// relative), four real products per complex product with the signs from the instruction descriptor's negate
+// bit; the (Re, Im) accumulators, 128 x 32 fp32 each, live in tensor memory.  Operands are K-major without
+// swizzle in shared memory: element (row, k) of a plane at float offset kb_off(row, k).
+//
+// One 256-thread CTA per item, two CTAs per SM (about 105 KB of shared memory and 128 TMEM columns each), so the
+// latency-bound steps of one item (diagonal inverses, triangular solves, the FP64 residual) overlap the other
+// item's tiles.  Every wait on a tile's completion barrier is bounded; a CTA whose wait runs out issues no more
+// tiles, flags its items DGA_ITEM_WAIT_TIMEOUT and drains what it issued before exiting.
+#include "bse_core.cuh"
+#include "tc_tile.cuh"
+
+namespace dga {
+
+constexpr int KT = 256;        // threads per CTA
+constexpr int KW = KT / 32;    // warps
+constexpr int KB = 32;         // diagonal block size (the pivot search stays inside it) = K of every product
+constexpr int KTM = 128;       // tile rows (TMEM lanes)
+constexpr int KTN = 32;        // tile complex columns
+constexpr int KAP = KTM * KB;  // floats of one A plane (128 x 32)
+constexpr int KBP = KTN * KB;  // floats of one B plane (32 x 32)
+constexpr int K_REGION = 4 * KAP * 4 + 2 * 4 * KBP * 4;  // A planes (64 KB) + two B plane sets (2 x 16 KB)
+constexpr int K_DLD = 33;                                 // leading dimension of the diagonal inverse in smem
+constexpr uint32_t K_SBO = 1024;                          // 8 rows x 32 floats: stride byte offset of a plane
+constexpr uint32_t K_TMEM_COLS = 128;                     // two tiles in flight x (Re, Im) x 32 columns
+
+// kind::tf32, D fp32, A and B tf32 K-major, M = 128, N = 32; bit 13 negates A.
+constexpr uint32_t K_IDESC_POS = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(KTN >> 3) << 17) |
+                                 ((uint32_t)(KTM >> 4) << 24);
+constexpr uint32_t K_IDESC_NEG = K_IDESC_POS | (1u << 13);
+
+__host__ __device__ __forceinline__ int kb_off(int row, int k) {
+  return (row >> 3) * 256 + (k >> 2) * 32 + (row & 7) * 4 + (k & 3);
+}
+
+__host__ __device__ inline size_t block_smem_bytes() {
+  return (size_t)K_REGION + KB * K_DLD * sizeof(float2) + 16 /*bars*/ + 16 /*probe*/ + 16 /*tslot*/ +
+         16 /*misc*/ + 8 * sizeof(double) /*redd*/;
+}
+
+// Solve-phase use of the region: y [NR][N] complex64 | ys [32][NR] + colsum [NR][NR] complex128 | two staged
+// diagonal inverses [2][32][32] complex64.
+__host__ __device__ inline size_t block_solve_bytes(int N, int NR) {
+  const size_t y = (((size_t)NR * N * sizeof(float2)) + 15) & ~(size_t)15;
+  return y + (size_t)(32 * NR + NR * NR) * sizeof(double2) + 2 * KB * KB * sizeof(float2);
+}
+
+struct BlockSmem {
+  float* a_pl;    // [4][KAP] A planes (Re hi, Re lo, Im hi, Im lo); also the Gauss-Jordan workspace
+  float* b_pl;    // [2][4][KBP] B planes of two tiles in flight
+  float2* y;      // solve phase: right-hand sides [NR][N]
+  double2* ys;    // solve phase: [32][NR] staging of the residual
+  double2* colsum;  // solve phase: [NR][NR]
+  float2* sinv;   // solve phase: [2][32][32] staged diagonal inverses
+  float2* dinv;   // [32][K_DLD] current diagonal inverse, row-major
+  uint64_t* bar;  // [2] completion barriers of the tiles in flight
+  uint64_t* probe;  // test hook: a barrier nothing arrives on
+  uint32_t* tslot;  // TMEM base address
+  int* misc;      // [0] a wait ran out, [1] status bits of the item, [2] the item met a singular diagonal block
+  double* redd;   // [8] block reductions
+  long long wait_limit, inject;
+
+  __device__ BlockSmem(unsigned char* base, int N, int NR, long long wl)
+      : wait_limit(wl > 0 ? wl : TC_WAIT_LIMIT), inject(wl < 0 ? -wl : 0) {
+    unsigned char* p = base;
+    a_pl = reinterpret_cast<float*>(p);
+    b_pl = a_pl + 4 * KAP;
+    y = reinterpret_cast<float2*>(p);
+    const size_t yb = (((size_t)NR * N * sizeof(float2)) + 15) & ~(size_t)15;
+    ys = reinterpret_cast<double2*>(p + yb);
+    colsum = ys + 32 * NR;
+    sinv = reinterpret_cast<float2*>(colsum + NR * NR);
+    p += K_REGION;
+    dinv = reinterpret_cast<float2*>(p);
+    p += KB * K_DLD * sizeof(float2);
+    bar = reinterpret_cast<uint64_t*>(p);
+    p += 16;
+    probe = reinterpret_cast<uint64_t*>(p);
+    p += 16;
+    tslot = reinterpret_cast<uint32_t*>(p);
+    p += 16;
+    misc = reinterpret_cast<int*>(p);
+    p += 16;
+    redd = reinterpret_cast<double*>(p);
+  }
+};
+
+// Tile bookkeeping (same in every thread): commits issued and completions observed per barrier.
+struct TileCount {
+  uint32_t iss[2] = {0u, 0u}, obs[2] = {0u, 0u};
+};
+
+// slot: A with its NR selector columns (N x (N + NR) complex64, column-major) | D_k^-1 per block (32 x 32
+// complex64, row-major) | B operands of the block row, split and laid out per 32-column strip (4 planes x 32 x 32
+// floats per strip) | Y, Rb (NR x N complex128 each)
+__host__ __device__ inline size_t block_a_bytes(int N, int NR) {
+  return ((size_t)N * (N + NR) * sizeof(float2) + 255) & ~(size_t)255;
+}
+__host__ __device__ inline int block_nblk(int N) { return (N + KB - 1) / KB; }
+__host__ __device__ inline int block_nstrips(int N, int NR) {
+  const int NC = N + NR;
+  return NC > KB ? (NC - KB + KTN - 1) / KTN : 1;
+}
+__host__ __device__ inline size_t block_slot_bytes(int N, int NR) {
+  return block_a_bytes(N, NR) + (size_t)block_nblk(N) * KB * KB * sizeof(float2) +
+         (size_t)block_nstrips(N, NR) * 4 * KBP * sizeof(float) + 2 * (size_t)NR * N * sizeof(double2);
+}
+
+__device__ __forceinline__ void split4(float4 x, float4& h, float4& l) {
+  h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+  l = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+}
+
+// Stores four consecutive-k complex values (K positions k .. k+3 of `row`) as the four planes of an operand.
+__device__ __forceinline__ void store_planes(float* planes, int plane_floats, int row, int k, float2 v0, float2 v1,
+                                             float2 v2, float2 v3) {
+  float4 h, l;
+  const int o = kb_off(row, k);
+  split4(make_float4(v0.x, v1.x, v2.x, v3.x), h, l);
+  *reinterpret_cast<float4*>(planes + o) = h;
+  *reinterpret_cast<float4*>(planes + plane_floats + o) = l;
+  split4(make_float4(v0.y, v1.y, v2.y, v3.y), h, l);
+  *reinterpret_cast<float4*>(planes + 2 * plane_floats + o) = h;
+  *reinterpret_cast<float4*>(planes + 3 * plane_floats + o) = l;
+}
+
+// The complex product of one 32-deep chunk into the (Re, Im) accumulators at TMEM columns d_re, d_im, issued by
+// one thread.  sign = -1: D -= A B (trailing update); sign = +1 with zero_init: D = A B (block row).
+//   D_re += s (Ar Br) - s (Ai Bi),  D_im += s (Ar Bi) + s (Ai Br)
+__device__ __forceinline__ void issue_planar(uint32_t d_re, uint32_t d_im, const float* a_pl, const float* b_pl,
+                                             bool negate, bool zero_init) {
+  const uint32_t a0 = smem_u32(a_pl), b0 = smem_u32(b_pl);
+  const uint32_t ar_h = a0, ar_l = a0 + KAP * 4, ai_h = a0 + 2 * KAP * 4, ai_l = a0 + 3 * KAP * 4;
+  const uint32_t br_h = b0, br_l = b0 + KBP * 4, bi_h = b0 + 2 * KBP * 4, bi_l = b0 + 3 * KBP * 4;
+  const uint32_t im = negate ? K_IDESC_NEG : K_IDESC_POS, ic = negate ? K_IDESC_POS : K_IDESC_NEG;
+#pragma unroll
+  for (int j = 0; j < KB / 8; ++j) {
+    const uint32_t o = 256u * j;  // K step of 8 reals = two core matrices along K
+    const uint32_t acc = (j > 0 || !zero_init) ? 1u : 0u;
+    tc_mma_desc(d_re, ar_l + o, br_h + o, K_SBO, im, acc);
+    tc_mma_desc(d_re, ar_h + o, br_l + o, K_SBO, im, 1u);
+    tc_mma_desc(d_re, ar_h + o, br_h + o, K_SBO, im, 1u);
+    tc_mma_desc(d_re, ai_l + o, bi_h + o, K_SBO, ic, 1u);
+    tc_mma_desc(d_re, ai_h + o, bi_l + o, K_SBO, ic, 1u);
+    tc_mma_desc(d_re, ai_h + o, bi_h + o, K_SBO, ic, 1u);
+    tc_mma_desc(d_im, ar_l + o, bi_h + o, K_SBO, im, acc);
+    tc_mma_desc(d_im, ar_h + o, bi_l + o, K_SBO, im, 1u);
+    tc_mma_desc(d_im, ar_h + o, bi_h + o, K_SBO, im, 1u);
+    tc_mma_desc(d_im, ai_l + o, br_h + o, K_SBO, im, 1u);
+    tc_mma_desc(d_im, ai_h + o, br_l + o, K_SBO, im, 1u);
+    tc_mma_desc(d_im, ai_h + o, br_h + o, K_SBO, im, 1u);
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Forming A (complex64, column-major) and the NR selector columns S[(p, nu)][s] = delta_ps
+// ----------------------------------------------------------------------------------------------
+// Element (i, j) as StructuredSource::element: (chi0^-1 [block diagonal] + Gamma / beta^2) + (-(U + V) / beta^2);
+// a thread owns two rows per pass with eight columns of Gamma loads in flight.
+template <int NR>
+__device__ void block_form_a(const StructuredSource& src, const WorkItem& wi, int N, int nv, float2* __restrict__ A) {
+  const int tid = threadIdx.x;
+  const double2* gam = src.gamma_cm + ((size_t)(wi.ch * src.W + wi.w) * N) * N;
+  const double2* c0 = src.chi0_inv + ((size_t)wi.q * src.W + wi.w) * nv * NR * NR;
+  const double2* uvq = src.uv + ((size_t)wi.ch * src.Q + wi.q) * NR * NR;
+  const double ib2 = src.inv_beta2;
+  for (int rbase = 0; rbase < N; rbase += 2 * KT) {
+    int ri[2], pr[2], vr[2];
+    bool rok[2];
+#pragma unroll
+    for (int a2 = 0; a2 < 2; ++a2) {
+      ri[a2] = rbase + tid + a2 * KT;
+      rok[a2] = ri[a2] < N;
+      pr[a2] = rok[a2] ? ri[a2] / nv : 0;
+      vr[a2] = rok[a2] ? ri[a2] - pr[a2] * nv : 0;
+    }
+    if (!rok[0]) break;
+    for (int j0 = 0; j0 < N; j0 += 8) {
+      double2 g[2][8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2)
+          g[a2][u] = (rok[a2] && j0 + u < N) ? __ldcg(gam + (size_t)(j0 + u) * N + ri[a2]) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + u;
+        if (j >= N) break;
+        const int pc = j / nv, vc = j - pc * nv;
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2) {
+          if (!rok[a2]) continue;
+          const double2 uu = uvq[pr[a2] * NR + pc];
+          double re = __dmul_rn(g[a2][u].x, ib2);
+          double im = __dmul_rn(g[a2][u].y, ib2);
+          if (vr[a2] == vc) {
+            const double2 c = c0[(size_t)vr[a2] * NR * NR + pr[a2] * NR + pc];
+            re = __dadd_rn(c.x, re);
+            im = __dadd_rn(c.y, im);
+          }
+          re = __dadd_rn(re, -__dmul_rn(uu.x, ib2));
+          im = __dadd_rn(im, -__dmul_rn(uu.y, ib2));
+          A[(size_t)j * N + ri[a2]] = make_float2((float)re, (float)im);
+        }
+      }
+    }
+#pragma unroll
+    for (int a2 = 0; a2 < 2; ++a2)
+      if (rok[a2])
+        for (int r = 0; r < NR; ++r) A[(size_t)(N + r) * N + ri[a2]] = make_float2(pr[a2] == r ? 1.f : 0.f, 0.f);
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// D_k^-1 by Gauss-Jordan elimination of [D | I] with the pivot search inside the block (warp 0; lane = row).
+// aug: [64][K_DLD] column-major workspace.  Writes D^-1 row-major to s.dinv (ld K_DLD) and inv (ld 32), zero
+// outside the nb x nb block.  Returns false if a pivot column was exactly zero or not finite.
+// ----------------------------------------------------------------------------------------------
+__device__ bool block_diag_inverse(const float2* __restrict__ A, int N, int k0, int nb, float2* aug, float2* dinv,
+                                   float2* __restrict__ inv) {
+  const int lane = threadIdx.x & 31;
+  for (int c = 0; c < KB; ++c) {
+    aug[c * K_DLD + lane] = (c < nb && lane < nb) ? __ldcg(A + (size_t)(k0 + c) * N + k0 + lane)
+                                                  : make_float2(c == lane ? 1.f : 0.f, 0.f);
+    aug[(KB + c) * K_DLD + lane] = make_float2(c == lane ? 1.f : 0.f, 0.f);
+  }
+  __syncwarp();
+  bool ok = true;
+  for (int jj = 0; jj < nb; ++jj) {
+    float v = (lane >= jj && lane < nb) ? cabs1(aug[jj * K_DLD + lane]) : -1.f;
+    int p = lane;
+    {  // largest |re| + |im|, ties to the smaller row; NaN is no candidate
+      const bool cand = v >= 0.f;
+      const unsigned key = cand ? __float_as_uint(v) : 0u;
+      const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+      const unsigned imin = __reduce_min_sync(0xffffffffu, (cand && key == kmax) ? (unsigned)lane : 0x7fffffffu);
+      v = __uint_as_float(kmax);
+      p = (int)imin;
+    }
+    const bool good = (v > 0.f) && isfinite(v) && p >= jj && p < nb;
+    if (!good) {
+      ok = false;
+      p = jj;
+    }
+    if (p != jj) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = lane + 32 * h;
+        const float2 t = aug[c * K_DLD + jj];
+        aug[c * K_DLD + jj] = aug[c * K_DLD + p];
+        aug[c * K_DLD + p] = t;
+      }
+    }
+    __syncwarp();
+    const float2 rinv = good ? crecip(aug[jj * K_DLD + jj]) : make_float2(0.f, 0.f);
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = lane + 32 * h;
+      aug[c * K_DLD + jj] = cmul(aug[c * K_DLD + jj], rinv);
+    }
+    __syncwarp();
+    const float2 f = aug[jj * K_DLD + lane];
+    __syncwarp();
+    if (lane != jj) {
+      for (int c = jj + 1; c < 2 * KB; ++c) {
+        float2 x = aug[c * K_DLD + lane];
+        cfms(x, f, aug[c * K_DLD + jj]);
+        aug[c * K_DLD + lane] = x;
+      }
+    }
+    __syncwarp();
+  }
+  for (int k = 0; k < KB; ++k) {
+    const float2 x = (lane < nb && k < nb) ? aug[(KB + k) * K_DLD + lane] : make_float2(0.f, 0.f);
+    dinv[lane * K_DLD + k] = x;
+    inv[lane * KB + k] = x;
+  }
+  return __all_sync(0xffffffffu, ok);
+}
+
+// ----------------------------------------------------------------------------------------------
+// Tile waits (bounded) and the drain at exit
+// ----------------------------------------------------------------------------------------------
+// A completion is counted only when this thread saw it; a wait that runs out (or is skipped because another
+// thread's ran out) leaves the phase outstanding for the drain at exit.  The result is made warp-uniform, since
+// the TMEM loads that follow are warp-collective.
+__device__ __forceinline__ bool tile_wait(BlockSmem& s, TileCount& tc, int b) {
+  bool ok = false;
+  if (s.misc[0] == 0) ok = mbar_wait(s.bar + b, tc.obs[b] & 1u, s.wait_limit);
+  if (ok) tc.obs[b] += 1;
+  ok = __all_sync(0xffffffffu, ok);
+  if (!ok) s.misc[0] = 1;
+  return ok;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Block row: W = D^-1 A[k0:k1, k1:NC] in place, plus its split planes per 32-column strip in bop (the B operands
+// of the trailing tiles).  Transposed tiles: D'(j, i) = sum_k A[k0 + k][j] D^-1[i][k], 128 columns j per tile.
+// ----------------------------------------------------------------------------------------------
+__device__ void block_row_w(float2* __restrict__ A, int N, int NC, int k0, int nb, int k1, BlockSmem& s,
+                            float* __restrict__ bop, TileCount& tc) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ncols = NC - k1;
+  if (ncols <= 0) return;
+  const int nst = (ncols + KTN - 1) / KTN;
+  float* bpl = s.b_pl;  // B' = (D^-1)^T: row i, k contiguous
+  for (int e = tid; e < KB * (KB / 4); e += KT) {
+    const int i = e >> 3, k = (e & 7) * 4;
+    const float2* d = s.dinv + i * K_DLD + k;
+    store_planes(bpl, KBP, i, k, d[0], d[1], d[2], d[3]);
+  }
+  const uint32_t tbase = *s.tslot;
+  const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
+  const int hh = warp >> 2;
+  const int ntile = (ncols + KTM - 1) / KTM;
+  for (int t = 0; t < ntile; ++t) {
+    const int j0 = k1 + t * KTM;
+    {  // A' planes: row = column j of the block row, k = row of the block (one 256-byte column per two threads)
+      const int jl = tid & (KTM - 1), h = tid >> 7, j = j0 + jl;
+      const bool jok = j < NC;
+      const float4* col = reinterpret_cast<const float4*>(A + (size_t)j * N + k0 + 16 * h);
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const int k = 16 * h + 4 * g;
+        float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
+        if (jok && k + 4 <= nb) {
+          x0 = __ldcg(col + 2 * g);
+          x1 = __ldcg(col + 2 * g + 1);
+        } else if (jok) {
+          const float2* c2 = A + (size_t)j * N + k0;
+          float2 v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) v[u] = (k + u < nb) ? __ldcg(c2 + k + u) : make_float2(0.f, 0.f);
+          x0 = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+          x1 = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+        }
+        store_planes(s.a_pl, KAP, jl, k, make_float2(x0.x, x0.y), make_float2(x0.z, x0.w), make_float2(x1.x, x1.y),
+                     make_float2(x1.z, x1.w));
+      }
+    }
+    tc_fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    const bool live = s.misc[0] == 0;
+    if (live && tid == 0) {
+      tc_fence_after();
+      issue_planar(tbase, tbase + 32, s.a_pl, bpl, false, true);
+      tc_commit(s.bar);
+    }
+    if (live) tc.iss[0] += 1;
+    const bool ok = live && tile_wait(s, tc, 0);
+    tc_fence_after();
+    if (ok) {
+      float re[16], im[16];
+      tmem_ld16(tl + 16 * hh, re);
+      tmem_ld16(tl + 32 + 16 * hh, im);
+      tmem_wait_ld();
+      const int jl = 32 * (warp & 3) + lane, j = j0 + jl;
+      if (j < NC) {
+        float2* col = A + (size_t)j * N + k0 + 16 * hh;
+#pragma unroll
+        for (int ii = 0; ii < 16; ++ii)
+          if (16 * hh + ii < nb) col[ii] = make_float2(re[ii], im[ii]);
+      }
+      const int st = (j - k1) >> 5, c = (j - k1) & 31;
+      if (st < nst) {
+        float* sp = bop + (size_t)st * 4 * KBP;
+        const bool jv = j < NC;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const int k = 16 * hh + 4 * g;
+          float2 v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            v[u] = (jv && k + u < nb) ? make_float2(re[4 * g + u], im[4 * g + u]) : make_float2(0.f, 0.f);
+          store_planes(sp, KBP, c, k, v[0], v[1], v[2], v[3]);
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Trailing update A[k1:N, k1:NC] -= A[k1:N, k0:k1] W: per 128-row block the A planes are staged once, then its
+// 32-column strips run two in flight (strip s stages its B planes and C while strip s - 1 multiplies).
+// ----------------------------------------------------------------------------------------------
+__device__ __forceinline__ void prefetch_tile_l2(const float2* A, int N, int NC, int r0, int c0) {
+  const int lane = threadIdx.x & 31;
+  const int c = c0 + lane;
+  if (c >= NC || r0 >= N) return;
+  const int r1 = min(N, r0 + KTM);
+  const uintptr_t a = reinterpret_cast<uintptr_t>(A + (size_t)c * N + r0) & ~(uintptr_t)15;
+  const uintptr_t e = (reinterpret_cast<uintptr_t>(A + (size_t)c * N + r1) + 15) & ~(uintptr_t)15;
+  bulk_prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(e - a));
+}
+
+__device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, int k1, BlockSmem& s,
+                               const float* __restrict__ bop, TileCount& tc) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (k1 >= N) return;
+  const int nrb = (N - k1 + KTM - 1) / KTM, nst = (NC - k1 + KTN - 1) / KTN;
+  const uint32_t tbase = *s.tslot;
+  const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
+  const int hh = warp >> 2;
+  const int row_t = 32 * (warp & 3) + lane;  // this thread's tile row (its TMEM lane)
+  auto finish = [&](int r0, int st) {
+    const int b = st & 1;
+    const bool ok = tile_wait(s, tc, b);
+    tc_fence_after();
+    if (!ok) return;
+    float re[16], im[16];
+    tmem_ld16(tl + 64 * b + 16 * hh, re);
+    tmem_ld16(tl + 64 * b + 32 + 16 * hh, im);
+    tmem_wait_ld();
+    const int r = r0 + row_t, cb = k1 + st * KTN + 16 * hh;
+    if (r < N) {
+#pragma unroll
+      for (int jj = 0; jj < 16; ++jj)
+        if (cb + jj < NC) A[(size_t)(cb + jj) * N + r] = make_float2(re[jj], im[jj]);
+    }
+  };
+  for (int rb = 0; rb < nrb; ++rb) {
+    const int r0 = k1 + rb * KTM;
+    {  // A planes: rows r0 .. r0 + 127 of the block column (16 k per thread, loads coalesced along the rows)
+      const int rl = tid & (KTM - 1), h = tid >> 7, r = r0 + rl;
+      const bool rok = r < N;
+      float2 v[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) v[u] = rok ? __ldcg(A + (size_t)(k0 + 16 * h + u) * N + r) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int g = 0; g < 4; ++g) store_planes(s.a_pl, KAP, rl, 16 * h + 4 * g, v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
+    }
+    if (warp == KW - 1) {
+      prefetch_tile_l2(A, N, NC, r0, k1);
+      if (nst > 1) prefetch_tile_l2(A, N, NC, r0, k1 + KTN);
+    }
+    for (int st = 0; st < nst; ++st) {
+      const int b = st & 1, c0 = k1 + st * KTN;
+      if (warp == KW - 1 && st + 2 < nst) prefetch_tile_l2(A, N, NC, r0, c0 + 2 * KTN);
+      {  // B planes of the strip (split by the block-row tiles): 16 KB copy
+        const float4* src4 = reinterpret_cast<const float4*>(bop + (size_t)st * 4 * KBP);
+        float4* dst4 = reinterpret_cast<float4*>(s.b_pl + b * 4 * KBP);
+#pragma unroll
+        for (int u = 0; u < (4 * KBP / 4) / KT; ++u) dst4[tid + u * KT] = __ldcg(src4 + tid + u * KT);
+      }
+      {  // C tile -> TMEM: row row_t, 16 complex columns per warp half
+        const int r = r0 + row_t, cb = c0 + 16 * hh;
+        float re[16], im[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          const float2 x = (r < N && cb + jj < NC) ? __ldcg(A + (size_t)(cb + jj) * N + r) : make_float2(0.f, 0.f);
+          re[jj] = x.x;
+          im[jj] = x.y;
+        }
+        tmem_st16(tl + 64 * b + 16 * hh, re);
+        tmem_st16(tl + 64 * b + 32 + 16 * hh, im);
+        tmem_wait_st();
+      }
+      tc_fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      const bool live = s.misc[0] == 0;
+      if (live && tid == 0) {
+        tc_fence_after();
+        issue_planar(tbase + 64 * b, tbase + 64 * b + 32, s.a_pl, s.b_pl + b * 4 * KBP, true, false);
+        tc_commit(s.bar + b);
+      }
+      if (live) tc.iss[b] += 1;
+      if (st > 0 && live) finish(r0, st - 1);
+    }
+    if (s.misc[0] == 0) finish(r0, nst - 1);
+    tc_fence_before();
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Triangular solves with the block factors for NR right-hand sides y[r * ldy + i] in shared memory.
+//   forward:  for each block b: y_b <- D_b^-1 y_b (warp per right-hand side, lane = row), then the rows below
+//             y_i -= A[i, b] y_b (thread per row); the next block's inverse is staged during the update;
+//   backward: for each block b from the last: the rows above y_i -= W[i, b] y_b.
+// ----------------------------------------------------------------------------------------------
+template <int NR>
+__device__ void block_solve(const float2* __restrict__ A, int N, float2* y, int ldy, const float2* __restrict__ inv,
+                            float2* sinv, bool forward) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = block_nblk(N);
+  auto update = [&](int k0, int nb, int i0, int i1) {
+    for (int i = i0 + tid; i < i1; i += KT) {
+      float2 acc[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) acc[r] = y[(size_t)r * ldy + i];
+      for (int k = 0; k < nb; k += 16) {
+        float2 l[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) l[u] = (k + u < nb) ? __ldcg(A + (size_t)(k0 + k + u) * N + i) : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+          if (k + u < nb) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) cfms(acc[r], l[u], y[(size_t)r * ldy + k0 + k + u]);
+          }
+      }
+#pragma unroll
+      for (int r = 0; r < NR; ++r) y[(size_t)r * ldy + i] = acc[r];
+    }
+  };
+  if (forward) {
+    for (int e = tid; e < KB * KB; e += KT) sinv[e] = inv[e];
+    __syncthreads();
+    for (int b = 0; b < nblk; ++b) {
+      const int k0 = b * KB, nb = min(KB, N - k0), k1 = k0 + nb;
+      const float2* sv = sinv + (b & 1) * KB * KB;
+      for (int r = warp; r < NR; r += KW) {
+        float2* yr = y + (size_t)r * ldy + k0;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int k = 0; k < nb; ++k) cfma(acc, sv[lane * KB + k], yr[k]);
+        __syncwarp();
+        if (lane < nb) yr[lane] = acc;
+      }
+      float2 nx[KB * KB / KT];
+      if (b + 1 < nblk) {
+#pragma unroll
+        for (int u = 0; u < KB * KB / KT; ++u) nx[u] = inv[(size_t)(b + 1) * KB * KB + tid + u * KT];
+      }
+      __syncthreads();
+      update(k0, nb, k1, N);
+      if (b + 1 < nblk) {
+        float2* dst = sinv + ((b + 1) & 1) * KB * KB;
+#pragma unroll
+        for (int u = 0; u < KB * KB / KT; ++u) dst[tid + u * KT] = nx[u];
+      }
+      __syncthreads();
+    }
+  }
+  for (int b = nblk - 1; b > 0; --b) {
+    const int k0 = b * KB, nb = min(KB, N - k0);
+    update(k0, nb, 0, k0);
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// One work item: form, factor, solve, refine.  Returns the status bits; *iters = number of corrections.
+// ----------------------------------------------------------------------------------------------
+template <int NR>
+__device__ int solve_item_block(const StructuredSource& src, const WorkItem& wi, int N, int nv, double beta,
+                                int max_iter, double tol, double2* __restrict__ o, unsigned char* slot, BlockSmem& s,
+                                TileCount& tc, int* iters) {
+  const int tid = threadIdx.x;
+  const int NC = N + NR;
+  float2* A = reinterpret_cast<float2*>(slot);
+  float2* inv = reinterpret_cast<float2*>(slot + block_a_bytes(N, NR));
+  float* bop = reinterpret_cast<float*>(inv + (size_t)block_nblk(N) * KB * KB);
+  double2* Y = reinterpret_cast<double2*>(bop + (size_t)block_nstrips(N, NR) * 4 * KBP);
+  double2* Rb = Y + (size_t)N * NR;
+  if (tid == 0) {
+    s.misc[1] = 0;
+    s.misc[2] = 0;
+  }
+  block_form_a<NR>(src, wi, N, nv, A);
+  __syncthreads();
+  // ---- factorisation ----
+  for (int k0 = 0; k0 < N; k0 += KB) {
+    const int nb = min(KB, N - k0), k1 = k0 + nb;
+    if (threadIdx.x < 32) {
+      const bool ok = block_diag_inverse(A, N, k0, nb, reinterpret_cast<float2*>(s.a_pl), s.dinv,
+                                         inv + (size_t)(k0 / KB) * KB * KB);
+      if (!ok && threadIdx.x == 0) s.misc[2] = 1;
+    }
+    __syncthreads();
+    block_row_w(A, N, NC, k0, nb, k1, s, bop, tc);
+    block_trailing(A, N, NC, k0, k1, s, bop, tc);
+  }
+  __syncthreads();
+  // ---- initial solve: the selector columns hold the forward result; back substitution only ----
+  const int ldy = N;
+  for (int e = tid; e < NR * N; e += KT) s.y[e] = A[(size_t)N * N + e];
+  __syncthreads();
+  block_solve<NR>(A, N, s.y, ldy, inv, s.sinv, false);
+  double prev = 0.0;
+  for (int e = tid; e < NR * N; e += KT) {
+    Y[e] = make_double2(s.y[e].x, s.y[e].y);
+    prev = fmax(prev, (double)fmaxf(fabsf(s.y[e].x), fabsf(s.y[e].y)));
+  }
+  prev = block_max(prev, s.redd);
+  int it = 0;
+  bool converged = false;
+  for (; it < max_iter; ++it) {
+    structured_residual_permuted<NR>(src, wi.ch, wi.q, wi.w, N, nv, Y, Rb, nullptr, s.colsum, s.ys);
+    for (int e = tid; e < NR * N; e += KT) s.y[e] = make_float2((float)Rb[e].x, (float)Rb[e].y);
+    __syncthreads();
+    block_solve<NR>(A, N, s.y, ldy, inv, s.sinv, true);
+    double dmax = 0.0, ymax = 0.0;
+    for (int e = tid; e < NR * N; e += KT) {
+      const double2 d = make_double2(s.y[e].x, s.y[e].y);
+      const double2 v = cadd(Y[e], d);
+      Y[e] = v;
+      dmax = fmax(dmax, fmax(fabs(d.x), fabs(d.y)));
+      ymax = fmax(ymax, fmax(fabs(v.x), fabs(v.y)));
+    }
+    dmax = block_max(dmax, s.redd);
+    ymax = block_max(ymax, s.redd);
+    if (isnan(dmax) || refine_converged(dmax, ymax, prev, tol)) {  // NaN is flagged below
+      converged = !isnan(dmax);
+      ++it;
+      break;
+    }
+    prev = dmax;
+  }
+  __syncthreads();
+  bool bad = false;
+  for (int e = tid; e < N * NR; e += KT) {
+    const int i = e / NR, r = e - i * NR;
+    double2 v = Y[(size_t)r * N + i];
+    v.x = v.x / beta;
+    v.y = v.y / beta;
+    if (!cfinite(v)) bad = true;
+    o[e] = v;
+  }
+  if (bad) atomicOr(&s.misc[1], DGA_ITEM_NONFINITE);
+  __syncthreads();
+  // a singular diagonal block is no proof of a singular matrix: such items go to the FP64 re-solve (with partial
+  // pivoting), which reports DGA_ITEM_SINGULAR if the matrix itself is
+  const int st = s.misc[1] | ((converged && !s.misc[2]) ? 0 : DGA_ITEM_NOCONVERGE) |
+                 (s.misc[0] ? DGA_ITEM_WAIT_TIMEOUT : 0);
+  *iters = it;
+  __syncthreads();
+  return st;
+}
+
+__device__ void block_kernel_begin(BlockSmem& s) {
+  if (threadIdx.x == 0) {
+    s.misc[0] = 0;
+    mbar_init(s.bar);
+    mbar_init(s.bar + 1);
+    if (s.inject) mbar_init(s.probe);
+  }
+  if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, K_TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (s.inject) {
+    // test hook (dga_bse_tuning.wait_limit < 0): a bounded wait on a phase that nothing completes runs out, and
+    // the CTA takes the path of a real timeout
+    if (!mbar_wait(s.probe, 0u, s.inject)) s.misc[0] = 1;
+    __syncthreads();
+  }
+}
+
+// Drains every tile still in flight (full limit) and frees TMEM; false if a drain wait ran out.
+__device__ bool block_kernel_end(BlockSmem& s, const TileCount& tc) {
+  tc_fence_before();
+  __syncthreads();
+  bool drained = true;
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+    if (tc.iss[b] > tc.obs[b]) drained &= mbar_wait(s.bar + b, (tc.iss[b] - 1u) & 1u);
+  tc_fence_after();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) tc_dealloc(*s.tslot, K_TMEM_COLS);
+  return __syncthreads_and(drained ? 1 : 0) != 0;
+}
+
+template <int NR>
+__global__ void __launch_bounds__(KT, 2)
+    bse_block_mixed_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int nv, int W,
+                           int Q, double beta, int max_iter, double tol, double2* __restrict__ out,
+                           int* __restrict__ status, int* __restrict__ iters, unsigned char* __restrict__ scratch,
+                           size_t slot_bytes, long long wait_limit) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  BlockSmem s(smem_raw, N, NR, wait_limit);
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  TileCount tc;
+  block_kernel_begin(s);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (s.misc[0]) {  // a wait ran out: the CTA issues nothing more, its remaining items go to the FP64 re-solve
+      if (threadIdx.x == 0) {
+        if (status) status[item] = DGA_ITEM_WAIT_TIMEOUT;
+        if (iters) iters[item] = 0;
+      }
+      continue;
+    }
+    const WorkItem wi = work[item];
+    double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * NR;
+    int it = 0;
+    const int st = solve_item_block<NR>(src, wi, N, nv, beta, max_iter, tol, o, slot, s, tc, &it);
+    if (threadIdx.x == 0) {
+      if (status) status[item] = st;
+      if (iters) iters[item] = it;
+    }
+  }
+  if (!block_kernel_end(s, tc) && status) {
+    for (int item = blockIdx.x + threadIdx.x * gridDim.x; item < n_items; item += blockDim.x * gridDim.x)
+      atomicOr(status + item, DGA_ITEM_WAIT_TIMEOUT);
+  }
+}
+
+}  // namespace dga
+
+using namespace dga;
+
+// ----------------------------------------------------------------------------------------------
+// Host side (called from bse.cu)
+// ----------------------------------------------------------------------------------------------
+bool dga_block_supported(int N, int n2) {
+  if (!(n2 == 1 || n2 == 4 || n2 == 9 || n2 == 16) || N <= 0 || N > 2048) return false;
+  return block_solve_bytes(N, n2) <= (size_t)K_REGION;
+}
+
+size_t dga_block_slot_bytes(int N, int n2) { return (block_slot_bytes(N, n2) + 255) & ~(size_t)255; }
+
+template <int NR>
+static int block_grid_nr(int n_items) {
+  const size_t smem = block_smem_bytes();
+  cudaFuncSetAttribute(bse_block_mixed_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bse_block_mixed_kernel<NR>, KT, smem);
+  if (per_sm < 1) per_sm = 1;
+  if (per_sm > 2) per_sm = 2;  // two CTAs hold 256 of the SM's 512 TMEM columns
+  const int g = device_sm_count() * per_sm;
+  return n_items < g ? n_items : g;
+}
+
+int dga_block_grid(int n2, int n_items) {
+  switch (n2) {
+    case 1: return block_grid_nr<1>(n_items);
+    case 4: return block_grid_nr<4>(n_items);
+    case 9: return block_grid_nr<9>(n_items);
+    default: return block_grid_nr<16>(n_items);
+  }
+}
+
+cudaError_t dga_block_launch(int grid, const StructuredSource& src, const WorkItem* work, int n_items, int N, int n2,
+                             int nv, int W, int Q, double beta, int max_iter, double tol, double2* out, int* status,
+                             int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
+                             long long wait_limit) {
+  const size_t smem = block_smem_bytes();
+#define DGA_BLOCK_CASE(R)                                                                                         \
+  case R:                                                                                                         \
+    cudaFuncSetAttribute(bse_block_mixed_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+    bse_block_mixed_kernel<R><<<grid, KT, smem, stream>>>(src, work, n_items, N, nv, W, Q, beta, max_iter, tol,    \
+                                                          out, status, iters, scratch, slot_bytes, wait_limit);   \
+    break;
+  switch (n2) {
+    DGA_BLOCK_CASE(1)
+    DGA_BLOCK_CASE(4)
+    DGA_BLOCK_CASE(9)
+    DGA_BLOCK_CASE(16)
+  }
+#undef DGA_BLOCK_CASE
+  return cudaGetLastError();
+}

@@ -185,7 +185,17 @@ int dga_panel_batch_grid(int n2, int n_max, int n_items, bool tc = false);
 cudaError_t dga_panel_launch(int grid, const dga::StructuredSource& src, const dga::WorkItem* work, int n_items, int N,
                              int n2, int nv, int W, int Q, double beta, int max_iter, double tol, double2* out,
                              int* status, int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
-                             bool tc = false);
+                             bool tc = false, long long wait_limit = 0);
+// Host side of the block-form mixed kernel (bse_block.cu): pivoting restricted to 32 x 32 diagonal blocks, every
+// update on the tensor cores, two 256-thread CTAs per SM.
+bool dga_block_supported(int N, int n2);
+size_t dga_block_slot_bytes(int N, int n2);
+int dga_block_grid(int n2, int n_items);
+cudaError_t dga_block_launch(int grid, const dga::StructuredSource& src, const dga::WorkItem* work, int n_items, int N,
+                             int n2, int nv, int W, int Q, double beta, int max_iter, double tol, double2* out,
+                             int* status, int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
+                             long long wait_limit = 0);
 cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const dga::MultiItem* work,
                                    int n_items, int n_max, int max_iter, double tol, int* status, int* iters,
-                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc = false);
+                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc = false,
+                                   long long wait_limit = 0);

@@ -82,8 +82,11 @@ struct PanelSmem {
   uint32_t* tslot;  // TMEM address of the two tile accumulators
   int* piv;     // [ldp] row interchanged with row j
   int ldp;
+  long long wait_limit;  // polls of the bounded waits inside an item (the drains at exit use TC_WAIT_LIMIT)
+  long long inject;      // > 0: the CTA's first wait is on a phase nothing completes (test hook), this many polls
 
-  __device__ PanelSmem(unsigned char* base, int ldp_, bool tc) : ldp(ldp_) {
+  __device__ PanelSmem(unsigned char* base, int ldp_, bool tc, long long wait_limit_)
+      : ldp(ldp_), wait_limit(wait_limit_ > 0 ? wait_limit_ : TC_WAIT_LIMIT), inject(wait_limit_ < 0 ? -wait_limit_ : 0) {
     unsigned char* p = base;
     P = reinterpret_cast<float2*>(p);
     p += panel_region_bytes(ldp, tc);
@@ -359,17 +362,26 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
     const int nb = min(PNB, N - k0), m = N - k0, k1 = k0 + nb;
     // ---- load the panel: one bulk copy (TMA engine) per column, global -> shared, completing on the panel
     // barrier; the fence orders every thread's earlier accesses (its writes of these columns, its reads of the
-    // panel region) before the copies ----
+    // panel region) before the copies.  Once any bounded wait of this CTA has run out (misc[2]) the CTA issues
+    // no more bulk copies or tiles: the panel is then read with plain loads, so the barrier's only phase that
+    // can still be pending is the one whose wait ran out (drained at exit) ----
     fence_proxy_async_all();
     __syncthreads();
-    if (tid < 32) {
-      if (tid == 0) mbar_expect_tx(s.pbar, (uint32_t)((size_t)m * nb * sizeof(float2)));
-      __syncwarp();
-      for (int c = tid; c < nb; c += 32)
-        bulk_g2s(s.P + (size_t)c * s.ldp, A + (size_t)(k0 + c) * N + k0, (uint32_t)(m * sizeof(float2)), s.pbar);
+    if (s.misc[2] == 0) {
+      if (tid < 32) {
+        if (tid == 0) mbar_expect_tx(s.pbar, (uint32_t)((size_t)m * nb * sizeof(float2)));
+        __syncwarp();
+        for (int c = tid; c < nb; c += 32)
+          bulk_g2s(s.P + (size_t)c * s.ldp, A + (size_t)(k0 + c) * N + k0, (uint32_t)(m * sizeof(float2)), s.pbar);
+      }
+      if (!mbar_wait(s.pbar, (parity >> 2) & 1u, s.wait_limit)) s.misc[2] = 1;  // flags the item
+      parity ^= 4u;
+    } else {
+      for (int e = tid; e < m * nb; e += PT) {
+        const int c = e / m, r = e - c * m;
+        s.P[(size_t)c * s.ldp + r] = __ldcg(A + (size_t)(k0 + c) * N + k0 + r);
+      }
     }
-    if (!mbar_wait(s.pbar, (parity >> 2) & 1u)) s.misc[2] = 1;  // flags the item; the CTA issues no more tiles
-    parity ^= 4u;
     __syncthreads();
     singular |= panel_factor(s, m, nb, k0);
     for (int e = tid; e < m * nb; e += PT) {
@@ -497,7 +509,7 @@ __device__ bool panel_lu(float2* __restrict__ A, int N, int NC, PanelSmem& s, ui
         };
         auto finish = [&](int i) {
           const int bsel = i & 1;
-          const bool ok = live && mbar_wait(s.bar + bsel, (parity >> bsel) & 1u);
+          const bool ok = live && mbar_wait(s.bar + bsel, (parity >> bsel) & 1u, s.wait_limit);
           if (live) parity ^= 1u << bsel;
           tc_fence_after();
           if (ok) {
@@ -829,9 +841,9 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
   }
   if (bad) atomicOr(&s.misc[1], DGA_ITEM_NONFINITE);
   __syncthreads();
-  // a tensor-core wait that ran out leaves the factors incomplete: flag the item for the FP64 re-solve
+  // a bounded wait that ran out leaves the factors incomplete: flag the item for the FP64 re-solve
   const int st = (singular ? DGA_ITEM_SINGULAR : 0) | s.misc[1] | (converged ? 0 : DGA_ITEM_NOCONVERGE) |
-                 (s.misc[2] ? DGA_ITEM_NONFINITE : 0);
+                 (s.misc[2] ? DGA_ITEM_WAIT_TIMEOUT : 0);
   *iters = it;
   __syncthreads();
   return st;
@@ -839,12 +851,15 @@ __device__ int solve_item_panel(const StructuredSource& src, const WorkItem& wi,
 
 // TMEM for the tensor-core tiles: one warp allocates 256 columns (two 128 x 128 fp32 accumulators, one per tile in
 // flight) for the CTA's lifetime; the two completion barriers are initialised once.  At exit, a CTA whose wait
-// ever ran out waits once more (bounded) for each tile still in flight before the columns are freed.
+// ever ran out waits once more, with the full limit, for the panel load and each tile still in flight before the
+// columns are freed; panel_kernel_end returns false if one of those waits also ran out (the launch is then
+// suspect: every item of the CTA is flagged DGA_ITEM_WAIT_TIMEOUT).
 template <bool TC>
 __device__ void panel_kernel_begin(PanelSmem& s) {
   if (threadIdx.x == 0) {
     s.misc[2] = 0;
     mbar_init(s.pbar);
+    if (s.inject) mbar_init(s.pbar + 1);  // the test hook's barrier: nothing ever arrives on it
   }
   if (TC) {
     if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, 2 * TC_NR);
@@ -856,20 +871,37 @@ __device__ void panel_kernel_begin(PanelSmem& s) {
   }
   __syncthreads();
   if (TC) tc_fence_after();
+  if (s.inject) {
+    // test hook (dga_bse_tuning.wait_limit < 0): a bounded wait on a phase that nothing completes runs out, and
+    // the CTA takes the path of a real timeout -- no more bulk copies or tiles, every item flagged
+    if (!mbar_wait(s.pbar + 1, 0u, s.inject)) s.misc[2] = 1;
+    __syncthreads();
+  }
 }
 
 template <bool TC>
-__device__ void panel_kernel_end(PanelSmem& s, uint32_t parity) {
+__device__ bool panel_kernel_end(PanelSmem& s, uint32_t parity) {
   __syncthreads();
-  if (s.misc[2]) mbar_wait(s.pbar, ((parity >> 2) & 1u) ^ 1u);  // a panel load that ran out may still be landing
-  if (!TC) return;
-  tc_fence_before();
-  __syncthreads();
-  if (s.misc[2]) {  // a wait ran out: give each tile still in flight one more bounded wait before freeing TMEM
-    mbar_wait(s.bar, (parity & 1u) ^ 1u);
-    mbar_wait(s.bar + 1, ((parity >> 1) & 1u) ^ 1u);
+  bool drained = true;
+  // a panel load whose wait ran out may still be landing
+  if (s.misc[2]) drained &= mbar_wait(s.pbar, ((parity >> 2) & 1u) ^ 1u);
+  if (TC) {
+    tc_fence_before();
+    __syncthreads();
+    if (s.misc[2]) {  // a wait ran out: give each tile still in flight one more full wait before freeing TMEM
+      drained &= mbar_wait(s.bar, (parity & 1u) ^ 1u);
+      drained &= mbar_wait(s.bar + 1, ((parity >> 1) & 1u) ^ 1u);
+    }
+    if ((threadIdx.x >> 5) == 0) tc_dealloc(*s.tslot, 2 * TC_NR);
   }
-  if ((threadIdx.x >> 5) == 0) tc_dealloc(*s.tslot, 2 * TC_NR);
+  return __syncthreads_and(drained ? 1 : 0) != 0;
+}
+
+// Flags every item the CTA processed when a drain wait at exit ran out.
+__device__ __forceinline__ void flag_cta_items(int* status, int n_items) {
+  if (!status) return;
+  for (int item = blockIdx.x + threadIdx.x * gridDim.x; item < n_items; item += blockDim.x * gridDim.x)
+    atomicOr(status + item, DGA_ITEM_WAIT_TIMEOUT);
 }
 
 template <int NR, bool TC>
@@ -877,9 +909,9 @@ __global__ void __launch_bounds__(PT, 1)
     bse_panel_mixed_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int nv, int W,
                            int Q, double beta, int max_iter, double tol, double2* __restrict__ out,
                            int* __restrict__ status, int* __restrict__ iters, unsigned char* __restrict__ scratch,
-                           size_t slot_bytes) {
+                           size_t slot_bytes, long long wait_limit) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  PanelSmem s(smem_raw, N, TC);
+  PanelSmem s(smem_raw, N, TC, wait_limit);
   unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
   uint32_t parity = 0;
   panel_kernel_begin<TC>(s);
@@ -893,7 +925,7 @@ __global__ void __launch_bounds__(PT, 1)
       if (iters) iters[item] = it;
     }
   }
-  panel_kernel_end<TC>(s, parity);
+  if (!panel_kernel_end<TC>(s, parity)) flag_cta_items(status, n_items);
 }
 
 // Heterogeneous batch (requests of one orbital count): see bse_multi_kernel in bse.cu.
@@ -901,9 +933,10 @@ template <int NR, bool TC>
 __global__ void __launch_bounds__(PT, 1)
     bse_panel_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work,
                            int n_items, int n_max, int max_iter, double tol, int* __restrict__ status,
-                           int* __restrict__ iters, unsigned char* __restrict__ scratch, size_t slot_bytes) {
+                           int* __restrict__ iters, unsigned char* __restrict__ scratch, size_t slot_bytes,
+                           long long wait_limit) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  PanelSmem s(smem_raw, n_max, TC);
+  PanelSmem s(smem_raw, n_max, TC, wait_limit);
   unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
   uint32_t parity = 0;
   panel_kernel_begin<TC>(s);
@@ -929,7 +962,7 @@ __global__ void __launch_bounds__(PT, 1)
       if (iters) iters[item] = it;
     }
   }
-  panel_kernel_end<TC>(s, parity);
+  if (!panel_kernel_end<TC>(s, parity)) flag_cta_items(status, n_items);
 }
 
 }  // namespace dga
@@ -995,12 +1028,13 @@ int dga_panel_batch_grid(int n2, int n_max, int n_items, bool tc) {
 template <bool TC>
 static void panel_launch_tc(int grid, const StructuredSource& src, const WorkItem* work, int n_items, int N, int n2,
                             int nv, int W, int Q, double beta, int max_iter, double tol, double2* out, int* status,
-                            int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream) {
+                            int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
+                            long long wait_limit) {
   const size_t smem = panel_smem_bytes(N, TC);
 #define DGA_PANEL_CASE(R)                                                                                          \
   case R:                                                                                                          \
     bse_panel_mixed_kernel<R, TC><<<grid, PT, smem, stream>>>(src, work, n_items, N, nv, W, Q, beta, max_iter, tol, \
-                                                              out, status, iters, scratch, slot_bytes);           \
+                                                              out, status, iters, scratch, slot_bytes, wait_limit); \
     break;
   switch (n2) {
     DGA_PANEL_CASE(1)
@@ -1013,25 +1047,26 @@ static void panel_launch_tc(int grid, const StructuredSource& src, const WorkIte
 
 cudaError_t dga_panel_launch(int grid, const StructuredSource& src, const WorkItem* work, int n_items, int N, int n2,
                              int nv, int W, int Q, double beta, int max_iter, double tol, double2* out, int* status,
-                             int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc) {
+                             int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc,
+                             long long wait_limit) {
   if (tc)
     panel_launch_tc<true>(grid, src, work, n_items, N, n2, nv, W, Q, beta, max_iter, tol, out, status, iters, scratch,
-                          slot_bytes, stream);
+                          slot_bytes, stream, wait_limit);
   else
     panel_launch_tc<false>(grid, src, work, n_items, N, n2, nv, W, Q, beta, max_iter, tol, out, status, iters,
-                           scratch, slot_bytes, stream);
+                           scratch, slot_bytes, stream, wait_limit);
   return cudaGetLastError();
 }
 
 template <bool TC>
 static void panel_batch_launch_tc(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
                                   int n_max, int max_iter, double tol, int* status, int* iters, unsigned char* scratch,
-                                  size_t slot_bytes, cudaStream_t stream) {
+                                  size_t slot_bytes, cudaStream_t stream, long long wait_limit) {
   const size_t smem = panel_smem_bytes(n_max, TC);
 #define DGA_PANEL_CASE(R)                                                                                           \
   case R:                                                                                                           \
     bse_panel_multi_kernel<R, TC><<<grid, PT, smem, stream>>>(probs, work, n_items, n_max, max_iter, tol, status, \
-                                                              iters, scratch, slot_bytes);                         \
+                                                              iters, scratch, slot_bytes, wait_limit);             \
     break;
   switch (n2) {
     DGA_PANEL_CASE(1)
@@ -1044,12 +1079,13 @@ static void panel_batch_launch_tc(int grid, int n2, const dga_bse_problem* probs
 
 cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
                                    int n_max, int max_iter, double tol, int* status, int* iters,
-                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc) {
+                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc,
+                                   long long wait_limit) {
   if (tc)
     panel_batch_launch_tc<true>(grid, n2, probs, work, n_items, n_max, max_iter, tol, status, iters, scratch,
-                                slot_bytes, stream);
+                                slot_bytes, stream, wait_limit);
   else
     panel_batch_launch_tc<false>(grid, n2, probs, work, n_items, n_max, max_iter, tol, status, iters, scratch,
-                                 slot_bytes, stream);
+                                 slot_bytes, stream, wait_limit);
   return cudaGetLastError();
 }

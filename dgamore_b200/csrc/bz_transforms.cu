@@ -359,7 +359,8 @@ static int launch_status(const char* who) {
 }
 
 static int grid_cap(long long work) {
-  long long g = work < 148LL * 8 ? work : 148LL * 8;
+  const long long cap = 8LL * device_sm_count();
+  long long g = work < cap ? work : cap;
   return (int)(g > 0 ? g : 1);
 }
 
@@ -421,7 +422,8 @@ int dga_bubble_c128(const void* g_r, int n_orb, int niv, int niw, int nx, int ny
   const size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + 3 * sizeof(int) * (size_t)n_qirr;
   cudaFuncSetAttribute(bubble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long work = (long long)(niw + 1) * 2 * niv * n_orb * n_orb;
-  bubble_kernel<<<(int)(work < 148LL * 64 ? work : 148LL * 64), BZ_THREADS, smem, stream>>>(
+  const long long cap = 64LL * device_sm_count();
+  bubble_kernel<<<(int)(work < cap ? work : cap), BZ_THREADS, smem, stream>>>(
       (const double2*)g_r, n_orb, niv, niw, g, q_irr, n_qirr, (const double2*)tw, beta, (double2*)out, os);
   return launch_status("dga_bubble_c128");
 }

@@ -19,6 +19,9 @@
 #define DGA_ITEM_SINGULAR 1    // exact zero pivot (numpy raises LinAlgError("Singular matrix"))
 #define DGA_ITEM_NONFINITE 2   // NaN or Inf in the result
 #define DGA_ITEM_NOCONVERGE 4  // iterative refinement did not reach its tolerance
+#define DGA_ITEM_WAIT_TIMEOUT 8  // a bounded wait on an asynchronous copy or tensor-core tile ran out
+// items a mixed-precision launch leaves for the FP64 re-solve
+#define DGA_ITEM_REDO (DGA_ITEM_NOCONVERGE | DGA_ITEM_NONFINITE | DGA_ITEM_WAIT_TIMEOUT)
 
 // One problem (request) of a heterogeneous BSE batch; the layout is part of the C ABI (include/dga_b200.h).
 typedef struct {
@@ -35,6 +38,7 @@ typedef struct {
   int kernel;       // 0 = default, 1 = shared-memory-panel kernel (mixed form only), 2 = 128-thread kernel,
                     // 3 = shared-memory-panel kernel with tensor-core (tcgen05) trailing tiles (mixed form only)
   int ctas_per_sm;  // CTAs per SM of the 128-thread kernels (0 = as many as fit)
+  long long wait_limit;  // polls of each bounded wait on a copy or tile inside an item (0 = the default limit)
 } dga_bse_tuning;
 
 namespace dga {
@@ -150,6 +154,9 @@ __device__ __forceinline__ float2 from_c64<float2>(double2 a) {
 }
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+// SMs of the current device (cached per device; 148 on B200).
+int device_sm_count();
 
 }  // namespace dga
 

@@ -217,7 +217,8 @@ static int eli_status(const char* who) {
 
 static int eli_blocks(long long work) {
   long long b = (work + 255) / 256;
-  if (b > 148LL * 16) b = 148LL * 16;
+  const long long cap = 16LL * device_sm_count();
+  if (b > cap) b = cap;
   return (int)(b > 0 ? b : 1);
 }
 
@@ -284,7 +285,8 @@ int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, in
   if (rc) return rc;
   const size_t smem = 2 * (size_t)M * sizeof(double2);
   cudaFuncSetAttribute(eli_vertex_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  eli_vertex_apply_kernel<<<nk < 148 * 8 ? nk : 148 * 8, ELI_APPLY_THREADS, smem, stream>>>(
+  const int apply_cap = 8 * device_sm_count();
+  eli_vertex_apply_kernel<<<nk < apply_cap ? nk : apply_cap, ELI_APPLY_THREADS, smem, stream>>>(
       (const double2*)mat, s1, n_orb, nvp, nk, s2, s3);
   if (eli_status("dga_eli_matvec_c128")) return DGA_ERR_LAUNCH;
   eli_combine_kernel<<<eli_blocks((long long)nk * M), 256, 0, stream>>>(s2, s3, M, nx, ny, nz, sign, s0);

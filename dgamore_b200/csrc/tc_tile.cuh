@@ -75,10 +75,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Bounded wait for the barrier phase with the given parity; false if it did not complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the barrier phase with the given parity (at most `limit` polls); false if it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = TC_WAIT_LIMIT) {
   const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < TC_WAIT_LIMIT; ++it) {
+  for (long long it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}"
@@ -134,6 +134,50 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 16 consecutive fp32 columns of this thread's TMEM lane (32x32b shape, as tmem_st32 / tmem_ld32).
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
+      "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]), "=f"(v[8]),
+        "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major without swizzle: 8-row x 16-byte core matrices, adjacent along K
+// 128 bytes apart (leading byte offset) and along rows sbo bytes apart (stride byte offset).
+__device__ __forceinline__ uint64_t tc_desc_sbo(uint32_t saddr, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) |
+         (1ull << 46);
+}
+
+// One MMA of kind::tf32 with an explicit instruction descriptor: D = (accum ? D : 0) + op(A) B, operands K-major
+// at the given shared-memory addresses (stride byte offset sbo).
+__device__ __forceinline__ void tc_mma_desc(uint32_t d_tmem, uint32_t a_addr, uint32_t b_addr, uint32_t sbo,
+                                            uint32_t idesc, uint32_t accum) {
+  const uint64_t ad = tc_desc_sbo(a_addr, sbo), bd = tc_desc_sbo(b_addr, sbo);
+  const uint32_t zero = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(zero), "r"(zero), "r"(zero), "r"(zero)
+      : "memory");
+}
+
+// Arrives on bar when every tcgen05 operation the calling thread issued before has completed.
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
 
 // One MMA D (+)= -A B over K = 8 (reals) at K step j, A and B descriptors at the operand buffers' bases.
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint32_t a_base, uint32_t b_base, int j) {

@@ -19,6 +19,25 @@ extern "C" const char* dga_last_error_string(void) { return g_last_error; }
 
 namespace dga {
 
+// Streaming multiprocessors of the current device, read once per device (grid sizes of the streaming kernels
+// are multiples of it).
+int device_sm_count() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148;
+  if (dev < 64 && cache[dev] > 0) return cache[dev];
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  if (dev < 64) cache[dev] = sms;
+  return sms;
+}
+
+}  // namespace dga
+
+extern "C" int dga_device_sm_count(void) { return dga::device_sm_count(); }
+
+namespace dga {
+
 constexpr int PERM_MAX_DIMS = 8;
 
 struct PermDesc {
@@ -76,7 +95,8 @@ int dga_strided_copy_c128(const void* src, void* dst, int ndim, const long long*
   }
   const int threads = 256;
   long long blocks = (total + threads - 1) / threads;
-  if (blocks > 148 * 32) blocks = 148 * 32;
+  const long long cap = 32LL * device_sm_count();
+  if (blocks > cap) blocks = cap;
   strided_copy_kernel<double2><<<(int)blocks, threads, 0, stream>>>((const double2*)src, (double2*)dst, d, total,
                                                                     scale);
   cudaError_t err = cudaGetLastError();

@@ -543,7 +543,7 @@ int dga_chi0_prep_c128(const void* chi0, int n_orb, int niv_core, int niv_shell,
   const long long n_qw = (long long)n_q * niw_half;
   const long long work = n_qw * n2 * n2;
   int blocks = (int)((work + 255) / 256);
-  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks > 16 * device_sm_count()) blocks = 16 * device_sm_count();
   chi0_sums_kernel<<<blocks, 256, 0, stream>>>((const double2*)chi0, n2, nvf, nv, niv_shell, n_qw, 1.0 / beta,
                                                (double2*)full_sum, (double2*)core_sum);
   return vstatus("dga_chi0_prep_c128");

@@ -117,12 +117,20 @@ def _blk(nbytes: int) -> int:
     return -(-int(nbytes) // _ALLOC_GRAIN) * _ALLOC_GRAIN
 
 
-def sigma_chunks_for(sh: PassShapes) -> int:
-    """(nu, i, j, w-chunk) CTAs of the Sigma contraction: at least four waves of its two resident CTAs per SM on
-    148 SMs (1,184 CTAs), so that the last wave's tail is short (the 3-orbital 32x32 pass has 360 (nu, i, j)
-    units: 4 chunks)."""
+def device_sm_count() -> int:
+    """SMs of the current CUDA device (the library's cached query); 148, the B200's count, without a GPU."""
+    if torch.cuda.is_available():
+        return int(lib().dga_device_sm_count())
+    return 148
+
+
+def sigma_chunks_for(sh: PassShapes, sm_count: int | None = None) -> int:
+    """(nu, i, j, w-chunk) CTAs of the Sigma contraction: at least four waves of its two resident CTAs per SM
+    (8 CTAs per SM in all: 1,184 on a 148-SM B200), so that the last wave's tail is short (the 3-orbital 32x32
+    pass has 360 (nu, i, j) units: 4 chunks)."""
+    sms = device_sm_count() if sm_count is None else int(sm_count)
     base = sh.niv * sh.n2
-    return max(1, min(2 * sh.niw + 1, -(-1184 // base)))
+    return max(1, min(2 * sh.niw + 1, -(-(8 * sms) // base)))
 
 
 def estimate_device_bytes(sh: PassShapes, precision: str = "fp64", keep_intermediates: bool = True,
@@ -307,11 +315,15 @@ class LadderPass:
         call("dga_dc_kernel_c128", _p(self.chi0), _p(self.u_perm), _p(self.fdc), sh.n_orb, sh.niv, sh.niv_shell, sh.W,
              sh.n_q, _p(self.k_dc), _p(self.dc_scratch), self.dc_scratch.numel() * 16, _s())
 
-    def set_tuning(self, choice) -> None:
-        """Uses the launch choice (kernel, ctas_per_sm) of dga_bse_tuning for this pass's BSE (see autotune.py)."""
+    def set_tuning(self, choice, wait_limit: int = 0) -> None:
+        """Uses the launch choice (kernel, ctas_per_sm) of dga_bse_tuning for this pass's BSE (see autotune.py).
+
+        ``wait_limit`` (polls, 0 = the library default) bounds each wait of the mixed kernels on a bulk copy or
+        a tensor-core tile inside an item; an item whose wait runs out is flagged DGA_ITEM_WAIT_TIMEOUT and
+        re-solved in FP64."""
         from ._lib import BseTuning
 
-        t = BseTuning(kernel=int(choice[0]), ctas_per_sm=int(choice[1]))
+        t = BseTuning(kernel=int(choice[0]), ctas_per_sm=int(choice[1]), wait_limit=int(wait_limit))
         sh = self.sh
         mixed = 1 if self.precision == "mixed" else 0
         nbytes = int(lib().dga_bse_tuned_scratch_bytes(sh.N, sh.n2, self.n_items, mixed, ctypes.byref(t)))

@@ -35,10 +35,15 @@ typedef struct CUstream_st* dga_stream_t; /* cudaStream_t */
 #define DGA_ITEM_SINGULAR 1
 #define DGA_ITEM_NONFINITE 2
 #define DGA_ITEM_NOCONVERGE 4
+#define DGA_ITEM_WAIT_TIMEOUT 8 /* a bounded wait on an asynchronous copy or tensor-core tile ran out */
 
 /* Library version (major*10000 + minor*100 + patch) and the last error message of the calling thread. */
 int dga_version(void);
 const char* dga_last_error_string(void);
+
+/* Streaming multiprocessors of the current device (cached per device); the grid sizes of the streaming kernels
+ * and the caller's chunking of the Sigma contraction are multiples of it.  No counterpart in the upstream. */
+int dga_device_sm_count(void);
 
 /* Generic strided complex copy dst[idx . dst_stride] = scale * src[idx . src_stride] over `shape`
  * (up to 8 dims, strides in complex elements).  Layout conversions at the boundary
@@ -93,7 +98,7 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
                                  int n_items, int max_iter, double tol, void* out, int* status, int* iters,
                                  void* scratch, size_t scratch_bytes, dga_stream_t stream);
 
-/* FP64 re-solve of the items a mixed launch flagged (status & (NOCONVERGE | NONFINITE)), leaving the others
+/* FP64 re-solve of the items a mixed launch flagged (status & (NOCONVERGE | NONFINITE | WAIT_TIMEOUT)), leaving the others
  * untouched; at most grid_limit CTAs (scratch: grid_limit * (N*N + N*n2) complex128). */
 int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
                               const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work, int n_items,
@@ -110,6 +115,12 @@ int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_c
 typedef struct {
   int kernel;
   int ctas_per_sm;
+  long long wait_limit; /* polls of each bounded wait on a copy or tensor-core tile inside an item (0 = default);
+                           an item whose wait runs out is flagged DGA_ITEM_WAIT_TIMEOUT for the FP64 re-solve,
+                           and the waits that drain the CTA's copies and tiles at exit always use the default.
+                           A negative value is a test hook: each CTA first waits -wait_limit polls on a barrier
+                           phase that nothing completes, so that wait runs out and the CTA takes the timeout
+                           path (no further copies or tiles, every item of the CTA flagged) */
 } dga_bse_tuning;
 
 /* dga_bse_solve_sum_c128 (mixed = 0) or dga_bse_solve_sum_mixed_c128 (mixed = 1) with an explicit tuning;
@@ -153,7 +164,9 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
  * (N above about 2040) are rejected with DGA_ERR_SCRATCH.  The first call on a device looks up the array's
  * device address (it can load the module): make it before any stream capture.  Calls share the array, so
  * calls that overlap on the GPU race; calls ordered on one stream are safe.  Nothing needs clearing between
- * calls (every item rewrites its slot before reading it). */
+ * calls (every item rewrites its slot before reading it).  The looked-up address is kept per device for the life
+ * of the process: after cudaDeviceReset (or after the primary context is released and created again) it is stale,
+ * so do not use this entry point across a device reset. */
 #define DGA_BSE_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int dga_bse_solve_sum_noalloc_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta,
                                    double inv_beta2, const void* gamma_cm, const void* chi0_inv, const void* uv,

@@ -27,7 +27,11 @@ import types
 
 import numpy as np
 
-REFERENCE_ROOT = "/root/reference"
+import os
+
+# Root of the upstream DGAmore sources (the directory holding the ``dgamore`` package); read from the
+# DGAMORE_REFERENCE_ROOT environment variable, with the mount point of the fixture-generating container as default.
+REFERENCE_ROOT = os.environ.get("DGAMORE_REFERENCE_ROOT", "/root/reference")
 
 
 class _InPlace:

@@ -1,7 +1,7 @@
 """Generates the golden fixtures under tests/golden/ by running the upstream DGAmore code itself.
 
-Run in a container that holds the upstream sources at /root/reference (they do not travel to the GPU box; the
-committed .npz files do):
+Run in a container that holds the upstream sources, at the path given by the DGAMORE_REFERENCE_ROOT environment
+variable (see _ref_harness.py); the sources are not needed where the tests run, the committed .npz files are:
 
     python tests/golden/make_golden.py
 

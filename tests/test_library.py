@@ -73,7 +73,7 @@ def test_batch_rejects_mixed_orbital_counts_without_launching():
 
 
 def test_tuning_struct_and_rejected_choices_without_gpu():
-    assert ctypes.sizeof(_lib.BseTuning) == 8
+    assert ctypes.sizeof(_lib.BseTuning) == 16  # int kernel, int ctas_per_sm, long long wait_limit
     lib = _lib.lib()
     bad = _lib.BseTuning(kernel=5, ctas_per_sm=0)
     assert lib.dga_bse_tuned_scratch_bytes(720, 9, 100, 1, ctypes.byref(bad)) == 0
