@@ -23,9 +23,10 @@ from ._lib import BseTuning, call, lib
 C128 = torch.complex128
 
 # (kernel, ctas_per_sm): kernel 1 = shared-memory panel (mixed only), 2 = 128-thread kernel, 3 = shared-memory
-# panel with tensor-core trailing tiles (mixed only)
+# panel with tensor-core trailing tiles (mixed only), 4 = block form with pivoting inside 32 x 32 diagonal blocks
+# and every update on the tensor cores (mixed only)
 CANDIDATES = {
-    "mixed": [(3, 0), (1, 0), (2, 0), (2, 2), (2, 1)],
+    "mixed": [(4, 0), (3, 0), (1, 0), (2, 0), (2, 2), (2, 1)],
     "fp64": [(2, 0), (2, 2), (2, 1)],
 }
 

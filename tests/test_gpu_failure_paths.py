@@ -80,7 +80,8 @@ def test_singular_matrix_raises_linalgerror():
         invert_and_sum_over_last_vn(mat, 5.0)
 
 
-def test_wait_that_runs_out_is_flagged_and_resolved(c3_small):
+@pytest.mark.parametrize("kernel", [3, 4])
+def test_wait_that_runs_out_is_flagged_and_resolved(c3_small, kernel):
     from dgamore_b200 import autotune
     from dgamore_b200._lib import BseTuning, call
     from dgamore_b200.pipeline import LadderPass
@@ -91,7 +92,7 @@ def test_wait_that_runs_out_is_flagged_and_resolved(c3_small):
     lp = LadderPass(c3_small, keep_intermediates=False, precision="mixed")
     lp.pre_bse()
     sh = lp.sh
-    t = BseTuning(kernel=3, ctas_per_sm=0, wait_limit=-1000)
+    t = BseTuning(kernel=kernel, ctas_per_sm=0, wait_limit=-1000)
     nbytes = int(autotune.lib().dga_bse_tuned_scratch_bytes(sh.N, sh.n2, lp.n_items, 1, ctypes.byref(t)))
     assert nbytes > 0
     scratch = torch.empty(nbytes // 16 + 1, dtype=torch.complex128, device="cuda")
@@ -112,7 +113,7 @@ def test_wait_that_runs_out_is_flagged_and_resolved(c3_small):
     assert int(lp.bse_status.abs().sum()) == 0
     assert rel_err(lp.X.cpu().numpy(), x64) < 1e-12
     # the same pass afterwards, with the default limit, is clean (the context and the kernel are still usable)
-    lp.set_tuning((3, 0))
+    lp.set_tuning((kernel, 0))
     lp.bse()
     torch.cuda.synchronize()
     assert int(lp.bse_status.abs().sum()) == 0
