@@ -21,6 +21,7 @@ PD = _c.c_void_p
 SIGNATURES = {
     "dga_version": (I, []),
     "dga_device_sm_count": (I, []),
+    "dga_bse_block_ctas_per_sm": (I, [I]),
     "dga_last_error_string": (_c.c_char_p, []),
     "dga_strided_copy_c128": (I, [VP, VP, I, PLL, PLL, PLL, D, VP]),
     "dga_dft_planes_c128": (I, [VP, LL, LL, LL, VP, LL, LL, LL, I, I, I, I, I, VP, D, VP]),
@@ -40,6 +41,7 @@ SIGNATURES = {
     "dga_dc_kernel_c128": (I, [VP, VP, VP, I, I, I, I, I, VP, VP, SZ, VP]),
     "dga_sigma_scratch_bytes": (SZ, [I, I, I, I]),
     "dga_sigma_c128": (I, [VP, VP, I, I, I, I, I, I, I, PI, VP, D, I, VP, VP, SZ, VP]),
+    "dga_sigma_rspace_c128": (I, [VP, VP, I, I, I, I, I, I, I, PI, VP, D, I, VP, VP, SZ, VP]),
     "dga_dft_planes_gather_c128": (I, [VP, LL, LL, LL, VP, LL, LL, LL, I, I, I, I, I, VP, D, PI, VP]),
     "dga_eli_vertex_scratch_bytes": (SZ, [I, I, I, I]),
     "dga_eli_full_vertex_c128": (I, [I, I, I, I, I, I, D, D, VP, VP, VP, VP, VP, PI, I, VP, PI, VP, SZ, VP]),
@@ -47,6 +49,8 @@ SIGNATURES = {
     "dga_eli_chi0pp_c128": (I, [VP, I, I, I, I, VP, VP]),
     "dga_eli_matvec_scratch_bytes": (SZ, [I, I, I]),
     "dga_eli_matvec_c128": (I, [VP, VP, VP, I, I, I, I, I, VP, VP, D, D, VP, VP, SZ, VP]),
+    "dga_eli_matvec_c64mat_c128": (I, [VP, VP, VP, I, I, I, I, I, VP, VP, D, D, VP, VP, SZ, VP]),
+    "dga_narrow_c128_to_c64": (I, [VP, VP, LL, VP]),
     "dga_bse_batch_scratch_bytes": (SZ, [VP, I, I, I]),
     "dga_bse_solve_sum_batch_c128": (I, [VP, VP, I, PI, I, I, I, D, PI, PI, VP, SZ, VP]),
     "dga_bse_tuned_scratch_bytes": (SZ, [I, I, I, I, VP]),

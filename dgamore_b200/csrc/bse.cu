@@ -672,17 +672,11 @@ __global__ void __launch_bounds__(BSE_THREADS, DGA_MIXED_MIN_BLOCKS)
 // descriptor carries the sizes, the resident inputs and the output.  The per-item body is the same as the
 // single-problem kernels.
 // ----------------------------------------------------------------------------------------------
+// One item of a batch: the problem's descriptor gives its sizes, inputs and output; returns the status bits.
 template <bool MIXED, int NR>
-__global__ void __launch_bounds__(BSE_THREADS, MIXED ? DGA_MIXED_MIN_BLOCKS : 3)
-    bse_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work, int n_items,
-                     int n_max, int max_iter, double tol, int* __restrict__ status, int* __restrict__ iters,
-                     unsigned char* __restrict__ scratch, size_t slot_bytes, int redo_only) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    if (redo_only && (status[item] & DGA_ITEM_REDO) == 0) continue;
-    const MultiItem mi = work[item];
-    const dga_bse_problem d = probs[mi.prob];
+__device__ __forceinline__ int multi_item(const dga_bse_problem& d, const MultiItem& mi, int n_max, int max_iter,
+                                          double tol, unsigned char* slot, unsigned char* smem_raw, int* it_out) {
+  {
     struct {
       StructuredSource src;
       int N, n2, nv, W, Q;
@@ -723,6 +717,53 @@ __global__ void __launch_bounds__(BSE_THREADS, MIXED ? DGA_MIXED_MIN_BLOCKS : 3)
       double2* A = reinterpret_cast<double2*>(slot);
       double2* Y = A + (size_t)pb.N * pb.N;
       st = solve_item_fp64<StructuredSource, NR>(pb.src, wi, pb.N, pb.nv, pb.beta, o, A, Y, sm, piv, perm);
+    }
+    *it_out = it;
+    return st;
+  }
+}
+
+template <bool MIXED, int NR>
+__global__ void __launch_bounds__(BSE_THREADS, MIXED ? DGA_MIXED_MIN_BLOCKS : 3)
+    bse_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work, int n_items,
+                     int n_max, int max_iter, double tol, int* __restrict__ status, int* __restrict__ iters,
+                     unsigned char* __restrict__ scratch, size_t slot_bytes, int redo_only) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (redo_only && (status[item] & DGA_ITEM_REDO) == 0) continue;
+    const MultiItem mi = work[item];
+    const dga_bse_problem d = probs[mi.prob];
+    int it = 0;
+    const int st = multi_item<MIXED, NR>(d, mi, n_max, max_iter, tol, slot, smem_raw, &it);
+    __syncthreads();  // every thread has read status[item] before it is rewritten
+    if (threadIdx.x == 0) {
+      status[item] = st;
+      if (iters && !redo_only) iters[item] = it;
+    }
+  }
+}
+
+// Batch whose problems differ in orbital count (the 2-orbital bilayer next to a 1-orbital lattice, say): the same
+// per-item body, with the right-hand-side count chosen per item from its problem's n_orb.  Shared memory and the
+// scratch slot are sized for the largest problem of the launch.
+template <bool MIXED>
+__global__ void __launch_bounds__(BSE_THREADS, MIXED ? DGA_MIXED_MIN_BLOCKS : 3)
+    bse_multi_any_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work, int n_items,
+                         int n_max, int max_iter, double tol, int* __restrict__ status, int* __restrict__ iters,
+                         unsigned char* __restrict__ scratch, size_t slot_bytes, int redo_only) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (redo_only && (status[item] & DGA_ITEM_REDO) == 0) continue;
+    const MultiItem mi = work[item];
+    const dga_bse_problem d = probs[mi.prob];
+    int it = 0, st = 0;
+    switch (d.n_orb) {
+      case 1: st = multi_item<MIXED, 1>(d, mi, n_max, max_iter, tol, slot, smem_raw, &it); break;
+      case 2: st = multi_item<MIXED, 4>(d, mi, n_max, max_iter, tol, slot, smem_raw, &it); break;
+      case 3: st = multi_item<MIXED, 9>(d, mi, n_max, max_iter, tol, slot, smem_raw, &it); break;
+      default: st = multi_item<MIXED, 16>(d, mi, n_max, max_iter, tol, slot, smem_raw, &it); break;
     }
     __syncthreads();  // every thread has read status[item] before it is rewritten
     if (threadIdx.x == 0) {
@@ -1231,24 +1272,34 @@ int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_
 // Launch geometry of a batch.  In the mixed form every request must have the same default kernel as when it runs
 // alone (default_mixed_kernel), so that a request's results are the same in a batch and alone; *kernel receives
 // it (1, 3: shared-memory panel, 2: 128-thread kernel; always 2 in FP64).  Returns false for an invalid batch.
-static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot, int* kernel) {
+// Problems may differ in orbital count (*n2_max receives the largest n_orb^2, *hetero whether they differ); such a
+// batch runs the 128-thread kernels with the right-hand-side count chosen per item, so in the mixed form every
+// problem of it must take the 128-thread kernel alone too (N below 320).
+static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot, int* kernel,
+                       int* n2_max = nullptr, bool* hetero = nullptr) {
   *n_max = 0;
   *slot = 0;
   *kernel = 2;
   if (n_prob <= 0) return false;
-  const int n2 = probs[0].n_orb * probs[0].n_orb;
+  int n2m = 0;
+  bool het = false;
   for (int p = 0; p < n_prob; ++p) {
+    const int n2 = probs[p].n_orb * probs[p].n_orb;
     const int N = n2 * 2 * probs[p].niv;
-    if (probs[p].n_orb != probs[0].n_orb || !supported_rhs(n2) || probs[p].niv <= 0 || N > BSE_MAX_N) return false;
+    if (probs[p].n_orb <= 0 || !supported_rhs(n2) || probs[p].niv <= 0 || N > BSE_MAX_N) return false;
+    het |= probs[p].n_orb != probs[0].n_orb;
     if (mixed) {
       const int k = default_mixed_kernel(N, n2);
       if (p == 0) *kernel = k;
       if (k != *kernel) return false;
     }
     if (N > *n_max) *n_max = N;
+    if (n2 > n2m) n2m = n2;
   }
   const bool panel = *kernel != 2;
+  if (het && panel) return false;
   for (int p = 0; p < n_prob; ++p) {
+    const int n2 = probs[p].n_orb * probs[p].n_orb;
     const int N = n2 * 2 * probs[p].niv;
     const size_t sl = panel ? dga_panel_slot_bytes(N, n2)
                       : mixed ? mixed_slot_bytes(N, n2)
@@ -1256,11 +1307,18 @@ static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int*
     if (sl > *slot) *slot = sl;
   }
   *slot = (*slot + 255) & ~(size_t)255;
+  if (n2_max) *n2_max = n2m;
+  if (hetero) *hetero = het;
   return true;
 }
 
 static size_t batch_smem(int n_max, int n2, int mixed) {
   return mixed ? mixed_smem_bytes(n_max, n2) : bse_smem_bytes(n_max);
+}
+
+static int batch_grid_hetero(int mixed, int n_items, size_t smem) {
+  return mixed ? grid_for(bse_multi_any_kernel<true>, n_items, smem)
+               : grid_for(bse_multi_any_kernel<false>, n_items, smem);
 }
 
 template <bool MIXED, int NR>
@@ -1283,14 +1341,17 @@ extern "C" {
 
 // Scratch bytes of dga_bse_solve_sum_batch_c128 (probs is a HOST array here); 0 for an invalid batch.
 size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int n_items, int mode) {
-  int n_max = 0, kernel = 2;
+  int n_max = 0, kernel = 2, n2_max = 0;
   size_t slot = 0;
+  bool hetero = false;
   const int mixed = mode == 1;
-  if (!probs || n_items <= 0 || mode < 0 || mode > 2 || !batch_dims(probs, n_prob, mixed, &n_max, &slot, &kernel))
+  if (!probs || n_items <= 0 || mode < 0 || mode > 2 ||
+      !batch_dims(probs, n_prob, mixed, &n_max, &slot, &kernel, &n2_max, &hetero))
     return 0;
   const int n2 = probs[0].n_orb * probs[0].n_orb;
   const bool panel = kernel != 2;
   if (panel) return (size_t)dga_panel_batch_grid(n2, n_max, n_items, kernel == 3) * slot;
+  if (hetero) return (size_t)batch_grid_hetero(mixed, n_items, batch_smem(n_max, n2_max, mixed)) * slot;
   return (size_t)batch_grid_any(mixed, n2, n_items, batch_smem(n_max, n2, mixed)) * slot;
 }
 
@@ -1304,13 +1365,14 @@ size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int
 int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* probs_dev, int n_prob, const int* work,
                                  int n_items, int mode, int max_iter, double tol, int* status, int* iters,
                                  void* scratch, size_t scratch_bytes, cudaStream_t stream) {
-  int n_max = 0, kernel = 2;
+  int n_max = 0, kernel = 2, n2_max = 0;
   size_t slot = 0;
+  bool hetero = false;
   const int mixed = mode == 1;
   if (!probs_host || !probs_dev || !work || !scratch || !status || n_items <= 0 || max_iter < 0 || mode < 0 ||
-      mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot, &kernel)) {
-    dga_set_error("dga_bse_solve_sum_batch_c128: invalid arguments (problems must share n_orb in {1,2,3,4}, and in "
-                  "the mixed form all have N below 320 or all from 320 up)");
+      mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot, &kernel, &n2_max, &hetero)) {
+    dga_set_error("dga_bse_solve_sum_batch_c128: invalid arguments (n_orb in {1,2,3,4}; in the mixed form all "
+                  "problems have N below 320 or all from 320 up, and problems of different n_orb all below 320)");
     return DGA_ERR_ARG;
   }
   for (int p = 0; p < n_prob; ++p) {
@@ -1321,9 +1383,11 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
     }
   }
   const int n2 = probs_host[0].n_orb * probs_host[0].n_orb;
-  const size_t smem = batch_smem(n_max, n2, mixed);
+  const size_t smem = batch_smem(n_max, hetero ? n2_max : n2, mixed);
   const bool panel = kernel != 2;
-  int grid = panel ? dga_panel_batch_grid(n2, n_max, n_items, kernel == 3) : batch_grid_any(mixed, n2, n_items, smem);
+  int grid = panel    ? dga_panel_batch_grid(n2, n_max, n_items, kernel == 3)
+             : hetero ? batch_grid_hetero(mixed, n_items, smem)
+                      : batch_grid_any(mixed, n2, n_items, smem);
   if (scratch_bytes < slot) {
     dga_set_error("dga_bse_solve_sum_batch_c128: scratch too small (%zu < one slot of %zu)", scratch_bytes, slot);
     return DGA_ERR_SCRATCH;
@@ -1336,6 +1400,20 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   if (panel) {
     cudaError_t err = dga_panel_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
                                              stream, kernel == 3);
+    if (err != cudaSuccess) {
+      dga_set_error("dga_bse_solve_sum_batch_c128: launch failed: %s", cudaGetErrorString(err));
+      return DGA_ERR_LAUNCH;
+    }
+    return DGA_OK;
+  }
+  if (hetero) {
+    if (mixed)
+      bse_multi_any_kernel<true><<<grid, BSE_THREADS, smem, stream>>>(pd, wk, n_items, n_max, max_iter, tol, status,
+                                                                      iters, sc, slot, 0);
+    else
+      bse_multi_any_kernel<false><<<grid, BSE_THREADS, smem, stream>>>(pd, wk, n_items, n_max, max_iter, tol, status,
+                                                                       iters, sc, slot, redo);
+    cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {
       dga_set_error("dga_bse_solve_sum_batch_c128: launch failed: %s", cudaGetErrorString(err));
       return DGA_ERR_LAUNCH;

@@ -7,13 +7,14 @@
 // products, and refined in FP64 until the correction is below tol max|Y|.
 //
 // Factorisation: block Gaussian elimination on 32 x 32 blocks in Schur-complement form.  Step k:
-//   D_k^-1                  inverse of the current diagonal block, by Gauss-Jordan elimination with partial
-//                           pivoting inside the block (one warp; the row interchanges end up inside D_k^-1);
-//   W_k = D_k^-1 A[k, >k]   the block row, overwritten in place (tensor cores, transposed 128-column tiles);
-//   A[>k, >k] -= A[>k, k] W_k   the trailing update (tensor cores, 128 x 32 tiles); the block column is kept.
-// Then A = L U with L = [I; A_ik D_k^-1] and U = [D_k, A_kj], so the solves are
-//   forward   y_k <- D_k^-1 y_k, then y_i -= A_ik y_k for i > k;
-//   backward  x_k = y_k - sum_{j > k} W_kj x_j.
+//   D_k^-1   inverse of the current diagonal block, by Gauss-Jordan elimination with partial pivoting inside the
+//            block (the whole CTA; the row interchanges end up inside D_k^-1);
+//   A[>k, >k] -= (A[>k, k] D_k^-1) A[k, >k]   the trailing update on the tensor cores: per 128-row block the
+//            product L' = A[rows, k] D_k^-1 is one tensor-core product whose result becomes the A operand of the
+//            block's 128 x 32 tiles, whose B operands are the block row's split planes (built once per step).
+// The block row and the block column stay as they are, so A = L U with L = [I; A_ik D_k^-1] and U = [D_k, A_kj]:
+//   forward   z_k = D_k^-1 y_k, then y_i -= A_ik z_k for i > k;
+//   backward  y_k <- D_k^-1 y_k, then y_i -= A_ik y_k for i < k.
 // The n2 selector columns ride along as extra columns, so after the factorisation they hold the forward result.
 // Restricting the pivot search to the diagonal block removes the CTA-wide, column-by-column pivot chain; the
 // FP64 refinement restores full accuracy (one correction at the 3-orbital size, as with partial pivoting).  An
@@ -62,10 +63,11 @@ __host__ __device__ inline size_t block_smem_bytes() {
 }
 
 // Solve-phase use of the region: y [NR][N] complex64 | ys [32][NR] + colsum [NR][NR] complex128 | two staged
-// diagonal inverses [2][32][32] complex64.
+// diagonal inverses [2][32][32] complex64 | the forward solve's D^-1 y_b [NR][32] complex64.
 __host__ __device__ inline size_t block_solve_bytes(int N, int NR) {
   const size_t y = (((size_t)NR * N * sizeof(float2)) + 15) & ~(size_t)15;
-  return y + (size_t)(32 * NR + NR * NR) * sizeof(double2) + 2 * KB * KB * sizeof(float2);
+  return y + (size_t)(32 * NR + NR * NR) * sizeof(double2) + 2 * KB * KB * sizeof(float2) +
+         (size_t)NR * KB * sizeof(float2);
 }
 
 struct BlockSmem {
@@ -75,6 +77,7 @@ struct BlockSmem {
   double2* ys;    // solve phase: [32][NR] staging of the residual
   double2* colsum;  // solve phase: [NR][NR]
   float2* sinv;   // solve phase: [2][32][32] staged diagonal inverses
+  float2* zb;     // solve phase: [NR][32] D^-1 y_b of the forward solve
   float2* dinv;   // [32][K_DLD] current diagonal inverse, row-major
   uint64_t* bar;  // [2] completion barriers of the tiles in flight
   uint64_t* probe;  // test hook: a barrier nothing arrives on
@@ -93,6 +96,7 @@ struct BlockSmem {
     ys = reinterpret_cast<double2*>(p + yb);
     colsum = ys + 32 * NR;
     sinv = reinterpret_cast<float2*>(colsum + NR * NR);
+    zb = sinv + 2 * KB * KB;
     p += K_REGION;
     dinv = reinterpret_cast<float2*>(p);
     p += KB * K_DLD * sizeof(float2);
@@ -179,127 +183,141 @@ __device__ __forceinline__ void issue_planar(uint32_t d_re, uint32_t d_im, const
 // Forming A (complex64, column-major) and the NR selector columns S[(p, nu)][s] = delta_ps
 // ----------------------------------------------------------------------------------------------
 // Element (i, j) as StructuredSource::element: (chi0^-1 [block diagonal] + Gamma / beta^2) + (-(U + V) / beta^2);
-// a thread owns two rows per pass with eight columns of Gamma loads in flight.
+// a thread owns rows tid, tid + KT, tid + 2 KT of a pass (a warp reads 512 contiguous bytes of a Gamma column per
+// load) with eight columns of Gamma loads in flight.
 template <int NR>
 __device__ void block_form_a(const StructuredSource& src, const WorkItem& wi, int N, int nv, float2* __restrict__ A) {
+  constexpr int RPT = 3, CPI = 8;  // rows per thread and pass, columns per iteration
   const int tid = threadIdx.x;
   const double2* gam = src.gamma_cm + ((size_t)(wi.ch * src.W + wi.w) * N) * N;
   const double2* c0 = src.chi0_inv + ((size_t)wi.q * src.W + wi.w) * nv * NR * NR;
   const double2* uvq = src.uv + ((size_t)wi.ch * src.Q + wi.q) * NR * NR;
   const double ib2 = src.inv_beta2;
-  for (int rbase = 0; rbase < N; rbase += 2 * KT) {
-    int ri[2], pr[2], vr[2];
-    bool rok[2];
+  for (int pass = 0; pass * RPT * KT < N; ++pass) {
+    int ri[RPT], pr[RPT], vr[RPT];
+    bool rok[RPT];
 #pragma unroll
-    for (int a2 = 0; a2 < 2; ++a2) {
-      ri[a2] = rbase + tid + a2 * KT;
-      rok[a2] = ri[a2] < N;
-      pr[a2] = rok[a2] ? ri[a2] / nv : 0;
-      vr[a2] = rok[a2] ? ri[a2] - pr[a2] * nv : 0;
+    for (int a = 0; a < RPT; ++a) {
+      ri[a] = pass * RPT * KT + tid + a * KT;
+      rok[a] = ri[a] < N;
+      pr[a] = rok[a] ? ri[a] / nv : 0;
+      vr[a] = rok[a] ? ri[a] - pr[a] * nv : 0;
     }
     if (!rok[0]) break;
-    for (int j0 = 0; j0 < N; j0 += 8) {
-      double2 g[2][8];
+    for (int j0 = 0; j0 < N; j0 += CPI) {
+      double2 g[CPI][RPT];
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
+      for (int u = 0; u < CPI; ++u)
 #pragma unroll
-        for (int a2 = 0; a2 < 2; ++a2)
-          g[a2][u] = (rok[a2] && j0 + u < N) ? __ldcg(gam + (size_t)(j0 + u) * N + ri[a2]) : make_double2(0.0, 0.0);
+        for (int a = 0; a < RPT; ++a)
+          g[u][a] = (rok[a] && j0 + u < N) ? __ldcg(gam + (size_t)(j0 + u) * N + ri[a]) : make_double2(0.0, 0.0);
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < CPI; ++u) {
         const int j = j0 + u;
         if (j >= N) break;
         const int pc = j / nv, vc = j - pc * nv;
 #pragma unroll
-        for (int a2 = 0; a2 < 2; ++a2) {
-          if (!rok[a2]) continue;
-          const double2 uu = uvq[pr[a2] * NR + pc];
-          double re = __dmul_rn(g[a2][u].x, ib2);
-          double im = __dmul_rn(g[a2][u].y, ib2);
-          if (vr[a2] == vc) {
-            const double2 c = c0[(size_t)vr[a2] * NR * NR + pr[a2] * NR + pc];
+        for (int a = 0; a < RPT; ++a) {
+          if (!rok[a]) continue;
+          const double2 uu = uvq[pr[a] * NR + pc];
+          double re = __dmul_rn(g[u][a].x, ib2);
+          double im = __dmul_rn(g[u][a].y, ib2);
+          if (vr[a] == vc) {
+            const double2 c = c0[(size_t)vr[a] * NR * NR + pr[a] * NR + pc];
             re = __dadd_rn(c.x, re);
             im = __dadd_rn(c.y, im);
           }
           re = __dadd_rn(re, -__dmul_rn(uu.x, ib2));
           im = __dadd_rn(im, -__dmul_rn(uu.y, ib2));
-          A[(size_t)j * N + ri[a2]] = make_float2((float)re, (float)im);
+          A[(size_t)j * N + ri[a]] = make_float2((float)re, (float)im);
         }
       }
     }
 #pragma unroll
-    for (int a2 = 0; a2 < 2; ++a2)
-      if (rok[a2])
-        for (int r = 0; r < NR; ++r) A[(size_t)(N + r) * N + ri[a2]] = make_float2(pr[a2] == r ? 1.f : 0.f, 0.f);
+    for (int a = 0; a < RPT; ++a)
+      if (rok[a])
+        for (int r = 0; r < NR; ++r) A[(size_t)(N + r) * N + ri[a]] = make_float2(pr[a] == r ? 1.f : 0.f, 0.f);
   }
 }
 
 // ----------------------------------------------------------------------------------------------
-// D_k^-1 by Gauss-Jordan elimination of [D | I] with the pivot search inside the block (warp 0; lane = row).
-// aug: [64][K_DLD] column-major workspace.  Writes D^-1 row-major to s.dinv (ld K_DLD) and inv (ld 32), zero
-// outside the nb x nb block.  Returns false if a pivot column was exactly zero or not finite.
+// D_k^-1 by Gauss-Jordan elimination of [D | I] with the pivot search inside the block, by the whole CTA: lane =
+// row, warp w owns the 16 columns w + 8t of the 64 (8 of D, 8 of I).  Per pivot step: the owner warp of column jj
+// finds the pivot (largest |re| + |im|, ties to the smaller row, NaN no candidate); every thread reads the old
+// values it needs; then writes row jj <- (old row p) / pivot and row i <- (old row i, or old row jj for i = p) -
+// f_i (new row jj).  aug: [64][K_DLD] column-major workspace; sp: {p, ok} and the pivot value, shared.
+// Writes D^-1 row-major to s.dinv (ld K_DLD) and inv (ld 32), zero outside the nb x nb block.  Returns false
+// (in every thread) if a pivot column was exactly zero or not finite.
 // ----------------------------------------------------------------------------------------------
 __device__ bool block_diag_inverse(const float2* __restrict__ A, int N, int k0, int nb, float2* aug, float2* dinv,
-                                   float2* __restrict__ inv) {
-  const int lane = threadIdx.x & 31;
-  for (int c = 0; c < KB; ++c) {
-    aug[c * K_DLD + lane] = (c < nb && lane < nb) ? __ldcg(A + (size_t)(k0 + c) * N + k0 + lane)
-                                                  : make_float2(c == lane ? 1.f : 0.f, 0.f);
-    aug[(KB + c) * K_DLD + lane] = make_float2(c == lane ? 1.f : 0.f, 0.f);
+                                   float2* __restrict__ inv, int* sp, float2* sd) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < 2 * KB / KW; ++t) {
+    const int c = warp + KW * t;  // t < 4: columns of D, t >= 4: columns of I
+    float2 x;
+    if (c < KB)
+      x = (c < nb && lane < nb) ? __ldcg(A + (size_t)(k0 + c) * N + k0 + lane) : make_float2(c == lane ? 1.f : 0.f, 0.f);
+    else
+      x = make_float2(c - KB == lane ? 1.f : 0.f, 0.f);
+    aug[c * K_DLD + lane] = x;
   }
-  __syncwarp();
-  bool ok = true;
+  if (threadIdx.x == 0) sp[1] = 1;
+  __syncthreads();
   for (int jj = 0; jj < nb; ++jj) {
-    float v = (lane >= jj && lane < nb) ? cabs1(aug[jj * K_DLD + lane]) : -1.f;
-    int p = lane;
-    {  // largest |re| + |im|, ties to the smaller row; NaN is no candidate
+    if (warp == (jj & (KW - 1))) {
+      float v = (lane >= jj && lane < nb) ? cabs1(aug[jj * K_DLD + lane]) : -1.f;
       const bool cand = v >= 0.f;
       const unsigned key = cand ? __float_as_uint(v) : 0u;
       const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
       const unsigned imin = __reduce_min_sync(0xffffffffu, (cand && key == kmax) ? (unsigned)lane : 0x7fffffffu);
       v = __uint_as_float(kmax);
-      p = (int)imin;
-    }
-    const bool good = (v > 0.f) && isfinite(v) && p >= jj && p < nb;
-    if (!good) {
-      ok = false;
-      p = jj;
-    }
-    if (p != jj) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int c = lane + 32 * h;
-        const float2 t = aug[c * K_DLD + jj];
-        aug[c * K_DLD + jj] = aug[c * K_DLD + p];
-        aug[c * K_DLD + p] = t;
+      int p = (int)imin;
+      const bool good = (v > 0.f) && isfinite(v) && p >= jj && p < nb;
+      if (!good) p = jj;
+      if (lane == 0) {
+        sp[0] = p;
+        if (!good) sp[1] = 0;
+        *sd = good ? aug[jj * K_DLD + p] : make_float2(0.f, 0.f);
       }
     }
-    __syncwarp();
-    const float2 rinv = good ? crecip(aug[jj * K_DLD + jj]) : make_float2(0.f, 0.f);
-    __syncwarp();
+    __syncthreads();
+    const int p = sp[0];
+    const float2 d = *sd;
+    const float2 rinv = (d.x != 0.f || d.y != 0.f) ? crecip(d) : make_float2(0.f, 0.f);
+    // old values: this row (row jj's for i = p), the factor in column jj, the new pivot row
+    const int i = lane;
+    const int src = (i == p) ? jj : i;
+    const float2 f = (i == jj) ? make_float2(0.f, 0.f) : aug[jj * K_DLD + src];
+    float2 old[2 * KB / KW], prow[2 * KB / KW];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int c = lane + 32 * h;
-      aug[c * K_DLD + jj] = cmul(aug[c * K_DLD + jj], rinv);
+    for (int t = 0; t < 2 * KB / KW; ++t) {
+      const int c = warp + KW * t;
+      old[t] = aug[c * K_DLD + src];
+      prow[t] = cmul(aug[c * K_DLD + p], rinv);
     }
-    __syncwarp();
-    const float2 f = aug[jj * K_DLD + lane];
-    __syncwarp();
-    if (lane != jj) {
-      for (int c = jj + 1; c < 2 * KB; ++c) {
-        float2 x = aug[c * K_DLD + lane];
-        cfms(x, f, aug[c * K_DLD + jj]);
-        aug[c * K_DLD + lane] = x;
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < 2 * KB / KW; ++t) {
+      const int c = warp + KW * t;
+      float2 x = prow[t];
+      if (i != jj) {
+        x = old[t];
+        cfms(x, f, prow[t]);
       }
+      aug[c * K_DLD + i] = x;
     }
-    __syncwarp();
+    __syncthreads();
   }
-  for (int k = 0; k < KB; ++k) {
-    const float2 x = (lane < nb && k < nb) ? aug[(KB + k) * K_DLD + lane] : make_float2(0.f, 0.f);
-    dinv[lane * K_DLD + k] = x;
-    inv[lane * KB + k] = x;
+  for (int e = threadIdx.x; e < KB * KB; e += KT) {
+    const int r = e >> 5, k = e & 31;
+    const float2 x = (r < nb && k < nb) ? aug[(KB + k) * K_DLD + r] : make_float2(0.f, 0.f);
+    dinv[r * K_DLD + k] = x;
+    inv[r * KB + k] = x;
   }
-  return __all_sync(0xffffffffu, ok);
+  const bool ok = sp[1] != 0;
+  __syncthreads();
+  return ok;
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -318,91 +336,29 @@ __device__ __forceinline__ bool tile_wait(BlockSmem& s, TileCount& tc, int b) {
 }
 
 // ----------------------------------------------------------------------------------------------
-// Block row: W = D^-1 A[k0:k1, k1:NC] in place, plus its split planes per 32-column strip in bop (the B operands
-// of the trailing tiles).  Transposed tiles: D'(j, i) = sum_k A[k0 + k][j] D^-1[i][k], 128 columns j per tile.
+// Split planes of the block row A[k0:k1, k1:NC] per 32-column strip, in bop (the B operands of the trailing tiles):
+// plane element (c, k) = A[k0 + k][k1 + 32 st + c]; zero beyond the row's columns.  Two threads per column, each a
+// 128-byte run of it.
 // ----------------------------------------------------------------------------------------------
-__device__ void block_row_w(float2* __restrict__ A, int N, int NC, int k0, int nb, int k1, BlockSmem& s,
-                            float* __restrict__ bop, TileCount& tc) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+__device__ void block_row_planes(const float2* __restrict__ A, int N, int NC, int k0, int k1, float* __restrict__ bop) {
   const int ncols = NC - k1;
-  if (ncols <= 0) return;
+  if (ncols <= 0 || k1 >= N) return;
   const int nst = (ncols + KTN - 1) / KTN;
-  float* bpl = s.b_pl;  // B' = (D^-1)^T: row i, k contiguous
-  for (int e = tid; e < KB * (KB / 4); e += KT) {
-    const int i = e >> 3, k = (e & 7) * 4;
-    const float2* d = s.dinv + i * K_DLD + k;
-    store_planes(bpl, KBP, i, k, d[0], d[1], d[2], d[3]);
-  }
-  const uint32_t tbase = *s.tslot;
-  const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
-  const int hh = warp >> 2;
-  const int ntile = (ncols + KTM - 1) / KTM;
-  for (int t = 0; t < ntile; ++t) {
-    const int j0 = k1 + t * KTM;
-    {  // A' planes: row = column j of the block row, k = row of the block (one 256-byte column per two threads)
-      const int jl = tid & (KTM - 1), h = tid >> 7, j = j0 + jl;
-      const bool jok = j < NC;
-      const float4* col = reinterpret_cast<const float4*>(A + (size_t)j * N + k0 + 16 * h);
+  for (int e = threadIdx.x; e < nst * KTN * 2; e += KT) {
+    const int jl = e >> 1, h = e & 1, j = k1 + jl;
+    const int st = jl >> 5, c = jl & 31;
+    float* sp = bop + (size_t)st * 4 * KBP;
+    const float4* col = reinterpret_cast<const float4*>(A + (size_t)j * N + k0 + 16 * h);
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        const int k = 16 * h + 4 * g;
-        float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
-        if (jok && k + 4 <= nb) {
-          x0 = __ldcg(col + 2 * g);
-          x1 = __ldcg(col + 2 * g + 1);
-        } else if (jok) {
-          const float2* c2 = A + (size_t)j * N + k0;
-          float2 v[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) v[u] = (k + u < nb) ? __ldcg(c2 + k + u) : make_float2(0.f, 0.f);
-          x0 = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
-          x1 = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
-        }
-        store_planes(s.a_pl, KAP, jl, k, make_float2(x0.x, x0.y), make_float2(x0.z, x0.w), make_float2(x1.x, x1.y),
-                     make_float2(x1.z, x1.w));
-      }
-    }
-    tc_fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    const bool live = s.misc[0] == 0;
-    if (live && tid == 0) {
-      tc_fence_after();
-      issue_planar(tbase, tbase + 32, s.a_pl, bpl, false, true);
-      tc_commit(s.bar);
-    }
-    if (live) tc.iss[0] += 1;
-    const bool ok = live && tile_wait(s, tc, 0);
-    tc_fence_after();
-    if (ok) {
-      float re[16], im[16];
-      tmem_ld16(tl + 16 * hh, re);
-      tmem_ld16(tl + 32 + 16 * hh, im);
-      tmem_wait_ld();
-      const int jl = 32 * (warp & 3) + lane, j = j0 + jl;
+    for (int g = 0; g < 4; ++g) {
+      float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
       if (j < NC) {
-        float2* col = A + (size_t)j * N + k0 + 16 * hh;
-#pragma unroll
-        for (int ii = 0; ii < 16; ++ii)
-          if (16 * hh + ii < nb) col[ii] = make_float2(re[ii], im[ii]);
+        x0 = __ldcg(col + 2 * g);
+        x1 = __ldcg(col + 2 * g + 1);
       }
-      const int st = (j - k1) >> 5, c = (j - k1) & 31;
-      if (st < nst) {
-        float* sp = bop + (size_t)st * 4 * KBP;
-        const bool jv = j < NC;
-#pragma unroll
-        for (int g = 0; g < 4; ++g) {
-          const int k = 16 * hh + 4 * g;
-          float2 v[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u)
-            v[u] = (jv && k + u < nb) ? make_float2(re[4 * g + u], im[4 * g + u]) : make_float2(0.f, 0.f);
-          store_planes(sp, KBP, c, k, v[0], v[1], v[2], v[3]);
-        }
-      }
+      store_planes(sp, KBP, c, 16 * h + 4 * g, make_float2(x0.x, x0.y), make_float2(x0.z, x0.w),
+                   make_float2(x1.x, x1.y), make_float2(x1.z, x1.w));
     }
-    tc_fence_before();
-    __syncthreads();
   }
 }
 
@@ -456,6 +412,40 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
 #pragma unroll
       for (int g = 0; g < 4; ++g) store_planes(s.a_pl, KAP, rl, 16 * h + 4 * g, v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
     }
+    // B planes of D^-1: element (i, k) = D^-1[k][i], so that the product below is A21 D^-1
+    for (int e = tid; e < KB * (KB / 4); e += KT) {
+      const int i = e >> 3, k = (e & 7) * 4;
+      const float2* d = s.dinv + i;
+      store_planes(s.b_pl + 4 * KBP, KBP, i, k, d[k * K_DLD], d[(k + 1) * K_DLD], d[(k + 2) * K_DLD],
+                   d[(k + 3) * K_DLD]);
+    }
+    tc_fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    {  // L21' = A21 D^-1 for the block's rows into TMEM buffer 0, then split back into the A planes
+      const bool live = s.misc[0] == 0;
+      if (live && tid == 0) {
+        tc_fence_after();
+        issue_planar(tbase, tbase + 32, s.a_pl, s.b_pl + 4 * KBP, false, true);
+        tc_commit(s.bar);
+      }
+      if (live) tc.iss[0] += 1;
+      const bool ok = live && tile_wait(s, tc, 0);
+      tc_fence_after();
+      if (ok) {
+        float re[16], im[16];
+        tmem_ld16(tl + 16 * hh, re);
+        tmem_ld16(tl + 32 + 16 * hh, im);
+        tmem_wait_ld();
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+          store_planes(s.a_pl, KAP, row_t, 16 * hh + 4 * g, make_float2(re[4 * g], im[4 * g]),
+                       make_float2(re[4 * g + 1], im[4 * g + 1]), make_float2(re[4 * g + 2], im[4 * g + 2]),
+                       make_float2(re[4 * g + 3], im[4 * g + 3]));
+      }
+      tc_fence_before();
+      __syncthreads();
+    }
     if (warp == KW - 1) {
       prefetch_tile_l2(A, N, NC, r0, k1);
       if (nst > 1) prefetch_tile_l2(A, N, NC, r0, k1 + KTN);
@@ -501,17 +491,21 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
 }
 
 // ----------------------------------------------------------------------------------------------
-// Triangular solves with the block factors for NR right-hand sides y[r * ldy + i] in shared memory.
-//   forward:  for each block b: y_b <- D_b^-1 y_b (warp per right-hand side, lane = row), then the rows below
-//             y_i -= A[i, b] y_b (thread per row); the next block's inverse is staged during the update;
-//   backward: for each block b from the last: the rows above y_i -= W[i, b] y_b.
+// Triangular solves with the block factors for NR right-hand sides y[r * ldy + i] in shared memory: with
+// `forward` the full solve (L then U), else the back substitution alone (the selector columns already hold L^-1 S).
+//   forward sweep (L y = r):  for each block b: z_b = D_b^-1 y_b (warp per right-hand side, lane = row, into zb),
+//                             then the rows below y_i -= A[i, b] z_b (thread per row);
+//   back substitution (U x = y): for each block b from the last: y_b <- D_b^-1 y_b, then the rows above
+//                             y_i -= A[i, b] y_b.
+// The inverse of the next block is staged into sinv (double buffered) during each update.
 // ----------------------------------------------------------------------------------------------
 template <int NR>
 __device__ void block_solve(const float2* __restrict__ A, int N, float2* y, int ldy, const float2* __restrict__ inv,
-                            float2* sinv, bool forward) {
+                            float2* sinv, float2* zb, bool forward) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nblk = block_nblk(N);
-  auto update = [&](int k0, int nb, int i0, int i1) {
+  // rows [i0, i1): y_i -= sum_k A[i][k0 + k] v[r][k], v = y + k0 (backward) or zb (forward)
+  auto update = [&](int k0, int nb, int i0, int i1, const float2* v, int ldv) {
     for (int i = i0 + tid; i < i1; i += KT) {
       float2 acc[NR];
 #pragma unroll
@@ -524,46 +518,51 @@ __device__ void block_solve(const float2* __restrict__ A, int N, float2* y, int 
         for (int u = 0; u < 16; ++u)
           if (k + u < nb) {
 #pragma unroll
-            for (int r = 0; r < NR; ++r) cfms(acc[r], l[u], y[(size_t)r * ldy + k0 + k + u]);
+            for (int r = 0; r < NR; ++r) cfms(acc[r], l[u], v[(size_t)r * ldv + k + u]);
           }
       }
 #pragma unroll
       for (int r = 0; r < NR; ++r) y[(size_t)r * ldy + i] = acc[r];
     }
   };
-  if (forward) {
-    for (int e = tid; e < KB * KB; e += KT) sinv[e] = inv[e];
+  // one sweep over the blocks: fwd = forward elimination (L), else back substitution (U)
+  auto sweep = [&](bool fwd) {
+    auto blk = [&](int st) { return fwd ? st : nblk - 1 - st; };
+    for (int e = tid; e < KB * KB; e += KT) sinv[e] = inv[(size_t)blk(0) * KB * KB + e];
     __syncthreads();
-    for (int b = 0; b < nblk; ++b) {
+    for (int st = 0; st < nblk; ++st) {
+      const int b = blk(st);
       const int k0 = b * KB, nb = min(KB, N - k0), k1 = k0 + nb;
-      const float2* sv = sinv + (b & 1) * KB * KB;
-      for (int r = warp; r < NR; r += KW) {
+      const float2* sv = sinv + (st & 1) * KB * KB;
+      for (int r = warp; r < NR; r += KW) {  // D_b^-1 y_b
         float2* yr = y + (size_t)r * ldy + k0;
         float2 acc = make_float2(0.f, 0.f);
         for (int k = 0; k < nb; ++k) cfma(acc, sv[lane * KB + k], yr[k]);
-        __syncwarp();
-        if (lane < nb) yr[lane] = acc;
+        if (fwd) {
+          zb[r * KB + lane] = acc;
+        } else {
+          __syncwarp();
+          if (lane < nb) yr[lane] = acc;
+        }
       }
       float2 nx[KB * KB / KT];
-      if (b + 1 < nblk) {
+      if (st + 1 < nblk) {
 #pragma unroll
-        for (int u = 0; u < KB * KB / KT; ++u) nx[u] = inv[(size_t)(b + 1) * KB * KB + tid + u * KT];
+        for (int u = 0; u < KB * KB / KT; ++u) nx[u] = inv[(size_t)blk(st + 1) * KB * KB + tid + u * KT];
       }
       __syncthreads();
-      update(k0, nb, k1, N);
-      if (b + 1 < nblk) {
-        float2* dst = sinv + ((b + 1) & 1) * KB * KB;
+      if (fwd) update(k0, nb, k1, N, zb, KB);
+      else update(k0, nb, 0, k0, y + k0, ldy);
+      if (st + 1 < nblk) {
+        float2* dst = sinv + ((st + 1) & 1) * KB * KB;
 #pragma unroll
         for (int u = 0; u < KB * KB / KT; ++u) dst[tid + u * KT] = nx[u];
       }
       __syncthreads();
     }
-  }
-  for (int b = nblk - 1; b > 0; --b) {
-    const int k0 = b * KB, nb = min(KB, N - k0);
-    update(k0, nb, 0, k0);
-    __syncthreads();
-  }
+  };
+  if (forward) sweep(true);
+  sweep(false);
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -589,21 +588,23 @@ __device__ int solve_item_block(const StructuredSource& src, const WorkItem& wi,
   // ---- factorisation ----
   for (int k0 = 0; k0 < N; k0 += KB) {
     const int nb = min(KB, N - k0), k1 = k0 + nb;
-    if (threadIdx.x < 32) {
+    {  // the block reductions' scratch holds the pivot step's broadcast here
       const bool ok = block_diag_inverse(A, N, k0, nb, reinterpret_cast<float2*>(s.a_pl), s.dinv,
-                                         inv + (size_t)(k0 / KB) * KB * KB);
+                                         inv + (size_t)(k0 / KB) * KB * KB, reinterpret_cast<int*>(s.redd),
+                                         reinterpret_cast<float2*>(s.redd + 2));
       if (!ok && threadIdx.x == 0) s.misc[2] = 1;
     }
     __syncthreads();
-    block_row_w(A, N, NC, k0, nb, k1, s, bop, tc);
+    block_row_planes(A, N, NC, k0, k1, bop);
+    __syncthreads();
     block_trailing(A, N, NC, k0, k1, s, bop, tc);
   }
   __syncthreads();
-  // ---- initial solve: the selector columns hold the forward result; back substitution only ----
+  // ---- initial solve: the selector columns hold the forward result L^-1 S; back substitution only ----
   const int ldy = N;
   for (int e = tid; e < NR * N; e += KT) s.y[e] = A[(size_t)N * N + e];
   __syncthreads();
-  block_solve<NR>(A, N, s.y, ldy, inv, s.sinv, false);
+  block_solve<NR>(A, N, s.y, ldy, inv, s.sinv, s.zb, false);
   double prev = 0.0;
   for (int e = tid; e < NR * N; e += KT) {
     Y[e] = make_double2(s.y[e].x, s.y[e].y);
@@ -616,7 +617,7 @@ __device__ int solve_item_block(const StructuredSource& src, const WorkItem& wi,
     structured_residual_permuted<NR>(src, wi.ch, wi.q, wi.w, N, nv, Y, Rb, nullptr, s.colsum, s.ys);
     for (int e = tid; e < NR * N; e += KT) s.y[e] = make_float2((float)Rb[e].x, (float)Rb[e].y);
     __syncthreads();
-    block_solve<NR>(A, N, s.y, ldy, inv, s.sinv, true);
+    block_solve<NR>(A, N, s.y, ldy, inv, s.sinv, s.zb, true);
     double dmax = 0.0, ymax = 0.0;
     for (int e = tid; e < NR * N; e += KT) {
       const double2 d = make_double2(s.y[e].x, s.y[e].y);
@@ -736,16 +737,46 @@ bool dga_block_supported(int N, int n2) {
 
 size_t dga_block_slot_bytes(int N, int n2) { return (block_slot_bytes(N, n2) + 255) & ~(size_t)255; }
 
+// Two CTAs per SM need the whole shared-memory carve-out of the SM's unified L1/shared storage.
+template <int NR>
+static void block_set_attributes() {
+  cudaFuncSetAttribute(bse_block_mixed_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)block_smem_bytes());
+  cudaFuncSetAttribute(bse_block_mixed_kernel<NR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
+}
+
 template <int NR>
 static int block_grid_nr(int n_items) {
   const size_t smem = block_smem_bytes();
-  cudaFuncSetAttribute(bse_block_mixed_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  block_set_attributes<NR>();
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bse_block_mixed_kernel<NR>, KT, smem);
   if (per_sm < 1) per_sm = 1;
   if (per_sm > 2) per_sm = 2;  // two CTAs hold 256 of the SM's 512 TMEM columns
   const int g = device_sm_count() * per_sm;
   return n_items < g ? n_items : g;
+}
+
+template <int NR>
+static int block_ctas_per_sm_nr() {
+  block_set_attributes<NR>();
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bse_block_mixed_kernel<NR>, KT, block_smem_bytes()) !=
+      cudaSuccess)
+    return -1;
+  return per_sm;
+}
+
+// Resident CTAs per SM of the block-form kernel for n2 right-hand sides (the occupancy the launch gets).
+extern "C" int dga_bse_block_ctas_per_sm(int n2) {
+  switch (n2) {
+    case 1: return block_ctas_per_sm_nr<1>();
+    case 4: return block_ctas_per_sm_nr<4>();
+    case 9: return block_ctas_per_sm_nr<9>();
+    case 16: return block_ctas_per_sm_nr<16>();
+    default: return -1;
+  }
 }
 
 int dga_block_grid(int n2, int n_items) {
@@ -764,7 +795,7 @@ cudaError_t dga_block_launch(int grid, const StructuredSource& src, const WorkIt
   const size_t smem = block_smem_bytes();
 #define DGA_BLOCK_CASE(R)                                                                                         \
   case R:                                                                                                         \
-    cudaFuncSetAttribute(bse_block_mixed_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+    block_set_attributes<R>();                                                                                    \
     bse_block_mixed_kernel<R><<<grid, KT, smem, stream>>>(src, work, n_items, N, nv, W, Q, beta, max_iter, tol,    \
                                                           out, status, iters, scratch, slot_bytes, wait_limit);   \
     break;

@@ -433,6 +433,58 @@ size_t dga_sigma_scratch_bytes(int n_orb, int niv, int nk, int n_chunks) {
   return (size_t)n_chunks * niv * n_orb * n_orb * nk * sizeof(double2) * 2;
 }
 
+}  // extern "C"
+
+// The real-space contraction of the Sigma computation: partial sums per bosonic chunk, then their sum times
+// -1/(2 beta Nk) into sig[nu >= 0][(i,j)][R] (planes contiguous in R).
+static int sigma_contract(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, Grid3 g,
+                          const int* irrk_inv, const void* tw_inv, double beta, int n_chunks, double2* part,
+                          double2* sig, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb;
+  const size_t smem = (2 * (size_t)g.nk + g.nx + g.ny + g.nz) * sizeof(double2) + sizeof(int) * (size_t)g.nk;
+  const long long work = (long long)niv * n2 * n_chunks;
+  auto partial = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<grid_cap(work), BZ_THREADS, smem, stream>>>((const double2*)kern, (const double2*)g_r, n_orb, niv, niw,
+                                                         n_q, g, irrk_inv, (const double2*)tw_inv, n_chunks, part);
+  };
+  static_assert(16 * BZ_THREADS >= BZ_MAX_NK, "the largest accumulator set covers the largest grid");
+  if (g.nk <= 4 * BZ_THREADS) partial(sigma_partial_kernel<4>);
+  else if (g.nk <= 8 * BZ_THREADS) partial(sigma_partial_kernel<8>);
+  else partial(sigma_partial_kernel<16>);
+  if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
+  const long long n_out = (long long)niv * n2 * g.nk;
+  const double factor = -0.5 / beta / (double)g.nk;
+  sigma_reduce_kernel<<<grid_cap((n_out + 255) / 256), 256, 0, stream>>>(part, n_chunks, n_out, factor, sig);
+  return launch_status("dga_sigma_c128");
+}
+
+extern "C" {
+
+// Real-space Sigma for nu >= 0, the result of calculate_sigma_from_kernel_fft_cpu/_gpu/_auto
+// (dgamore/nonlocal_sde.py:544-652) before the caller's ifft and to_full_niv_range: out [niv][n2][Nk] (planes
+// contiguous in R, R in row-major grid order).  Arguments and scratch as dga_sigma_c128.
+int dga_sigma_rspace_c128(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, int nx, int ny,
+                          int nz, const int* irrk_inv, const void* tw_inv, double beta, int n_chunks, void* out,
+                          void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (check_grid(nx, ny, nz, "dga_sigma_rspace_c128")) return DGA_ERR_ARG;
+  if (!kern || !g_r || !irrk_inv || !tw_inv || !out || !scratch || n_orb <= 0 || niv <= 0 || niw < 0 ||
+      n_chunks <= 0) {
+    dga_set_error("dga_sigma_rspace_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  Grid3 g{nx, ny, nz, nx * ny * nz};
+  const size_t need = dga_sigma_scratch_bytes(n_orb, niv, g.nk, n_chunks);
+  if (scratch_bytes < need) {
+    dga_set_error("dga_sigma_rspace_c128: scratch too small (%zu < %zu)", scratch_bytes, need);
+    return DGA_ERR_SCRATCH;
+  }
+  return sigma_contract(kern, g_r, n_orb, niv, niw, n_q, g, irrk_inv, tw_inv, beta, n_chunks, (double2*)scratch,
+                        (double2*)out, stream)
+             ? DGA_ERR_LAUNCH
+             : DGA_OK;
+}
+
 // Sigma(k, nu) from the irreducible kernel (nonlocal_sde.py:544-594 and 876-879).
 //   kern:   [Q][niw+1][2 niv][n2][n2] (row (a,i), column (d,j));  irrk_inv: [Nk]
 //   g_r:    [niv + 2 niw][n][n][Nk] forward transforms of G(k) for nu indices [-niw, niv + niw)
@@ -456,24 +508,11 @@ int dga_sigma_c128(const void* kern, const void* g_r, int n_orb, int niv, int ni
   }
   double2* part = (double2*)scratch;
   double2* sig = part + (size_t)n_chunks * niv * n2 * g.nk;
-  size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + sizeof(int) * (size_t)g.nk;
-  const long long work = (long long)niv * n2 * n_chunks;
-  auto partial = [&](auto kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kernel<<<grid_cap(work), BZ_THREADS, smem, stream>>>((const double2*)kern, (const double2*)g_r, n_orb, niv, niw,
-                                                         n_q, g, irrk_inv, (const double2*)tw_inv, n_chunks, part);
-  };
-  static_assert(16 * BZ_THREADS >= BZ_MAX_NK, "the largest accumulator set covers the largest grid");
-  if (g.nk <= 4 * BZ_THREADS) partial(sigma_partial_kernel<4>);
-  else if (g.nk <= 8 * BZ_THREADS) partial(sigma_partial_kernel<8>);
-  else partial(sigma_partial_kernel<16>);
-  if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
+  if (sigma_contract(kern, g_r, n_orb, niv, niw, n_q, g, irrk_inv, tw_inv, beta, n_chunks, part, sig, stream))
+    return DGA_ERR_LAUNCH;
   const long long n_out = (long long)niv * n2 * g.nk;
-  const double factor = -0.5 / beta / (double)g.nk;
-  sigma_reduce_kernel<<<grid_cap((n_out + 255) / 256), 256, 0, stream>>>(part, n_chunks, n_out, factor, sig);
-  if (launch_status("dga_sigma_c128")) return DGA_ERR_LAUNCH;
   // inverse transform over R (normalised 1/Nk), planes contiguous; result back into `part`
-  smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2);
+  size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2);
   cudaFuncSetAttribute(dft_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   PlaneAddr pa{(long long)g.nk, 0, 1, 1};
   dft_planes_kernel<<<grid_cap(niv * n2), BZ_THREADS, smem, stream>>>(sig, pa, part, pa, niv * n2, g,

@@ -117,8 +117,12 @@ __global__ void eli_apply_chi0pp_kernel(const double2* __restrict__ chi0pp, cons
 // over J and eight 16-byte loads of Mat(R) per lane in flight, so the Gamma(R) stream keeps enough bytes in
 // flight per SM to run at HBM bandwidth.
 //   gR: [Nk][n2][nvp] (forward transform of v), mat: [Nk][M][M]
+// MT = double2: Gamma(R) in complex128; MT = float2: Gamma(R) stored in complex64 (half the bytes of the stream),
+// widened on load, FP64 accumulation.  U loads of Mat(R) per lane and row in flight (16 bytes each for complex128,
+// 8 for complex64, so U doubles with the narrower storage to keep the same bytes in flight).
 constexpr int ELI_APPLY_THREADS = 256;
-__global__ void __launch_bounds__(ELI_APPLY_THREADS) eli_vertex_apply_kernel(const double2* __restrict__ mat,
+template <typename MT, int U>
+__global__ void __launch_bounds__(ELI_APPLY_THREADS) eli_vertex_apply_kernel(const MT* __restrict__ mat,
                                                                               const double2* __restrict__ gR, int nb,
                                                                               int nvp, int nk,
                                                                               double2* __restrict__ direct,
@@ -128,6 +132,7 @@ __global__ void __launch_bounds__(ELI_APPLY_THREADS) eli_vertex_apply_kernel(con
   double2* g = reinterpret_cast<double2*>(smem_raw);
   double2* gt = g + M;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const MT zero = {};
   for (int R = blockIdx.x; R < nk; R += gridDim.x) {
     __syncthreads();
     for (int J = threadIdx.x; J < M; J += blockDim.x) {
@@ -137,22 +142,22 @@ __global__ void __launch_bounds__(ELI_APPLY_THREADS) eli_vertex_apply_kernel(con
       gt[J] = gR[(size_t)R * M + (d * nb + c) * nvp + (nvp - 1 - nup)];
     }
     __syncthreads();
-    const double2* m = mat + (size_t)R * M * M;
+    const MT* m = mat + (size_t)R * M * M;
     for (int I0 = 2 * warp; I0 < M; I0 += 2 * nw) {
       const bool two = I0 + 1 < M;
-      const double2* row0 = m + (size_t)I0 * M;
-      const double2* row1 = row0 + M;
+      const MT* row0 = m + (size_t)I0 * M;
+      const MT* row1 = row0 + M;
       double2 a1 = make_double2(0.0, 0.0), a2 = a1, b1 = a1, b2 = a1;
-      for (int J0 = 0; J0 < M; J0 += 128) {
-        double2 x0[4], x1[4];
+      for (int J0 = 0; J0 < M; J0 += 32 * U) {
+        double2 x0[U], x1[U];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < U; ++u) {
           const int J = J0 + 32 * u + lane;
-          x0[u] = J < M ? row0[J] : make_double2(0.0, 0.0);
-          x1[u] = (two && J < M) ? row1[J] : make_double2(0.0, 0.0);
+          x0[u] = to_c64(J < M ? row0[J] : zero);
+          x1[u] = to_c64((two && J < M) ? row1[J] : zero);
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < U; ++u) {
           const int J = J0 + 32 * u + lane;
           if (J < M) {
             const double2 gj = g[J], gtj = gt[J];
@@ -262,16 +267,20 @@ int dga_dft_planes_c128(const void* in, long long in_s_hi, long long in_s_lo, lo
                         long long out_s_hi, long long out_s_lo, long long out_s_r, int n_lo, int n_planes, int nx,
                         int ny, int nz, const void* tw, double scale, cudaStream_t stream);
 
-int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, int n_orb, int niv_pp, int nx, int ny,
-                        int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign, void* gap_out,
-                        void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+}  // extern "C"
+
+// The gap-equation application with Gamma(R) stored as MT (complex128 or complex64); everything else FP64.
+template <typename MT, int U>
+static int eli_matvec(const char* who, const void* mat, const void* chi0pp, const void* gap, int n_orb, int niv_pp,
+                      int nx, int ny, int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign,
+                      void* gap_out, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
   const int n2 = n_orb * n_orb, nvp = 2 * niv_pp, M = n2 * nvp, nk = nx * ny * nz;
   if (!mat || !chi0pp || !gap || !gap_out || !scratch || !tw_fwd || !tw_inv || n_orb <= 0 || niv_pp <= 0 || nk <= 0) {
-    dga_set_error("dga_eli_matvec_c128: invalid arguments");
+    dga_set_error("%s: invalid arguments", who);
     return DGA_ERR_ARG;
   }
   if (scratch_bytes < dga_eli_matvec_scratch_bytes(n_orb, niv_pp, nk)) {
-    dga_set_error("dga_eli_matvec_c128: scratch too small");
+    dga_set_error("%s: scratch too small", who);
     return DGA_ERR_SCRATCH;
   }
   double2* s0 = (double2*)scratch;
@@ -280,20 +289,52 @@ int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, in
   double2* s3 = s2 + (size_t)nk * M;
   eli_apply_chi0pp_kernel<<<eli_blocks((long long)nk * M), 256, 0, stream>>>(
       (const double2*)chi0pp, (const double2*)gap, n2, nvp, nk, s0);
-  if (eli_status("dga_eli_matvec_c128")) return DGA_ERR_LAUNCH;
+  if (eli_status(who)) return DGA_ERR_LAUNCH;
   int rc = dga_dft_planes_c128(s0, 1, 0, M, s1, 1, 0, M, 1, M, nx, ny, nz, tw_fwd, 1.0, stream);
   if (rc) return rc;
   const size_t smem = 2 * (size_t)M * sizeof(double2);
-  cudaFuncSetAttribute(eli_vertex_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(eli_vertex_apply_kernel<MT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int apply_cap = 8 * device_sm_count();
-  eli_vertex_apply_kernel<<<nk < apply_cap ? nk : apply_cap, ELI_APPLY_THREADS, smem, stream>>>(
-      (const double2*)mat, s1, n_orb, nvp, nk, s2, s3);
-  if (eli_status("dga_eli_matvec_c128")) return DGA_ERR_LAUNCH;
+  eli_vertex_apply_kernel<MT, U><<<nk < apply_cap ? nk : apply_cap, ELI_APPLY_THREADS, smem, stream>>>(
+      (const MT*)mat, s1, n_orb, nvp, nk, s2, s3);
+  if (eli_status(who)) return DGA_ERR_LAUNCH;
   eli_combine_kernel<<<eli_blocks((long long)nk * M), 256, 0, stream>>>(s2, s3, M, nx, ny, nz, sign, s0);
-  if (eli_status("dga_eli_matvec_c128")) return DGA_ERR_LAUNCH;
+  if (eli_status(who)) return DGA_ERR_LAUNCH;
   // ifftn(norm * new) with norm = 0.5 / (Nk beta) (eliashberg_solver.py:418, 428)
   const double norm = 0.5 / (double)nk / beta;
   return dga_dft_planes_c128(s0, 1, 0, M, gap_out, 1, 0, M, 1, M, nx, ny, nz, tw_inv, norm / (double)nk, stream);
+}
+
+// complex128 -> complex64 narrowing (round to nearest) of n elements.
+__global__ void narrow_c64_kernel(const double2* __restrict__ src, float2* __restrict__ dst, long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    dst[e] = make_float2((float)src[e].x, (float)src[e].y);
+}
+
+extern "C" {
+
+int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, int n_orb, int niv_pp, int nx, int ny,
+                        int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign, void* gap_out,
+                        void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  return eli_matvec<double2, 4>("dga_eli_matvec_c128", mat, chi0pp, gap, n_orb, niv_pp, nx, ny, nz, tw_fwd, tw_inv,
+                                beta, sign, gap_out, scratch, scratch_bytes, stream);
+}
+
+int dga_eli_matvec_c64mat_c128(const void* mat_c64, const void* chi0pp, const void* gap, int n_orb, int niv_pp, int nx,
+                               int ny, int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign,
+                               void* gap_out, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  return eli_matvec<float2, 8>("dga_eli_matvec_c64mat_c128", mat_c64, chi0pp, gap, n_orb, niv_pp, nx, ny, nz, tw_fwd,
+                               tw_inv, beta, sign, gap_out, scratch, scratch_bytes, stream);
+}
+
+int dga_narrow_c128_to_c64(const void* src, void* dst, long long n, cudaStream_t stream) {
+  if (!src || !dst || n < 0) {
+    dga_set_error("dga_narrow_c128_to_c64: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  if (n == 0) return DGA_OK;
+  narrow_c64_kernel<<<eli_blocks(n), 256, 0, stream>>>((const double2*)src, (float2*)dst, n);
+  return eli_status("dga_narrow_c128_to_c64") ? DGA_ERR_LAUNCH : DGA_OK;
 }
 
 }  // extern "C"

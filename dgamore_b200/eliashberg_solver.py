@@ -63,7 +63,12 @@ def initial_gap(nk: tuple, n_bands: int, niv_pp: int, channel: str, symmetry: st
 class EliashbergSolver:
     """Pairing vertices and gap-equation operators of one request, resident on the device."""
 
-    def __init__(self, lp: LadderPass, niv_pp: int | None = None):
+    def __init__(self, lp: LadderPass, niv_pp: int | None = None, precision: str = "fp64"):
+        """precision 'fp64': Gamma(R) in complex128; 'mixed': Gamma(R) stored in complex64 (half the bytes the
+        operator streams), with FP64 products, sums, vectors and normalisation."""
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+        self.precision = precision
         if lp.gamma3 is None:
             raise ValueError("the Eliashberg stage needs the three-leg vertex: build LadderPass(keep_intermediates=True)")
         self.lp = lp
@@ -97,6 +102,10 @@ class EliashbergSolver:
         for st, sign in ((0, 1.0), (1, -1.0)):
             call("dga_dft_planes_gather_c128", _p(self.gamma_pp_irr[st]), 1, 0, M * M, _p(self.mat[st]), 1, 0, M * M,
                  1, M * M, nx, ny, nz, _p(lp.tw_fwd), sign, _p(lp.irrk_inv), _s())
+        if precision == "mixed":
+            mat64 = torch.empty((2, sh.nk_tot, M, M), dtype=torch.complex64, device=dev)
+            call("dga_narrow_c128_to_c64", _p(self.mat), _p(mat64), self.mat.numel(), _s())
+            self.mat = mat64
         self.chi0pp = torch.empty((sh.nk_tot, 2 * P, n2, n2), dtype=C128, device=dev)
         call("dga_eli_chi0pp_c128", _p(lp.g_k), n, sh.niv_g, P, sh.nk_tot, _p(self.chi0pp), _s())
         self.mv_scratch = torch.empty(int(lib().dga_eli_matvec_scratch_bytes(n, P, sh.nk_tot)) // 16 + 1, dtype=C128,
@@ -112,7 +121,8 @@ class EliashbergSolver:
         x = x.contiguous()
         out = torch.empty_like(x) if out is None else out
         nx, ny, nz = sh.nk
-        call("dga_eli_matvec_c128", _p(self.mat[st]), _p(self.chi0pp), _p(x), sh.n_orb, self.P, nx, ny, nz,
+        entry = "dga_eli_matvec_c64mat_c128" if self.precision == "mixed" else "dga_eli_matvec_c128"
+        call(entry, _p(self.mat[st]), _p(self.chi0pp), _p(x), sh.n_orb, self.P, nx, ny, nz,
              _p(self.lp.tw_fwd), _p(self.lp.tw_inv), sh.beta, sign, _p(out), _p(self.mv_scratch),
              self.mv_scratch.numel() * 16, _s())
         self.n_matvec += 1

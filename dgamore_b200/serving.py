@@ -52,9 +52,12 @@ PANEL_MIN_N = 320
 
 
 def launch_class(lp: LadderPass, precision: str) -> tuple:
-    """Requests of one class share a batch launch: orbital count, precision and, in the mixed form, the side of
-    PANEL_MIN_N their compound size is on."""
-    return (lp.sh.n_orb, precision, precision == "mixed" and lp.sh.N >= PANEL_MIN_N)
+    """Requests of one class share a batch launch.  The 128-thread kernels (the FP64 form, and the mixed form
+    below PANEL_MIN_N) choose the right-hand-side count per item, so their requests share one launch whatever
+    their orbital counts; the shared-memory-panel kernel of the mixed form (from PANEL_MIN_N up) is compiled per
+    orbital count, so there the class also holds n_orb."""
+    panel = precision == "mixed" and lp.sh.N >= PANEL_MIN_N
+    return (precision, panel, lp.sh.n_orb if panel else 0)
 
 
 def item_cost(sh: PassShapes) -> float:
@@ -113,6 +116,9 @@ class BseBatch:
         self.work = torch.cat(rows).index_select(0, order.to(dev)).contiguous()
         self.owner = torch.cat(owners).index_select(0, order)
         self.local = torch.cat(local).index_select(0, order.to(dev))
+        # per pass, the batch positions of its items (device index lists, so that launch() copies nothing from the
+        # host and can be captured in a CUDA graph)
+        self.sel = [(self.owner == p).nonzero().squeeze(1).to(dev) for p in range(len(passes))]
         self.n_items = int(self.work.shape[0])
         self.status = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
         self.iters = torch.zeros(self.n_items, dtype=torch.int32, device=dev)
@@ -133,9 +139,8 @@ class BseBatch:
                  _ptr(self.work), self.n_items, _RESOLVE, self.refine_max_iter, self.refine_tol, _ptr(self.status),
                  _ptr(self.iters), _ptr(scratch), nbytes, _stream())
         # scatter the status words back to the passes
-        owner_dev = self.owner.to(self.status.device)
         for p, lp in enumerate(self.passes):
-            sel = (owner_dev == p).nonzero().squeeze(1)
+            sel = self.sel[p]
             lp.bse_status.index_copy_(0, self.local.index_select(0, sel), self.status.index_select(0, sel))
             lp.bse_iters.index_copy_(0, self.local.index_select(0, sel), self.iters.index_select(0, sel))
 
@@ -155,6 +160,55 @@ def solve_bse_batch(passes: list[LadderPass], precision: str = "fp64", scratch: 
             need = max(batch.scratch_bytes(), batch.scratch_bytes(_RESOLVE) if precision == "mixed" else 0)
             sc = torch.empty(need // 16 + 1, dtype=torch.complex128, device=dev)
         batch.launch(sc)
+
+
+class BatchedPasses:
+    """Whole nonlocal passes of several requests as one device schedule: every pass's pre-BSE stages, one batch
+    launch per launch class over all their BSE items (requests of different orbital counts below N = 320 -- the
+    2-orbital bilayer next to a 1-orbital lattice, say -- share a single launch), every pass's post-BSE stages.
+    ``capture()`` records the whole schedule in one CUDA graph; ``replay()`` runs it again on refreshed inputs
+    (the passes' resident G(k) and vertices are read in place)."""
+
+    def __init__(self, passes: list[LadderPass], precision: str = "fp64", **kw):
+        if any(lp.own_bse_scratch for lp in passes):
+            raise ValueError("build the passes with own_bse_scratch=False: the batch launch brings the scratch")
+        self.passes = passes
+        self.precision = precision
+        groups: dict[tuple, list[LadderPass]] = {}
+        for lp in passes:
+            groups.setdefault(launch_class(lp, precision), []).append(lp)
+        dev = passes[0].dev
+        self.batches = [BseBatch([(lp, torch.arange(lp.n_items, device=dev)) for lp in g], precision, **kw)
+                        for g in groups.values()]
+        need = max(max(b.scratch_bytes(), b.scratch_bytes(_RESOLVE) if precision == "mixed" else 0)
+                   for b in self.batches)
+        self.scratch = torch.empty(need // 16 + 1, dtype=torch.complex128, device=dev)
+        self.graph = None
+
+    @property
+    def n_solves(self) -> int:
+        return sum(lp.sh.n_solves for lp in self.passes)
+
+    def run(self) -> None:
+        for lp in self.passes:
+            lp.pre_bse()
+        for b in self.batches:
+            b.launch(self.scratch)
+        for lp in self.passes:
+            lp.post_bse()
+
+    def capture(self) -> "torch.cuda.CUDAGraph":
+        self.run()  # module loading and kernel attributes outside the capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            self.run()
+        torch.cuda.synchronize()
+        self.graph = g
+        return g
+
+    def replay(self) -> None:
+        self.graph.replay()
 
 
 # ------------------------------------------------------------------------------------------------------------
@@ -270,7 +324,7 @@ class LadderServer:
             self.running.append(_Running(req, lp))
 
     def step(self) -> list[Request]:
-        """One iteration: admit, one batch launch per (orbital count, precision), finish completed requests.
+        """One iteration: admit, one batch launch per launch class (``launch_class``), finish completed requests.
         Synchronises the stream once at the end; returns the requests completed in this iteration."""
         self._admit()
         if not self.running:
@@ -281,7 +335,7 @@ class LadderServer:
             take = left if self.items_per_request is None else min(left, self.items_per_request)
             if take > 0:
                 groups.setdefault(launch_class(r.lp, r.req.precision), []).append((r, take))
-        for (_, precision, _), members in groups.items():
+        for (precision, _, _), members in groups.items():
             items = []
             for r, take in members:
                 items.append((r.lp, torch.arange(r.cursor, r.cursor + take, device=self.dev)))

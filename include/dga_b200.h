@@ -45,6 +45,10 @@ const char* dga_last_error_string(void);
  * and the caller's chunking of the Sigma contraction are multiples of it.  No counterpart in the upstream. */
 int dga_device_sm_count(void);
 
+/* Resident CTAs per SM of the block-form mixed BSE kernel (tuning kernel 4) for n2 = n_orb^2 right-hand sides,
+ * as the occupancy calculator gives it on the current device (-1 on error).  No counterpart in the upstream. */
+int dga_bse_block_ctas_per_sm(int n2);
+
 /* Generic strided complex copy dst[idx . dst_stride] = scale * src[idx . src_stride] over `shape`
  * (up to 8 dims, strides in complex elements).  Layout conversions at the boundary
  * (FourPoint.to_compound_indices / to_full_indices, dgamore/four_point.py:166-293). */
@@ -145,7 +149,9 @@ typedef struct {
 
 /* Ladder BSE of several requests in ONE persistent launch (the serving path's continuous batch; the upstream
  * runs one create_auxiliary_chi_r_q_sum call per request, dgamore/nonlocal_sde.py:85-156).  Requests may differ
- * in niv, niw, Q, beta and inputs but share n_orb (1..4).  probs_host: the descriptors on the host (launch
+ * in niv, niw, Q, beta, inputs and n_orb (1..4): the 128-thread kernels choose the right-hand-side count per item,
+ * so in the FP64 form, and in the mixed form when every request has N < 320, any orbital counts share a launch;
+ * mixed-form requests with N >= 320 (shared-memory-panel kernel) must share n_orb.  probs_host: the descriptors on the host (launch
  * geometry); probs_dev: the same array copied to device memory; work: [n_items][4] ints (request, ch, q, w);
  * mode 0 runs the FP64 LU of dga_bse_solve_sum_c128, mode 1 the FP32 LU + FP64 refinement of
  * dga_bse_solve_sum_mixed_c128 (max_iter, tol), mode 2 the FP64 re-solve of the items a mode-1 launch flagged;
@@ -224,6 +230,14 @@ int dga_sigma_c128(const void* kern, const void* g_r, int n_orb, int niv, int ni
                    const int* irrk_inv, const void* tw_inv, double beta, int n_chunks, void* out, void* scratch,
                    size_t scratch_bytes, dga_stream_t stream);
 
+/* The real-space half of dga_sigma_c128: Sigma(R, nu >= 0) = -1/(2 beta Nk) sum_w sum_ad G_ad(R, nu - w)
+ * K_aijd(-R, w, nu), the result of nonlocal_sde.calculate_sigma_from_kernel_fft_cpu/_gpu/_auto
+ * (dgamore/nonlocal_sde.py:544-652) before the caller's ifft().to_full_niv_range(); out: [niv][n2][Nk] (planes
+ * contiguous in R).  Arguments and scratch as dga_sigma_c128. */
+int dga_sigma_rspace_c128(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, int nx, int ny,
+                          int nz, const int* irrk_inv, const void* tw_inv, double beta, int n_chunks, void* out,
+                          void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
 /* dga_dft_planes_c128 with the input point of output R read from gather[R]: the IBZ -> FBZ expansion
  * (IAmNonLocal._map_to_full_bz, dgamore/n_point_base.py:489-494) folded into the transform's load. */
 int dga_dft_planes_gather_c128(const void* in, long long in_s_hi, long long in_s_lo, long long in_s_r, void* out,
@@ -260,6 +274,17 @@ size_t dga_eli_matvec_scratch_bytes(int n_orb, int niv_pp, int nk);
 int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, int n_orb, int niv_pp, int nx, int ny,
                         int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign, void* gap_out,
                         void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
+/* dga_eli_matvec_c128 with Gamma(R) stored in complex64 (mat_c64 [Nk][M][M], made by dga_narrow_c128_to_c64):
+ * half the bytes of the operator's dominant stream, every product and sum in FP64 and the vectors complex128,
+ * so the Krylov normalisation and Rayleigh quotients stay FP64 (the power-iteration form of
+ * solve_eliashberg_lanczos, dgamore/eliashberg_solver.py:420-428, with its operator in complex64 storage). */
+int dga_eli_matvec_c64mat_c128(const void* mat_c64, const void* chi0pp, const void* gap, int n_orb, int niv_pp,
+                               int nx, int ny, int nz, const void* tw_fwd, const void* tw_inv, double beta,
+                               double sign, void* gap_out, void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
+/* dst[e] = complex64(src[e]) for e < n (round to nearest); no counterpart in the upstream. */
+int dga_narrow_c128_to_c64(const void* src, void* dst, long long n, dga_stream_t stream);
 
 #ifdef __cplusplus
 }

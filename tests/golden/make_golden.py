@@ -81,7 +81,9 @@ def _setup_config(cfg: synthetic.DgaConfig, inp: dict):
     config.lambda_correction.perform_lambda_correction = False
 
 
-def run_reference_pass(name: str) -> dict:
+def run_reference_pass(name: str, variants: bool = True) -> dict:
+    """The upstream pass in FP64; with ``variants`` also its alternative forms (direct-q bubble, v3 BSE, direct
+    Sigma), which the at-size fixtures skip because they cost far more than the pass at 64x64."""
     cfg = synthetic.CONFIGS[name]
     inp = synthetic.make_inputs(cfg)
     _setup_config(cfg, inp)
@@ -103,8 +105,10 @@ def run_reference_pass(name: str) -> dict:
     gchi0_q = BubbleGenerator.create_generalized_chi0_q_fft_cpu(dist, giwk, cfg.niw, cfg.niv_full, grid, beta)
     out["chi0"] = gchi0_q.mat.copy()
     # direct-q bubble variant (bubble_gen.py:147-183)
-    gchi0_direct = BubbleGenerator.create_generalized_chi0_q_cpu(giwk, cfg.niw, cfg.niv_full, irr_q_list, grid, beta)
-    out["chi0_direct"] = gchi0_direct.mat.copy()
+    if variants:
+        gchi0_direct = BubbleGenerator.create_generalized_chi0_q_cpu(giwk, cfg.niw, cfg.niv_full, irr_q_list, grid,
+                                                                     beta)
+        out["chi0_direct"] = gchi0_direct.mat.copy()
 
     # double-counting kernel (nonlocal_sde.py:817-820)
     f_dc_loc = 2 * LocalFourPoint(inp["f_magn_loc"], SpinChannel.NONE, 1, 2, False, True).permute_orbitals("abcd->cbad")
@@ -124,9 +128,10 @@ def run_reference_pass(name: str) -> dict:
         keep[ch] = {"gamma": gamma_r}
         # calculate_sigma_kernel_r_q (nonlocal_sde.py:257-336), both BSE variants
         aux = nonlocal_sde.create_auxiliary_chi_r_q_sum_v1(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc)
-        aux3 = nonlocal_sde.create_auxiliary_chi_r_q_sum_v3(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc, dist)
         out[f"chi_aux_sum_{ch}"] = aux.mat.copy()
-        out[f"chi_aux_sum_v3_{ch}"] = aux3.mat.copy()
+        if variants:
+            aux3 = nonlocal_sde.create_auxiliary_chi_r_q_sum_v3(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc, dist)
+            out[f"chi_aux_sum_v3_{ch}"] = aux3.mat.copy()
         vrg_q = nonlocal_sde.create_vrg_r_q(aux, gchi0_q_core_inv)
         out[f"vrg_{ch}"] = vrg_q.mat.copy()
         chi_phys = aux.sum_over_all_vn(beta)
@@ -152,8 +157,9 @@ def run_reference_pass(name: str) -> dict:
     sigma = sigma_r.ifft().to_full_niv_range()
     out["sigma"] = sigma.compress_q_dimension().mat.copy()
     # direct Sigma variant (nonlocal_sde.py:430-469) on the full q list
-    sig_direct = nonlocal_sde.calculate_sigma_from_kernel_cpu(deepcopy(kernel_full), giwk, grid.get_q_list())
-    out["sigma_direct"] = sig_direct.compress_q_dimension().mat.copy()
+    if variants:
+        sig_direct = nonlocal_sde.calculate_sigma_from_kernel_cpu(deepcopy(kernel_full), giwk, grid.get_q_list())
+        out["sigma_direct"] = sig_direct.compress_q_dimension().mat.copy()
 
     if name in ELIASHBERG_CONFIGS:
         out.update(run_reference_eliashberg(cfg, inp, giwk, u_loc, v_nonloc, gchi0_q_core_inv, keep, grid))
@@ -258,7 +264,44 @@ def hf_fixtures() -> dict:
     return out
 
 
+AT_SIZE_Q = {"c1": 45, "c2": 4}  # irreducible q whose X is stored (c1: all of them)
+
+
+def input_digest(inp: dict) -> dict:
+    """Sums of the seeded inputs, stored beside the at-size outputs so a test can see that it regenerated the
+    same inputs (synthetic.make_inputs is deterministic; machines differ at most in the last bits)."""
+    return {f"digest_{k}": np.sum(np.asarray(inp[k], dtype=np.complex128))
+            for k in ("g_k", "gamma_dens", "gamma_magn", "f_dc", "u", "v_q_irr")}
+
+
+def run_reference_at_size(name: str) -> dict:
+    """The upstream pass at a benchmark configuration's own size (c1: 1 orbital 16x16, niv = niw = 20 with the
+    spch lambda-correction; c2: 64x64, niv = niw = 60), in FP64.  Stored: Sigma on the irreducible k points,
+    lambda_d and lambda_m, X = sum_nu' chi* for the first AT_SIZE_Q[name] irreducible q, and the input digest;
+    the inputs themselves are regenerated from their seed by the tests."""
+    full = run_reference_pass(name, variants=False)
+    ref = {k[4:]: v for k, v in full.items() if k.startswith("ref_")}
+    inp = synthetic.make_inputs(synthetic.CONFIGS[name])
+    nq = AT_SIZE_Q[name]
+    out = {
+        "sigma_irr": ref["sigma"][inp["irrk_ind"]],
+        "lambda_dens": ref["lambda_dens"],
+        "lambda_magn": ref["lambda_magn"],
+        "chi_aux_sum_dens_q": ref["chi_aux_sum_dens"][:nq],
+        "chi_aux_sum_magn_q": ref["chi_aux_sum_magn"][:nq],
+        "chi_phys_magn": ref["chi_phys_magn"],
+        "n_q_stored": np.int64(nq),
+    }
+    out.update(input_digest(inp))
+    return {f"ref_{k}": v for k, v in out.items()}
+
+
 def main():
+    if "--at-size" in sys.argv:
+        for name in sys.argv[sys.argv.index("--at-size") + 1:]:
+            np.savez_compressed(os.path.join(HERE, f"{name}_size.npz"), **run_reference_at_size(name))
+            print("wrote", f"{name}_size.npz")
+        return
     if "--only-hf" in sys.argv:
         np.savez_compressed(os.path.join(HERE, "hartree_fock.npz"), **hf_fixtures())
         print("wrote hartree_fock.npz")

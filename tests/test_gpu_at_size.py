@@ -1,0 +1,74 @@
+"""GPU parity at the benchmark configurations' own sizes against the upstream run in FP64.
+
+* c1: 1 orbital, 16x16, niv = niw = 20, with the spch lambda-correction (the CPU-runnable configuration);
+* c2: 1 orbital, 64x64 reduced to its 561 irreducible q, niv = niw = 60 (the FP64 drop-in at scale).
+
+tests/golden/make_golden.py (``--at-size c1 c2``) ran the upstream pass on the seeded inputs and stored Sigma on
+the irreducible k points, lambda_d and lambda_m, X = sum_nu' chi* for some irreducible q, and a digest of the
+inputs; the test regenerates the inputs from the same seed, checks the digest, and runs the device pass.
+Bounds: the FP64 drop-in form to 1e-10 relative (lambda to 1e-10 absolute); the mixed form Sigma to 1e-8 relative
+and lambda_d, lambda_m to 1e-6 absolute, the bounds the benchmark states for it.
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _golden(name):
+    path = os.path.join(GOLDEN, f"{name}_size.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"{name}_size.npz has not been generated")
+    return {k[4:]: v for k, v in np.load(path).items()}
+
+
+@pytest.fixture(scope="module", params=["c1", "c2"])
+def case(request):
+    from dgamore_b200 import synthetic
+
+    ref = _golden(request.param)
+    inp = synthetic.make_inputs(request.param)
+    for key in ("g_k", "gamma_dens", "gamma_magn", "f_dc", "u", "v_q_irr"):
+        got = np.sum(np.asarray(inp[key], dtype=np.complex128))
+        assert abs(got - ref[f"digest_{key}"]) <= 1e-12 * max(1.0, abs(ref[f"digest_{key}"])), key
+    return request.param, inp, ref
+
+
+def _pass(inp, precision):
+    from dgamore_b200.pipeline import LadderPass
+
+    lp = LadderPass(inp, keep_intermediates=False, precision=precision)
+    lp.run()
+    torch.cuda.synchronize()
+    assert int(lp.bse_status.abs().sum()) == 0 and int(lp.status.abs().sum()) == 0
+    return lp
+
+
+def test_fp64_pass_at_size(case):
+    name, inp, ref = case
+    lp = _pass(inp, "fp64")
+    sigma = lp.sigma.cpu().numpy()[inp["irrk_ind"]]
+    assert rel_err(sigma, ref["sigma_irr"]) < 1e-10
+    lam = lp.lambdas.cpu().numpy()
+    assert abs(lam[0] - float(ref["lambda_dens"])) < 1e-10 * max(1.0, abs(float(ref["lambda_dens"])))
+    assert abs(lam[1] - float(ref["lambda_magn"])) < 1e-10 * max(1.0, abs(float(ref["lambda_magn"])))
+    nq = int(ref["n_q_stored"])
+    for ch, chname in ((0, "dens"), (1, "magn")):
+        assert rel_err(lp.x_ref_layout(ch)[:nq], ref[f"chi_aux_sum_{chname}_q"]) < 1e-10, chname
+    assert rel_err(lp.chi_phys_ref_layout(lp.chi_lam, 1), ref["chi_phys_magn"]) < 1e-10
+
+
+def test_mixed_pass_at_size(case):
+    name, inp, ref = case
+    lp = _pass(inp, "mixed")
+    sigma = lp.sigma.cpu().numpy()[inp["irrk_ind"]]
+    assert rel_err(sigma, ref["sigma_irr"]) < 1e-8
+    lam = lp.lambdas.cpu().numpy()
+    assert abs(lam[0] - float(ref["lambda_dens"])) < 1e-6
+    assert abs(lam[1] - float(ref["lambda_magn"])) < 1e-6

@@ -56,15 +56,19 @@ def test_batch_descriptor_matches_the_c_struct():
     assert _lib.BseProblem.beta.offset == 48 and _lib.BseProblem.n_q.offset == 44
 
 
-def test_batch_rejects_mixed_orbital_counts_without_launching():
+def test_batch_rejects_unsupported_mixes_without_launching():
     lib = _lib.lib()
+    # orbital counts may differ where the 128-thread kernels run; the mixed form's panel kernel (N >= 320) is
+    # compiled per orbital count, so a mixed-precision batch of 2- and 3-orbital problems of that size is refused
     arr = (_lib.BseProblem * 2)(
-        _lib.BseProblem(n_orb=1, niv=4, niw_half=3, n_q=2, beta=1.0),
-        _lib.BseProblem(n_orb=2, niv=4, niw_half=3, n_q=2, beta=1.0),
+        _lib.BseProblem(n_orb=2, niv=40, niw_half=3, n_q=2, beta=1.0),
+        _lib.BseProblem(n_orb=3, niv=20, niw_half=3, n_q=2, beta=1.0),
     )
-    assert lib.dga_bse_batch_scratch_bytes(arr, 2, 10, 0) == 0
-    rc = lib.dga_bse_solve_sum_batch_c128(arr, None, 2, None, 10, 0, 0, 0.0, None, None, None, 0, None)
+    assert lib.dga_bse_batch_scratch_bytes(arr, 2, 10, 1) == 0
+    rc = lib.dga_bse_solve_sum_batch_c128(arr, None, 2, None, 10, 1, 0, 0.0, None, None, None, 0, None)
     assert rc == 1 and b"n_orb" in lib.dga_last_error_string()
+    five = (_lib.BseProblem * 1)(_lib.BseProblem(n_orb=5, niv=4, niw_half=3, n_q=2, beta=1.0))
+    assert lib.dga_bse_batch_scratch_bytes(five, 1, 10, 0) == 0
     one = (_lib.BseProblem * 1)(_lib.BseProblem(n_orb=1, niv=4, niw_half=3, n_q=2, beta=1.0))
     # null input pointers are caught before any CUDA call; an unknown mode too
     rc = lib.dga_bse_solve_sum_batch_c128(one, 1, 1, 1, 10, 0, 0, 0.0, 1, None, 1, 1 << 30, None)
