@@ -299,17 +299,21 @@ DRAM_BYTES_PER_ITEM = {
     "bse_panel_mixed_kernel": (5.670e9 + 4.917e9) / 132,
     "bse_panel_mixed_kernel<TC> (tcgen05 trailing tiles)": (6.093e9 + 4.978e9) / 132,
     "bse_solve_sum_mixed_kernel": 11.79e9 / 132,
+    # same 132-item case, one item per CTA: ncu dram__bytes_read.sum + dram__bytes_write.sum
+    "bse_block_mixed_kernel (tcgen05, pivoting inside 32x32 blocks)": (7.053e9 + 4.934e9) / 132,
 }
 
 
 def kernel_name(lp) -> str:
     if lp.precision == "fp64":
         return "bse_solve_sum_fp64_kernel"
-    kernel = lp.tuning.kernel if lp.tuning is not None else (3 if lp.sh.N >= 320 else 2)
+    kernel = lp.tuning.kernel if lp.tuning is not None else (4 if lp.sh.N >= 320 else 2)
     if kernel == 2:
         return "bse_solve_sum_mixed_kernel"
     if kernel == 3:
         return "bse_panel_mixed_kernel<TC> (tcgen05 trailing tiles)"
+    if kernel == 4:
+        return "bse_block_mixed_kernel (tcgen05, pivoting inside 32x32 blocks)"
     return "bse_panel_mixed_kernel"
 
 
@@ -333,6 +337,56 @@ def serving_leg(precision: str, n_requests: int) -> dict:
     stats = srv.serve(reqs, realtime=True)
     out = stats.summary()
     out["bse_status_nonzero"] = int(sum(int(np.abs(r.bse_status).sum()) for r in stats.completed))
+    return out
+
+
+def c4_batch_leg(precision: str, steps: int = 3) -> dict:
+    """The 2-orbital bilayer (48x48, niv = niw = 30, N = 240) and the 1-orbital lattice (32x32, niv = niw = 50,
+    N = 100) as one device schedule: both passes' stages and ONE persistent BSE launch over the items of both,
+    replayed from one captured CUDA graph; each request's X is compared bitwise with its single-request pass."""
+    import torch
+
+    from dgamore_b200 import synthetic
+    from dgamore_b200.pipeline import LadderPass
+    from dgamore_b200.serving import BatchedPasses
+
+    inps = [synthetic.make_inputs("c4_bilayer"), synthetic.make_inputs("c4_single")]
+    alone = []
+    for inp in inps:
+        lp = LadderPass(inp, precision=precision, keep_intermediates=False)
+        lp.run()
+        torch.cuda.synchronize()
+        alone.append(lp.X.cpu())
+        del lp
+    torch.cuda.empty_cache()
+    passes = [LadderPass(inp, precision=precision, keep_intermediates=False, own_bse_scratch=False) for inp in inps]
+    bp = BatchedPasses(passes, precision)
+    bp.capture()
+    for _ in range(2):
+        bp.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        bp.replay()
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    bitwise = all(torch.equal(lp.X.cpu(), x) for lp, x in zip(passes, alone))
+    status = sum(int(lp.bse_status.abs().sum()) for lp in passes)
+    out = {
+        "workload": "2-orbital bilayer 48x48 niv=niw=30 (N=240) + 1-orbital 32x32 niv=niw=50 (N=100), one graph",
+        "precision": precision,
+        "bse_launches_per_step": len(bp.batches),
+        "solves_per_step": bp.n_solves,
+        "ms_per_step": ms,
+        "solves_per_s": bp.n_solves / (ms / 1e3),
+        "x_bitwise_equal_to_single_requests": bool(bitwise),
+        "bse_status_nonzero": status,
+    }
+    bp.graph = None
+    del bp, passes
+    torch.cuda.empty_cache()
     return out
 
 
@@ -373,6 +427,19 @@ def eliashberg_leg(config: str = "c4_bilayer") -> dict:
     ls, lt, _, _ = es.solve(n_eig=4, tol=1e-6)
     b.record()
     b.synchronize()
+    solve_ms = a.elapsed_time(b)
+    # the operator with Gamma(R) stored in complex64 (FP64 products, vectors and normalisation)
+    es32 = EliashbergSolver(lp, precision="mixed")
+    for _ in range(3):
+        es32.matvec("sing", x, out)
+    a.record()
+    for _ in range(reps):
+        es32.matvec("sing", x, out)
+    b.record()
+    b.synchronize()
+    mv32_ms = a.elapsed_time(b) / reps
+    ls32, lt32, _, _ = es32.solve(n_eig=4, tol=1e-9)
+    del es32
     hbm = measured_peaks().get("hbm_gbs")
     gbs = bytes_mv / (mv_ms / 1e3) / 1e9
     return {
@@ -381,10 +448,17 @@ def eliashberg_leg(config: str = "c4_bilayer") -> dict:
         "matvec_ms": mv_ms,
         "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
                      "frac": gbs / hbm if hbm else None, "bytes_per_matvec": bytes_mv},
-        "solve_ms": a.elapsed_time(b),
+        "solve_ms": solve_ms,
         "matvecs_in_solve": es.n_matvec,
         "lambda_sing": [float(v) for v in ls],
         "lambda_trip": [float(v) for v in lt],
+        "complex64_operator": {
+            "matvec_ms": mv32_ms,
+            "speedup_vs_fp64_matvec": mv_ms / mv32_ms,
+            "lambda_max_sing": float(ls32[0]),
+            "lambda_max_trip": float(lt32[0]),
+            "lambda_max_abs_err_vs_fp64": max(abs(float(ls32[0]) - float(ls[0])), abs(float(lt32[0]) - float(lt[0]))),
+        },
         "status": {k: int(v) for k, v in es.status.items()},
     }
 
@@ -457,6 +531,10 @@ def run_ours(args, rank: int, world: int, local: int):
         for prec in ("fp64", "mixed"):
             serving[prec] = serving_leg(prec, args.serve_requests)
     eliashberg = eliashberg_leg() if (args.eliashberg and rank == 0) else None
+    c4 = {}
+    if args.c4 and rank == 0:
+        for prec in ("fp64", "mixed"):
+            c4[prec] = c4_batch_leg(prec)
     line = {
         "metric": "(q,w) ladder solves/s",
         "value": value,
@@ -524,6 +602,7 @@ def run_ours(args, rank: int, world: int, local: int):
         "clocks": clocks.summary(),
         "serving": serving,
         "eliashberg": eliashberg,
+        "c4_batch": c4,
     }
     if rank == 0:
         line["cpu_baseline"] = cpu_baseline_sample(inp, args.cpu_items)
@@ -543,6 +622,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving leg (0: skip)")
     ap.add_argument("--tune-cache", action="store_true", help="keep autotuner choices in _build/tuning.json")
     ap.add_argument("--eliashberg", type=int, default=1, help="run the Eliashberg leg (0: skip)")
+    ap.add_argument("--c4", type=int, default=1, help="run the uneven-orbital batch leg under one graph (0: skip)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     try:

@@ -1096,9 +1096,18 @@ static size_t mixed_slot_bytes(int N, int n2) {
 // else the panel kernel with FP32 tiles (1), else the 128-thread kernel (2).
 static int default_mixed_kernel(int N, int n2) {
   if (N < 320) return 2;
+  if (dga_block_supported(N, n2)) return 4;
   if (dga_panel_supported(N, n2, true)) return 3;
   if (dga_panel_supported(N, n2)) return 1;
   return 2;
+}
+
+// Grid and scratch slot of the mixed kernels that own their launch geometry (1, 3: panel; 4: block form).
+static int owned_grid(int kernel, int n2, int N, int n_items) {
+  return kernel == 4 ? dga_block_grid(n2, n_items) : dga_panel_grid(n2, N, n_items, kernel == 3);
+}
+static size_t owned_slot(int kernel, int N, int n2) {
+  return kernel == 4 ? dga_block_slot_bytes(N, n2) : dga_panel_slot_bytes(N, n2);
 }
 
 static int mixed_grid(int n_items, size_t smem) {
@@ -1116,7 +1125,7 @@ extern "C" {
 size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items) {
   if (N <= 0 || n2 <= 0 || n_items <= 0) return 0;
   const int kernel = default_mixed_kernel(N, n2);
-  if (kernel != 2) return (size_t)dga_panel_grid(n2, N, n_items, kernel == 3) * dga_panel_slot_bytes(N, n2);
+  if (kernel != 2) return (size_t)owned_grid(kernel, n2, N, n_items) * owned_slot(kernel, N, n2);
   const size_t smem = mixed_smem_bytes(N, n2);
   return (size_t)mixed_grid(n_items, smem) * mixed_slot_bytes(N, n2);
 }
@@ -1141,8 +1150,8 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
   const int kernel = default_mixed_kernel(N, n2);
   const bool panel = kernel != 2;
   const size_t smem = mixed_smem_bytes(N, n2);
-  const int grid = panel ? dga_panel_grid(n2, N, n_items, kernel == 3) : mixed_grid(n_items, smem);
-  const size_t slot = panel ? dga_panel_slot_bytes(N, n2) : mixed_slot_bytes(N, n2);
+  const int grid = panel ? owned_grid(kernel, n2, N, n_items) : mixed_grid(n_items, smem);
+  const size_t slot = panel ? owned_slot(kernel, N, n2) : mixed_slot_bytes(N, n2);
   if (scratch_bytes < (size_t)grid * slot) {
     dga_set_error("dga_bse_solve_sum_mixed_c128: scratch too small (%zu < %zu)", scratch_bytes, (size_t)grid * slot);
     return DGA_ERR_SCRATCH;
@@ -1157,8 +1166,13 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
   src.Q = n_q;
   src.inv_beta2 = inv_beta2;
   if (panel) {
-    // N fits the shared-memory panel: one 512-thread CTA per SM (bse_panel.cu)
-    cudaError_t err = dga_panel_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta,
+    // from N = 320: the block-form kernel (bse_block.cu, two 256-thread CTAs per SM), or where it does not fit the
+    // shared-memory panel (bse_panel.cu, one 512-thread CTA per SM)
+    cudaError_t err =
+        kernel == 4 ? dga_block_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta,
+                                       max_iter, tol, (double2*)out, status, iters, (unsigned char*)scratch, slot,
+                                       stream)
+                    : dga_panel_launch(grid, src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta,
                                        max_iter, tol, (double2*)out, status, iters, (unsigned char*)scratch, slot,
                                        stream, kernel == 3);
     if (err != cudaSuccess) {
@@ -1301,7 +1315,7 @@ static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int*
   for (int p = 0; p < n_prob; ++p) {
     const int n2 = probs[p].n_orb * probs[p].n_orb;
     const int N = n2 * 2 * probs[p].niv;
-    const size_t sl = panel ? dga_panel_slot_bytes(N, n2)
+    const size_t sl = panel ? owned_slot(*kernel, N, n2)
                       : mixed ? mixed_slot_bytes(N, n2)
                               : ((size_t)N * N + (size_t)N * n2) * sizeof(double2);
     if (sl > *slot) *slot = sl;
@@ -1350,7 +1364,9 @@ size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int
     return 0;
   const int n2 = probs[0].n_orb * probs[0].n_orb;
   const bool panel = kernel != 2;
-  if (panel) return (size_t)dga_panel_batch_grid(n2, n_max, n_items, kernel == 3) * slot;
+  if (panel)
+    return (size_t)(kernel == 4 ? dga_block_grid(n2, n_items) : dga_panel_batch_grid(n2, n_max, n_items, kernel == 3)) *
+           slot;
   if (hetero) return (size_t)batch_grid_hetero(mixed, n_items, batch_smem(n_max, n2_max, mixed)) * slot;
   return (size_t)batch_grid_any(mixed, n2, n_items, batch_smem(n_max, n2, mixed)) * slot;
 }
@@ -1385,7 +1401,7 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   const int n2 = probs_host[0].n_orb * probs_host[0].n_orb;
   const size_t smem = batch_smem(n_max, hetero ? n2_max : n2, mixed);
   const bool panel = kernel != 2;
-  int grid = panel    ? dga_panel_batch_grid(n2, n_max, n_items, kernel == 3)
+  int grid = panel    ? (kernel == 4 ? dga_block_grid(n2, n_items) : dga_panel_batch_grid(n2, n_max, n_items, kernel == 3))
              : hetero ? batch_grid_hetero(mixed, n_items, smem)
                       : batch_grid_any(mixed, n2, n_items, smem);
   if (scratch_bytes < slot) {
@@ -1398,7 +1414,10 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   const MultiItem* wk = (const MultiItem*)work;
   unsigned char* sc = (unsigned char*)scratch;
   if (panel) {
-    cudaError_t err = dga_panel_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
+    cudaError_t err =
+        kernel == 4 ? dga_block_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
+                                             stream)
+                    : dga_panel_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
                                              stream, kernel == 3);
     if (err != cudaSuccess) {
       dga_set_error("dga_bse_solve_sum_batch_c128: launch failed: %s", cudaGetErrorString(err));

@@ -47,6 +47,7 @@ constexpr int K_REGION = 4 * KAP * 4 + 2 * 4 * KBP * 4;  // A planes (64 KB) + t
 constexpr int K_DLD = 33;                                 // leading dimension of the diagonal inverse in smem
 constexpr uint32_t K_SBO = 1024;                          // 8 rows x 32 floats: stride byte offset of a plane
 constexpr uint32_t K_TMEM_COLS = 128;                     // two tiles in flight x (Re, Im) x 32 columns
+constexpr uint32_t K_A2_COL = 128;                        // TMEM A operand planes of a step pair (4 x 32 columns)
 
 // kind::tf32, D fp32, A and B tf32 K-major, M = 128, N = 32; bit 13 negates A.
 constexpr uint32_t K_IDESC_POS = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(KTN >> 3) << 17) |
@@ -376,15 +377,94 @@ __device__ __forceinline__ void prefetch_tile_l2(const float2* A, int N, int NC,
   bulk_prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(e - a));
 }
 
+// L' = A[r0 : r0 + 128, kc : kc + 32] D^-1 on the tensor cores (D^-1 row-major in global memory, dinv), into TMEM
+// buffer 0, then split back either into the shared-memory A planes (to_tmem false) or into the tensor-memory A
+// planes at column a2 of the CTA's allocation (to_tmem true: Re hi, Re lo, Im hi, Im lo at a2 + 0, 32, 64, 96).
+// Uses the A planes and B buffer 1 of shared memory; every thread takes part; ends with a barrier.
+__device__ void block_l21(const float2* __restrict__ A, int N, int r0, int kc, const float2* __restrict__ dinv,
+                          BlockSmem& s, TileCount& tc, bool to_tmem) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tbase = *s.tslot;
+  const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
+  const int hh = warp >> 2;
+  const int row_t = 32 * (warp & 3) + lane;
+  {  // A planes: rows r0 .. r0 + 127 of the block column (16 k per thread, loads coalesced along the rows)
+    const int rl = tid & (KTM - 1), h = tid >> 7, r = r0 + rl;
+    const bool rok = r < N;
+    float2 v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) v[u] = rok ? __ldcg(A + (size_t)(kc + 16 * h + u) * N + r) : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int g = 0; g < 4; ++g) store_planes(s.a_pl, KAP, rl, 16 * h + 4 * g, v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
+  }
+  // B planes of D^-1: element (i, k) = D^-1[k][i], so that the product below is A21 D^-1
+  for (int e = tid; e < KB * (KB / 4); e += KT) {
+    const int i = e >> 3, k = (e & 7) * 4;
+    store_planes(s.b_pl + 4 * KBP, KBP, i, k, __ldcg(dinv + k * KB + i), __ldcg(dinv + (k + 1) * KB + i),
+                 __ldcg(dinv + (k + 2) * KB + i), __ldcg(dinv + (k + 3) * KB + i));
+  }
+  tc_fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  const bool live = s.misc[0] == 0;
+  if (live && tid == 0) {
+    tc_fence_after();
+    issue_planar(tbase, tbase + 32, s.a_pl, s.b_pl + 4 * KBP, false, true);
+    tc_commit(s.bar);
+  }
+  if (live) tc.iss[0] += 1;
+  const bool ok = live && tile_wait(s, tc, 0);
+  tc_fence_after();
+  if (ok) {
+    float re[16], im[16];
+    tmem_ld16(tl + 16 * hh, re);
+    tmem_ld16(tl + 32 + 16 * hh, im);
+    tmem_wait_ld();
+    if (to_tmem) {
+      float rh[16], rlo[16], ih[16], il[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        rh[j] = tf32_hi(re[j]);
+        rlo[j] = re[j] - rh[j];
+        ih[j] = tf32_hi(im[j]);
+        il[j] = im[j] - ih[j];
+      }
+      const uint32_t a2 = tl + K_A2_COL + 16 * hh;
+      tmem_st16(a2, rh);
+      tmem_st16(a2 + 32, rlo);
+      tmem_st16(a2 + 64, ih);
+      tmem_st16(a2 + 96, il);
+      tmem_wait_st();
+    } else {
+#pragma unroll
+      for (int g = 0; g < 4; ++g)
+        store_planes(s.a_pl, KAP, row_t, 16 * hh + 4 * g, make_float2(re[4 * g], im[4 * g]),
+                     make_float2(re[4 * g + 1], im[4 * g + 1]), make_float2(re[4 * g + 2], im[4 * g + 2]),
+                     make_float2(re[4 * g + 3], im[4 * g + 3]));
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+}
+
+// The K = 32 trailing pass of step k (block column k0, first trailing row and column k1).  With k2 = 0 it is the
+// whole trailing update rows [k1, N) x columns [k1, NC).  With k2 = k1 + 32 it is the first half of a pair of
+// steps: only block column k + 1 (columns [k1, k2), every row from k1) and block row k + 1 (rows [k1, k2), every
+// column) take step k's product here; the rest of the trailing matrix takes steps k and k + 1 together in
+// block_trailing_pair.
 __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, int k1, BlockSmem& s,
-                               const float* __restrict__ bop, TileCount& tc) {
+                               const float* __restrict__ bop, const float2* __restrict__ dinv, TileCount& tc,
+                               int k2 = 0) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (k1 >= N) return;
-  const int nrb = (N - k1 + KTM - 1) / KTM, nst = (NC - k1 + KTN - 1) / KTN;
+  const int nrb = (N - k1 + KTM - 1) / KTM, nst_all = (NC - k1 + KTN - 1) / KTN;
   const uint32_t tbase = *s.tslot;
   const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
   const int hh = warp >> 2;
   const int row_t = 32 * (warp & 3) + lane;  // this thread's tile row (its TMEM lane)
+  // rows of strip st that take this pass's product: all from k1, or for a pair's panel pass beyond strip 0 only
+  // the rows of block row k + 1
+  auto row_end = [&](int st) { return (k2 > 0 && st > 0) ? k2 : N; };
   auto finish = [&](int r0, int st) {
     const int b = st & 1;
     const bool ok = tile_wait(s, tc, b);
@@ -395,7 +475,7 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
     tmem_ld16(tl + 64 * b + 32 + 16 * hh, im);
     tmem_wait_ld();
     const int r = r0 + row_t, cb = k1 + st * KTN + 16 * hh;
-    if (r < N) {
+    if (r < row_end(st)) {
 #pragma unroll
       for (int jj = 0; jj < 16; ++jj)
         if (cb + jj < NC) A[(size_t)(cb + jj) * N + r] = make_float2(re[jj], im[jj]);
@@ -403,49 +483,8 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
   };
   for (int rb = 0; rb < nrb; ++rb) {
     const int r0 = k1 + rb * KTM;
-    {  // A planes: rows r0 .. r0 + 127 of the block column (16 k per thread, loads coalesced along the rows)
-      const int rl = tid & (KTM - 1), h = tid >> 7, r = r0 + rl;
-      const bool rok = r < N;
-      float2 v[16];
-#pragma unroll
-      for (int u = 0; u < 16; ++u) v[u] = rok ? __ldcg(A + (size_t)(k0 + 16 * h + u) * N + r) : make_float2(0.f, 0.f);
-#pragma unroll
-      for (int g = 0; g < 4; ++g) store_planes(s.a_pl, KAP, rl, 16 * h + 4 * g, v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
-    }
-    // B planes of D^-1: element (i, k) = D^-1[k][i], so that the product below is A21 D^-1
-    for (int e = tid; e < KB * (KB / 4); e += KT) {
-      const int i = e >> 3, k = (e & 7) * 4;
-      const float2* d = s.dinv + i;
-      store_planes(s.b_pl + 4 * KBP, KBP, i, k, d[k * K_DLD], d[(k + 1) * K_DLD], d[(k + 2) * K_DLD],
-                   d[(k + 3) * K_DLD]);
-    }
-    tc_fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    {  // L21' = A21 D^-1 for the block's rows into TMEM buffer 0, then split back into the A planes
-      const bool live = s.misc[0] == 0;
-      if (live && tid == 0) {
-        tc_fence_after();
-        issue_planar(tbase, tbase + 32, s.a_pl, s.b_pl + 4 * KBP, false, true);
-        tc_commit(s.bar);
-      }
-      if (live) tc.iss[0] += 1;
-      const bool ok = live && tile_wait(s, tc, 0);
-      tc_fence_after();
-      if (ok) {
-        float re[16], im[16];
-        tmem_ld16(tl + 16 * hh, re);
-        tmem_ld16(tl + 32 + 16 * hh, im);
-        tmem_wait_ld();
-#pragma unroll
-        for (int g = 0; g < 4; ++g)
-          store_planes(s.a_pl, KAP, row_t, 16 * hh + 4 * g, make_float2(re[4 * g], im[4 * g]),
-                       make_float2(re[4 * g + 1], im[4 * g + 1]), make_float2(re[4 * g + 2], im[4 * g + 2]),
-                       make_float2(re[4 * g + 3], im[4 * g + 3]));
-      }
-      tc_fence_before();
-      __syncthreads();
-    }
+    const int nst = (k2 > 0 && rb > 0) ? 1 : nst_all;
+    block_l21(A, N, r0, k0, dinv, s, tc, false);
     if (warp == KW - 1) {
       prefetch_tile_l2(A, N, NC, r0, k1);
       if (nst > 1) prefetch_tile_l2(A, N, NC, r0, k1 + KTN);
@@ -461,10 +500,11 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
       }
       {  // C tile -> TMEM: row row_t, 16 complex columns per warp half
         const int r = r0 + row_t, cb = c0 + 16 * hh;
+        const bool rok = r < row_end(st);
         float re[16], im[16];
 #pragma unroll
         for (int jj = 0; jj < 16; ++jj) {
-          const float2 x = (r < N && cb + jj < NC) ? __ldcg(A + (size_t)(cb + jj) * N + r) : make_float2(0.f, 0.f);
+          const float2 x = (rok && cb + jj < NC) ? __ldcg(A + (size_t)(cb + jj) * N + r) : make_float2(0.f, 0.f);
           re[jj] = x.x;
           im[jj] = x.y;
         }
@@ -597,7 +637,7 @@ __device__ int solve_item_block(const StructuredSource& src, const WorkItem& wi,
     __syncthreads();
     block_row_planes(A, N, NC, k0, k1, bop);
     __syncthreads();
-    block_trailing(A, N, NC, k0, k1, s, bop, tc);
+    block_trailing(A, N, NC, k0, k1, s, bop, inv + (size_t)(k0 / KB) * KB * KB, tc);
   }
   __syncthreads();
   // ---- initial solve: the selector columns hold the forward result L^-1 S; back substitution only ----
@@ -723,6 +763,55 @@ __global__ void __launch_bounds__(KT, 2)
   }
 }
 
+// Heterogeneous batch (requests of one orbital count, see bse_multi_kernel in bse.cu): each item reads its
+// request's descriptor; shared memory and the scratch slot are sized for the largest request of the launch.
+template <int NR>
+__global__ void __launch_bounds__(KT, 2)
+    bse_block_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work,
+                           int n_items, int n_max, int max_iter, double tol, int* __restrict__ status,
+                           int* __restrict__ iters, unsigned char* __restrict__ scratch, size_t slot_bytes,
+                           long long wait_limit) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  BlockSmem s0(smem_raw, n_max, NR, wait_limit);
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  TileCount tc;
+  block_kernel_begin(s0);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (s0.misc[0]) {
+      if (threadIdx.x == 0) {
+        status[item] = DGA_ITEM_WAIT_TIMEOUT;
+        if (iters) iters[item] = 0;
+      }
+      continue;
+    }
+    const MultiItem mi = work[item];
+    const dga_bse_problem d = probs[mi.prob];
+    StructuredSource src;
+    src.gamma_cm = (const double2*)d.gamma_cm;
+    src.chi0_inv = (const double2*)d.chi0_inv;
+    src.uv = (const double2*)d.uv;
+    src.n2 = NR;
+    src.nv = 2 * d.niv;
+    src.W = d.niw_half;
+    src.Q = d.n_q;
+    src.inv_beta2 = d.inv_beta2;
+    const int N = NR * src.nv;
+    BlockSmem s(smem_raw, N, NR, wait_limit);  // the same shared memory, solve-phase offsets for this N
+    const WorkItem wi{mi.ch, mi.q, mi.w};
+    double2* o = (double2*)d.out + (((size_t)wi.ch * src.Q + wi.q) * src.W + wi.w) * (size_t)N * NR;
+    int it = 0;
+    const int st = solve_item_block<NR>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, tc, &it);
+    if (threadIdx.x == 0) {
+      status[item] = st;
+      if (iters) iters[item] = it;
+    }
+  }
+  if (!block_kernel_end(s0, tc)) {
+    for (int item = blockIdx.x + threadIdx.x * gridDim.x; item < n_items; item += blockDim.x * gridDim.x)
+      atomicOr(status + item, DGA_ITEM_WAIT_TIMEOUT);
+  }
+}
+
 }  // namespace dga
 
 using namespace dga;
@@ -744,28 +833,43 @@ static void block_set_attributes() {
                        (int)block_smem_bytes());
   cudaFuncSetAttribute(bse_block_mixed_kernel<NR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                        (int)cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(bse_block_multi_kernel<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)block_smem_bytes());
+  cudaFuncSetAttribute(bse_block_multi_kernel<NR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
 }
 
 template <int NR>
+static int block_ctas_per_sm_nr();
+
+template <int NR>
 static int block_grid_nr(int n_items) {
-  const size_t smem = block_smem_bytes();
-  block_set_attributes<NR>();
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bse_block_mixed_kernel<NR>, KT, smem);
+  int per_sm = block_ctas_per_sm_nr<NR>();
   if (per_sm < 1) per_sm = 1;
-  if (per_sm > 2) per_sm = 2;  // two CTAs hold 256 of the SM's 512 TMEM columns
   const int g = device_sm_count() * per_sm;
   return n_items < g ? n_items : g;
 }
 
+// Resident CTAs per SM from the kernel's registers and shared memory (two at most: two CTAs hold 256 of the SM's
+// 512 TMEM columns).  Computed here rather than by cudaOccupancyMaxActiveBlocksPerMultiprocessor, which answers 1
+// for this kernel although its register and shared-memory limits both allow 2 (as the profiler's occupancy
+// section reports).
 template <int NR>
 static int block_ctas_per_sm_nr() {
   block_set_attributes<NR>();
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bse_block_mixed_kernel<NR>, KT, block_smem_bytes()) !=
-      cudaSuccess)
+  cudaFuncAttributes fa;
+  int dev = 0, regs_sm = 0, smem_sm = 0, reserved = 0;
+  if (cudaFuncGetAttributes(&fa, bse_block_mixed_kernel<NR>) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess)
     return -1;
-  return per_sm;
+  const long long regs_cta = (long long)((fa.numRegs + 7) / 8 * 8) * KT;
+  const long long smem_cta = (long long)block_smem_bytes() + fa.sharedSizeBytes + reserved;
+  long long per_sm = 2;
+  if (regs_cta * per_sm > regs_sm) per_sm = regs_sm / regs_cta;
+  if (smem_cta * per_sm > smem_sm) per_sm = smem_sm / smem_cta;
+  return per_sm < 1 ? 1 : (int)per_sm;
 }
 
 // Resident CTAs per SM of the block-form kernel for n2 right-hand sides (the occupancy the launch gets).
@@ -798,6 +902,27 @@ cudaError_t dga_block_launch(int grid, const StructuredSource& src, const WorkIt
     block_set_attributes<R>();                                                                                    \
     bse_block_mixed_kernel<R><<<grid, KT, smem, stream>>>(src, work, n_items, N, nv, W, Q, beta, max_iter, tol,    \
                                                           out, status, iters, scratch, slot_bytes, wait_limit);   \
+    break;
+  switch (n2) {
+    DGA_BLOCK_CASE(1)
+    DGA_BLOCK_CASE(4)
+    DGA_BLOCK_CASE(9)
+    DGA_BLOCK_CASE(16)
+  }
+#undef DGA_BLOCK_CASE
+  return cudaGetLastError();
+}
+
+cudaError_t dga_block_batch_launch(int grid, int n2, const dga_bse_problem* probs, const MultiItem* work, int n_items,
+                                   int n_max, int max_iter, double tol, int* status, int* iters,
+                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
+                                   long long wait_limit) {
+  const size_t smem = block_smem_bytes();
+#define DGA_BLOCK_CASE(R)                                                                                          \
+  case R:                                                                                                          \
+    block_set_attributes<R>();                                                                                     \
+    bse_block_multi_kernel<R><<<grid, KT, smem, stream>>>(probs, work, n_items, n_max, max_iter, tol, status,     \
+                                                          iters, scratch, slot_bytes, wait_limit);                 \
     break;
   switch (n2) {
     DGA_BLOCK_CASE(1)

@@ -195,6 +195,10 @@ cudaError_t dga_block_launch(int grid, const dga::StructuredSource& src, const d
                              int n2, int nv, int W, int Q, double beta, int max_iter, double tol, double2* out,
                              int* status, int* iters, unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
                              long long wait_limit = 0);
+cudaError_t dga_block_batch_launch(int grid, int n2, const dga_bse_problem* probs, const dga::MultiItem* work,
+                                   int n_items, int n_max, int max_iter, double tol, int* status, int* iters,
+                                   unsigned char* scratch, size_t slot_bytes, cudaStream_t stream,
+                                   long long wait_limit = 0);
 cudaError_t dga_panel_batch_launch(int grid, int n2, const dga_bse_problem* probs, const dga::MultiItem* work,
                                    int n_items, int n_max, int max_iter, double tol, int* status, int* iters,
                                    unsigned char* scratch, size_t slot_bytes, cudaStream_t stream, bool tc = false,
