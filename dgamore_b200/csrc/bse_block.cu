@@ -46,8 +46,8 @@ constexpr int KBP = KTN * KB;  // floats of one B plane (32 x 32)
 constexpr int K_REGION = 4 * KAP * 4 + 2 * 4 * KBP * 4;  // A planes (64 KB) + two B plane sets (2 x 16 KB)
 constexpr int K_DLD = 33;                                 // leading dimension of the diagonal inverse in smem
 constexpr uint32_t K_SBO = 1024;                          // 8 rows x 32 floats: stride byte offset of a plane
-constexpr uint32_t K_TMEM_COLS = 128;                     // two tiles in flight x (Re, Im) x 32 columns
-constexpr uint32_t K_A2_COL = 128;                        // TMEM A operand planes of a step pair (4 x 32 columns)
+constexpr uint32_t K_A_COL = 128;      // TMEM A operand planes (4 x 32 columns) after the accumulators
+constexpr uint32_t K_TMEM_COLS = 256;  // two tiles in flight x (Re, Im) x 32 columns, then the A operand planes
 
 // kind::tf32, D fp32, A and B tf32 K-major, M = 128, N = 32; bit 13 negates A.
 constexpr uint32_t K_IDESC_POS = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(KTN >> 3) << 17) |
@@ -59,7 +59,7 @@ __host__ __device__ __forceinline__ int kb_off(int row, int k) {
 }
 
 __host__ __device__ inline size_t block_smem_bytes() {
-  return (size_t)K_REGION + KB * K_DLD * sizeof(float2) + 16 /*bars*/ + 16 /*probe*/ + 16 /*tslot*/ +
+  return (size_t)K_REGION + KB * K_DLD * sizeof(float2) + 32 /*bars*/ + 16 /*probe*/ + 16 /*tslot*/ +
          16 /*misc*/ + 8 * sizeof(double) /*redd*/;
 }
 
@@ -72,15 +72,16 @@ __host__ __device__ inline size_t block_solve_bytes(int N, int NR) {
 }
 
 struct BlockSmem {
-  float* a_pl;    // [4][KAP] A planes (Re hi, Re lo, Im hi, Im lo); also the Gauss-Jordan workspace
-  float* b_pl;    // [2][4][KBP] B planes of two tiles in flight
+  float* a_pl;    // [4][KAP] A planes (Re hi, Re lo, Im hi, Im lo) of L'; also the Gauss-Jordan workspace
+  float2* cbuf;   // [2][32][128] the C tiles of two strips in flight, column-major (aliases a_pl)
+  float* b_pl;    // [2][4][KBP] B planes of two strips in flight
   float2* y;      // solve phase: right-hand sides [NR][N]
   double2* ys;    // solve phase: [32][NR] staging of the residual
   double2* colsum;  // solve phase: [NR][NR]
   float2* sinv;   // solve phase: [2][32][32] staged diagonal inverses
   float2* zb;     // solve phase: [NR][32] D^-1 y_b of the forward solve
   float2* dinv;   // [32][K_DLD] current diagonal inverse, row-major
-  uint64_t* bar;  // [2] completion barriers of the tiles in flight
+  uint64_t* bar;  // [4] completion barriers: [0, 1] products of the tiles in flight, [2, 3] their bulk copies
   uint64_t* probe;  // test hook: a barrier nothing arrives on
   uint32_t* tslot;  // TMEM base address
   int* misc;      // [0] a wait ran out, [1] status bits of the item, [2] the item met a singular diagonal block
@@ -91,6 +92,7 @@ struct BlockSmem {
       : wait_limit(wl > 0 ? wl : TC_WAIT_LIMIT), inject(wl < 0 ? -wl : 0) {
     unsigned char* p = base;
     a_pl = reinterpret_cast<float*>(p);
+    cbuf = reinterpret_cast<float2*>(p);
     b_pl = a_pl + 4 * KAP;
     y = reinterpret_cast<float2*>(p);
     const size_t yb = (((size_t)NR * N * sizeof(float2)) + 15) & ~(size_t)15;
@@ -102,7 +104,7 @@ struct BlockSmem {
     dinv = reinterpret_cast<float2*>(p);
     p += KB * K_DLD * sizeof(float2);
     bar = reinterpret_cast<uint64_t*>(p);
-    p += 16;
+    p += 32;
     probe = reinterpret_cast<uint64_t*>(p);
     p += 16;
     tslot = reinterpret_cast<uint32_t*>(p);
@@ -113,9 +115,10 @@ struct BlockSmem {
   }
 };
 
-// Tile bookkeeping (same in every thread): commits issued and completions observed per barrier.
+// Tile bookkeeping (same in every thread): phases issued and completions observed per barrier.
+constexpr int K_NBAR = 4;
 struct TileCount {
-  uint32_t iss[2] = {0u, 0u}, obs[2] = {0u, 0u};
+  uint32_t iss[K_NBAR] = {}, obs[K_NBAR] = {};
 };
 
 // slot: A with its NR selector columns (N x (N + NR) complex64, column-major) | D_k^-1 per block (32 x 32
@@ -152,31 +155,51 @@ __device__ __forceinline__ void store_planes(float* planes, int plane_floats, in
   *reinterpret_cast<float4*>(planes + 3 * plane_floats + o) = l;
 }
 
-// The complex product of one 32-deep chunk into the (Re, Im) accumulators at TMEM columns d_re, d_im, issued by
-// one thread.  sign = -1: D -= A B (trailing update); sign = +1 with zero_init: D = A B (block row).
-//   D_re += s (Ar Br) - s (Ai Bi),  D_im += s (Ar Bi) + s (Ai Br)
-__device__ __forceinline__ void issue_planar(uint32_t d_re, uint32_t d_im, const float* a_pl, const float* b_pl,
-                                             bool negate, bool zero_init) {
+// One half of the complex product of a 32-deep chunk, issued by one thread: part 0 the real accumulator d (Ar Br
+// - Ai Bi), part 1 the imaginary one (Ar Bi + Ai Br).  The two parts go to different accumulators, so two threads
+// issue them side by side (a single thread issues a tcgen05.mma only every ~50 cycles, while the tensor pipe takes
+// an M = 128, N = 32 product every ~16).  Each of the four real products is the three-term split (lo hi + hi lo +
+// hi hi), six MMAs per K step of 8.
+//   issue_planar_part: A planes in shared memory, D = A B (the first product initialises d);
+//   issue_planar_tmem_part: A planes in tensor memory (Re hi, Re lo, Im hi, Im lo at a_tm + 0, 32, 64, 96),
+//   D -= A B.
+__device__ __forceinline__ void issue_planar_part(uint32_t d, const float* a_pl, const float* b_pl, int part) {
   const uint32_t a0 = smem_u32(a_pl), b0 = smem_u32(b_pl);
   const uint32_t ar_h = a0, ar_l = a0 + KAP * 4, ai_h = a0 + 2 * KAP * 4, ai_l = a0 + 3 * KAP * 4;
   const uint32_t br_h = b0, br_l = b0 + KBP * 4, bi_h = b0 + 2 * KBP * 4, bi_l = b0 + 3 * KBP * 4;
-  const uint32_t im = negate ? K_IDESC_NEG : K_IDESC_POS, ic = negate ? K_IDESC_POS : K_IDESC_NEG;
+  // part 0: (Ar, Br) +, (Ai, Bi) -;  part 1: (Ar, Bi) +, (Ai, Br) +
+  const uint32_t b1h = part ? bi_h : br_h, b1l = part ? bi_l : br_l;
+  const uint32_t b2h = part ? br_h : bi_h, b2l = part ? br_l : bi_l;
+  const uint32_t s2 = part ? K_IDESC_POS : K_IDESC_NEG;
 #pragma unroll
   for (int j = 0; j < KB / 8; ++j) {
     const uint32_t o = 256u * j;  // K step of 8 reals = two core matrices along K
-    const uint32_t acc = (j > 0 || !zero_init) ? 1u : 0u;
-    tc_mma_desc(d_re, ar_l + o, br_h + o, K_SBO, im, acc);
-    tc_mma_desc(d_re, ar_h + o, br_l + o, K_SBO, im, 1u);
-    tc_mma_desc(d_re, ar_h + o, br_h + o, K_SBO, im, 1u);
-    tc_mma_desc(d_re, ai_l + o, bi_h + o, K_SBO, ic, 1u);
-    tc_mma_desc(d_re, ai_h + o, bi_l + o, K_SBO, ic, 1u);
-    tc_mma_desc(d_re, ai_h + o, bi_h + o, K_SBO, ic, 1u);
-    tc_mma_desc(d_im, ar_l + o, bi_h + o, K_SBO, im, acc);
-    tc_mma_desc(d_im, ar_h + o, bi_l + o, K_SBO, im, 1u);
-    tc_mma_desc(d_im, ar_h + o, bi_h + o, K_SBO, im, 1u);
-    tc_mma_desc(d_im, ai_l + o, br_h + o, K_SBO, im, 1u);
-    tc_mma_desc(d_im, ai_h + o, br_l + o, K_SBO, im, 1u);
-    tc_mma_desc(d_im, ai_h + o, br_h + o, K_SBO, im, 1u);
+    tc_mma_desc(d, ar_l + o, b1h + o, K_SBO, K_IDESC_POS, j > 0 ? 1u : 0u);
+    tc_mma_desc(d, ar_h + o, b1l + o, K_SBO, K_IDESC_POS, 1u);
+    tc_mma_desc(d, ar_h + o, b1h + o, K_SBO, K_IDESC_POS, 1u);
+    tc_mma_desc(d, ai_l + o, b2h + o, K_SBO, s2, 1u);
+    tc_mma_desc(d, ai_h + o, b2l + o, K_SBO, s2, 1u);
+    tc_mma_desc(d, ai_h + o, b2h + o, K_SBO, s2, 1u);
+  }
+}
+
+__device__ __forceinline__ void issue_planar_tmem_part(uint32_t d, uint32_t a_tm, const float* b_pl, int part) {
+  const uint32_t b0 = smem_u32(b_pl);
+  const uint32_t ar_h = a_tm, ar_l = a_tm + 32, ai_h = a_tm + 64, ai_l = a_tm + 96;
+  const uint32_t br_h = b0, br_l = b0 + KBP * 4, bi_h = b0 + 2 * KBP * 4, bi_l = b0 + 3 * KBP * 4;
+  // part 0: (Ar, Br) -, (Ai, Bi) +;  part 1: (Ar, Bi) -, (Ai, Br) -
+  const uint32_t b1h = part ? bi_h : br_h, b1l = part ? bi_l : br_l;
+  const uint32_t b2h = part ? br_h : bi_h, b2l = part ? br_l : bi_l;
+  const uint32_t s2 = part ? K_IDESC_NEG : K_IDESC_POS;
+#pragma unroll
+  for (int j = 0; j < KB / 8; ++j) {
+    const uint32_t o = 256u * j, t = 8u * j;  // K step of 8: 256 bytes of a shared plane, 8 TMEM columns
+    tc_mma_tmem_a(d, ar_l + t, b1h + o, K_SBO, K_IDESC_NEG, 1u);
+    tc_mma_tmem_a(d, ar_h + t, b1l + o, K_SBO, K_IDESC_NEG, 1u);
+    tc_mma_tmem_a(d, ar_h + t, b1h + o, K_SBO, K_IDESC_NEG, 1u);
+    tc_mma_tmem_a(d, ai_l + t, b2h + o, K_SBO, s2, 1u);
+    tc_mma_tmem_a(d, ai_h + t, b2l + o, K_SBO, s2, 1u);
+    tc_mma_tmem_a(d, ai_h + t, b2h + o, K_SBO, s2, 1u);
   }
 }
 
@@ -364,9 +387,9 @@ __device__ void block_row_planes(const float2* __restrict__ A, int N, int NC, in
 }
 
 // ----------------------------------------------------------------------------------------------
-// Trailing update A[k1:N, k1:NC] -= A[k1:N, k0:k1] W: per 128-row block the A planes are staged once, then its
-// 32-column strips run two in flight (strip s stages its B planes and C while strip s - 1 multiplies).
+// Trailing update (below): L' in tensor memory, strips of C and B by bulk copy, two strips in flight.
 // ----------------------------------------------------------------------------------------------
+// Hint to bring the C tile A[r0 : r0 + 128, c0 : c0 + 32] into L2 (one prefetch per column, by one warp).
 __device__ __forceinline__ void prefetch_tile_l2(const float2* A, int N, int NC, int r0, int c0) {
   const int lane = threadIdx.x & 31;
   const int c = c0 + lane;
@@ -378,16 +401,15 @@ __device__ __forceinline__ void prefetch_tile_l2(const float2* A, int N, int NC,
 }
 
 // L' = A[r0 : r0 + 128, kc : kc + 32] D^-1 on the tensor cores (D^-1 row-major in global memory, dinv), into TMEM
-// buffer 0, then split back either into the shared-memory A planes (to_tmem false) or into the tensor-memory A
-// planes at column a2 of the CTA's allocation (to_tmem true: Re hi, Re lo, Im hi, Im lo at a2 + 0, 32, 64, 96).
-// Uses the A planes and B buffer 1 of shared memory; every thread takes part; ends with a barrier.
+// buffer 0, then split into the tensor-memory A operand planes (Re hi, Re lo, Im hi, Im lo at columns K_A_COL + 0,
+// 32, 64, 96 of the CTA's allocation).  Stages A21 in the shared A planes and D^-1 in B buffer 1; every thread takes
+// part; ends with a barrier.
 __device__ void block_l21(const float2* __restrict__ A, int N, int r0, int kc, const float2* __restrict__ dinv,
-                          BlockSmem& s, TileCount& tc, bool to_tmem) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+                          BlockSmem& s, TileCount& tc) {
+  const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t tbase = *s.tslot;
   const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
   const int hh = warp >> 2;
-  const int row_t = 32 * (warp & 3) + lane;
   {  // A planes: rows r0 .. r0 + 127 of the block column (16 k per thread, loads coalesced along the rows)
     const int rl = tid & (KTM - 1), h = tid >> 7, r = r0 + rl;
     const bool rok = r < N;
@@ -407,9 +429,10 @@ __device__ void block_l21(const float2* __restrict__ A, int N, int r0, int kc, c
   tc_fence_before();
   __syncthreads();
   const bool live = s.misc[0] == 0;
-  if (live && tid == 0) {
+  if (live && (tid == 0 || tid == 32)) {  // real part by thread 0, imaginary part by thread 32
+    const int part = tid >> 5;
     tc_fence_after();
-    issue_planar(tbase, tbase + 32, s.a_pl, s.b_pl + 4 * KBP, false, true);
+    issue_planar_part(tbase + 32 * part, s.a_pl, s.b_pl + 4 * KBP, part);
     tc_commit(s.bar);
   }
   if (live) tc.iss[0] += 1;
@@ -420,109 +443,128 @@ __device__ void block_l21(const float2* __restrict__ A, int N, int r0, int kc, c
     tmem_ld16(tl + 16 * hh, re);
     tmem_ld16(tl + 32 + 16 * hh, im);
     tmem_wait_ld();
-    if (to_tmem) {
-      float rh[16], rlo[16], ih[16], il[16];
+    float rh[16], rlo[16], ih[16], il[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        rh[j] = tf32_hi(re[j]);
-        rlo[j] = re[j] - rh[j];
-        ih[j] = tf32_hi(im[j]);
-        il[j] = im[j] - ih[j];
-      }
-      const uint32_t a2 = tl + K_A2_COL + 16 * hh;
-      tmem_st16(a2, rh);
-      tmem_st16(a2 + 32, rlo);
-      tmem_st16(a2 + 64, ih);
-      tmem_st16(a2 + 96, il);
-      tmem_wait_st();
-    } else {
-#pragma unroll
-      for (int g = 0; g < 4; ++g)
-        store_planes(s.a_pl, KAP, row_t, 16 * hh + 4 * g, make_float2(re[4 * g], im[4 * g]),
-                     make_float2(re[4 * g + 1], im[4 * g + 1]), make_float2(re[4 * g + 2], im[4 * g + 2]),
-                     make_float2(re[4 * g + 3], im[4 * g + 3]));
+    for (int j = 0; j < 16; ++j) {
+      rh[j] = tf32_hi(re[j]);
+      rlo[j] = re[j] - rh[j];
+      ih[j] = tf32_hi(im[j]);
+      il[j] = im[j] - ih[j];
     }
+    const uint32_t a2 = tl + K_A_COL + 16 * hh;
+    tmem_st16(a2, rh);
+    tmem_st16(a2 + 32, rlo);
+    tmem_st16(a2 + 64, ih);
+    tmem_st16(a2 + 96, il);
+    tmem_wait_st();
   }
   tc_fence_before();
   __syncthreads();
 }
 
-// The K = 32 trailing pass of step k (block column k0, first trailing row and column k1).  With k2 = 0 it is the
-// whole trailing update rows [k1, N) x columns [k1, NC).  With k2 = k1 + 32 it is the first half of a pair of
-// steps: only block column k + 1 (columns [k1, k2), every row from k1) and block row k + 1 (rows [k1, k2), every
-// column) take step k's product here; the rest of the trailing matrix takes steps k and k + 1 together in
-// block_trailing_pair.
+// Bulk copies of strip st's operands into buffer b (issued by warp 0): the B planes of the block row (16 KB, one
+// copy) and the C tile A[r0 : r0 + rows, c0 : c0 + 32] (one copy of rows x 8 bytes per column inside the matrix,
+// column-major in cbuf); all of them complete on load barrier 2 + b.  rows and r0 are even and N is even, so every
+// copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
+__device__ __forceinline__ void trailing_copies(const float2* __restrict__ A, int N, int NC, int r0, int rows, int c0,
+                                                const float* __restrict__ bsrc, BlockSmem& s, int b) {
+  const int lane = threadIdx.x & 31;
+  const int ncols = min(KTN, NC - c0);
+  uint64_t* bar = s.bar + 2 + b;
+  if (lane == 0)
+    mbar_expect_tx(bar, (uint32_t)(4 * KBP * sizeof(float)) + (uint32_t)(ncols * rows) * (uint32_t)sizeof(float2));
+  __syncwarp();
+  if (lane == 0) bulk_g2s(s.b_pl + b * 4 * KBP, bsrc, 4 * KBP * sizeof(float), bar);
+  if (lane < ncols)
+    bulk_g2s(s.cbuf + (size_t)b * KTN * KTM + lane * KTM, A + (size_t)(c0 + lane) * N + r0,
+             (uint32_t)(rows * sizeof(float2)), bar);
+}
+
+// Trailing update A[k1:N, k1:NC] -= (A[k1:N, k0:k1] D^-1) A[k0:k1, k1:NC]: per 128-row block, L' goes to the
+// tensor-memory A operand; then its 32-column strips run two in flight.  Strip st's B planes and C tile arrive by
+// bulk copy in buffer st & 1 (issued one strip ahead, once the product that read the buffer has completed).  Warp
+// roles in the strip loop: threads 0 and 32 issue the real and imaginary halves of each product (warps 0 and 1 do
+// nothing else); the other six warps move the C tiles between shared memory, tensor memory and A (a warp reaches
+// the TMEM lanes 32 (warp % 4) ..: warps 2, 3, 6, 7 one 16-column half each, warps 4 and 5 both halves of the
+// lanes of warps 0 and 1), and warp 2 issues the bulk copies.
 __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, int k1, BlockSmem& s,
-                               const float* __restrict__ bop, const float2* __restrict__ dinv, TileCount& tc,
-                               int k2 = 0) {
+                               const float* __restrict__ bop, const float2* __restrict__ dinv, TileCount& tc) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (k1 >= N) return;
-  const int nrb = (N - k1 + KTM - 1) / KTM, nst_all = (NC - k1 + KTN - 1) / KTN;
+  const int nrb = (N - k1 + KTM - 1) / KTM, nst = (NC - k1 + KTN - 1) / KTN;
   const uint32_t tbase = *s.tslot;
   const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
-  const int hh = warp >> 2;
   const int row_t = 32 * (warp & 3) + lane;  // this thread's tile row (its TMEM lane)
-  // rows of strip st that take this pass's product: all from k1, or for a pair's panel pass beyond strip 0 only
-  // the rows of block row k + 1
-  auto row_end = [&](int st) { return (k2 > 0 && st > 0) ? k2 : N; };
+  const bool mover = warp >= 2;
+  const int h0 = (warp == 4 || warp == 5) ? 0 : (warp >> 2), h1 = (warp == 4 || warp == 5) ? 1 : (warp >> 2);
+  constexpr int COPIER = 2;
   auto finish = [&](int r0, int st) {
     const int b = st & 1;
     const bool ok = tile_wait(s, tc, b);
     tc_fence_after();
-    if (!ok) return;
-    float re[16], im[16];
-    tmem_ld16(tl + 64 * b + 16 * hh, re);
-    tmem_ld16(tl + 64 * b + 32 + 16 * hh, im);
-    tmem_wait_ld();
-    const int r = r0 + row_t, cb = k1 + st * KTN + 16 * hh;
-    if (r < row_end(st)) {
+    if (!ok || !mover) return ok;
+    for (int hh = h0; hh <= h1; ++hh) {
+      float re[16], im[16];
+      tmem_ld16(tl + 64 * b + 16 * hh, re);
+      tmem_ld16(tl + 64 * b + 32 + 16 * hh, im);
+      tmem_wait_ld();
+      const int r = r0 + row_t, cb = k1 + st * KTN + 16 * hh;
+      if (r < N) {
 #pragma unroll
-      for (int jj = 0; jj < 16; ++jj)
-        if (cb + jj < NC) A[(size_t)(cb + jj) * N + r] = make_float2(re[jj], im[jj]);
+        for (int jj = 0; jj < 16; ++jj)
+          if (cb + jj < NC) A[(size_t)(cb + jj) * N + r] = make_float2(re[jj], im[jj]);
+      }
     }
+    return true;
   };
   for (int rb = 0; rb < nrb; ++rb) {
-    const int r0 = k1 + rb * KTM;
-    const int nst = (k2 > 0 && rb > 0) ? 1 : nst_all;
-    block_l21(A, N, r0, k0, dinv, s, tc, false);
-    if (warp == KW - 1) {
-      prefetch_tile_l2(A, N, NC, r0, k1);
-      if (nst > 1) prefetch_tile_l2(A, N, NC, r0, k1 + KTN);
+    const int r0 = k1 + rb * KTM, rows = min(KTM, N - r0);
+    block_l21(A, N, r0, k0, dinv, s, tc);  // every product of the previous row block has completed
+    if (s.misc[0] == 0) {
+      if (warp == COPIER) {
+        trailing_copies(A, N, NC, r0, rows, k1, bop, s, 0);
+        if (nst > 1) trailing_copies(A, N, NC, r0, rows, k1 + KTN, bop + 4 * KBP, s, 1);
+      }
+      tc.iss[2] += 1;
+      if (nst > 1) tc.iss[3] += 1;
     }
     for (int st = 0; st < nst; ++st) {
       const int b = st & 1, c0 = k1 + st * KTN;
       if (warp == KW - 1 && st + 2 < nst) prefetch_tile_l2(A, N, NC, r0, c0 + 2 * KTN);
-      {  // B planes of the strip (split by the block-row tiles): 16 KB copy
-        const float4* src4 = reinterpret_cast<const float4*>(bop + (size_t)st * 4 * KBP);
-        float4* dst4 = reinterpret_cast<float4*>(s.b_pl + b * 4 * KBP);
+      if (tile_wait(s, tc, 2 + b) && mover) {  // C tile -> TMEM buffer b
+        for (int hh = h0; hh <= h1; ++hh) {
+          const float2* cb = s.cbuf + (size_t)b * KTN * KTM + (16 * hh) * KTM + row_t;
+          float re[16], im[16];
 #pragma unroll
-        for (int u = 0; u < (4 * KBP / 4) / KT; ++u) dst4[tid + u * KT] = __ldcg(src4 + tid + u * KT);
-      }
-      {  // C tile -> TMEM: row row_t, 16 complex columns per warp half
-        const int r = r0 + row_t, cb = c0 + 16 * hh;
-        const bool rok = r < row_end(st);
-        float re[16], im[16];
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-          const float2 x = (rok && cb + jj < NC) ? __ldcg(A + (size_t)(cb + jj) * N + r) : make_float2(0.f, 0.f);
-          re[jj] = x.x;
-          im[jj] = x.y;
+          for (int jj = 0; jj < 16; ++jj) {
+            const float2 x = cb[jj * KTM];
+            re[jj] = x.x;
+            im[jj] = x.y;
+          }
+          tmem_st16(tl + 64 * b + 16 * hh, re);
+          tmem_st16(tl + 64 * b + 32 + 16 * hh, im);
         }
-        tmem_st16(tl + 64 * b + 16 * hh, re);
-        tmem_st16(tl + 64 * b + 32 + 16 * hh, im);
         tmem_wait_st();
       }
-      tc_fence_async_smem();
       tc_fence_before();
       __syncthreads();
       const bool live = s.misc[0] == 0;
-      if (live && tid == 0) {
+      if (live && (tid == 0 || tid == 32)) {
+        const int part = tid >> 5;
         tc_fence_after();
-        issue_planar(tbase + 64 * b, tbase + 64 * b + 32, s.a_pl, s.b_pl + b * 4 * KBP, true, false);
+        issue_planar_tmem_part(tbase + 64 * b + 32 * part, tbase + K_A_COL, s.b_pl + b * 4 * KBP, part);
         tc_commit(s.bar + b);
       }
       if (live) tc.iss[b] += 1;
-      if (st > 0 && live) finish(r0, st - 1);
+      if (st > 0 && live) {
+        // once strip st - 1's product has completed, its buffers take strip st + 1
+        const bool ok = finish(r0, st - 1);
+        if (st + 1 < nst) {
+          if (warp == COPIER && ok)
+            trailing_copies(A, N, NC, r0, rows, c0 + KTN, bop + (size_t)(st + 1) * 4 * KBP, s, b ^ 1);
+          tc.iss[2 + (b ^ 1)] += 1;
+        }
+      }
     }
     if (s.misc[0] == 0) finish(r0, nst - 1);
     tc_fence_before();
@@ -699,8 +741,8 @@ __device__ int solve_item_block(const StructuredSource& src, const WorkItem& wi,
 __device__ void block_kernel_begin(BlockSmem& s) {
   if (threadIdx.x == 0) {
     s.misc[0] = 0;
-    mbar_init(s.bar);
-    mbar_init(s.bar + 1);
+#pragma unroll
+    for (int b = 0; b < K_NBAR; ++b) mbar_init(s.bar + b, b < 2 ? 2u : 1u);  // products: two issuing threads
     if (s.inject) mbar_init(s.probe);
   }
   if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, K_TMEM_COLS);
@@ -721,7 +763,7 @@ __device__ bool block_kernel_end(BlockSmem& s, const TileCount& tc) {
   __syncthreads();
   bool drained = true;
 #pragma unroll
-  for (int b = 0; b < 2; ++b)
+  for (int b = 0; b < K_NBAR; ++b)
     if (tc.iss[b] > tc.obs[b]) drained &= mbar_wait(s.bar + b, (tc.iss[b] - 1u) & 1u);
   tc_fence_after();
   __syncthreads();

@@ -70,8 +70,8 @@ __device__ __forceinline__ void tc_dealloc(uint32_t taddr, uint32_t ncols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1) : "memory");
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count = 1) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
@@ -170,6 +170,18 @@ __device__ __forceinline__ void tc_mma_desc(uint32_t d_tmem, uint32_t a_addr, ui
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
       "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(zero), "r"(zero), "r"(zero), "r"(zero)
+      : "memory");
+}
+
+// One MMA of kind::tf32 with A in tensor memory (lane = row, one fp32 column per K element, a_tmem the column of
+// the K step) and B K-major in shared memory: D = (accum ? D : 0) + op(A) B.
+__device__ __forceinline__ void tc_mma_tmem_a(uint32_t d_tmem, uint32_t a_tmem, uint32_t b_addr, uint32_t sbo,
+                                              uint32_t idesc, uint32_t accum) {
+  const uint64_t bd = tc_desc_sbo(b_addr, sbo);
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bd), "r"(idesc), "r"(accum)
       : "memory");
 }
 
