@@ -46,6 +46,7 @@ constexpr int KBP = KTN * KB;  // floats of one B plane (32 x 32)
 constexpr int K_REGION = 4 * KAP * 4 + 2 * 4 * KBP * 4;  // A planes (64 KB) + two B plane sets (2 x 16 KB)
 constexpr int K_DLD = 33;                                 // leading dimension of the diagonal inverse in smem
 constexpr uint32_t K_SBO = 1024;                          // 8 rows x 32 floats: stride byte offset of a plane
+constexpr uint32_t K_WAIT_HINT_NS = 1000;  // longest suspension of one poll of a tile wait
 constexpr uint32_t K_A_COL = 128;      // TMEM A operand planes (4 x 32 columns) after the accumulators
 constexpr uint32_t K_TMEM_COLS = 256;  // two tiles in flight x (Re, Im) x 32 columns, then the A operand planes
 
@@ -115,10 +116,17 @@ struct BlockSmem {
   }
 };
 
-// Tile bookkeeping (same in every thread): phases issued and completions observed per barrier.
+// Tile bookkeeping of one thread, in two registers (bit i for barrier i): pend, a phase has been issued that this
+// thread has not yet seen complete; par, the parity of the next phase to wait for.  By construction a barrier has
+// at most one phase in flight.
 constexpr int K_NBAR = 4;
 struct TileCount {
-  uint32_t iss[K_NBAR] = {}, obs[K_NBAR] = {};
+  uint32_t pend = 0u, par = 0u;
+  __device__ __forceinline__ void issued(int i) { pend |= 1u << i; }
+  __device__ __forceinline__ void observed(int i) {
+    pend &= ~(1u << i);
+    par ^= 1u << i;
+  }
 };
 
 // slot: A with its NR selector columns (N x (N + NR) complex64, column-major) | D_k^-1 per block (32 x 32
@@ -210,8 +218,8 @@ __device__ __forceinline__ void issue_planar_tmem_part(uint32_t d, uint32_t a_tm
 // a thread owns rows tid, tid + KT, tid + 2 KT of a pass (a warp reads 512 contiguous bytes of a Gamma column per
 // load) with eight columns of Gamma loads in flight.
 template <int NR>
-__device__ void block_form_a(const StructuredSource& src, const WorkItem& wi, int N, int nv, float2* __restrict__ A) {
-  constexpr int RPT = 3, CPI = 8;  // rows per thread and pass, columns per iteration
+__device__ __forceinline__ void block_form_a(const StructuredSource& src, const WorkItem& wi, int N, int nv, float2* __restrict__ A) {
+  constexpr int RPT = 3, CPI = 4;  // rows per thread and pass, columns per iteration
   const int tid = threadIdx.x;
   const double2* gam = src.gamma_cm + ((size_t)(wi.ch * src.W + wi.w) * N) * N;
   const double2* c0 = src.chi0_inv + ((size_t)wi.q * src.W + wi.w) * nv * NR * NR;
@@ -273,7 +281,7 @@ __device__ void block_form_a(const StructuredSource& src, const WorkItem& wi, in
 // Writes D^-1 row-major to s.dinv (ld K_DLD) and inv (ld 32), zero outside the nb x nb block.  Returns false
 // (in every thread) if a pivot column was exactly zero or not finite.
 // ----------------------------------------------------------------------------------------------
-__device__ bool block_diag_inverse(const float2* __restrict__ A, int N, int k0, int nb, float2* aug, float2* dinv,
+__device__ __forceinline__ bool block_diag_inverse(const float2* __restrict__ A, int N, int k0, int nb, float2* aug, float2* dinv,
                                    float2* __restrict__ inv, int* sp, float2* sd) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -352,8 +360,8 @@ __device__ bool block_diag_inverse(const float2* __restrict__ A, int N, int k0, 
 // the TMEM loads that follow are warp-collective.
 __device__ __forceinline__ bool tile_wait(BlockSmem& s, TileCount& tc, int b) {
   bool ok = false;
-  if (s.misc[0] == 0) ok = mbar_wait(s.bar + b, tc.obs[b] & 1u, s.wait_limit);
-  if (ok) tc.obs[b] += 1;
+  if (s.misc[0] == 0) ok = mbar_wait_sleep(s.bar + b, (tc.par >> b) & 1u, s.wait_limit, K_WAIT_HINT_NS);
+  if (ok) tc.observed(b);
   ok = __all_sync(0xffffffffu, ok);
   if (!ok) s.misc[0] = 1;
   return ok;
@@ -364,7 +372,7 @@ __device__ __forceinline__ bool tile_wait(BlockSmem& s, TileCount& tc, int b) {
 // plane element (c, k) = A[k0 + k][k1 + 32 st + c]; zero beyond the row's columns.  Two threads per column, each a
 // 128-byte run of it.
 // ----------------------------------------------------------------------------------------------
-__device__ void block_row_planes(const float2* __restrict__ A, int N, int NC, int k0, int k1, float* __restrict__ bop) {
+__device__ __forceinline__ void block_row_planes(const float2* __restrict__ A, int N, int NC, int k0, int k1, float* __restrict__ bop) {
   const int ncols = NC - k1;
   if (ncols <= 0 || k1 >= N) return;
   const int nst = (ncols + KTN - 1) / KTN;
@@ -404,7 +412,7 @@ __device__ __forceinline__ void prefetch_tile_l2(const float2* A, int N, int NC,
 // buffer 0, then split into the tensor-memory A operand planes (Re hi, Re lo, Im hi, Im lo at columns K_A_COL + 0,
 // 32, 64, 96 of the CTA's allocation).  Stages A21 in the shared A planes and D^-1 in B buffer 1; every thread takes
 // part; ends with a barrier.
-__device__ void block_l21(const float2* __restrict__ A, int N, int r0, int kc, const float2* __restrict__ dinv,
+__device__ __forceinline__ void block_l21(const float2* __restrict__ A, int N, int r0, int kc, const float2* __restrict__ dinv,
                           BlockSmem& s, TileCount& tc) {
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t tbase = *s.tslot;
@@ -435,7 +443,7 @@ __device__ void block_l21(const float2* __restrict__ A, int N, int r0, int kc, c
     issue_planar_part(tbase + 32 * part, s.a_pl, s.b_pl + 4 * KBP, part);
     tc_commit(s.bar);
   }
-  if (live) tc.iss[0] += 1;
+  if (live) tc.issued(0);
   const bool ok = live && tile_wait(s, tc, 0);
   tc_fence_after();
   if (ok) {
@@ -487,7 +495,7 @@ __device__ __forceinline__ void trailing_copies(const float2* __restrict__ A, in
 // nothing else); the other six warps move the C tiles between shared memory, tensor memory and A (a warp reaches
 // the TMEM lanes 32 (warp % 4) ..: warps 2, 3, 6, 7 one 16-column half each, warps 4 and 5 both halves of the
 // lanes of warps 0 and 1), and warp 2 issues the bulk copies.
-__device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, int k1, BlockSmem& s,
+__device__ __forceinline__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, int k1, BlockSmem& s,
                                const float* __restrict__ bop, const float2* __restrict__ dinv, TileCount& tc) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (k1 >= N) return;
@@ -498,11 +506,13 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
   const bool mover = warp >= 2;
   const int h0 = (warp == 4 || warp == 5) ? 0 : (warp >> 2), h1 = (warp == 4 || warp == 5) ? 1 : (warp >> 2);
   constexpr int COPIER = 2;
-  auto finish = [&](int r0, int st) {
+  // the product of strip st back to A once it has completed; `then` runs between the wait and the epilogue
+  auto finish = [&](int r0, int st, auto&& then) {
     const int b = st & 1;
     const bool ok = tile_wait(s, tc, b);
     tc_fence_after();
-    if (!ok || !mover) return ok;
+    then(ok);
+    if (!ok || !mover) return;
     for (int hh = h0; hh <= h1; ++hh) {
       float re[16], im[16];
       tmem_ld16(tl + 64 * b + 16 * hh, re);
@@ -515,7 +525,6 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
           if (cb + jj < NC) A[(size_t)(cb + jj) * N + r] = make_float2(re[jj], im[jj]);
       }
     }
-    return true;
   };
   for (int rb = 0; rb < nrb; ++rb) {
     const int r0 = k1 + rb * KTM, rows = min(KTM, N - r0);
@@ -525,8 +534,8 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
         trailing_copies(A, N, NC, r0, rows, k1, bop, s, 0);
         if (nst > 1) trailing_copies(A, N, NC, r0, rows, k1 + KTN, bop + 4 * KBP, s, 1);
       }
-      tc.iss[2] += 1;
-      if (nst > 1) tc.iss[3] += 1;
+      tc.issued(2);
+      if (nst > 1) tc.issued(3);
     }
     for (int st = 0; st < nst; ++st) {
       const int b = st & 1, c0 = k1 + st * KTN;
@@ -555,18 +564,19 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
         issue_planar_tmem_part(tbase + 64 * b + 32 * part, tbase + K_A_COL, s.b_pl + b * 4 * KBP, part);
         tc_commit(s.bar + b);
       }
-      if (live) tc.iss[b] += 1;
+      if (live) tc.issued(b);
       if (st > 0 && live) {
-        // once strip st - 1's product has completed, its buffers take strip st + 1
-        const bool ok = finish(r0, st - 1);
-        if (st + 1 < nst) {
-          if (warp == COPIER && ok)
-            trailing_copies(A, N, NC, r0, rows, c0 + KTN, bop + (size_t)(st + 1) * 4 * KBP, s, b ^ 1);
-          tc.iss[2 + (b ^ 1)] += 1;
-        }
+        // once strip st - 1's product has completed, its buffers take strip st + 1 (before the epilogue's stores)
+        finish(r0, st - 1, [&](bool ok) {
+          if (st + 1 < nst) {
+            if (warp == COPIER && ok)
+              trailing_copies(A, N, NC, r0, rows, c0 + KTN, bop + (size_t)(st + 1) * 4 * KBP, s, b ^ 1);
+            tc.issued(2 + (b ^ 1));
+          }
+        });
       }
     }
-    if (s.misc[0] == 0) finish(r0, nst - 1);
+    if (s.misc[0] == 0) finish(r0, nst - 1, [](bool) {});
     tc_fence_before();
     __syncthreads();
   }
@@ -582,7 +592,7 @@ __device__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, in
 // The inverse of the next block is staged into sinv (double buffered) during each update.
 // ----------------------------------------------------------------------------------------------
 template <int NR>
-__device__ void block_solve(const float2* __restrict__ A, int N, float2* y, int ldy, const float2* __restrict__ inv,
+__device__ __forceinline__ void block_solve(const float2* __restrict__ A, int N, float2* y, int ldy, const float2* __restrict__ inv,
                             float2* sinv, float2* zb, bool forward) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nblk = block_nblk(N);
@@ -651,7 +661,7 @@ __device__ void block_solve(const float2* __restrict__ A, int N, float2* y, int 
 // One work item: form, factor, solve, refine.  Returns the status bits; *iters = number of corrections.
 // ----------------------------------------------------------------------------------------------
 template <int NR>
-__device__ int solve_item_block(const StructuredSource& src, const WorkItem& wi, int N, int nv, double beta,
+__device__ __forceinline__ int solve_item_block(const StructuredSource& src, const WorkItem& wi, int N, int nv, double beta,
                                 int max_iter, double tol, double2* __restrict__ o, unsigned char* slot, BlockSmem& s,
                                 TileCount& tc, int* iters) {
   const int tid = threadIdx.x;
@@ -738,7 +748,7 @@ __device__ int solve_item_block(const StructuredSource& src, const WorkItem& wi,
   return st;
 }
 
-__device__ void block_kernel_begin(BlockSmem& s) {
+__device__ __forceinline__ void block_kernel_begin(BlockSmem& s) {
   if (threadIdx.x == 0) {
     s.misc[0] = 0;
 #pragma unroll
@@ -758,13 +768,13 @@ __device__ void block_kernel_begin(BlockSmem& s) {
 }
 
 // Drains every tile still in flight (full limit) and frees TMEM; false if a drain wait ran out.
-__device__ bool block_kernel_end(BlockSmem& s, const TileCount& tc) {
+__device__ __forceinline__ bool block_kernel_end(BlockSmem& s, const TileCount& tc) {
   tc_fence_before();
   __syncthreads();
   bool drained = true;
 #pragma unroll
   for (int b = 0; b < K_NBAR; ++b)
-    if (tc.iss[b] > tc.obs[b]) drained &= mbar_wait(s.bar + b, (tc.iss[b] - 1u) & 1u);
+    if ((tc.pend >> b) & 1u) drained &= mbar_wait(s.bar + b, (tc.par >> b) & 1u);
   tc_fence_after();
   __syncthreads();
   if ((threadIdx.x >> 5) == 0) tc_dealloc(*s.tslot, K_TMEM_COLS);

@@ -90,6 +90,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
   return false;
 }
 
+// As mbar_wait, but each poll may suspend the thread for up to hint_ns nanoseconds while the phase is incomplete
+// (it resumes as soon as the phase completes), so waiting warps leave the issue slots to the others: at most
+// limit x hint_ns in all.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, long long limit, uint32_t hint_ns) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\tselp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity), "r"(hint_ns)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Bulk copies between global and shared memory (the TMA engine, untiled form): the barrier expects `bytes` of
 // transactions, then each copy (16-byte aligned addresses, size a multiple of 16) completes on it.  Source and
 // destination are this CTA's own memory on this GPU; no multicast.
