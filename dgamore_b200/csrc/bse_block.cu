@@ -65,10 +65,11 @@ __host__ __device__ inline size_t block_smem_bytes() {
 }
 
 // Solve-phase use of the region: y [NR][N] complex64 | ys [32][NR] + colsum [NR][NR] complex128 | two staged
-// diagonal inverses [2][32][32] complex64 | the forward solve's D^-1 y_b [NR][32] complex64.
+// diagonal inverses [2][32][33] complex64 (rows padded against bank conflicts) | the forward solve's D^-1 y_b
+// [NR][32] complex64.
 __host__ __device__ inline size_t block_solve_bytes(int N, int NR) {
   const size_t y = (((size_t)NR * N * sizeof(float2)) + 15) & ~(size_t)15;
-  return y + (size_t)(32 * NR + NR * NR) * sizeof(double2) + 2 * KB * KB * sizeof(float2) +
+  return y + (size_t)(32 * NR + NR * NR) * sizeof(double2) + 2 * KB * K_DLD * sizeof(float2) +
          (size_t)NR * KB * sizeof(float2);
 }
 
@@ -79,7 +80,7 @@ struct BlockSmem {
   float2* y;      // solve phase: right-hand sides [NR][N]
   double2* ys;    // solve phase: [32][NR] staging of the residual
   double2* colsum;  // solve phase: [NR][NR]
-  float2* sinv;   // solve phase: [2][32][32] staged diagonal inverses
+  float2* sinv;   // solve phase: [2][32][K_DLD] staged diagonal inverses
   float2* zb;     // solve phase: [NR][32] D^-1 y_b of the forward solve
   float2* dinv;   // [32][K_DLD] current diagonal inverse, row-major
   uint64_t* bar;  // [4] completion barriers: [0, 1] products of the tiles in flight, [2, 3] their bulk copies
@@ -100,7 +101,7 @@ struct BlockSmem {
     ys = reinterpret_cast<double2*>(p + yb);
     colsum = ys + 32 * NR;
     sinv = reinterpret_cast<float2*>(colsum + NR * NR);
-    zb = sinv + 2 * KB * KB;
+    zb = sinv + 2 * KB * K_DLD;
     p += K_REGION;
     dinv = reinterpret_cast<float2*>(p);
     p += KB * K_DLD * sizeof(float2);
@@ -237,6 +238,9 @@ __device__ __forceinline__ void block_form_a(const StructuredSource& src, const 
     }
     if (!rok[0]) break;
     for (int j0 = 0; j0 < N; j0 += CPI) {
+      // L2 prefetch of Gamma columns 8 iterations ahead (one bulk prefetch per column)
+      if (tid < CPI && j0 + 8 * CPI + tid < N)
+        bulk_prefetch_l2(gam + (size_t)(j0 + 8 * CPI + tid) * N, (uint32_t)(N * sizeof(double2)));
       double2 g[CPI][RPT];
 #pragma unroll
       for (int u = 0; u < CPI; ++u)
@@ -618,18 +622,28 @@ __device__ __forceinline__ void block_solve(const float2* __restrict__ A, int N,
     }
   };
   // one sweep over the blocks: fwd = forward elimination (L), else back substitution (U)
+  // L2 prefetch of the column panel of block bb that a sweep's update reads: rows below it (forward) or above it
+  auto prefetch_panel = [&](int bb, bool fwd) {
+    if (warp != KW - 1) return;
+    const int p0 = bb * KB, pn = min(KB, N - p0);
+    const int rlo = fwd ? p0 + pn : 0, rhi = fwd ? N : p0;
+    if (lane < pn && rhi > rlo)
+      bulk_prefetch_l2(A + (size_t)(p0 + lane) * N + rlo, (uint32_t)((rhi - rlo) * sizeof(float2)));
+  };
   auto sweep = [&](bool fwd) {
     auto blk = [&](int st) { return fwd ? st : nblk - 1 - st; };
-    for (int e = tid; e < KB * KB; e += KT) sinv[e] = inv[(size_t)blk(0) * KB * KB + e];
+    prefetch_panel(blk(0), fwd);
+    for (int e = tid; e < KB * KB; e += KT) sinv[(e >> 5) * K_DLD + (e & 31)] = inv[(size_t)blk(0) * KB * KB + e];
     __syncthreads();
     for (int st = 0; st < nblk; ++st) {
       const int b = blk(st);
       const int k0 = b * KB, nb = min(KB, N - k0), k1 = k0 + nb;
-      const float2* sv = sinv + (st & 1) * KB * KB;
+      const float2* sv = sinv + (st & 1) * KB * K_DLD;
+      if (st + 1 < nblk) prefetch_panel(blk(st + 1), fwd);
       for (int r = warp; r < NR; r += KW) {  // D_b^-1 y_b
         float2* yr = y + (size_t)r * ldy + k0;
         float2 acc = make_float2(0.f, 0.f);
-        for (int k = 0; k < nb; ++k) cfma(acc, sv[lane * KB + k], yr[k]);
+        for (int k = 0; k < nb; ++k) cfma(acc, sv[lane * K_DLD + k], yr[k]);
         if (fwd) {
           zb[r * KB + lane] = acc;
         } else {
@@ -646,9 +660,12 @@ __device__ __forceinline__ void block_solve(const float2* __restrict__ A, int N,
       if (fwd) update(k0, nb, k1, N, zb, KB);
       else update(k0, nb, 0, k0, y + k0, ldy);
       if (st + 1 < nblk) {
-        float2* dst = sinv + ((st + 1) & 1) * KB * KB;
+        float2* dst = sinv + ((st + 1) & 1) * KB * K_DLD;
 #pragma unroll
-        for (int u = 0; u < KB * KB / KT; ++u) dst[tid + u * KT] = nx[u];
+        for (int u = 0; u < KB * KB / KT; ++u) {
+          const int e = tid + u * KT;
+          dst[(e >> 5) * K_DLD + (e & 31)] = nx[u];
+        }
       }
       __syncthreads();
     }

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "dga_common.cuh"
+#include "tc_tile.cuh"
 
 namespace dga {
 
@@ -130,9 +131,12 @@ __device__ void structured_residual_permuted(const StructuredSource& src, int ch
     double2 acc[NR];
 #pragma unroll
     for (int sidx = 0; sidx < NR; ++sidx) acc[sidx] = make_double2(0.0, 0.0);
-    // Gamma part: sum_j Gamma[i][j] Y[j][s], Y staged 32 rows at a time
+    // Gamma part: sum_j Gamma[i][j] Y[j][s], Y staged 32 rows at a time; the next 32 Gamma columns are
+    // prefetched into L2 (one bulk prefetch per column by the last warp) while this chunk is summed
     for (int j0 = 0; j0 < N; j0 += 32) {
       const int jw = min(32, N - j0);
+      if ((tid >> 5) == (T >> 5) - 1 && j0 + 32 + (tid & 31) < N)
+        bulk_prefetch_l2(gam + (size_t)(j0 + 32 + (tid & 31)) * N, (uint32_t)(N * sizeof(double2)));
       for (int e = tid; e < jw * NR; e += T) {
         const int jj = e % jw, sidx = e / jw;
         ys[jj * NR + sidx] = Y[(size_t)sidx * N + j0 + jj];
