@@ -75,15 +75,16 @@ __host__ __device__ inline size_t block_solve_bytes(int N, int NR) {
 
 struct BlockSmem {
   float* a_pl;    // [4][KAP] A planes (Re hi, Re lo, Im hi, Im lo) of L'; also the Gauss-Jordan workspace
-  float2* cbuf;   // [2][32][128] the C tiles of two strips in flight, column-major (aliases a_pl)
-  float* b_pl;    // [2][4][KBP] B planes of two strips in flight
+  float2* cbuf;   // [2][32][128] the C tiles of a strip pair, column-major (aliases a_pl)
+  float* b_pl;    // [2][4][KBP] B planes of a strip pair
   float2* y;      // solve phase: right-hand sides [NR][N]
   double2* ys;    // solve phase: [32][NR] staging of the residual
   double2* colsum;  // solve phase: [NR][NR]
   float2* sinv;   // solve phase: [2][32][K_DLD] staged diagonal inverses
   float2* zb;     // solve phase: [NR][32] D^-1 y_b of the forward solve
   float2* dinv;   // [32][K_DLD] current diagonal inverse, row-major
-  uint64_t* bar;  // [4] completion barriers: [0, 1] products of the tiles in flight, [2, 3] their bulk copies
+  uint64_t* bar;  // [4] completion barriers: [0] the products of a strip pair (four issuing threads), [1] the L'
+                  // product (two), [2] bulk copies of a pair's C tiles, [3] those of its B planes
   uint64_t* probe;  // test hook: a barrier nothing arrives on
   uint32_t* tslot;  // TMEM base address
   int* misc;      // [0] a wait ran out, [1] status bits of the item, [2] the item met a singular diagonal block
@@ -226,6 +227,7 @@ __device__ __forceinline__ void block_form_a(const StructuredSource& src, const 
   const double2* c0 = src.chi0_inv + ((size_t)wi.q * src.W + wi.w) * nv * NR * NR;
   const double2* uvq = src.uv + ((size_t)wi.ch * src.Q + wi.q) * NR * NR;
   const double ib2 = src.inv_beta2;
+  const uint64_t keep = l2_policy_evict_last();  // Gamma_r(w) is shared by every q of the (channel, w)
   for (int pass = 0; pass * RPT * KT < N; ++pass) {
     int ri[RPT], pr[RPT], vr[RPT];
     bool rok[RPT];
@@ -246,7 +248,7 @@ __device__ __forceinline__ void block_form_a(const StructuredSource& src, const 
       for (int u = 0; u < CPI; ++u)
 #pragma unroll
         for (int a = 0; a < RPT; ++a)
-          g[u][a] = (rok[a] && j0 + u < N) ? __ldcg(gam + (size_t)(j0 + u) * N + ri[a]) : make_double2(0.0, 0.0);
+          g[u][a] = (rok[a] && j0 + u < N) ? ld_d2_hint(gam + (size_t)(j0 + u) * N + ri[a], keep) : make_double2(0.0, 0.0);
 #pragma unroll
       for (int u = 0; u < CPI; ++u) {
         const int j = j0 + u;
@@ -445,10 +447,10 @@ __device__ __forceinline__ void block_l21(const float2* __restrict__ A, int N, i
     const int part = tid >> 5;
     tc_fence_after();
     issue_planar_part(tbase + 32 * part, s.a_pl, s.b_pl + 4 * KBP, part);
-    tc_commit(s.bar);
+    tc_commit(s.bar + 1);
   }
-  if (live) tc.issued(0);
-  const bool ok = live && tile_wait(s, tc, 0);
+  if (live) tc.issued(1);
+  const bool ok = live && tile_wait(s, tc, 1);
   tc_fence_after();
   if (ok) {
     float re[16], im[16];
@@ -474,79 +476,68 @@ __device__ __forceinline__ void block_l21(const float2* __restrict__ A, int N, i
   __syncthreads();
 }
 
-// Bulk copies of strip st's operands into buffer b (issued by warp 0): the B planes of the block row (16 KB, one
-// copy) and the C tile A[r0 : r0 + rows, c0 : c0 + 32] (one copy of rows x 8 bytes per column inside the matrix,
-// column-major in cbuf); all of them complete on load barrier 2 + b.  rows and r0 are even and N is even, so every
-// copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
-__device__ __forceinline__ void trailing_copies(const float2* __restrict__ A, int N, int NC, int r0, int rows, int c0,
-                                                const float* __restrict__ bsrc, BlockSmem& s, int b) {
+// Bulk copies (issued by one warp) of a strip pair's operands, strips st and st + 1 (if it exists) into buffers 0
+// and 1: the C tiles A[r0 : r0 + rows, c0 : c0 + 32] (one copy of rows x 8 bytes per column inside the matrix,
+// column-major in cbuf) on barrier 2, and the block row's B planes (16 KB per strip, one copy) on barrier 3.  rows
+// and r0 are even and N is even, so every copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
+__device__ __forceinline__ void copy_c_pair(const float2* __restrict__ A, int N, int NC, int r0, int rows, int c0,
+                                            BlockSmem& s) {
   const int lane = threadIdx.x & 31;
-  const int ncols = min(KTN, NC - c0);
-  uint64_t* bar = s.bar + 2 + b;
-  if (lane == 0)
-    mbar_expect_tx(bar, (uint32_t)(4 * KBP * sizeof(float)) + (uint32_t)(ncols * rows) * (uint32_t)sizeof(float2));
+  const int ncols = min(2 * KTN, NC - c0);
+  if (lane == 0) mbar_expect_tx(s.bar + 2, (uint32_t)(ncols * rows) * (uint32_t)sizeof(float2));
   __syncwarp();
-  if (lane == 0) bulk_g2s(s.b_pl + b * 4 * KBP, bsrc, 4 * KBP * sizeof(float), bar);
-  if (lane < ncols)
-    bulk_g2s(s.cbuf + (size_t)b * KTN * KTM + lane * KTM, A + (size_t)(c0 + lane) * N + r0,
-             (uint32_t)(rows * sizeof(float2)), bar);
+  const uint64_t pol = l2_policy_evict_first();  // the slot's matrix streams through L2
+  for (int c = lane; c < ncols; c += 32)
+    bulk_g2s_hint(s.cbuf + (size_t)c * KTM, A + (size_t)(c0 + c) * N + r0, (uint32_t)(rows * sizeof(float2)), s.bar + 2,
+                  pol);
+}
+__device__ __forceinline__ void copy_b_pair(const float* __restrict__ bsrc, int nstrips, BlockSmem& s) {
+  if ((threadIdx.x & 31) == 0) {
+    mbar_expect_tx(s.bar + 3, (uint32_t)(nstrips * 4 * KBP * sizeof(float)));
+    bulk_g2s(s.b_pl, bsrc, (uint32_t)(nstrips * 4 * KBP * sizeof(float)), s.bar + 3);
+  }
 }
 
 // Trailing update A[k1:N, k1:NC] -= (A[k1:N, k0:k1] D^-1) A[k0:k1, k1:NC]: per 128-row block, L' goes to the
-// tensor-memory A operand; then its 32-column strips run two in flight.  Strip st's B planes and C tile arrive by
-// bulk copy in buffer st & 1 (issued one strip ahead, once the product that read the buffer has completed).  Warp
-// roles in the strip loop: threads 0 and 32 issue the real and imaginary halves of each product (warps 0 and 1 do
-// nothing else); the other six warps move the C tiles between shared memory, tensor memory and A (a warp reaches
-// the TMEM lanes 32 (warp % 4) ..: warps 2, 3, 6, 7 one 16-column half each, warps 4 and 5 both halves of the
-// lanes of warps 0 and 1), and warp 2 issues the bulk copies.
+// tensor-memory A operand; then its 32-column strips go two at a time.  A strip pair's C tiles and B planes arrive
+// by bulk copy; all eight warps move the C tiles into tensor memory (warp w: TMEM lanes 32 (w % 4) .., tile w / 4);
+// threads 0, 32, 64, 96 issue the real and imaginary halves of the two tiles' products (a single thread issues a
+// tcgen05.mma only every ~50 cycles or more, so the products of a pair go out four at a time); once they have
+// completed, the next pair's B planes are copied in (its C tiles went out as soon as this pair's had moved on) and
+// all warps move the results back to A.  The second CTA on the SM fills the tensor pipe while this one moves tiles.
 __device__ __forceinline__ void block_trailing(float2* __restrict__ A, int N, int NC, int k0, int k1, BlockSmem& s,
-                               const float* __restrict__ bop, const float2* __restrict__ dinv, TileCount& tc) {
+                                               const float* __restrict__ bop, const float2* __restrict__ dinv,
+                                               TileCount& tc) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (k1 >= N) return;
-  const int nrb = (N - k1 + KTM - 1) / KTM, nst = (NC - k1 + KTN - 1) / KTN;
+  const int nrb = (N - k1 + KTM - 1) / KTM, nst = (NC - k1 + KTN - 1) / KTN, npair = (nst + 1) / 2;
   const uint32_t tbase = *s.tslot;
   const uint32_t tl = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
   const int row_t = 32 * (warp & 3) + lane;  // this thread's tile row (its TMEM lane)
-  const bool mover = warp >= 2;
-  const int h0 = (warp == 4 || warp == 5) ? 0 : (warp >> 2), h1 = (warp == 4 || warp == 5) ? 1 : (warp >> 2);
-  constexpr int COPIER = 2;
-  // the product of strip st back to A once it has completed; `then` runs between the wait and the epilogue
-  auto finish = [&](int r0, int st, auto&& then) {
-    const int b = st & 1;
-    const bool ok = tile_wait(s, tc, b);
-    tc_fence_after();
-    then(ok);
-    if (!ok || !mover) return;
-    for (int hh = h0; hh <= h1; ++hh) {
-      float re[16], im[16];
-      tmem_ld16(tl + 64 * b + 16 * hh, re);
-      tmem_ld16(tl + 64 * b + 32 + 16 * hh, im);
-      tmem_wait_ld();
-      const int r = r0 + row_t, cb = k1 + st * KTN + 16 * hh;
-      if (r < N) {
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj)
-          if (cb + jj < NC) A[(size_t)(cb + jj) * N + r] = make_float2(re[jj], im[jj]);
-      }
-    }
-  };
+  const int tile = warp >> 2;                // the tile of the pair this warp moves
+  constexpr int COPIER = KW - 1;
   for (int rb = 0; rb < nrb; ++rb) {
     const int r0 = k1 + rb * KTM, rows = min(KTM, N - r0);
     block_l21(A, N, r0, k0, dinv, s, tc);  // every product of the previous row block has completed
     if (s.misc[0] == 0) {
       if (warp == COPIER) {
-        trailing_copies(A, N, NC, r0, rows, k1, bop, s, 0);
-        if (nst > 1) trailing_copies(A, N, NC, r0, rows, k1 + KTN, bop + 4 * KBP, s, 1);
+        copy_c_pair(A, N, NC, r0, rows, k1, s);
+        copy_b_pair(bop, min(2, nst), s);
       }
       tc.issued(2);
-      if (nst > 1) tc.issued(3);
+      tc.issued(3);
     }
-    for (int st = 0; st < nst; ++st) {
-      const int b = st & 1, c0 = k1 + st * KTN;
-      if (warp == KW - 1 && st + 2 < nst) prefetch_tile_l2(A, N, NC, r0, c0 + 2 * KTN);
-      if (tile_wait(s, tc, 2 + b) && mover) {  // C tile -> TMEM buffer b
-        for (int hh = h0; hh <= h1; ++hh) {
-          const float2* cb = s.cbuf + (size_t)b * KTN * KTM + (16 * hh) * KTM + row_t;
+    for (int p = 0; p < npair; ++p) {
+      const int st = 2 * p + tile, c0 = k1 + st * KTN;
+      const bool has = st < nst;  // this warp's tile exists (the last pair may hold one strip)
+      if (warp == KW - 2 && 2 * p + 4 < nst) {
+        prefetch_tile_l2(A, N, NC, r0, k1 + (2 * p + 4) * KTN);
+        if (2 * p + 5 < nst) prefetch_tile_l2(A, N, NC, r0, k1 + (2 * p + 5) * KTN);
+      }
+      if (tile_wait(s, tc, 2) && has) {  // C tile -> TMEM: row row_t, 32 complex columns
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+          const float2* cb = s.cbuf + (size_t)(tile * KTN + 16 * hh) * KTM + row_t;
           float re[16], im[16];
 #pragma unroll
           for (int jj = 0; jj < 16; ++jj) {
@@ -554,33 +545,58 @@ __device__ __forceinline__ void block_trailing(float2* __restrict__ A, int N, in
             re[jj] = x.x;
             im[jj] = x.y;
           }
-          tmem_st16(tl + 64 * b + 16 * hh, re);
-          tmem_st16(tl + 64 * b + 32 + 16 * hh, im);
+          tmem_st16(tl + 64 * tile + 16 * hh, re);
+          tmem_st16(tl + 64 * tile + 32 + 16 * hh, im);
         }
         tmem_wait_st();
       }
+      tile_wait(s, tc, 3);
       tc_fence_before();
       __syncthreads();
       const bool live = s.misc[0] == 0;
-      if (live && (tid == 0 || tid == 32)) {
-        const int part = tid >> 5;
-        tc_fence_after();
-        issue_planar_tmem_part(tbase + 64 * b + 32 * part, tbase + K_A_COL, s.b_pl + b * 4 * KBP, part);
-        tc_commit(s.bar + b);
-      }
-      if (live) tc.issued(b);
-      if (st > 0 && live) {
-        // once strip st - 1's product has completed, its buffers take strip st + 1 (before the epilogue's stores)
-        finish(r0, st - 1, [&](bool ok) {
-          if (st + 1 < nst) {
-            if (warp == COPIER && ok)
-              trailing_copies(A, N, NC, r0, rows, c0 + KTN, bop + (size_t)(st + 1) * 4 * KBP, s, b ^ 1);
-            tc.issued(2 + (b ^ 1));
+      if (live) {
+        if (tid < 128 && lane == 0) {  // threads 0, 32, 64, 96: tile tid / 64, part (tid / 32) % 2
+          const int t = tid >> 6, part = (tid >> 5) & 1;
+          if (2 * p + t < nst) {
+            tc_fence_after();
+            issue_planar_tmem_part(tbase + 64 * t + 32 * part, tbase + K_A_COL, s.b_pl + t * 4 * KBP, part);
+            tc_commit(s.bar);
+          } else {
+            mbar_arrive(s.bar);
           }
-        });
+        }
+        tc.issued(0);
+        // the pair's C buffers have moved on: the next pair's C tiles go out now
+        if (p + 1 < npair) {
+          if (warp == COPIER) copy_c_pair(A, N, NC, r0, rows, k1 + (2 * p + 2) * KTN, s);
+          tc.issued(2);
+        }
+        const bool done = tile_wait(s, tc, 0);
+        tc_fence_after();
+        // the products have completed: the next pair's B planes go out, then the results go back to A
+        if (p + 1 < npair) {
+          if (warp == COPIER && done) copy_b_pair(bop + (size_t)(2 * p + 2) * 4 * KBP, min(2, nst - 2 * p - 2), s);
+          tc.issued(3);
+        }
+        if (done && has) {
+          const int r = r0 + row_t;
+          const uint64_t pol = l2_policy_evict_first();
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            float re[16], im[16];
+            tmem_ld16(tl + 64 * tile + 16 * hh, re);
+            tmem_ld16(tl + 64 * tile + 32 + 16 * hh, im);
+            tmem_wait_ld();
+            const int cb = c0 + 16 * hh;
+            if (r < N) {
+#pragma unroll
+              for (int jj = 0; jj < 16; ++jj)
+                if (cb + jj < NC) st_f2_hint(A + (size_t)(cb + jj) * N + r, make_float2(re[jj], im[jj]), pol);
+            }
+          }
+        }
       }
     }
-    if (s.misc[0] == 0) finish(r0, nst - 1, [](bool) {});
     tc_fence_before();
     __syncthreads();
   }
@@ -769,7 +785,7 @@ __device__ __forceinline__ void block_kernel_begin(BlockSmem& s) {
   if (threadIdx.x == 0) {
     s.misc[0] = 0;
 #pragma unroll
-    for (int b = 0; b < K_NBAR; ++b) mbar_init(s.bar + b, b < 2 ? 2u : 1u);  // products: two issuing threads
+    for (int b = 0; b < K_NBAR; ++b) mbar_init(s.bar + b, b == 0 ? 4u : b == 1 ? 2u : 1u);  // issuing threads
     if (s.inject) mbar_init(s.probe);
   }
   if ((threadIdx.x >> 5) == 0) tc_alloc(s.tslot, K_TMEM_COLS);

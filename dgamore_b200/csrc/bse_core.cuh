@@ -124,6 +124,7 @@ __device__ void structured_residual_permuted(const StructuredSource& src, int ch
   __syncthreads();
   const double2* gam = src.gamma_cm + (size_t)(ch * src.W + w) * N * N;
   const double2* uvq = src.uv + ((size_t)ch * src.Q + q) * n2 * n2;
+  const uint64_t keep = l2_policy_evict_last();  // Gamma_r(w) is shared by every q of the (channel, w)
   for (int pos0 = 0; pos0 < N; pos0 += T) {
     const int pos = pos0 + tid;
     const bool active = pos < N;
@@ -147,7 +148,7 @@ __device__ void structured_residual_permuted(const StructuredSource& src, int ch
           double2 g[8];
 #pragma unroll
           for (int u = 0; u < 8; ++u)
-            g[u] = (jj0 + u < jw) ? __ldcg(gam + (size_t)(j0 + jj0 + u) * N + i) : make_double2(0.0, 0.0);
+            g[u] = (jj0 + u < jw) ? ld_d2_hint(gam + (size_t)(j0 + jj0 + u) * N + i, keep) : make_double2(0.0, 0.0);
 #pragma unroll
           for (int u = 0; u < 8; ++u)
             if (jj0 + u < jw) {
