@@ -1091,12 +1091,12 @@ static size_t mixed_smem_bytes(int N, int n2) { return mixed_colsum_offset(N) + 
 static size_t mixed_slot_bytes(int N, int n2) {
   return (((size_t)N * N * sizeof(float2) + 255) & ~(size_t)255) + 2 * (size_t)N * n2 * sizeof(double2);
 }
-// Default launch of the mixed form: below N = 320 the 128-thread kernel keeps several items per SM in flight and
-// wins; above it the shared-memory-panel kernel with tensor-core trailing tiles (3), if its shared memory fits,
-// else the panel kernel with FP32 tiles (1), else the 128-thread kernel (2).
+// Default launch of the mixed form: the block-form kernel (4) wherever its solve phase fits shared memory (it is
+// the fastest at every size measured, N = 40 to 720); else, from N = 320, the shared-memory-panel kernel with
+// tensor-core trailing tiles (3) or FP32 tiles (1), else the 128-thread kernel (2).
 static int default_mixed_kernel(int N, int n2) {
-  if (N < 320) return 2;
   if (dga_block_supported(N, n2)) return 4;
+  if (N < 320) return 2;
   if (dga_panel_supported(N, n2, true)) return 3;
   if (dga_panel_supported(N, n2)) return 1;
   return 2;
@@ -1285,10 +1285,11 @@ int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_
 // ------------------------------------------------------------------------------------------------
 // Launch geometry of a batch.  In the mixed form every request must have the same default kernel as when it runs
 // alone (default_mixed_kernel), so that a request's results are the same in a batch and alone; *kernel receives
-// it (1, 3: shared-memory panel, 2: 128-thread kernel; always 2 in FP64).  Returns false for an invalid batch.
-// Problems may differ in orbital count (*n2_max receives the largest n_orb^2, *hetero whether they differ); such a
-// batch runs the 128-thread kernels with the right-hand-side count chosen per item, so in the mixed form every
-// problem of it must take the 128-thread kernel alone too (N below 320).
+// it (1, 3: shared-memory panel, 4: block form, 2: 128-thread kernel; always 2 in FP64).  Returns false for an
+// invalid batch.  Problems may differ in orbital count (*n2_max receives the largest n_orb^2, *hetero whether they
+// differ); such a batch runs kernels that choose the right-hand-side count per item: the 128-thread kernels, or
+// the block-form kernel for orbital counts 1 to 3 (the 4-orbital block kernel is compiled alone).  The
+// shared-memory-panel kernels take one orbital count per launch.
 static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int* n_max, size_t* slot, int* kernel,
                        int* n2_max = nullptr, bool* hetero = nullptr) {
   *n_max = 0;
@@ -1311,7 +1312,7 @@ static bool batch_dims(const dga_bse_problem* probs, int n_prob, int mixed, int*
     if (n2 > n2m) n2m = n2;
   }
   const bool panel = *kernel != 2;
-  if (het && panel) return false;
+  if (het && panel && (*kernel != 4 || n2m > 9)) return false;
   for (int p = 0; p < n_prob; ++p) {
     const int n2 = probs[p].n_orb * probs[p].n_orb;
     const int N = n2 * 2 * probs[p].niv;
@@ -1365,7 +1366,8 @@ size_t dga_bse_batch_scratch_bytes(const dga_bse_problem* probs, int n_prob, int
   const int n2 = probs[0].n_orb * probs[0].n_orb;
   const bool panel = kernel != 2;
   if (panel)
-    return (size_t)(kernel == 4 ? dga_block_grid(n2, n_items) : dga_panel_batch_grid(n2, n_max, n_items, kernel == 3)) *
+    return (size_t)(kernel == 4 ? dga_block_grid(hetero ? 0 : n2, n_items)
+                                : dga_panel_batch_grid(n2, n_max, n_items, kernel == 3)) *
            slot;
   if (hetero) return (size_t)batch_grid_hetero(mixed, n_items, batch_smem(n_max, n2_max, mixed)) * slot;
   return (size_t)batch_grid_any(mixed, n2, n_items, batch_smem(n_max, n2, mixed)) * slot;
@@ -1388,7 +1390,8 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   if (!probs_host || !probs_dev || !work || !scratch || !status || n_items <= 0 || max_iter < 0 || mode < 0 ||
       mode > 2 || !batch_dims(probs_host, n_prob, mixed, &n_max, &slot, &kernel, &n2_max, &hetero)) {
     dga_set_error("dga_bse_solve_sum_batch_c128: invalid arguments (n_orb in {1,2,3,4}; in the mixed form all "
-                  "problems have N below 320 or all from 320 up, and problems of different n_orb all below 320)");
+                  "problems take the same default kernel, and problems of different n_orb take the block-form or "
+                  "the 128-thread kernel with n_orb at most 3)");
     return DGA_ERR_ARG;
   }
   for (int p = 0; p < n_prob; ++p) {
@@ -1401,7 +1404,8 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   const int n2 = probs_host[0].n_orb * probs_host[0].n_orb;
   const size_t smem = batch_smem(n_max, hetero ? n2_max : n2, mixed);
   const bool panel = kernel != 2;
-  int grid = panel    ? (kernel == 4 ? dga_block_grid(n2, n_items) : dga_panel_batch_grid(n2, n_max, n_items, kernel == 3))
+  int grid = panel    ? (kernel == 4 ? dga_block_grid(hetero ? 0 : n2, n_items)
+                                     : dga_panel_batch_grid(n2, n_max, n_items, kernel == 3))
              : hetero ? batch_grid_hetero(mixed, n_items, smem)
                       : batch_grid_any(mixed, n2, n_items, smem);
   if (scratch_bytes < slot) {
@@ -1415,8 +1419,8 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
   unsigned char* sc = (unsigned char*)scratch;
   if (panel) {
     cudaError_t err =
-        kernel == 4 ? dga_block_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
-                                             stream)
+        kernel == 4 ? dga_block_batch_launch(grid, hetero ? 0 : n2, pd, wk, n_items, n_max, max_iter, tol, status,
+                                             iters, sc, slot, stream)
                     : dga_panel_batch_launch(grid, n2, pd, wk, n_items, n_max, max_iter, tol, status, iters, sc, slot,
                                              stream, kernel == 3);
     if (err != cudaSuccess) {
@@ -1464,6 +1468,12 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
 }
 
 }  // extern "C"
+
+extern "C" int dga_bse_default_kernel(int n_orb, int niv, int mixed) {
+  const int n2 = n_orb * n_orb, N = n2 * 2 * niv;
+  if (n_orb <= 0 || niv <= 0 || !supported_rhs(n2) || N > BSE_MAX_N) return -1;
+  return mixed ? default_mixed_kernel(N, n2) : 2;
+}
 
 // ------------------------------------------------------------------------------------------------
 // Tuned entry: the same solves with an explicit kernel choice and CTAs per SM (the autotuner's knobs)

@@ -848,8 +848,29 @@ __global__ void __launch_bounds__(KT, 2)
   }
 }
 
-// Heterogeneous batch (requests of one orbital count, see bse_multi_kernel in bse.cu): each item reads its
-// request's descriptor; shared memory and the scratch slot are sized for the largest request of the launch.
+// Batches (see bse_multi_kernel in bse.cu): each item reads its request's descriptor; shared memory and the
+// scratch slot are sized for the largest request of the launch.  bse_block_multi_kernel<NR> takes one orbital
+// count; bse_block_multi_any_kernel chooses the right-hand-side count per item (orbital counts 1 to 3).
+template <int NR>
+__device__ __forceinline__ void block_batch_item(const dga_bse_problem& d, const MultiItem& mi, int max_iter,
+                                                 double tol, unsigned char* slot, unsigned char* smem_raw,
+                                                 long long wait_limit, TileCount& tc, int* st, int* it) {
+  StructuredSource src;
+  src.gamma_cm = (const double2*)d.gamma_cm;
+  src.chi0_inv = (const double2*)d.chi0_inv;
+  src.uv = (const double2*)d.uv;
+  src.n2 = NR;
+  src.nv = 2 * d.niv;
+  src.W = d.niw_half;
+  src.Q = d.n_q;
+  src.inv_beta2 = d.inv_beta2;
+  const int N = NR * src.nv;
+  BlockSmem s(smem_raw, N, NR, wait_limit);  // the same shared memory, solve-phase offsets for this N
+  const WorkItem wi{mi.ch, mi.q, mi.w};
+  double2* o = (double2*)d.out + (((size_t)wi.ch * src.Q + wi.q) * src.W + wi.w) * (size_t)N * NR;
+  *st = solve_item_block<NR>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, tc, it);
+}
+
 template <int NR>
 __global__ void __launch_bounds__(KT, 2)
     bse_block_multi_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work,
@@ -870,22 +891,45 @@ __global__ void __launch_bounds__(KT, 2)
       continue;
     }
     const MultiItem mi = work[item];
+    int st = 0, it = 0;
+    block_batch_item<NR>(probs[mi.prob], mi, max_iter, tol, slot, smem_raw, wait_limit, tc, &st, &it);
+    if (threadIdx.x == 0) {
+      status[item] = st;
+      if (iters) iters[item] = it;
+    }
+  }
+  if (!block_kernel_end(s0, tc)) {
+    for (int item = blockIdx.x + threadIdx.x * gridDim.x; item < n_items; item += blockDim.x * gridDim.x)
+      atomicOr(status + item, DGA_ITEM_WAIT_TIMEOUT);
+  }
+}
+
+__global__ void __launch_bounds__(KT, 2)
+    bse_block_multi_any_kernel(const dga_bse_problem* __restrict__ probs, const MultiItem* __restrict__ work,
+                               int n_items, int n_max, int max_iter, double tol, int* __restrict__ status,
+                               int* __restrict__ iters, unsigned char* __restrict__ scratch, size_t slot_bytes,
+                               long long wait_limit) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  BlockSmem s0(smem_raw, n_max, 1, wait_limit);
+  unsigned char* slot = scratch + (size_t)blockIdx.x * slot_bytes;
+  TileCount tc;
+  block_kernel_begin(s0);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (s0.misc[0]) {
+      if (threadIdx.x == 0) {
+        status[item] = DGA_ITEM_WAIT_TIMEOUT;
+        if (iters) iters[item] = 0;
+      }
+      continue;
+    }
+    const MultiItem mi = work[item];
     const dga_bse_problem d = probs[mi.prob];
-    StructuredSource src;
-    src.gamma_cm = (const double2*)d.gamma_cm;
-    src.chi0_inv = (const double2*)d.chi0_inv;
-    src.uv = (const double2*)d.uv;
-    src.n2 = NR;
-    src.nv = 2 * d.niv;
-    src.W = d.niw_half;
-    src.Q = d.n_q;
-    src.inv_beta2 = d.inv_beta2;
-    const int N = NR * src.nv;
-    BlockSmem s(smem_raw, N, NR, wait_limit);  // the same shared memory, solve-phase offsets for this N
-    const WorkItem wi{mi.ch, mi.q, mi.w};
-    double2* o = (double2*)d.out + (((size_t)wi.ch * src.Q + wi.q) * src.W + wi.w) * (size_t)N * NR;
-    int it = 0;
-    const int st = solve_item_block<NR>(src, wi, N, src.nv, d.beta, max_iter, tol, o, slot, s, tc, &it);
+    int st = 0, it = 0;
+    switch (d.n_orb) {
+      case 1: block_batch_item<1>(d, mi, max_iter, tol, slot, smem_raw, wait_limit, tc, &st, &it); break;
+      case 2: block_batch_item<4>(d, mi, max_iter, tol, slot, smem_raw, wait_limit, tc, &st, &it); break;
+      default: block_batch_item<9>(d, mi, max_iter, tol, slot, smem_raw, wait_limit, tc, &st, &it); break;
+    }
     if (threadIdx.x == 0) {
       status[item] = st;
       if (iters) iters[item] = it;
@@ -968,8 +1012,10 @@ extern "C" int dga_bse_block_ctas_per_sm(int n2) {
   }
 }
 
+// n2 = 0: the batch kernel that chooses the right-hand-side count per item (same launch bounds and shared memory).
 int dga_block_grid(int n2, int n_items) {
   switch (n2) {
+    case 0: return block_grid_nr<9>(n_items);
     case 1: return block_grid_nr<1>(n_items);
     case 4: return block_grid_nr<4>(n_items);
     case 9: return block_grid_nr<9>(n_items);
@@ -1010,6 +1056,13 @@ cudaError_t dga_block_batch_launch(int grid, int n2, const dga_bse_problem* prob
                                                           iters, scratch, slot_bytes, wait_limit);                 \
     break;
   switch (n2) {
+    case 0:  // orbital counts 1 to 3 in one launch
+      cudaFuncSetAttribute(bse_block_multi_any_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(bse_block_multi_any_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
+      bse_block_multi_any_kernel<<<grid, KT, smem, stream>>>(probs, work, n_items, n_max, max_iter, tol, status,
+                                                             iters, scratch, slot_bytes, wait_limit);
+      break;
     DGA_BLOCK_CASE(1)
     DGA_BLOCK_CASE(4)
     DGA_BLOCK_CASE(9)

@@ -10,7 +10,7 @@ temperatures, interactions -- on one GPU is done here the way LLM servers batch 
   server's budget next to the requests already running; otherwise it waits in FIFO order.
 * **One persistent launch per iteration.**  Every iteration gathers BSE work items (request, channel, q, w)
   from all running requests of the same launch class (orbital count; in the mixed form also the side of
-  ``PANEL_MIN_N`` the compound size is on) into one ``dga_bse_solve_sum_batch_c128`` launch.
+  the compound size takes) into one ``dga_bse_solve_sum_batch_c128`` launch.
   Items are taken round-robin, a bounded number per request per iteration (``items_per_request``), so a
   small request that arrives while a large one runs finishes in a few iterations instead of waiting for
   the large one to drain (the chunked scheduling of long prompts in LLM serving).
@@ -48,16 +48,16 @@ def _stream() -> ctypes.c_void_p:
 
 # Compound size from which the mixed form runs the shared-memory-panel kernel when alone (the library's default
 # rule); a batch launch serves requests on one side of it only, so each gets the kernel it gets alone.
-PANEL_MIN_N = 320
-
-
 def launch_class(lp: LadderPass, precision: str) -> tuple:
-    """Requests of one class share a batch launch.  The 128-thread kernels (the FP64 form, and the mixed form
-    below PANEL_MIN_N) choose the right-hand-side count per item, so their requests share one launch whatever
-    their orbital counts; the shared-memory-panel kernel of the mixed form (from PANEL_MIN_N up) is compiled per
-    orbital count, so there the class also holds n_orb."""
-    panel = precision == "mixed" and lp.sh.N >= PANEL_MIN_N
-    return (precision, panel, lp.sh.n_orb if panel else 0)
+    """Requests of one class share a batch launch: the same kernel as each would take alone
+    (dga_bse_default_kernel), so that a request's results are bitwise the same in a batch and alone.  The
+    128-thread kernels and the mixed form's block kernel for 1 to 3 orbitals choose the right-hand-side count per
+    item, so their requests share one launch whatever their orbital counts; the shared-memory-panel kernels and
+    the 4-orbital block kernel are compiled per orbital count, so there the class also holds n_orb."""
+    mixed = precision == "mixed"
+    kernel = int(lib().dga_bse_default_kernel(lp.sh.n_orb, lp.sh.niv, 1 if mixed else 0))
+    per_orbital = kernel in (1, 3) or (kernel == 4 and lp.sh.n_orb > 3)
+    return (precision, kernel, lp.sh.n_orb if per_orbital else 0)
 
 
 def item_cost(sh: PassShapes) -> float:
@@ -147,8 +147,7 @@ class BseBatch:
 
 def solve_bse_batch(passes: list[LadderPass], precision: str = "fp64", scratch: torch.Tensor | None = None,
                     **kw) -> None:
-    """BSE of several whole passes (all their items), one launch per launch class (orbital count, and in the
-    mixed form the side of PANEL_MIN_N)."""
+    """BSE of several whole passes (all their items), one launch per launch class (``launch_class``)."""
     groups: dict[tuple, list[LadderPass]] = {}
     for lp in passes:
         groups.setdefault(launch_class(lp, precision), []).append(lp)
@@ -164,8 +163,8 @@ def solve_bse_batch(passes: list[LadderPass], precision: str = "fp64", scratch: 
 
 class BatchedPasses:
     """Whole nonlocal passes of several requests as one device schedule: every pass's pre-BSE stages, one batch
-    launch per launch class over all their BSE items (requests of different orbital counts below N = 320 -- the
-    2-orbital bilayer next to a 1-orbital lattice, say -- share a single launch), every pass's post-BSE stages.
+    launch per launch class over all their BSE items (requests of different orbital counts -- the 2-orbital
+    bilayer next to a 1-orbital lattice, say -- share a single launch), every pass's post-BSE stages.
     ``capture()`` records the whole schedule in one CUDA graph; ``replay()`` runs it again on refreshed inputs
     (the passes' resident G(k) and vertices are read in place)."""
 

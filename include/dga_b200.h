@@ -92,15 +92,21 @@ int dga_bse_solve_sum_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, 
  * trailing updates, then FP64 iterative refinement -- residuals r = S - A Y with A formed in FP64 from Gamma_r,
  * chi0^-1 and U_r + V_r^q -- until the correction, or the error left after it estimated from the observed
  * contraction rho = |d_k|/|d_(k-1)| as |d_k| rho/(1-rho), is at most tol max|Y|, or max_iter corrections; items
- * that do not converge are flagged DGA_ITEM_NOCONVERGE.  Items with 320 <= N <= about 790 run the
- * shared-memory-panel kernel (one 512-thread CTA per SM) with tensor-core trailing tiles, the others the
- * 128-thread kernel.  Replaces the same upstream functions as dga_bse_solve_sum_c128.  iters: optional per-item
- * number of corrections. */
+ * that do not converge are flagged DGA_ITEM_NOCONVERGE.  The launch runs the block-form kernel (kernel 4 of
+ * dga_bse_tuning) wherever its solve phase fits shared memory (every size of the benchmark configurations; see
+ * dga_bse_default_kernel), else the shared-memory-panel kernel (320 <= N <= about 790) or the 128-thread kernel.
+ * Replaces the same upstream functions as dga_bse_solve_sum_c128.  iters: optional per-item number of
+ * corrections. */
 size_t dga_bse_mixed_scratch_bytes(int N, int n2, int n_items);
 int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
                                  const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
                                  int n_items, int max_iter, double tol, void* out, int* status, int* iters,
                                  void* scratch, size_t scratch_bytes, dga_stream_t stream);
+
+/* The kernel a single request of n_orb orbitals and niv positive fermionic frequencies takes by default (the
+ * kernel numbers of dga_bse_tuning; the FP64 form always 2); -1 for an unsupported size.  A batch launch runs each
+ * request with this same kernel, so requests whose defaults differ go to different launches. */
+int dga_bse_default_kernel(int n_orb, int niv, int mixed);
 
 /* FP64 re-solve of the items a mixed launch flagged (status & (NOCONVERGE | NONFINITE | WAIT_TIMEOUT)), leaving the others
  * untouched; at most grid_limit CTAs (scratch: grid_limit * (N*N + N*n2) complex128). */
@@ -110,12 +116,13 @@ int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_c
                               dga_stream_t stream);
 
 /* Launch choices of the BSE solvers, the search space of the autotuner (dgamore_b200/autotune.py); no
- * counterpart in the upstream.  kernel: 0 = default (mixed form: kernel 3 for 320 <= N when it fits, else the
- * 128-thread kernel; FP64: the 128-thread kernel), 1 = shared-memory-panel kernel (mixed form only,
- * N up to about 790), 2 = 128-thread kernel, 3 = shared-memory-panel kernel whose trailing tiles run on the
- * tensor cores (tcgen05.mma kind::tf32 with a three-term split for FP32-level products, accumulators in tensor
- * memory; mixed form only); ctas_per_sm: CTAs per SM of the 128-thread kernel (0 = all that fit).  The choices
- * change the speed only: every choice computes the same solves (the mixed ones to the refinement tolerance). */
+ * counterpart in the upstream.  kernel: 0 = default (dga_bse_default_kernel), 1 = shared-memory-panel kernel
+ * (mixed form only, N up to about 790), 2 = 128-thread kernel, 3 = shared-memory-panel kernel whose trailing
+ * tiles run on the tensor cores (tcgen05.mma kind::tf32 with a three-term split for FP32-level products,
+ * accumulators in tensor memory; mixed form only), 4 = block-form kernel (pivoting inside 32 x 32 diagonal
+ * blocks, every update on the tensor cores, two 256-thread CTAs per SM; mixed form only); ctas_per_sm: CTAs per
+ * SM of the 128-thread kernel (0 = all that fit).  The choices change the speed only: every choice computes the
+ * same solves (the mixed ones to the refinement tolerance). */
 typedef struct {
   int kernel;
   int ctas_per_sm;
@@ -149,9 +156,11 @@ typedef struct {
 
 /* Ladder BSE of several requests in ONE persistent launch (the serving path's continuous batch; the upstream
  * runs one create_auxiliary_chi_r_q_sum call per request, dgamore/nonlocal_sde.py:85-156).  Requests may differ
- * in niv, niw, Q, beta, inputs and n_orb (1..4): the 128-thread kernels choose the right-hand-side count per item,
- * so in the FP64 form, and in the mixed form when every request has N < 320, any orbital counts share a launch;
- * mixed-form requests with N >= 320 (shared-memory-panel kernel) must share n_orb.  probs_host: the descriptors on the host (launch
+ * in niv, niw, Q, beta, inputs and n_orb (1..4), but every request must take the same default kernel
+ * (dga_bse_default_kernel).  The 128-thread kernels (the FP64 form) and the mixed form's block kernel for 1 to 3
+ * orbitals choose the right-hand-side count per item, so their requests share a launch whatever their orbital
+ * counts; the shared-memory-panel kernels and the 4-orbital block kernel take one n_orb per launch.
+ * probs_host: the descriptors on the host (launch
  * geometry); probs_dev: the same array copied to device memory; work: [n_items][4] ints (request, ch, q, w);
  * mode 0 runs the FP64 LU of dga_bse_solve_sum_c128, mode 1 the FP32 LU + FP64 refinement of
  * dga_bse_solve_sum_mixed_c128 (max_iter, tol), mode 2 the FP64 re-solve of the items a mode-1 launch flagged;

@@ -58,11 +58,12 @@ def test_batch_descriptor_matches_the_c_struct():
 
 def test_batch_rejects_unsupported_mixes_without_launching():
     lib = _lib.lib()
-    # orbital counts may differ where the 128-thread kernels run; the mixed form's panel kernel (N >= 320) is
-    # compiled per orbital count, so a mixed-precision batch of 2- and 3-orbital problems of that size is refused
+    # orbital counts may differ where the kernels choose the right-hand-side count per item (the 128-thread
+    # kernels, and the mixed form's block kernel for 1 to 3 orbitals); the 4-orbital block kernel is compiled
+    # alone, so a mixed-precision batch of 4- and 2-orbital problems is refused
     arr = (_lib.BseProblem * 2)(
+        _lib.BseProblem(n_orb=4, niv=10, niw_half=3, n_q=2, beta=1.0),
         _lib.BseProblem(n_orb=2, niv=40, niw_half=3, n_q=2, beta=1.0),
-        _lib.BseProblem(n_orb=3, niv=20, niw_half=3, n_q=2, beta=1.0),
     )
     assert lib.dga_bse_batch_scratch_bytes(arr, 2, 10, 1) == 0
     rc = lib.dga_bse_solve_sum_batch_c128(arr, None, 2, None, 10, 1, 0, 0.0, None, None, None, 0, None)
