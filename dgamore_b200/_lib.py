@@ -23,6 +23,7 @@ SIGNATURES = {
     "dga_device_sm_count": (I, []),
     "dga_bse_block_ctas_per_sm": (I, [I]),
     "dga_bse_default_kernel": (I, [I, I, I]),
+    "dga_bse_preload": (I, []),
     "dga_last_error_string": (_c.c_char_p, []),
     "dga_strided_copy_c128": (I, [VP, VP, I, PLL, PLL, PLL, D, VP]),
     "dga_dft_planes_c128": (I, [VP, LL, LL, LL, VP, LL, LL, LL, I, I, I, I, I, VP, D, VP]),

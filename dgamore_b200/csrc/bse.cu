@@ -1469,6 +1469,15 @@ int dga_bse_solve_sum_batch_c128(const dga_bse_problem* probs_host, const void* 
 
 }  // extern "C"
 
+// Loads the code of the block-form BSE kernels ahead of their first launch (see include/dga_b200.h).
+extern "C" int dga_bse_preload(void) {
+  if (dga_block_preload()) {
+    dga_set_error("dga_bse_preload: a kernel could not be loaded: %s", cudaGetErrorString(cudaGetLastError()));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
 extern "C" int dga_bse_default_kernel(int n_orb, int niv, int mixed) {
   const int n2 = n_orb * n_orb, N = n2 * 2 * niv;
   if (n_orb <= 0 || niv <= 0 || !supported_rhs(n2) || N > BSE_MAX_N) return -1;

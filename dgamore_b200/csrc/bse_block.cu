@@ -1012,6 +1012,23 @@ extern "C" int dga_bse_block_ctas_per_sm(int n2) {
   }
 }
 
+// Loads every block-form kernel now (CUDA loads a kernel's code at its first launch otherwise, which can take tens
+// of milliseconds for these): cudaFuncGetAttributes brings each function in.
+int dga_block_preload() {
+  cudaFuncAttributes fa;
+  int bad = 0;
+  bad |= cudaFuncGetAttributes(&fa, bse_block_multi_any_kernel) != cudaSuccess;
+#define DGA_BLOCK_LOAD(R)                                                               \
+  bad |= cudaFuncGetAttributes(&fa, bse_block_mixed_kernel<R>) != cudaSuccess;          \
+  bad |= cudaFuncGetAttributes(&fa, bse_block_multi_kernel<R>) != cudaSuccess;
+  DGA_BLOCK_LOAD(1)
+  DGA_BLOCK_LOAD(4)
+  DGA_BLOCK_LOAD(9)
+  DGA_BLOCK_LOAD(16)
+#undef DGA_BLOCK_LOAD
+  return bad;
+}
+
 // n2 = 0: the batch kernel that chooses the right-hand-side count per item (same launch bounds and shared memory).
 int dga_block_grid(int n2, int n_items) {
   switch (n2) {

@@ -194,6 +194,7 @@ cudaError_t dga_panel_launch(int grid, const dga::StructuredSource& src, const d
 // Host side of the block-form mixed kernel (bse_block.cu): pivoting restricted to 32 x 32 diagonal blocks, every
 // update on the tensor cores, two 256-thread CTAs per SM.
 bool dga_block_supported(int N, int n2);
+int dga_block_preload();  // nonzero if a kernel could not be loaded
 size_t dga_block_slot_bytes(int N, int n2);
 int dga_block_grid(int n2, int n_items);
 cudaError_t dga_block_launch(int grid, const dga::StructuredSource& src, const dga::WorkItem* work, int n_items, int N,

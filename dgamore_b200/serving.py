@@ -282,8 +282,9 @@ class LadderServer:
 
     def __init__(self, hbm_budget: int, scratch_bytes: int = 4 << 30, items_per_request: int | None = 256,
                  device: str = "cuda", refine_max_iter: int = 6, refine_tol: float = 1e-10):
-        lib()
         self.dev = torch.device(device)
+        with torch.cuda.device(self.dev):
+            call("dga_bse_preload")  # the BSE kernels' code is loaded at start-up, not inside a request
         self.hbm_budget = int(hbm_budget)
         self.items_per_request = items_per_request
         self.refine_max_iter = refine_max_iter

@@ -108,6 +108,11 @@ int dga_bse_solve_sum_mixed_c128(int n_orb, int niv, int niw_half, int n_q, int 
  * request with this same kernel, so requests whose defaults differ go to different launches. */
 int dga_bse_default_kernel(int n_orb, int niv, int mixed);
 
+/* Loads the code of the mixed form's block-form kernels on the current device now.  CUDA otherwise loads a kernel
+ * at its first launch, which for these large kernels takes tens of milliseconds inside that launch; a server calls
+ * this once at start-up so that no request pays it.  Returns 0 or DGA_ERR_LAUNCH. */
+int dga_bse_preload(void);
+
 /* FP64 re-solve of the items a mixed launch flagged (status & (NOCONVERGE | NONFINITE | WAIT_TIMEOUT)), leaving the others
  * untouched; at most grid_limit CTAs (scratch: grid_limit * (N*N + N*n2) complex128). */
 int dga_bse_resolve_fp64_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
