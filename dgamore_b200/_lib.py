@@ -57,6 +57,9 @@ SIGNATURES = {
     "dga_bse_solve_sum_batch_c128": (I, [VP, VP, I, PI, I, I, I, D, PI, PI, VP, SZ, VP]),
     "dga_bse_tuned_scratch_bytes": (SZ, [I, I, I, I, VP]),
     "dga_hartree_fock_c128": (I, [VP, VP, VP, VP, I, I, I, I, VP, VP, VP, I, VP]),
+    "dga_g_full_c128": (I, [VP, VP, I, I, I, D, D, VP, VP]),
+    "dga_fill_sums_c128": (I, [VP, VP, PD, I, I, I, D, D, PD, PD, VP]),
+    "dga_sigma_kmean_c128": (I, [VP, I, I, I, I, I, VP, VP]),
     "dga_bse_solve_sum_tuned_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, I, I, D, VP, PI, PI, VP, VP, SZ, VP]),
 }
 

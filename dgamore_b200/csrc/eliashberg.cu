@@ -118,10 +118,11 @@ __global__ void eli_apply_chi0pp_kernel(const double2* __restrict__ chi0pp, cons
 // flight per SM to run at HBM bandwidth.
 //   gR: [Nk][n2][nvp] (forward transform of v), mat: [Nk][M][M]
 // MT = double2: Gamma(R) in complex128; MT = float2: Gamma(R) stored in complex64 (half the bytes of the stream),
-// widened on load, FP64 accumulation.  U loads of Mat(R) per lane and row in flight (16 bytes each for complex128,
-// 8 for complex64, so U doubles with the narrower storage to keep the same bytes in flight).
+// widened on use, FP64 accumulation.  A warp takes RW rows at a time with U loads per lane and row in flight
+// (U = 4 covers a row of up to 128 columns in one pass: M = 120 in the bilayer configuration); the complex64 form
+// takes twice the rows so that the bytes in flight stay the same.
 constexpr int ELI_APPLY_THREADS = 256;
-template <typename MT, int U>
+template <typename MT, int U, int RW>
 __global__ void __launch_bounds__(ELI_APPLY_THREADS) eli_vertex_apply_kernel(const MT* __restrict__ mat,
                                                                               const double2* __restrict__ gR, int nb,
                                                                               int nvp, int nk,
@@ -143,48 +144,48 @@ __global__ void __launch_bounds__(ELI_APPLY_THREADS) eli_vertex_apply_kernel(con
     }
     __syncthreads();
     const MT* m = mat + (size_t)R * M * M;
-    for (int I0 = 2 * warp; I0 < M; I0 += 2 * nw) {
-      const bool two = I0 + 1 < M;
-      const MT* row0 = m + (size_t)I0 * M;
-      const MT* row1 = row0 + M;
-      double2 a1 = make_double2(0.0, 0.0), a2 = a1, b1 = a1, b2 = a1;
-      for (int J0 = 0; J0 < M; J0 += 32 * U) {
-        double2 x0[U], x1[U];
+    for (int I0 = RW * warp; I0 < M; I0 += RW * nw) {
+      double2 a[RW], b[RW];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int J = J0 + 32 * u + lane;
-          x0[u] = to_c64(J < M ? row0[J] : zero);
-          x1[u] = to_c64((two && J < M) ? row1[J] : zero);
-        }
+      for (int r = 0; r < RW; ++r) a[r] = b[r] = make_double2(0.0, 0.0);
+      for (int J0 = 0; J0 < M; J0 += 32 * U) {
+        MT x[RW][U];
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int J = J0 + 32 * u + lane;
+            x[r][u] = (I0 + r < M && J < M) ? m[(size_t)(I0 + r) * M + J] : zero;
+          }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int J = J0 + 32 * u + lane;
           if (J < M) {
             const double2 gj = g[J], gtj = gt[J];
-            cfma(a1, x0[u], gj);
-            cfma(a2, x0[u], gtj);
-            cfma(b1, x1[u], gj);
-            cfma(b2, x1[u], gtj);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) {
+              const double2 xv = to_c64(x[r][u]);
+              cfma(a[r], xv, gj);
+              cfma(b[r], xv, gtj);
+            }
           }
         }
       }
-      for (int off = 16; off > 0; off >>= 1) {
-        a1.x += __shfl_down_sync(0xffffffffu, a1.x, off);
-        a1.y += __shfl_down_sync(0xffffffffu, a1.y, off);
-        a2.x += __shfl_down_sync(0xffffffffu, a2.x, off);
-        a2.y += __shfl_down_sync(0xffffffffu, a2.y, off);
-        b1.x += __shfl_down_sync(0xffffffffu, b1.x, off);
-        b1.y += __shfl_down_sync(0xffffffffu, b1.y, off);
-        b2.x += __shfl_down_sync(0xffffffffu, b2.x, off);
-        b2.y += __shfl_down_sync(0xffffffffu, b2.y, off);
-      }
-      if (lane == 0) {
-        direct[(size_t)R * M + I0] = a1;
-        flip[(size_t)R * M + I0] = a2;
-        if (two) {
-          direct[(size_t)R * M + I0 + 1] = b1;
-          flip[(size_t)R * M + I0 + 1] = b2;
+#pragma unroll
+      for (int r = 0; r < RW; ++r)
+        for (int off = 16; off > 0; off >>= 1) {
+          a[r].x += __shfl_down_sync(0xffffffffu, a[r].x, off);
+          a[r].y += __shfl_down_sync(0xffffffffu, a[r].y, off);
+          b[r].x += __shfl_down_sync(0xffffffffu, b[r].x, off);
+          b[r].y += __shfl_down_sync(0xffffffffu, b[r].y, off);
         }
+      if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+          if (I0 + r < M) {
+            direct[(size_t)R * M + I0 + r] = a[r];
+            flip[(size_t)R * M + I0 + r] = b[r];
+          }
       }
     }
   }
@@ -270,7 +271,7 @@ int dga_dft_planes_c128(const void* in, long long in_s_hi, long long in_s_lo, lo
 }  // extern "C"
 
 // The gap-equation application with Gamma(R) stored as MT (complex128 or complex64); everything else FP64.
-template <typename MT, int U>
+template <typename MT, int U, int RW>
 static int eli_matvec(const char* who, const void* mat, const void* chi0pp, const void* gap, int n_orb, int niv_pp,
                       int nx, int ny, int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign,
                       void* gap_out, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
@@ -293,9 +294,9 @@ static int eli_matvec(const char* who, const void* mat, const void* chi0pp, cons
   int rc = dga_dft_planes_c128(s0, 1, 0, M, s1, 1, 0, M, 1, M, nx, ny, nz, tw_fwd, 1.0, stream);
   if (rc) return rc;
   const size_t smem = 2 * (size_t)M * sizeof(double2);
-  cudaFuncSetAttribute(eli_vertex_apply_kernel<MT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(eli_vertex_apply_kernel<MT, U, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int apply_cap = 8 * device_sm_count();
-  eli_vertex_apply_kernel<MT, U><<<nk < apply_cap ? nk : apply_cap, ELI_APPLY_THREADS, smem, stream>>>(
+  eli_vertex_apply_kernel<MT, U, RW><<<nk < apply_cap ? nk : apply_cap, ELI_APPLY_THREADS, smem, stream>>>(
       (const MT*)mat, s1, n_orb, nvp, nk, s2, s3);
   if (eli_status(who)) return DGA_ERR_LAUNCH;
   eli_combine_kernel<<<eli_blocks((long long)nk * M), 256, 0, stream>>>(s2, s3, M, nx, ny, nz, sign, s0);
@@ -316,14 +317,14 @@ extern "C" {
 int dga_eli_matvec_c128(const void* mat, const void* chi0pp, const void* gap, int n_orb, int niv_pp, int nx, int ny,
                         int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign, void* gap_out,
                         void* scratch, size_t scratch_bytes, cudaStream_t stream) {
-  return eli_matvec<double2, 4>("dga_eli_matvec_c128", mat, chi0pp, gap, n_orb, niv_pp, nx, ny, nz, tw_fwd, tw_inv,
+  return eli_matvec<double2, 4, 2>("dga_eli_matvec_c128", mat, chi0pp, gap, n_orb, niv_pp, nx, ny, nz, tw_fwd, tw_inv,
                                 beta, sign, gap_out, scratch, scratch_bytes, stream);
 }
 
 int dga_eli_matvec_c64mat_c128(const void* mat_c64, const void* chi0pp, const void* gap, int n_orb, int niv_pp, int nx,
                                int ny, int nz, const void* tw_fwd, const void* tw_inv, double beta, double sign,
                                void* gap_out, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
-  return eli_matvec<float2, 8>("dga_eli_matvec_c64mat_c128", mat_c64, chi0pp, gap, n_orb, niv_pp, nx, ny, nz, tw_fwd,
+  return eli_matvec<float2, 4, 4>("dga_eli_matvec_c64mat_c128", mat_c64, chi0pp, gap, n_orb, niv_pp, nx, ny, nz, tw_fwd,
                                tw_inv, beta, sign, gap_out, scratch, scratch_bytes, stream);
 }
 

@@ -214,6 +214,22 @@ int dga_chi_phys_c128(const void* X, const void* uv, const void* full_sum, const
 int dga_hartree_fock_c128(const void* u, const void* v_q, const void* occ, const void* occ_k, int n_orb, int nx,
                           int ny, int nz, void* hartree, void* fock, void* sigma, int nv2, dga_stream_t stream);
 
+/* Self-consistency glue (dgamore_b200/selfconsistency.py holds the host side).  sigma, g: [Nk][n][n][2 niv]
+ * complex128 (compressed k, nu = (2m+1) pi/beta for m = -niv .. niv-1); ek: [Nk][n][n] complex128; n_orb 1..4.
+ * dga_g_full_c128: G(k,nu) = [i nu + mu - e_k - Sigma(k,nu)]^-1, as GreensFunction.get_g_full
+ *   (dgamore/greens_function.py:110-124).
+ * dga_fill_sums_c128: s_out[k] = sum_nu Re G(k,nu) and t_out[k] = sum_nu Re [i nu + mu - e_k - s0]^-1 ([Nk][n][n]
+ *   float64; s0: [n][n] float64, the self-energy's zeroth tail moment), the frequency sums behind get_total_fill
+ *   and get_fill_nonlocal (greens_function.py:20-52, 212-240).
+ * dga_sigma_kmean_c128: out[n][n][nvs] = mean over k of sigma[k][.][.][v0 .. v0+nvs), the k-average the tail-moment
+ *   fit reads (SelfEnergy.fit_smom, dgamore/self_energy.py:51-75); nv = 2 niv. */
+int dga_g_full_c128(const void* sigma, const void* ek, int n_orb, int nk, int niv, double mu, double beta, void* g,
+                    dga_stream_t stream);
+int dga_fill_sums_c128(const void* sigma, const void* ek, const double* s0, int n_orb, int nk, int niv, double mu,
+                       double beta, double* s_out, double* t_out, dga_stream_t stream);
+int dga_sigma_kmean_c128(const void* sigma, int n_orb, int nk, int nv, int v0, int nvs, void* out,
+                         dga_stream_t stream);
+
 /* Single-band lambda correction (FP64 Newton with delta halving); replaces lambda_correction.find_lambda and
  * perform_single_lambda_correction (dgamore/lambda_correction.py:28-73).  chi: [n_ch][Q][W]; weights: [Q]
  * multiplicities (irrk_count); target: [n_ch] complex; outputs lambda [n_ch], iterations, corrected chi. */
