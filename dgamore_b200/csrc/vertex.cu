@@ -405,29 +405,32 @@ kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __re
 }
 
 // ------------------------------------------------------------------------------------------------
-// K1 = (U_adcb / beta^2) @ chi0 for every (q, w, nu_full): one warp per matrix
+// K1 = (U_adcb / beta^2) @ chi0 for every (q, w, nu_full): one warp per matrix, written as the row-major GEMM
+// operand K1[w][(q, p)][(m, nu)] (row (q, p), column (m, nu), Kd = n2 * nvf columns)
 // ------------------------------------------------------------------------------------------------
-__global__ void dc_left_kernel(const double2* __restrict__ chi0, const double2* __restrict__ u_perm, int n2,
-                               long long n_mats, double2* __restrict__ k1) {
-  // one warp per matrix, lane l computing the elements l, l + 32, ... (coalesced along the matrix)
+__global__ void dc_left_kernel(const double2* __restrict__ chi0, const double2* __restrict__ u_perm, int n2, int Q,
+                               int W, int nvf, double2* __restrict__ k1) {
+  // one warp per matrix t = (q, w, nu), lane l computing the elements l, l + 32, ...
   const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (t >= n_mats) return;
-  const int nn = n2 * n2;
+  if (t >= (long long)Q * W * nvf) return;
+  const int nu = (int)(t % nvf), qw = (int)(t / nvf), w = qw % W, q = qw / W;
+  const int nn = n2 * n2, Kd = n2 * nvf;
   const double2* c = chi0 + (size_t)t * nn;
-  double2* o = k1 + (size_t)t * nn;
+  double2* o = k1 + ((size_t)w * Q + q) * n2 * Kd + nu;
   for (int e = lane; e < nn; e += 32) {
     const int i = e / n2, j = e - i * n2;
     double2 a = make_double2(0.0, 0.0);
     for (int k = 0; k < n2; ++k) cfma(a, u_perm[i * n2 + k], c[k * n2 + j]);
-    o[e] = a;
+    o[(size_t)i * Kd + (size_t)j * nvf] = a;
   }
 }
 
-// Batched complex GEMM C = A @ B over w with two-level row/column addressing:
-//   A(r, k): r = (q, p) -> q*a_q + p*a_p;  k = (m, nu) -> m*a_m + nu*a_nu   (K1: [Q][W][nvf][n2][n2])
-//   B(k, c): row k = m*nvf + nu, column c = s*nv + nu'  (F_dc compound matrix [W][Nf][Nf], row-major)
-//   C(r, c): r = (q, p), c = (s, nu')  -> K_dc [Q][W][nv][n2][n2]
+// Batched complex GEMM over w: C(r, c) = sum_k K1[w][r][k] F_dc[w][k][col(c)]
+//   r = (q, p) (M = Q n2 rows), k = (m, nu) (Kd = n2 nvf), c = (s, nu') (Nc = n2 nv), col(c) = s nvf + shell + nu'
+//   C(r, c) -> K_dc [Q][W][nv][n2][n2] at (q, w, nu', p, s)
+// 64 x 64 complex outputs per 256-thread CTA, 4 x 4 per thread; K in steps of 16, the next step's operands loaded
+// into registers while the current one multiplies.  A-tile rows are 16 consecutive k (256 contiguous bytes per row).
 struct DcGemmArgs {
   const double2* k1;
   const double2* fdc;
@@ -437,42 +440,48 @@ struct DcGemmArgs {
 
 constexpr int DG_TM = 64, DG_TN = 64, DG_TK = 16;
 
-__global__ void __launch_bounds__(256) dc_gemm_kernel(DcGemmArgs a) {
-  __shared__ double2 As[DG_TK][DG_TM];
+__global__ void __launch_bounds__(256, 2) dc_gemm_kernel(DcGemmArgs a) {
+  __shared__ double2 As[DG_TK][DG_TM + 1];
   __shared__ double2 Bs[DG_TK][DG_TN];
   const int w = blockIdx.z;
   const int M = a.Q * a.n2, Kd = a.n2 * a.nvf, Nc = a.n2 * a.nv;
   const int r0 = blockIdx.y * DG_TM, c0 = blockIdx.x * DG_TN;
   const int tid = threadIdx.x, ty = tid & 15, tx = tid >> 4;
   const int Nf = a.n2 * a.nvf;
+  const double2* A = a.k1 + (size_t)w * M * Kd;
+  const double2* B = a.fdc + (size_t)w * Nf * Nf;
+  // this thread's loads: A rows ra + 16 i (k = ka), B column cb (k rows kb + 4 i)
+  const int ka = tid & 15, ra = tid >> 4;
+  const int cb = tid & 63, kb = tid >> 6;
+  int bcol = -1;
+  if (c0 + cb < Nc) {
+    const int col = c0 + cb, sidx = col / a.nv, nup = col - sidx * a.nv;
+    bcol = sidx * a.nvf + a.shell + nup;
+  }
+  double2 ra_v[4], rb_v[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = r0 + ra + 16 * i, k = k0 + ka;
+      ra_v[i] = (row < M && k < Kd) ? A[(size_t)row * Kd + k] : make_double2(0.0, 0.0);
+      const int kr = k0 + kb + 4 * i;
+      rb_v[i] = (bcol >= 0 && kr < Kd) ? B[(size_t)kr * Nf + bcol] : make_double2(0.0, 0.0);
+    }
+  };
   double2 acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+  load(0);
   for (int k0 = 0; k0 < Kd; k0 += DG_TK) {
-    for (int e = tid; e < DG_TK * DG_TM; e += 256) {
-      const int r = e % DG_TM, kk = e / DG_TM;
-      const int row = r0 + r, k = k0 + kk;
-      double2 val = make_double2(0.0, 0.0);
-      if (row < M && k < Kd) {
-        const int q = row / a.n2, p = row - q * a.n2;
-        const int m = k / a.nvf, nu = k - m * a.nvf;
-        val = a.k1[((((size_t)q * a.W + w) * a.nvf + nu) * a.n2 + p) * a.n2 + m];
-      }
-      As[kk][r] = val;
-    }
-    for (int e = tid; e < DG_TK * DG_TN; e += 256) {
-      const int c = e % DG_TN, kk = e / DG_TN;
-      const int col = c0 + c, k = k0 + kk;
-      double2 val = make_double2(0.0, 0.0);
-      if (col < Nc && k < Kd) {
-        const int sidx = col / a.nv, nup = col - sidx * a.nv;
-        val = a.fdc[((size_t)w * Nf + k) * Nf + sidx * a.nvf + a.shell + nup];
-      }
-      Bs[kk][c] = val;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      As[ka][ra + 16 * i] = ra_v[i];
+      Bs[kb + 4 * i][cb] = rb_v[i];
     }
     __syncthreads();
+    if (k0 + DG_TK < Kd) load(k0 + DG_TK);
 #pragma unroll
     for (int kk = 0; kk < DG_TK; ++kk) {
       double2 av[4], bv[4];
@@ -618,7 +627,7 @@ int dga_dc_kernel_c128(const void* chi0, const void* u_perm, const void* fdc, in
   }
   const long long n_mats = (long long)n_q * niw_half * nvf;
   dc_left_kernel<<<(int)((n_mats * 32 + 255) / 256), 256, 0, stream>>>((const double2*)chi0, (const double2*)u_perm, n2,
-                                                                  n_mats, (double2*)scratch);
+                                                                  n_q, niw_half, nvf, (double2*)scratch);
   if (vstatus("dga_dc_kernel_c128")) return DGA_ERR_LAUNCH;
   DcGemmArgs a;
   a.k1 = (const double2*)scratch;
