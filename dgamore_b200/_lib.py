@@ -61,6 +61,14 @@ SIGNATURES = {
     "dga_fill_sums_c128": (I, [VP, VP, PD, I, I, I, D, D, PD, PD, VP]),
     "dga_sigma_kmean_c128": (I, [VP, I, I, I, I, I, VP, VP]),
     "dga_bse_solve_sum_tuned_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, I, I, D, VP, PI, PI, VP, VP, SZ, VP]),
+    "dga_lu_batched_c128": (I, [VP, I, I, LL, PI, PI, VP]),
+    "dga_lu_solve_batched_c128": (I, [VP, PI, I, I, LL, VP, LL, LL, LL, I, VP, LL, PI, VP]),
+    "dga_local_bubble_c128": (I, [VP, I, I, I, I, D, VP, VP]),
+    "dga_local_chi_c128": (I, [VP, I, I, I, I, I, VP, I, D, I, VP, VP]),
+    "dga_local_ucorr_c128": (I, [VP, VP, VP, I, I, VP, PI, VP]),
+    "dga_local_gamma_c128": (I, [VP, LL, VP, VP, I, I, I, D, VP, VP]),
+    "dga_local_fvertex_operands_c128": (I, [VP, VP, VP, I, I, I, I, D, VP, VP, VP]),
+    "dga_local_sigma_c128": (I, [VP, VP, VP, VP, VP, VP, I, I, I, I, D, VP, VP, VP]),
 }
 
 

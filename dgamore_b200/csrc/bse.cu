@@ -909,6 +909,84 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   }
 }
 
+// ----------------------------------------------------------------------------------------------
+// Dense batched LU and solves with many right-hand sides (the local Schwinger-Dyson equation's full inverses,
+// numpy.linalg.inv behind LocalFourPoint.invert, local_four_point.py:298-310).  The factorisation is lu_factor
+// (LAPACK's pivot order) with one CTA per matrix; the solves spread over (matrix, block of DENSE_RHS right-hand
+// sides) CTAs, each streaming the factors once for its block.
+// ----------------------------------------------------------------------------------------------
+constexpr int DENSE_RHS = 16;
+
+__global__ void __launch_bounds__(BSE_THREADS, 3)
+    dense_lu_kernel(double2* __restrict__ a, int N, int n_mat, long long mat_stride, int* __restrict__ piv_out,
+                    int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BseSmem<double2>& sm = *reinterpret_cast<BseSmem<double2>*>(smem_raw);
+  int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<double2>));
+  for (int m = blockIdx.x; m < n_mat; m += gridDim.x) {
+    const bool singular = lu_factor<double2>(a + (size_t)m * mat_stride, N, N, piv, sm);
+    __syncthreads();
+    for (int i = threadIdx.x; i < N; i += blockDim.x) piv_out[(size_t)m * N + i] = piv[i];
+    if (threadIdx.x == 0) status[m] = singular ? DGA_ITEM_SINGULAR : DGA_ITEM_OK;
+    __syncthreads();
+  }
+}
+
+// out_m[:, k] = A_m^-1 B_m[:, k] for k < n_rhs, column-major with leading dimension N, in blocks of DENSE_RHS
+// columns (columns n_rhs .. of the last block are solved for zero right-hand sides).  B_m(r, k) =
+// b[m b_sm + r b_sr + k b_sk], or the identity when b is null.  A non-finite solution element sets
+// DGA_ITEM_NONFINITE in status[m].
+__global__ void __launch_bounds__(BSE_THREADS, 3)
+    dense_solve_kernel(const double2* __restrict__ lu, const int* __restrict__ piv, int N, int n_mat,
+                       long long lu_stride, const double2* __restrict__ b, long long b_sm, long long b_sr,
+                       long long b_sk, int n_rhs, double2* __restrict__ out, long long out_stride,
+                       int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BseSmem<double2>& sm = *reinterpret_cast<BseSmem<double2>*>(smem_raw);
+  int* perm = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<double2>));
+  const int tid = threadIdx.x, T = blockDim.x;
+  const int n_blk = (n_rhs + DENSE_RHS - 1) / DENSE_RHS;
+  for (int t = blockIdx.x; t < n_mat * n_blk; t += gridDim.x) {
+    const int m = t / n_blk, k0 = (t - m * n_blk) * DENSE_RHS;
+    const int* pv = piv + (size_t)m * N;
+    for (int i = tid; i < N; i += T) perm[i] = i;
+    __syncthreads();
+    if (tid == 0) {
+      for (int i = 0; i < N; ++i) {
+        const int p = pv[i];
+        if (p != i) {
+          const int s = perm[i];
+          perm[i] = perm[p];
+          perm[p] = s;
+        }
+      }
+    }
+    __syncthreads();
+    double2* Y = out + (size_t)m * out_stride + (size_t)k0 * N;
+    for (int e = tid; e < N * DENSE_RHS; e += T) {
+      const int i = e % N, k = e / N, col = k0 + k;
+      double2 v = make_double2(0.0, 0.0);
+      if (col < n_rhs) {
+        const int r = perm[i];
+        if (b)
+          v = b[m * b_sm + r * b_sr + col * b_sk];
+        else if (r == col)
+          v.x = 1.0;
+      }
+      Y[(size_t)k * N + i] = v;
+    }
+    __syncthreads();
+    lu_solve_inplace<double2, double2, DENSE_RHS>(lu + (size_t)m * lu_stride, N, N, Y, sm);
+    int bad = 0;
+    for (int e = tid; e < N * DENSE_RHS; e += T) {
+      const double2 v = Y[e];
+      bad |= !(isfinite(v.x) && isfinite(v.y));
+    }
+    if (__syncthreads_or(bad) && tid == 0) atomicOr(status + m, DGA_ITEM_NONFINITE);
+    __syncthreads();
+  }
+}
+
 }  // namespace dga
 
 using namespace dga;
@@ -1708,6 +1786,55 @@ int dga_bse_solve_sum_noalloc_c128(int n_orb, int niv, int niw_half, int n_q, in
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     dga_set_error("dga_bse_solve_sum_noalloc_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Batched dense LU with partial pivoting of n_mat N x N column-major matrices a + m*mat_stride (in place).
+int dga_lu_batched_c128(void* a, int N, int n_mat, long long mat_stride, int* piv, int* status, cudaStream_t stream) {
+  if (!a || !piv || !status || N <= 0 || N > DGA_DENSE_MAX_N || n_mat <= 0 || mat_stride < (long long)N * N) {
+    dga_set_error("dga_lu_batched_c128: invalid arguments (N=%d n_mat=%d)", N, n_mat);
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = bse_smem_bytes(N);
+  const int grid = grid_for(dense_lu_kernel, n_mat, smem);
+  dense_lu_kernel<<<grid, BSE_THREADS, smem, stream>>>((double2*)a, N, n_mat, mat_stride, piv, status);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_lu_batched_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+// Solves with the factors of dga_lu_batched_c128 for n_rhs right-hand sides (b null: the identity).
+int dga_lu_solve_batched_c128(const void* lu, const int* piv, int N, int n_mat, long long lu_stride, const void* b,
+                              long long b_stride_m, long long b_stride_r, long long b_stride_k, int n_rhs, void* out,
+                              long long out_stride, int* status, cudaStream_t stream) {
+  const long long cols = ((long long)n_rhs + DENSE_RHS - 1) / DENSE_RHS * DENSE_RHS;
+  if (!lu || !piv || !out || !status || N <= 0 || N > DGA_DENSE_MAX_N || n_mat <= 0 || n_rhs <= 0 ||
+      lu_stride < (long long)N * N || out_stride < cols * N || (!b && n_rhs > N)) {
+    dga_set_error("dga_lu_solve_batched_c128: invalid arguments (N=%d n_mat=%d n_rhs=%d)", N, n_mat, n_rhs);
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = bse_smem_bytes(N);
+  const long long n_tasks = (long long)n_mat * (cols / DENSE_RHS);
+  if (n_tasks > 0x7fffffffLL) {
+    dga_set_error("dga_lu_solve_batched_c128: too many right-hand-side blocks");
+    return DGA_ERR_ARG;
+  }
+  const int grid = grid_for(dense_solve_kernel, (int)n_tasks, smem);
+  dense_solve_kernel<<<grid, BSE_THREADS, smem, stream>>>((const double2*)lu, piv, N, n_mat, lu_stride,
+                                                          (const double2*)b, b_stride_m, b_stride_r, b_stride_k,
+                                                          n_rhs, (double2*)out, out_stride, status);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_lu_solve_batched_c128: launch failed: %s", cudaGetErrorString(err));
     return DGA_ERR_LAUNCH;
   }
   return DGA_OK;

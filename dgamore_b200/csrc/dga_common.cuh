@@ -23,6 +23,9 @@
 // items a mixed-precision launch leaves for the FP64 re-solve
 #define DGA_ITEM_REDO (DGA_ITEM_NOCONVERGE | DGA_ITEM_NONFINITE | DGA_ITEM_WAIT_TIMEOUT)
 
+// largest matrix of the dense batched LU / solves (pivot and permutation arrays in shared memory)
+#define DGA_DENSE_MAX_N 8192
+
 // One problem (request) of a heterogeneous BSE batch; the layout is part of the C ABI (include/dga_b200.h).
 typedef struct {
   const void* gamma_cm;  // [2][W][N][N] column-major compound Gamma_r

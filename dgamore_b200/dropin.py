@@ -26,6 +26,8 @@ nonlocal_sde.get_hartree_fock (nonlocal_sde.py:31-69)  dga_hartree_fock_c128
 lambda_correction.find_lambda,                      dga_lambda_c128
   perform_single_lambda_correction (:28-73)
 eliashberg_solver.solve_eliashberg_lanczos (:376-471)  device gap-equation matvec + Krylov-Schur
+local_sde.perform_local_schwinger_dyson             local_sde.LocalSde: local bubble, batched dense LU,
+  (local_sde.py:175-217)                            the BSE at q = 0, local Sigma kernels
 =================================================  ==================================================
 
 Arguments are the upstream's objects, duck-typed: a function reads only ``.mat`` and the metadata the original
@@ -437,6 +439,36 @@ def perform_single_lambda_correction(chi_r, chi_r_loc_sum: complex):
 
 
 # ------------------------------------------------------------------------------------------------
+# local_sde
+# ------------------------------------------------------------------------------------------------
+def perform_local_schwinger_dyson(g_dmft, g2_dens, g2_magn, u_loc):
+    """local_sde.perform_local_schwinger_dyson (local_sde.py:175-217) on the device (``local_sde.LocalSde``):
+    returns gamma_d, gamma_m, chi_d, chi_m, vrg_d, vrg_m, f_d, f_m, gchi_d, gchi_m (LocalFourPoint, half w range)
+    and sigma_loc (SelfEnergy), reading config.sys.beta / occ_dmft, config.box.niw_core / niv_core / niv_shell
+    and, like the original, saving the local bubble as ``gchi0_loc`` when config.eliashberg.perform_eliashberg.
+    Orbital symmetrisation (config.dmft.symmetrize_orbitals) raises NotImplementedError."""
+    from .local_sde import LocalSde
+    from .outputs import save_npoint
+
+    cfg = _cfg()
+    dmft = getattr(cfg, "dmft", None)
+    if dmft is not None and len(getattr(dmft, "symmetrize_orbitals", []) or []) > 0:
+        raise NotImplementedError("orbital symmetrisation of the local vertices is not part of the device form")
+    box = cfg.box
+    sde = LocalSde(np.asarray(g_dmft.mat), np.asarray(g2_dens.mat), np.asarray(g2_magn.mat), np.asarray(u_loc.mat),
+                   cfg.sys.beta, box.niw_core, box.niv_core, box.niv_shell, cfg.sys.occ_dmft).run()
+    res = sde.results()
+    eli = getattr(cfg, "eliashberg", None)
+    if eli is not None and getattr(eli, "perform_eliashberg", False):
+        save_npoint(sde.bubble().cpu().numpy(), cfg.output.output_path, "gchi0_loc")
+    dens, magn = _enum("SpinChannel", "DENS"), _enum("SpinChannel", "MAGN")
+    n_vn = (2, 2, 0, 0, 1, 1, 2, 2, 2, 2)
+    chans = (dens, magn) * 5
+    four = [_make("LocalFourPoint", m, c, 1, nv, False) for m, c, nv in zip(res[:10], chans, n_vn)]
+    return (*four, _make("SelfEnergy", res[10]))
+
+
+# ------------------------------------------------------------------------------------------------
 # eliashberg_solver
 # ------------------------------------------------------------------------------------------------
 class PairingOperator:
@@ -512,6 +544,7 @@ PATCHES = [
     ("lambda_correction", None, "find_lambda", find_lambda, False),
     ("lambda_correction", None, "perform_single_lambda_correction", perform_single_lambda_correction, False),
     ("eliashberg_solver", None, "solve_eliashberg_lanczos", solve_eliashberg_lanczos, False),
+    ("local_sde", None, "perform_local_schwinger_dyson", perform_local_schwinger_dyson, False),
 ]
 
 
@@ -524,10 +557,11 @@ def install(package: str = "dgamore", precision: str = "fp64") -> list:
     set_precision(precision)
     mods = {m: importlib.import_module(f"{package}.{m}") for m in
             ("bubble_gen", "four_point", "nonlocal_sde", "lambda_correction", "eliashberg_solver", "self_energy",
-             "gap_function", "n_point_base")}
+             "gap_function", "n_point_base", "local_sde", "local_four_point")}
     use_config(importlib.import_module(f"{package}.config"))
     use_classes(FourPoint=mods["four_point"].FourPoint, SelfEnergy=mods["self_energy"].SelfEnergy,
                 GapFunction=mods["gap_function"].GapFunction, SpinChannel=mods["n_point_base"].SpinChannel,
+                LocalFourPoint=mods["local_four_point"].LocalFourPoint,
                 FrequencyNotation=mods["n_point_base"].FrequencyNotation)
     replaced = []
     for mod, cls, name, fn, static in PATCHES:

@@ -316,6 +316,67 @@ int dga_eli_matvec_c64mat_c128(const void* mat_c64, const void* chi0pp, const vo
 /* dst[e] = complex64(src[e]) for e < n (round to nearest); no counterpart in the upstream. */
 int dga_narrow_c128_to_c64(const void* src, void* dst, long long n, dga_stream_t stream);
 
+/* ---- dense batched LU (the full inverses of the local Schwinger-Dyson equation) ---- */
+
+/* LU with partial pivoting (LAPACK's pivot order, the zgetrf behind numpy.linalg.inv in LocalFourPoint.invert,
+ * dgamore/local_four_point.py:298-310) of n_mat column-major N x N matrices a + m*mat_stride, in place (N <= 8192);
+ * piv [n_mat][N]; status [n_mat]: DGA_ITEM_SINGULAR on an exact zero pivot. */
+int dga_lu_batched_c128(void* a, int N, int n_mat, long long mat_stride, int* piv, int* status, dga_stream_t stream);
+
+/* X_m = A_m^-1 B_m with the factors of dga_lu_batched_c128 for n_rhs right-hand sides B_m(r, k) =
+ * b[m*b_stride_m + r*b_stride_r + k*b_stride_k] (b null: the identity, n_rhs <= N, giving the inverse), written
+ * column-major (leading dimension N) to out + m*out_stride in blocks of 16 columns: out holds ceil(n_rhs/16)*16
+ * columns, those past n_rhs solved for zero right-hand sides.  A non-finite element of X_m ORs DGA_ITEM_NONFINITE
+ * into status[m]. */
+int dga_lu_solve_batched_c128(const void* lu, const int* piv, int N, int n_mat, long long lu_stride, const void* b,
+                              long long b_stride_m, long long b_stride_r, long long b_stride_k, int n_rhs, void* out,
+                              long long out_stride, int* status, dga_stream_t stream);
+
+/* ---- local Schwinger-Dyson equation (dgamore/local_sde.py:17-217), W = niw_core + 1 frequencies w >= 0 ----
+ * Compound orbital index p = (a,b), s = (d,c); N = n^2 * 2 niv_core; matrices of both channels ordered
+ * m = ch*W + w (ch 0 = density, 1 = magnetic); uv [2][n2][n2] = U_dens, U_magn (interaction.py:43-65). */
+
+/* chi0[w][nu][p][s] = -beta G_ad(nu) G_cb(nu - w) over the box of 2*niv_box frequencies, entries with both parts
+ * below 1e-12 set to zero; replaces BubbleGenerator.create_generalized_chi0 (dgamore/bubble_gen.py:20-30) in the
+ * half w range.  g: [n][n][2 niv_g], niv_g >= niv_box + niw_half. */
+int dga_local_bubble_c128(const void* g, int n_orb, int niv_g, int niw_half, int niv_box, double beta, void* chi0,
+                          dga_stream_t stream);
+
+/* chi_cm[w] (column-major compound N x N) = beta G2[a,b,c,d,w0+w,nu,nu'] - 2 beta G_ab(nu) G_cd(nu') at w = 0 if
+ * dens; replaces create_generalized_chi (dgamore/local_sde.py:17-29).  g2: [n][n][n][n][n_wg][2niv][2niv] with
+ * w = 0 at index w0 (w0 = niw for the full range, 0 for the half range). */
+int dga_local_chi_c128(const void* g2, int n_orb, int niv, int niw_half, int w0, int n_wg, const void* g, int niv_g,
+                       double beta, int dens, void* chi_cm, dga_stream_t stream);
+
+/* ucorr[ch][w] = U_r - U_r [1 + (full_sum - core_sum) U_r]^-1 (n2 x n2; full/core sums [W][n2][n2] of
+ * dga_chi0_prep_c128 with one q): the shell correction of create_gamma_r_with_shell_correction
+ * (dgamore/local_sde.py:49-51) in closed form.  status [2][W]: DGA_ITEM_SINGULAR if the bracket is singular. */
+int dga_local_ucorr_c128(const void* uv, const void* full_sum, const void* core_sum, int n_orb, int niw_half,
+                         void* ucorr, int* status, dga_stream_t stream);
+
+/* gamma_cm[m] = beta^2 chi_inv[m] - delta_{nu nu'} beta^2 chi0_inv[w][nu] + ucorr[m] (column-major compound, the
+ * layout dga_bse_solve_sum_c128 reads); chi_inv column-major at m*inv_stride; chi0_inv [W][nv][n2][n2].  Replaces
+ * create_gamma_r_with_shell_correction (dgamore/local_sde.py:40-51). */
+int dga_local_gamma_c128(const void* chi_inv, long long inv_stride, const void* chi0_inv, const void* ucorr,
+                         int n_orb, int niv, int niw_half, double beta, void* gamma_cm, dga_stream_t stream);
+
+/* Operands of F = Gamma_u [1 + chi0 Gamma_u / beta^2]^-1 over the full box (create_full_vertex_from_gamma,
+ * dgamore/local_sde.py:75-82): gamma_u (Gamma_r in the core box, U_r outside it, pad_with_u) and mt = the
+ * transpose of 1 + chi0 Gamma_u / beta^2, both column-major [2W][Nf][Nf], Nf = n^2 * 2(niv_core + niv_shell);
+ * chi0 [W][nvf][n2][n2] from dga_local_bubble_c128 over the full box.  F follows as the solve mt X = gamma_u^T
+ * (X = F^T) of dga_lu_solve_batched_c128. */
+int dga_local_fvertex_operands_c128(const void* gamma_cm, const void* uv, const void* chi0, int n_orb, int niv_core,
+                                    int niv_shell, int niw_half, double beta, void* mt, void* gamma_u,
+                                    dga_stream_t stream);
+
+/* Local self-energy from the three-leg vertices vrg [2][W][nv][n2][n2] and susceptibilities chi_phys
+ * [2][W][n2][n2] (get_loc_self_energy_vrg, dgamore/local_sde.py:150-172): sigma [n][n][2niv] = Hartree term
+ * U_dens occ + the SDE sum over the full w range; u [n][n][n][n] (plain U), g [n][n][2niv_g], occ [n][n];
+ * inner: scratch [W][nv][n2][n2]. */
+int dga_local_sigma_c128(const void* vrg, const void* chi_phys, const void* uv, const void* u, const void* g,
+                         const void* occ, int n_orb, int niv, int niw_half, int niv_g, double beta, void* inner,
+                         void* sigma, dga_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
