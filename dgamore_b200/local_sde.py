@@ -130,19 +130,24 @@ class LocalSde:
         call("dga_local_gamma_c128", _p(chi_inv), cols * N, _p(self.chi0_inv), _p(self.ucorr), n, self.niv, W, beta,
              _p(self.gamma_cm), _s())
         del chi_inv
-        # full vertex over the full box (create_full_vertex_from_gamma): F^T = (1 + chi0 Gamma_u / beta^2)^-T Gamma_u^T
+        # full vertex over the full box (create_full_vertex_from_gamma): F^T = (1 + chi0 Gamma_u / beta^2)^-T Gamma_u^T.
+        # It depends on Gamma_r only, like the BSE below: it runs on a second stream so that the two sets of
+        # single-CTA LUs share the GPU.  Its buffers come from the main stream and are freed after the join.
         mt = torch.empty((M, Nf, Nf), dtype=C128, device=dev)
         gamma_u = torch.empty((M, Nf, Nf), dtype=C128, device=dev)
-        call("dga_local_fvertex_operands_c128", _p(self.gamma_cm), _p(self.uv), _p(self.chi0), n, self.niv,
-             self.niv_shell, W, beta, _p(mt), _p(gamma_u), _s())
         pivf = torch.empty((M, Nf), dtype=torch.int32, device=dev)
         self.f_status = torch.zeros(M, dtype=torch.int32, device=dev)
-        call("dga_lu_batched_c128", _p(mt), Nf, M, Nf * Nf, _p(pivf), _p(self.f_status), _s())
         colsf = _cols(Nf)
         self.f_rm = torch.empty((M, colsf, Nf), dtype=C128, device=dev)  # row c of F at [m][c][:]
-        call("dga_lu_solve_batched_c128", _p(mt), _p(pivf), Nf, M, Nf * Nf, _p(gamma_u), Nf * Nf, Nf, 1, Nf,
-             _p(self.f_rm), colsf * Nf, _p(self.f_status), _s())
-        del mt, gamma_u
+        main = torch.cuda.current_stream()
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            call("dga_local_fvertex_operands_c128", _p(self.gamma_cm), _p(self.uv), _p(self.chi0), n, self.niv,
+                 self.niv_shell, W, beta, _p(mt), _p(gamma_u), _s())
+            call("dga_lu_batched_c128", _p(mt), Nf, M, Nf * Nf, _p(pivf), _p(self.f_status), _s())
+            call("dga_lu_solve_batched_c128", _p(mt), _p(pivf), Nf, M, Nf * Nf, _p(gamma_u), Nf * Nf, Nf, 1, Nf,
+                 _p(self.f_rm), colsf * Nf, _p(self.f_status), _s())
         # auxiliary susceptibility's nu' sum: the ladder BSE at q = 0 with V = 0 (create_auxiliary_chi, create_vrg)
         work = torch.tensor([[ch, 0, w] for ch in range(2) for w in range(W)], dtype=torch.int32, device=dev)
         self.X = torch.empty((2, 1, W, N, n2), dtype=C128, device=dev)
@@ -168,6 +173,8 @@ class LocalSde:
         self.sigma = torch.empty((n, n, nv), dtype=C128, device=dev)
         call("dga_local_sigma_c128", _p(self.vrg), _p(self.chi_phys), _p(self.uv), _p(self.u), _p(self.g),
              _p(self.occ), n, self.niv, W, self.niv_g, beta, _p(inner), _p(self.sigma), _s())
+        main.wait_stream(side)
+        del mt, gamma_u, pivf
         self._ran = True
         return self
 
@@ -180,10 +187,10 @@ class LocalSde:
                 raise np.linalg.LinAlgError("Singular matrix")
 
     # ------------------------------------------------------------------ upstream layouts
-    def _copy(self, src: torch.Tensor, shape: tuple, strides: tuple) -> torch.Tensor:
+    def _copy(self, src: torch.Tensor, shape: tuple, strides: tuple, scale: float = 1.0) -> torch.Tensor:
         dst = torch.empty(shape, dtype=C128, device=self.dev)
         call("dga_strided_copy_c128", _p(src), _p(dst), len(shape), ll_array(shape), ll_array(strides),
-             ll_array(list(dst.stride())), 1.0, _s())
+             ll_array(list(dst.stride())), scale, _s())
         return dst
 
     def _four_point(self, src: torch.Tensor, nvb: int, ld: int, row_major: bool) -> torch.Tensor:
@@ -226,6 +233,37 @@ class LocalSde:
     def sigma_loc(self) -> torch.Tensor:
         """Sigma_loc [1, 1, 1, n, n, 2 niv_core] (get_loc_self_energy_vrg)."""
         return self.sigma.reshape(1, 1, 1, self.n, self.n, self.nv)
+
+    def f_dc(self) -> torch.Tensor:
+        """2 F_magn permuted abcd -> cbad [a,b,c,d,w>=0,nu,nu'] over the full box, the double-counting vertex the
+        nonlocal pass reads (nonlocal_sde.py:817-819), made on the device from F_magn in one strided copy."""
+        n, nvf, Nf = self.n, self.nvf, self.Nf
+        ld = self.f_rm.shape[1] * Nf
+        # destination (i, j, k, l) takes F_magn[k, j, i, l]: row-major strides of (a, b, c, d) are
+        # (n nvf Nf, nvf Nf, nvf, n nvf)
+        st = (nvf, nvf * Nf, n * nvf * Nf, n * nvf, ld, Nf, 1)
+        return self._copy(self.f_rm[self.W], (n, n, n, n, self.W, nvf, nvf), st, 2.0)
+
+    def chi_loc_sum(self, ch: int) -> complex:
+        """sum over orbitals and the full w range of chi_r / beta, the local sum the lambda-correction compares
+        with (nonlocal_sde.py:383-392; w < 0 by conjugation, local_n_point.py:191-225)."""
+        c = self.chi(ch).cpu().numpy()
+        return complex((c.sum() + np.conj(c[..., 1:]).sum()) / self.beta)
+
+    def nonlocal_inputs(self, base: dict) -> dict:
+        """``base`` (an input dict of pipeline.LadderPass) with its local vertices replaced by this equation's
+        results, kept on the device: gamma_dens / gamma_magn, f_dc and the local susceptibility sums (the
+        upstream passes them through gamma_*_loc.npy, f_magn_loc.npy and chi_*_loc.npy, DGAmore.py:257-277)."""
+        if not self._ran:
+            self.run()
+        self.check()
+        if (base["niw"], base["niv_core"], base["niv_shell"]) != (self.niw, self.niv, self.niv_shell):
+            raise ValueError("the nonlocal pass and the local equation must share the frequency boxes")
+        out = dict(base)
+        out["gamma_dens"], out["gamma_magn"] = self.gamma(0), self.gamma(1)
+        out["f_dc"] = self.f_dc()
+        out["chi_loc_sum_dens"], out["chi_loc_sum_magn"] = self.chi_loc_sum(0), self.chi_loc_sum(1)
+        return out
 
     def results(self) -> tuple:
         """The upstream's 11 results as numpy arrays, in its order: gamma_d, gamma_m, chi_d, chi_m, vrg_d, vrg_m,

@@ -42,6 +42,14 @@ def twiddles(nk: tuple, sign: int) -> np.ndarray:
     return np.concatenate(parts).astype(np.complex128)
 
 
+def _resident(x, dev) -> torch.Tensor:
+    """A complex128 input on the device: a device tensor (the local equation's results, local_sde.LocalSde) as it
+    is, host arrays copied once."""
+    if isinstance(x, torch.Tensor):
+        return x.to(device=dev, dtype=C128).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=np.complex128)).to(dev)
+
+
 def compound_orb(x: np.ndarray) -> np.ndarray:
     """[..., a, b, c, d] -> [..., (a,b), (d,c)] compound orbital matrices."""
     nb = x.shape[-1]
@@ -218,7 +226,7 @@ class LadderPass:
         n, nv, W, N = sh.n_orb, sh.nv, sh.W, sh.N
         self.gamma_cm = torch.empty((2, W, N, N), dtype=C128, device=dev)
         for ich, ch in enumerate(("dens", "magn")):
-            g_ref = torch.from_numpy(np.ascontiguousarray(inp[f"gamma_{ch}"], dtype=np.complex128)).to(dev)
+            g_ref = _resident(inp[f"gamma_{ch}"], dev)
             src_strides = list(g_ref.stride())
             dst = self.gamma_cm[ich]
             # dims (a, b, c, d, w, nu, nu')
@@ -228,7 +236,7 @@ class LadderPass:
         # F_dc (upstream [d,c,e,f,w,nu,nu']) -> row-major compound [W][Nf][Nf]
         nvf = sh.nvf
         Nf = sh.n2 * nvf
-        f_ref = torch.from_numpy(np.ascontiguousarray(inp["f_dc"], dtype=np.complex128)).to(dev)
+        f_ref = _resident(inp["f_dc"], dev)
         self.fdc = torch.empty((W, Nf, Nf), dtype=C128, device=dev)
         call("dga_strided_copy_c128", _p(f_ref), _p(self.fdc), 7, ll_array(f_ref.shape), ll_array(list(f_ref.stride())),
              ll_array([n * nvf * Nf, nvf * Nf, nvf, n * nvf, Nf * Nf, Nf, 1]), 1.0, _s())

@@ -8,7 +8,8 @@
 * at size: the 3-orbital configuration's box (niv_core = 40, N = 720) on a reduced bosonic range against the
   oracle to 1e-10, and the full box (niw_core = niv_core = 40) through size-independent properties: the vertex
   the inputs were made from comes back (Gamma_r = Gamma_model) and F satisfies F (1 + chi0 Gamma_u / beta^2) =
-  Gamma_u, checked with torch matrix products.
+  Gamma_u, checked with torch matrix products;
+* the hand-off to the nonlocal pass on the device: Sigma equal to the pass fed host copies, and to the oracle.
 """
 
 import dataclasses
@@ -125,7 +126,7 @@ def _model_inputs(name: str, niw: int, niv: int, niv_shell: int, seed_offset: in
         if ch == "dens":
             gs = g[..., g.shape[-1] // 2 - niv : g.shape[-1] // 2 + niv]
             g2[:, :, :, :, 0] += 2.0 * gs[:, :, None, None, :, None] * gs[None, None, :, :, None, :]
-        g2s.append(g2)
+        g2s.append(osde.full_niw(g2, 3))  # the full w range, as the upstream reads G2
         gammas.append(gamma)
     occ = synthetic.make_occupations(cfg)[0]
     return (g, g2s[0], g2s[1], u, beta, niw, niv, niv_shell, occ), gammas
@@ -165,3 +166,39 @@ def test_local_sde_full_box_properties(name, niw, niv, shell):
         lhs = f @ (eye + c0 @ gu / beta**2)
         assert rel_err(lhs.cpu().numpy(), gu.cpu().numpy()) < 1e-10, ch
         assert f.shape == (W, Nf, Nf)
+
+
+def test_local_results_feed_the_nonlocal_pass_on_the_device():
+    """The local equation's vertices reach the nonlocal pass on the device (no .npy hand-off): the pass built from
+    LocalSde.nonlocal_inputs gives the same Sigma as the pass built from host copies of the same results, and
+    both match the oracle's pass (pinned to the upstream) on those inputs."""
+    from dgamore_b200 import synthetic
+    from dgamore_b200.local_sde import LocalSde
+    from dgamore_b200.pipeline import LadderPass
+    from oracle import ladder, local_sde as osde
+
+    cfg = synthetic.CONFIGS["t1"]  # 1 orbital, 4x4, niw = niv = 4, niv_shell = 2, lambda-corrected
+    base = synthetic.make_inputs(cfg)
+    g_loc = np.asarray(base["g_k"]).mean(axis=(0, 1, 2))
+    beta, niw, niv, sh = base["beta"], base["niw"], base["niv_core"], base["niv_shell"]
+    u = np.asarray(base["u"])
+    chi0h = osde.half_niw(osde.local_bubble(g_loc, niw, niv + sh, beta), 2)
+    g2 = []
+    for ch in ("dens", "magn"):
+        u_r = osde.u_as_channel(u, ch)
+        a = osde.chi_tilde_core_inv(chi0h, u_r, beta, niv) + (base[f"gamma_{ch}"] - u_r[..., None, None, None]) / beta**2
+        x = osde.inv_dense(a) / beta
+        if ch == "dens":
+            gs = g_loc[..., g_loc.shape[-1] // 2 - niv : g_loc.shape[-1] // 2 + niv]
+            x[:, :, :, :, 0] += 2.0 * gs[:, :, None, None, :, None] * gs[None, None, :, :, None, :]
+        g2.append(osde.full_niw(x, 3))
+    sde = LocalSde(g_loc, g2[0], g2[1], u, beta, niw, niv, sh, synthetic.make_occupations(cfg)[0]).run()
+    dev_inp = sde.nonlocal_inputs(base)
+    assert isinstance(dev_inp["gamma_dens"], torch.Tensor) and dev_inp["gamma_dens"].is_cuda
+    host_inp = {k: (v.cpu().numpy() if isinstance(v, torch.Tensor) else v) for k, v in dev_inp.items()}
+    sig_dev = LadderPass(dev_inp).run().cpu().numpy()
+    sig_host = LadderPass(host_inp).run().cpu().numpy()
+    assert np.array_equal(sig_dev, sig_host)
+    ref = ladder.sde_pass(host_inp)
+    assert rel_err(sig_dev, ref["sigma"]) < 1e-10
+    assert rel_err(host_inp["gamma_magn"], base["gamma_magn"]) < 1e-10  # the round trip through the local ladder
