@@ -155,10 +155,17 @@ __global__ void __launch_bounds__(BZ_THREADS) dft_planes_kernel(const double2* _
 // ------------------------------------------------------------------------------------------------
 // bubble: one CTA per (w, nu, a, d), looping over (c, b)
 //   g_r: [T][n][n][Nk] with slot t = nu_index + niv + niw (nu_index in [-niv-niw, niv))
+// Per (c, b) plane P(R) = G_ad(R) G_cb(-R), stored transposed as P[(y, z)][x] so that reads across x are
+// conflict-free; the (y, z) sums are taken only at the distinct (qy, qz) pairs of the irreducible q list
+// (T[x][j] = sum_yz P[(y,z)][x] e^{i (qy_j y + qz_j z)}), then one x sum per irreducible q.  Work per plane
+// Nk * n_pairs + Q * nx complex FMAs (the wedge of a 32 x 32 grid has 17 pairs: 22K instead of a full x transform
+// plus the q sums, 38K).
 // ------------------------------------------------------------------------------------------------
 struct OutStrides7 {
   long long q, w, v, a, b, c, d;
 };
+
+constexpr int BUB_GR = 4;  // (qy, qz) pairs per thread in the (y, z) sums
 
 __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __restrict__ g_r, int nb, int niv,
                                                              int niw, Grid3 g, const int* __restrict__ q_irr,
@@ -166,12 +173,44 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
                                                              double beta, double2* __restrict__ out,
                                                              OutStrides7 os) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* P = reinterpret_cast<double2*>(smem_raw);
-  double2* T1 = P + g.nk;
-  double2* s_tw = T1 + g.nk;
-  int* s_q = reinterpret_cast<int*>(s_tw + g.nx + g.ny + g.nz);
+  double2* P = reinterpret_cast<double2*>(smem_raw);  // [yz][x]
+  double2* Tt = P + g.nk;                               // [x][pair]
+  double2* s_tw = Tt + g.nk;
+  int* s_q = reinterpret_cast<int*>(s_tw + g.nx + g.ny + g.nz);  // [n_qirr][3]
+  int* s_j = s_q + 3 * n_qirr;                                    // pair index of each q
+  int* s_pair = s_j + n_qirr;                                     // [n_pairs][2] (qy, qz)
+  int* s_np = s_pair + 2 * n_qirr;
   load_twiddles(s_tw, tw, g);
   for (int i = threadIdx.x; i < 3 * n_qirr; i += blockDim.x) s_q[i] = q_irr[i];
+  __syncthreads();
+  // distinct (qy, qz) pairs in order of first appearance: s_j[i] = the first q with the same pair (i itself for
+  // that first q), then, in q order, the first q of a pair numbers it and every later q copies its number (its
+  // first q, at a smaller index, is already numbered)
+  for (int i = threadIdx.x; i < n_qirr; i += blockDim.x) {
+    int lead = i;
+    for (int k = 0; k < i; ++k)
+      if (s_q[3 * k + 1] == s_q[3 * i + 1] && s_q[3 * k + 2] == s_q[3 * i + 2]) {
+        lead = k;
+        break;
+      }
+    s_j[i] = lead;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int np = 0;
+    for (int i = 0; i < n_qirr; ++i) {
+      if (s_j[i] == i) {
+        s_pair[2 * np] = s_q[3 * i + 1];
+        s_pair[2 * np + 1] = s_q[3 * i + 2];
+        s_j[i] = np++;
+      } else {
+        s_j[i] = s_j[s_j[i]];
+      }
+    }
+    *s_np = np;
+  }
+  __syncthreads();
+  const int np = *s_np;
 
   const int nv = 2 * niv, W = niw + 1;
   const int n2 = nb * nb;
@@ -179,6 +218,10 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
   const int nyz = g.ny * g.nz;
   const double inv_nk = 1.0 / (double)g.nk;
   const double pref = -beta / (double)g.nk;
+  const double2* twx = s_tw;
+  const double2* twy = s_tw + g.nx;
+  const double2* twz = s_tw + g.nx + g.ny;
+  const int ngp = (np + BUB_GR - 1) / BUB_GR;
   for (int blk = blockIdx.x; blk < total; blk += gridDim.x) {
     const int ad = blk % n2;
     const int v = (blk / n2) % nv;
@@ -192,31 +235,56 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
       const double2* gcb = g_r + (((size_t)t2 * nb + c) * nb + b) * g.nk;
       __syncthreads();
       for (int r = threadIdx.x; r < g.nk; r += blockDim.x) {
-        const int x = r / nyz, rem = r - x * nyz, y = rem / g.nz, z = rem - y * g.nz;
+        const int x = r / nyz, yz = r - x * nyz, y = yz / g.nz, z = yz - y * g.nz;
         const int xm = x ? g.nx - x : 0, ym = y ? g.ny - y : 0, zm = z ? g.nz - z : 0;
-        P[r] = cmul(gad[r], gcb[(xm * g.ny + ym) * g.nz + zm]);
+        P[yz * g.nx + x] = cmul(gad[r], gcb[(xm * g.ny + ym) * g.nz + zm]);
       }
       __syncthreads();
-      dft_axis_x(P, T1, s_tw, g);  // x axis in full (P -> T1)
-      // y and z axes only at the irreducible q points
-      const double2* twy = s_tw + g.nx;
-      const double2* twz = s_tw + g.nx + g.ny;
-      for (int iq = threadIdx.x; iq < n_qirr; iq += blockDim.x) {
-        const int qx = s_q[3 * iq], qy = s_q[3 * iq + 1], qz = s_q[3 * iq + 2];
-        double2 acc = make_double2(0.0, 0.0);
-        int my = 0;
+      // T[x][j] for BUB_GR pairs j per thread: consecutive threads take consecutive x (conflict-free P reads)
+      for (int t = threadIdx.x; t < g.nx * ngp; t += blockDim.x) {
+        const int x = t % g.nx, jg = t / g.nx;
+        double2 acc[BUB_GR];
+        int jy[BUB_GR], jz[BUB_GR], my[BUB_GR], mz[BUB_GR];
+#pragma unroll
+        for (int u = 0; u < BUB_GR; ++u) {
+          const int j = min(jg * BUB_GR + u, np - 1);  // pairs past np are computed on a valid pair and dropped
+          acc[u] = make_double2(0.0, 0.0);
+          jy[u] = s_pair[2 * j];
+          jz[u] = s_pair[2 * j + 1];
+          my[u] = 0;
+        }
         for (int y = 0; y < g.ny; ++y) {
-          double2 accz = make_double2(0.0, 0.0);
-          int mz = 0;
-          const double2* row = T1 + qx * nyz + y * g.nz;
+#pragma unroll
+          for (int u = 0; u < BUB_GR; ++u) mz[u] = 0;
           for (int z = 0; z < g.nz; ++z) {
-            cfma(accz, row[z], twz[mz]);
-            mz += qz;
-            if (mz >= g.nz) mz -= g.nz;
+            const double2 pv = P[(y * g.nz + z) * g.nx + x];
+#pragma unroll
+            for (int u = 0; u < BUB_GR; ++u) {
+              const double2 tt = g.nz > 1 ? cmul(twy[my[u]], twz[mz[u]]) : twy[my[u]];
+              cfma(acc[u], pv, tt);
+              mz[u] += jz[u];
+              if (mz[u] >= g.nz) mz[u] -= g.nz;
+            }
           }
-          cfma(acc, accz, twy[my]);
-          my += qy;
-          if (my >= g.ny) my -= g.ny;
+#pragma unroll
+          for (int u = 0; u < BUB_GR; ++u) {
+            my[u] += jy[u];
+            if (my[u] >= g.ny) my[u] -= g.ny;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < BUB_GR; ++u)
+          if (jg * BUB_GR + u < np) Tt[x * np + jg * BUB_GR + u] = acc[u];
+      }
+      __syncthreads();
+      for (int iq = threadIdx.x; iq < n_qirr; iq += blockDim.x) {
+        const int qx = s_q[3 * iq], j = s_j[iq];
+        double2 acc = make_double2(0.0, 0.0);
+        int mx = 0;
+        for (int x = 0; x < g.nx; ++x) {
+          cfma(acc, Tt[x * np + j], twx[mx]);
+          mx += qx;
+          if (mx >= g.nx) mx -= g.nx;
         }
         double re = (acc.x * inv_nk) * pref;
         double im = (acc.y * inv_nk) * pref;
@@ -419,7 +487,12 @@ int dga_bubble_c128(const void* g_r, int n_orb, int niv, int niw, int nx, int ny
   Grid3 g{nx, ny, nz, nx * ny * nz};
   OutStrides7 os{out_strides[0], out_strides[1], out_strides[2], out_strides[3],
                  out_strides[4], out_strides[5], out_strides[6]};
-  const size_t smem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + 3 * sizeof(int) * (size_t)n_qirr;
+  if ((long long)n_qirr > (long long)g.nk) {
+    dga_set_error("dga_bubble_c128: more irreducible q points (%d) than grid points", n_qirr);
+    return DGA_ERR_ARG;
+  }
+  const size_t smem =
+      (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + (6 * (size_t)n_qirr + 1) * sizeof(int);
   cudaFuncSetAttribute(bubble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long work = (long long)(niw + 1) * 2 * niv * n_orb * n_orb;
   const long long cap = 64LL * device_sm_count();

@@ -313,15 +313,18 @@ __global__ void lambda_kernel(const double2* __restrict__ chi, int Q, int W, con
 //   chi0_inv: [Q][W][nv][n2][n2]; X: [2][Q][W][N][n2]; uv: [2][Q][n2][n2]; chi_phys: [2][Q][W][n2][n2]
 //   k_dc: [Q][W][nv][n2][n2] or null;  out K: [Q][W][nv][n2][n2];  gamma_out (optional): [2][Q][W][nv][n2][n2]
 // ------------------------------------------------------------------------------------------------
-constexpr int KA_WARPS = 8;                            // matrices per block
-constexpr int KA_EPL = (MAX_N2 * MAX_N2 + 31) / 32;    // elements per lane
-__global__ void __launch_bounds__(32 * KA_WARPS, 2)
+constexpr int KA_WARPS = 8;  // matrices per block
+// One warp per matrix (q, w, nu); the n2 x n2 products run with the orbital-pair count NN2 fixed at compile time
+// (elements per lane EPL), four blocks per SM (two for 4 orbitals, whose accumulators need the registers) to hide
+// the latency of the dependent product chain.
+template <int NN2>
+__global__ void __launch_bounds__(32 * KA_WARPS, NN2 > 9 ? 2 : 4)
 kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __restrict__ X,
                                        const double2* __restrict__ uv, const double2* __restrict__ chi_phys,
-                                       const double2* __restrict__ k_dc, int n2, int nv, int W, int Q, double beta,
+                                       const double2* __restrict__ k_dc, int nv, int W, int Q, double beta,
                                        double2* __restrict__ K, double2* __restrict__ gamma_out) {
+  constexpr int n2 = NN2, nn = NN2 * NN2, EPL = (nn + 31) / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nn = n2 * n2;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double2* g3 = reinterpret_cast<double2*>(smem_raw) + (size_t)wib * 3 * nn;
   double2* t1 = g3 + nn;
@@ -334,9 +337,9 @@ kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __re
   const int q = (int)(qw / W);
   const int N = n2 * nv;
   const double2* c0i = chi0_inv + (size_t)t * nn;
-  double2 acc[KA_EPL];
+  double2 acc[EPL];
 #pragma unroll
-  for (int j = 0; j < KA_EPL; ++j) {
+  for (int j = 0; j < EPL; ++j) {
     const int e = lane + 32 * j;
     acc[j] = make_double2(0.0, 0.0);
     if (e < nn && k_dc) {
@@ -344,6 +347,7 @@ kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __re
       acc[j] = make_double2(-z.x, -z.y);
     }
   }
+#pragma unroll 1
   for (int ch = 0; ch < 2; ++ch) {
     const double2* x = X + ((size_t)ch * Q * W + qw) * N * n2;
     const double2* u = uv + ((size_t)ch * Q + q) * nn;
@@ -351,54 +355,63 @@ kernel_assembly_kernel(const double2* __restrict__ chi0_inv, const double2* __re
     double2* go = gamma_out ? gamma_out + ((size_t)ch * Q * W * nv + t) * nn : nullptr;
     // gamma = beta * (chi0_inv @ X_nu)
 #pragma unroll
-    for (int j = 0; j < KA_EPL; ++j) {
+    for (int j = 0; j < EPL; ++j) {
       const int e = lane + 32 * j;
-      if (e >= nn) break;
-      const int p = e / n2, sidx = e - p * n2;
-      double2 a = make_double2(0.0, 0.0);
-      for (int m = 0; m < n2; ++m) cfma(a, c0i[p * n2 + m], x[(size_t)(m * nv + v) * n2 + sidx]);
-      g3[e] = make_double2(beta * a.x, beta * a.y);
-      if (go) go[e] = g3[e];
+      if (e < nn) {
+        const int p = e / n2, sidx = e - p * n2;
+        double2 a = make_double2(0.0, 0.0);
+#pragma unroll 3
+        for (int m = 0; m < n2; ++m) cfma(a, c0i[p * n2 + m], x[(size_t)(m * nv + v) * n2 + sidx]);
+        const double2 g = make_double2(beta * a.x, beta * a.y);
+        g3[e] = g;
+        if (go) go[e] = g;
+      }
     }
     __syncwarp();
 #pragma unroll
-    for (int j = 0; j < KA_EPL; ++j) {  // t1 = gamma @ U_r
+    for (int j = 0; j < EPL; ++j) {  // t1 = gamma @ U_r
       const int e = lane + 32 * j;
-      if (e >= nn) break;
-      const int p = e / n2, sidx = e - p * n2;
-      double2 a = make_double2(0.0, 0.0);
-      for (int k = 0; k < n2; ++k) cfma(a, g3[p * n2 + k], u[k * n2 + sidx]);
-      t1[e] = a;
+      if (e < nn) {
+        const int p = e / n2, sidx = e - p * n2;
+        double2 a = make_double2(0.0, 0.0);
+#pragma unroll 3
+        for (int k = 0; k < n2; ++k) cfma(a, g3[p * n2 + k], u[k * n2 + sidx]);
+        t1[e] = a;
+      }
     }
     __syncwarp();
 #pragma unroll
-    for (int j = 0; j < KA_EPL; ++j) {  // t2 = gamma - t1 @ chi_r  (- 2/3 on the diagonal in the magnetic channel)
+    for (int j = 0; j < EPL; ++j) {  // t2 = gamma - t1 @ chi_r  (- 2/3 on the diagonal in the magnetic channel)
       const int e = lane + 32 * j;
-      if (e >= nn) break;
-      const int p = e / n2, sidx = e - p * n2;
-      double2 a = make_double2(0.0, 0.0);
-      for (int k = 0; k < n2; ++k) cfma(a, t1[p * n2 + k], cp[k * n2 + sidx]);
-      double2 r = csub(g3[e], a);
-      if (ch == 1 && p == sidx) r.x += -(2.0 / 3.0);
-      t2[e] = r;
+      if (e < nn) {
+        const int p = e / n2, sidx = e - p * n2;
+        double2 a = make_double2(0.0, 0.0);
+#pragma unroll 3
+        for (int k = 0; k < n2; ++k) cfma(a, t1[p * n2 + k], cp[k * n2 + sidx]);
+        double2 r = csub(g3[e], a);
+        if (ch == 1 && p == sidx) r.x += -(2.0 / 3.0);
+        t2[e] = r;
+      }
     }
     __syncwarp();
     const double f = ch == 0 ? 1.0 : 3.0;
 #pragma unroll
-    for (int j = 0; j < KA_EPL; ++j) {  // K += f U_r @ t2
+    for (int j = 0; j < EPL; ++j) {  // K += f U_r @ t2
       const int e = lane + 32 * j;
-      if (e >= nn) break;
-      const int p = e / n2, sidx = e - p * n2;
-      double2 a = make_double2(0.0, 0.0);
-      for (int k = 0; k < n2; ++k) cfma(a, u[p * n2 + k], t2[k * n2 + sidx]);
-      acc[j].x += f * a.x;
-      acc[j].y += f * a.y;
+      if (e < nn) {
+        const int p = e / n2, sidx = e - p * n2;
+        double2 a = make_double2(0.0, 0.0);
+#pragma unroll 3
+        for (int k = 0; k < n2; ++k) cfma(a, u[p * n2 + k], t2[k * n2 + sidx]);
+        acc[j].x += f * a.x;
+        acc[j].y += f * a.y;
+      }
     }
     __syncwarp();  // g3, t1, t2 are rewritten by the next channel
   }
   double2* o = K + (size_t)t * nn;
 #pragma unroll
-  for (int j = 0; j < KA_EPL; ++j) {
+  for (int j = 0; j < EPL; ++j) {
     const int e = lane + 32 * j;
     if (e < nn) o[e] = acc[j];
   }
@@ -600,10 +613,24 @@ int dga_kernel_assembly_c128(const void* chi0_inv, const void* X, const void* uv
   }
   const long long total = (long long)n_q * niw_half * 2 * niv_core;
   const size_t smem = (size_t)KA_WARPS * 3 * n2 * n2 * sizeof(double2);
-  cudaFuncSetAttribute(kernel_assembly_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kernel_assembly_kernel<<<(int)((total + KA_WARPS - 1) / KA_WARPS), 32 * KA_WARPS, smem, stream>>>(
-      (const double2*)chi0_inv, (const double2*)X, (const double2*)uv, (const double2*)chi_phys,
-      (const double2*)k_dc, n2, 2 * niv_core, niw_half, n_q, beta, (double2*)K, (double2*)gamma_out);
+  const int blocks = (int)((total + KA_WARPS - 1) / KA_WARPS);
+#define DGA_KA_CASE(NN)                                                                                        \
+  case NN:                                                                                                     \
+    cudaFuncSetAttribute(kernel_assembly_kernel<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+    kernel_assembly_kernel<NN><<<blocks, 32 * KA_WARPS, smem, stream>>>(                                       \
+        (const double2*)chi0_inv, (const double2*)X, (const double2*)uv, (const double2*)chi_phys,             \
+        (const double2*)k_dc, 2 * niv_core, niw_half, n_q, beta, (double2*)K, (double2*)gamma_out);            \
+    break;
+  switch (n2) {
+    DGA_KA_CASE(1)
+    DGA_KA_CASE(4)
+    DGA_KA_CASE(9)
+    DGA_KA_CASE(16)
+    default:
+      dga_set_error("dga_kernel_assembly_c128: unsupported orbital count (n_orb = %d)", n_orb);
+      return DGA_ERR_ARG;
+  }
+#undef DGA_KA_CASE
   return vstatus("dga_kernel_assembly_c128");
 }
 
