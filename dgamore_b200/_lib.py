@@ -61,6 +61,9 @@ SIGNATURES = {
     "dga_fill_sums_c128": (I, [VP, VP, PD, I, I, I, D, D, PD, PD, VP]),
     "dga_sigma_kmean_c128": (I, [VP, I, I, I, I, I, VP, VP]),
     "dga_bse_solve_sum_tuned_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, I, I, D, VP, PI, PI, VP, VP, SZ, VP]),
+    "dga_bse_eli_scratch_bytes": (SZ, [I, I, I]),
+    "dga_bse_solve_sum_eli_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, I, I, VP, VP, PI, VP, SZ, VP]),
+    "dga_eli_ladder_term_c128": (I, [VP, VP, VP, I, I, I, I, I, I, VP, VP]),
     "dga_lu_batched_c128": (I, [VP, I, I, LL, PI, PI, VP]),
     "dga_lu_solve_batched_c128": (I, [VP, PI, I, I, LL, VP, LL, LL, LL, I, VP, LL, PI, VP]),
     "dga_local_bubble_c128": (I, [VP, I, I, I, I, D, VP, VP]),

@@ -987,6 +987,128 @@ __global__ void __launch_bounds__(BSE_THREADS, 3)
   }
 }
 
+// ----------------------------------------------------------------------------------------------
+// Eliashberg full vertex fused into the FP64 BSE (eliashberg_solver.py:175-204): an item with w < Wpp keeps its LU
+// factors after the selector solve and solves the unit vectors of the pp box with them, writing
+//   f1[(p,nu),(s,nu')] = beta^2 (delta_{nu nu'} c0(nu)[p][s] - sum_{m,m'} c0(nu)[p][m] chi*[(m,nu),(m',nu')] c0(nu')[m'][s])
+// for nu, nu' in [niv - P, niv + P).  The ladder term (Z G3(nu) G3(nu'), which needs the lambda-corrected chi_r and
+// the three-leg vertex of the whole pass) is added afterwards by eli_ladder_term_kernel; f1 + term is the sum
+// eli_full_vertex_kernel forms, in the same order, from the same factors.
+// ----------------------------------------------------------------------------------------------
+template <int NRB>
+__device__ void eli_box_epilogue(const StructuredSource& src, const WorkItem& wi, int N, int n2, int nv, int W, int P,
+                                 double beta2, const double2* __restrict__ A, double2* __restrict__ Y,
+                                 const int* __restrict__ perm, double2* __restrict__ o, BseSmem<double2>& sm) {
+  const int tid = threadIdx.x, T = blockDim.x;
+  const int nvp = 2 * P, Mb = n2 * nvp, KB = NRB / n2, off = nv / 2 - P;
+  for (int v0 = 0; v0 < nvp; v0 += KB) {
+    for (int e = tid; e < N * NRB; e += T) {
+      const int i = e % N, sidx = e / N;
+      const int kk = sidx / n2, mp = sidx - kk * n2;
+      const int vb = v0 + kk;
+      const int j = mp * nv + off + vb;
+      Y[(size_t)sidx * N + i] = make_double2((kk < KB && vb < nvp && perm[i] == j) ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    lu_solve_inplace<double2, double2, NRB>(A, N, N, Y, sm);
+    for (int e = tid; e < Mb * KB * n2; e += T) {
+      const int sidx = e % n2;
+      const int kk = (e / n2) % KB;
+      const int row = e / (n2 * KB);
+      const int vbp = v0 + kk;
+      if (vbp >= nvp) continue;
+      const int p = row / nvp, vb = row - p * nvp;
+      const int vr = off + vb, vc = off + vbp;
+      const double2* c0r = src.chi0_inv + (((size_t)wi.q * W + wi.w) * nv + vr) * n2 * n2;
+      const double2* c0c = src.chi0_inv + (((size_t)wi.q * W + wi.w) * nv + vc) * n2 * n2;
+      double2 t = make_double2(0.0, 0.0);
+      for (int m = 0; m < n2; ++m) {
+        double2 inner = make_double2(0.0, 0.0);
+        for (int mp = 0; mp < n2; ++mp) cfma(inner, Y[(size_t)(kk * n2 + mp) * N + m * nv + vr], c0c[mp * n2 + sidx]);
+        cfma(t, c0r[p * n2 + m], inner);
+      }
+      double2 f1 = make_double2(-t.x, -t.y);
+      if (vb == vbp) f1 = cadd(f1, c0r[p * n2 + sidx]);
+      o[(size_t)row * Mb + sidx * nvp + vbp] = cscale(f1, beta2);
+    }
+    __syncthreads();
+  }
+}
+
+// FP64 BSE (as bse_solve_sum_fp64_kernel) with the pp-box epilogue for items w < Wpp; NRB = box columns per solve
+// (KB = NRB / n2 box frequencies).  out_pp: [2][Q][Wpp][Mb][Mb].
+template <int NR, int NRB>
+__global__ void __launch_bounds__(BSE_THREADS, 3)
+    bse_fp64_eli_kernel(StructuredSource src, const WorkItem* __restrict__ work, int n_items, int N, int n2, int nv,
+                        int W, int Q, double beta, double2* __restrict__ out, int P, int Wpp,
+                        double2* __restrict__ out_pp, int* __restrict__ status, double2* __restrict__ scratch,
+                        size_t slot_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BseSmem<double2>& sm = *reinterpret_cast<BseSmem<double2>*>(smem_raw);
+  int* piv = reinterpret_cast<int*>(smem_raw + sizeof(BseSmem<double2>));
+  int* perm = piv + N;
+  double2* A = scratch + (size_t)blockIdx.x * slot_elems;
+  double2* Y = A + (size_t)N * N;
+  const int Mb = n2 * 2 * P;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const WorkItem wi = work[item];
+    double2* o = out + (((size_t)wi.ch * Q + wi.q) * W + wi.w) * (size_t)N * n2;
+    const int st = solve_item_fp64<StructuredSource, NR>(src, wi, N, nv, beta, o, A, Y, sm, piv, perm);
+    if (wi.w < Wpp) {
+      double2* opp = out_pp + (((size_t)wi.ch * Q + wi.q) * Wpp + wi.w) * (size_t)Mb * Mb;
+      eli_box_epilogue<NRB>(src, wi, N, n2, nv, W, P, beta * beta, A, Y, perm, opp, sm);
+    }
+    if (threadIdx.x == 0 && status) status[item] = st;
+  }
+}
+
+// f[ch][q][w] += (Z G3(nu)) G3(nu') over the pp box, Z = U_r - U_r chi_r U_r (the second term of the full vertex,
+// eliashberg_solver.py:175-204); one CTA per (ch, q, w < Wpp), Z and H(nu) = Z G3(nu) in shared memory.
+//   g3: [2][Q][W][nv][n2][n2]; chi_phys: [2][Q][W][n2][n2]; uv: [2][Q][n2][n2]; f: [2][Q][Wpp][Mb][Mb]
+__global__ void eli_ladder_term_kernel(const double2* __restrict__ uv, const double2* __restrict__ g3,
+                                       const double2* __restrict__ chi_phys, int n2, int nv, int W, int Q, int P,
+                                       int Wpp, double2* __restrict__ f) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* Z = reinterpret_cast<double2*>(smem_raw);
+  double2* H = Z + n2 * n2;
+  const int wq = blockIdx.x, w = wq % Wpp, q = (wq / Wpp) % Q, ch = wq / (Wpp * Q);
+  const int tid = threadIdx.x, T = blockDim.x;
+  const int nvp = 2 * P, Mb = n2 * nvp, off = nv / 2 - P;
+  const double2* uvq = uv + ((size_t)ch * Q + q) * n2 * n2;
+  const double2* cp = chi_phys + (((size_t)ch * Q + q) * W + w) * n2 * n2;
+  for (int e = tid; e < n2 * n2; e += T) {
+    const int p = e / n2, s = e - p * n2;
+    double2 acc = uvq[e];
+    for (int t = 0; t < n2; ++t) {
+      double2 cu = make_double2(0.0, 0.0);
+      for (int u = 0; u < n2; ++u) cfma(cu, cp[t * n2 + u], uvq[u * n2 + s]);
+      cfms(acc, uvq[p * n2 + t], cu);
+    }
+    Z[e] = acc;
+  }
+  __syncthreads();
+  const double2* g3q = g3 + ((((size_t)ch * Q + q) * W + w) * nv) * n2 * n2;
+  for (int e = tid; e < nvp * n2 * n2; e += T) {
+    const int vb = e / (n2 * n2), ps = e - vb * n2 * n2, p = ps / n2, s = ps - p * n2;
+    const double2* g = g3q + (size_t)(off + vb) * n2 * n2;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int t = 0; t < n2; ++t) cfma(acc, Z[p * n2 + t], g[t * n2 + s]);
+    H[e] = acc;
+  }
+  __syncthreads();
+  double2* o = f + (size_t)wq * Mb * Mb;
+  for (int e = tid; e < Mb * Mb; e += T) {
+    const int row = e / Mb, colx = e - row * Mb;  // column index sidx * nvp + vbp
+    const int sidx = colx / nvp, vbp = colx - sidx * nvp;
+    const int p = row / nvp, vb = row - p * nvp;
+    const double2* hrow = H + (size_t)vb * n2 * n2 + p * n2;
+    const double2* gcol = g3q + (size_t)(off + vbp) * n2 * n2;
+    double2 f2 = make_double2(0.0, 0.0);
+    for (int u = 0; u < n2; ++u) cfma(f2, hrow[u], gcol[u * n2 + sidx]);
+    o[e] = cadd(o[e], f2);
+  }
+}
+
 }  // namespace dga
 
 using namespace dga;
@@ -1835,6 +1957,99 @@ int dga_lu_solve_batched_c128(const void* lu, const int* piv, int N, int n_mat, 
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     dga_set_error("dga_lu_solve_batched_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Scratch bytes of dga_bse_solve_sum_eli_c128 for n_items items of size N.
+size_t dga_bse_eli_scratch_bytes(int N, int n2, int n_items) {
+  if (N <= 0 || !supported_rhs(n2) || n_items <= 0) return 0;
+  const size_t smem = bse_smem_bytes(N);
+  const int grid = grid_for(bse_fp64_eli_kernel<9, 9>, n_items, smem);
+  return (size_t)grid * ((size_t)N * N + (size_t)N * eli_rhs(n2)) * sizeof(double2);
+}
+
+// dga_bse_solve_sum_c128 whose items with w < w_pp also write the chi* part of the Eliashberg full vertex in the pp
+// box (niv_pp) from the same LU factors: out_pp [2][Q][w_pp][Mb][Mb], Mb = n2 * 2 niv_pp; dga_eli_ladder_term_c128
+// completes it to the vertex dga_eli_full_vertex_c128 computes.
+int dga_bse_solve_sum_eli_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                               const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
+                               int n_items, int niv_pp, int w_pp, void* out, void* out_pp, int* status, void* scratch,
+                               size_t scratch_bytes, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv, N = n2 * nv;
+  if (!supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 || n_ch != 2 || n_items <= 0 ||
+      N > BSE_MAX_N || niv_pp <= 0 || niv_pp > niv || w_pp <= 0 || w_pp > niw_half || !gamma_cm || !chi0_inv ||
+      !uv || !work || !out || !out_pp || !scratch) {
+    dga_set_error("dga_bse_solve_sum_eli_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = bse_smem_bytes(N);
+  const size_t slot = (size_t)N * N + (size_t)N * eli_rhs(n2);
+  int grid = 0;
+  switch (n2) {
+    case 1: grid = grid_for(bse_fp64_eli_kernel<1, 16>, n_items, smem); break;
+    case 4: grid = grid_for(bse_fp64_eli_kernel<4, 16>, n_items, smem); break;
+    case 9: grid = grid_for(bse_fp64_eli_kernel<9, 9>, n_items, smem); break;
+    default: grid = grid_for(bse_fp64_eli_kernel<16, 16>, n_items, smem); break;
+  }
+  if (scratch_bytes < (size_t)grid * slot * sizeof(double2)) {
+    dga_set_error("dga_bse_solve_sum_eli_c128: scratch too small");
+    return DGA_ERR_SCRATCH;
+  }
+  StructuredSource src;
+  src.gamma_cm = (const double2*)gamma_cm;
+  src.chi0_inv = (const double2*)chi0_inv;
+  src.uv = (const double2*)uv;
+  src.n2 = n2;
+  src.nv = nv;
+  src.W = niw_half;
+  src.Q = n_q;
+  src.inv_beta2 = inv_beta2;
+#define DGA_ELI_CASE(NRV, NRB)                                                                                 \
+  case NRV:                                                                                                    \
+    bse_fp64_eli_kernel<NRV, NRB><<<grid, BSE_THREADS, smem, stream>>>(                                        \
+        src, (const WorkItem*)work, n_items, N, n2, nv, niw_half, n_q, beta, (double2*)out, niv_pp, w_pp,      \
+        (double2*)out_pp, status, (double2*)scratch, slot);                                                    \
+    break;
+  switch (n2) {
+    DGA_ELI_CASE(1, 16)
+    DGA_ELI_CASE(4, 16)
+    DGA_ELI_CASE(9, 9)
+    DGA_ELI_CASE(16, 16)
+  }
+#undef DGA_ELI_CASE
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_bse_solve_sum_eli_c128: launch failed: %s", cudaGetErrorString(err));
+    return DGA_ERR_LAUNCH;
+  }
+  return DGA_OK;
+}
+
+// f += (Z G3(nu)) G3(nu') over the pp box for every (ch, q, w < w_pp), Z = U_r - U_r chi_r U_r: completes the
+// out_pp of dga_bse_solve_sum_eli_c128 to the full vertex (g3 [2][Q][W][nv][n2][n2], chi_phys [2][Q][W][n2][n2]
+// lambda-corrected, uv [2][Q][n2][n2]).
+int dga_eli_ladder_term_c128(const void* uv, const void* g3, const void* chi_phys, int n_orb, int niv, int niw_half,
+                             int n_q, int niv_pp, int w_pp, void* f, cudaStream_t stream) {
+  const int n2 = n_orb * n_orb, nv = 2 * niv;
+  if (!uv || !g3 || !chi_phys || !f || !supported_rhs(n2) || n_orb <= 0 || niv <= 0 || niw_half <= 0 || n_q <= 0 ||
+      niv_pp <= 0 || niv_pp > niv || w_pp <= 0 || w_pp > niw_half) {
+    dga_set_error("dga_eli_ladder_term_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = ((size_t)n2 * n2 + (size_t)2 * niv_pp * n2 * n2) * sizeof(double2);
+  cudaFuncSetAttribute(eli_ladder_term_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  eli_ladder_term_kernel<<<2 * n_q * w_pp, 256, smem, stream>>>((const double2*)uv, (const double2*)g3,
+                                                              (const double2*)chi_phys, n2, nv, niw_half, n_q,
+                                                              niv_pp, w_pp, (double2*)f);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    dga_set_error("dga_eli_ladder_term_c128: launch failed: %s", cudaGetErrorString(err));
     return DGA_ERR_LAUNCH;
   }
   return DGA_OK;

@@ -11,6 +11,11 @@ Mirrors ``dgamore/eliashberg_solver.py``:
   (G. W. Stewart, SIAM J. Matrix Anal. Appl. 23, 601 (2001)) with the operator applied by
   ``dga_eli_matvec_c128`` on the device, FP64 throughout, and the same start vector construction.
 
+The full vertex comes from the pass itself when it was built with ``LadderPass(..., eliashberg_pp=niv_pp)``: its
+FP64 BSE then solves the pp-box unit vectors with each item's own LU factors (``dga_bse_solve_sum_eli_c128``) and
+this stage only adds the ladder term (``dga_eli_ladder_term_c128``), instead of factorising every (q, w < 2 niv_pp)
+item a second time (``dga_eli_full_vertex_c128``, the path for passes built without it).
+
 Every vertex and operator stage is a libdga_b200 kernel; torch provides device memory and the small vector
 algebra of the Arnoldi basis.
 """
@@ -85,17 +90,28 @@ class EliashbergSolver:
         work = [(ch, q, w) for w in range(self.w_pp) for ch in range(2) for q in range(Q)]
         self.work = torch.tensor(work, dtype=torch.int32, device=dev)
         n_items = len(work)
-        self.vertex_status = torch.zeros(n_items, dtype=torch.int32, device=dev)
-        sbytes = int(lib().dga_eli_vertex_scratch_bytes(n, sh.niv, P, n_items))
-        scratch = torch.empty(sbytes // 16 + 1, dtype=C128, device=dev)
-        fph = torch.empty((2, Q, self.w_pp, M, M), dtype=C128, device=dev)
-        call("dga_eli_full_vertex_c128", n, sh.niv, sh.W, Q, P, self.w_pp, sh.beta, lp.inv_beta2, _p(lp.gamma_cm),
-             _p(lp.chi0_inv), _p(lp.uv), _p(lp.gamma3), _p(chi_r), _p(self.work), n_items, _p(fph),
-             _p(self.vertex_status), _p(scratch), scratch.numel() * 16, _s())
-        del scratch
+        self.fused = bool(getattr(lp, "f_pp_ready", False)) and lp.eli_P == P
+        if self.fused:
+            # the pass's FP64 BSE already wrote the chi* part of the vertex from its own LU factors: add the
+            # ladder term in place (the buffer is consumed) instead of factorising every item again
+            fph = lp.f_pp
+            call("dga_eli_ladder_term_c128", _p(lp.uv), _p(lp.gamma3), _p(chi_r), n, sh.niv, sh.W, Q, P, self.w_pp,
+                 _p(fph), _s())
+            lp.f_pp_ready = False
+            self.vertex_status = lp.bse_status.clone()
+        else:
+            self.vertex_status = torch.zeros(n_items, dtype=torch.int32, device=dev)
+            sbytes = int(lib().dga_eli_vertex_scratch_bytes(n, sh.niv, P, n_items))
+            scratch = torch.empty(sbytes // 16 + 1, dtype=C128, device=dev)
+            fph = torch.empty((2, Q, self.w_pp, M, M), dtype=C128, device=dev)
+            call("dga_eli_full_vertex_c128", n, sh.niv, sh.W, Q, P, self.w_pp, sh.beta, lp.inv_beta2,
+                 _p(lp.gamma_cm), _p(lp.chi0_inv), _p(lp.uv), _p(lp.gamma3), _p(chi_r), _p(self.work), n_items,
+                 _p(fph), _p(self.vertex_status), _p(scratch), scratch.numel() * 16, _s())
+            del scratch
         self.gamma_pp_irr = torch.empty((2, Q, M, M), dtype=C128, device=dev)
         call("dga_eli_pairing_vertex_c128", _p(fph), n, P, Q, self.w_pp, _p(self.gamma_pp_irr), _s())
-        del fph
+        if not self.fused:
+            del fph
         # Gamma(R) = sign * FFT_q of the pairing vertex expanded to the full zone (eliashberg_solver.py:392-396)
         nx, ny, nz = sh.nk
         self.mat = torch.empty((2, sh.nk_tot, M, M), dtype=C128, device=dev)

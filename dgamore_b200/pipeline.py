@@ -182,7 +182,8 @@ class LadderPass:
 
     def __init__(self, inp: dict, device: str = "cuda", do_lambda: bool | None = None, sigma_chunks: int | None = None,
                  keep_intermediates: bool = True, precision: str = "fp64", refine_tol: float = 1e-10,
-                 refine_max_iter: int = 6, resolve_grid: int = 148, own_bse_scratch: bool = True):
+                 refine_max_iter: int = 6, resolve_grid: int = 148, own_bse_scratch: bool = True,
+                 eliashberg_pp: int | None = None):
         lib()  # fail loudly before anything else if the CUDA library is missing
         self.dev = torch.device(device)
         g_k = np.asarray(inp["g_k"])
@@ -267,6 +268,8 @@ class LadderPass:
         if not self.own_bse_scratch:
             # the BSE runs in a batch launch (serving.solve_bse_batch) that brings its own scratch
             self.bse_scratch = self.mixed_scratch = None
+        elif precision == "fp64" and eliashberg_pp:
+            self.bse_scratch_bytes = int(lib().dga_bse_eli_scratch_bytes(N, n2, self.n_items))
         elif precision == "fp64":
             self.bse_scratch_bytes = int(lib().dga_bse_scratch_bytes(N, n2, self.n_items))
         else:
@@ -285,6 +288,18 @@ class LadderPass:
         self.status = torch.zeros(4, dtype=torch.int32, device=dev)
         self.K = torch.empty((Q, W, nv, n2, n2), dtype=C128, device=dev)
         self.gamma3 = torch.empty((2, Q, W, nv, n2, n2), dtype=C128, device=dev) if keep_intermediates else None
+        # Eliashberg vertex fused into the FP64 BSE: the items w < 2 niv_pp also write the chi* part of the full
+        # vertex in the pp box from their own LU factors (eliashberg_solver.EliashbergSolver adds the ladder term)
+        self.eli_P = int(eliashberg_pp) if eliashberg_pp else 0
+        self.f_pp = None
+        if self.eli_P:
+            if precision != "fp64" or not own_bse_scratch or not keep_intermediates:
+                raise ValueError("the fused Eliashberg vertex needs the FP64 BSE, its own scratch and the three-leg vertex")
+            if 2 * self.eli_P > W or self.eli_P > sh.niv:
+                raise ValueError(f"eliashberg_pp={self.eli_P} needs 2 niv_pp <= niw + 1 and niv_pp <= niv")
+            mb = n2 * 2 * self.eli_P
+            self.f_pp = torch.empty((2, Q, 2 * self.eli_P, mb, mb), dtype=C128, device=dev)
+        self.f_pp_ready = False  # f_pp holds the chi* part of this pass's vertex (the fused BSE ran last)
         if sigma_chunks is None:
             sigma_chunks = sigma_chunks_for(sh)
         self.sigma_chunks = sigma_chunks
@@ -351,6 +366,7 @@ class LadderPass:
         sh = self.sh
         if not self.own_bse_scratch:
             raise RuntimeError("this pass was built without BSE scratch: run its BSE through serving.solve_bse_batch")
+        self.f_pp_ready = False
         if self.tuning is not None:
             mixed = 1 if self.precision == "mixed" else 0
             call("dga_bse_solve_sum_tuned_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
@@ -371,6 +387,13 @@ class LadderPass:
             call("dga_bse_resolve_fp64_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
                  _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, _p(self.X),
                  _p(self.bse_status), self.resolve_grid, _p(self.bse_scratch), self.bse_scratch.numel() * 16, _s())
+            return
+        if self.eli_P:
+            call("dga_bse_solve_sum_eli_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2,
+                 _p(self.gamma_cm), _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, self.eli_P,
+                 2 * self.eli_P, _p(self.X), _p(self.f_pp), _p(self.bse_status), _p(self.bse_scratch),
+                 self.bse_scratch.numel() * 16, _s())
+            self.f_pp_ready = True
             return
         call("dga_bse_solve_sum_c128", sh.n_orb, sh.niv, sh.W, sh.n_q, 2, sh.beta, self.inv_beta2, _p(self.gamma_cm),
              _p(self.chi0_inv), _p(self.uv), _p(self.work), self.n_items, _p(self.X), _p(self.bse_status),

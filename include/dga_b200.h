@@ -286,6 +286,20 @@ int dga_eli_full_vertex_c128(int n_orb, int niv, int niw_half, int n_q, int niv_
                              const void* g3, const void* chi_phys, const int* work, int n_items, void* out,
                              int* status, void* scratch, size_t scratch_bytes, dga_stream_t stream);
 
+/* The Eliashberg full vertex fused into the FP64 BSE: dga_bse_solve_sum_c128 (same inputs, X into out) whose items
+ * with w < w_pp also solve the unit vectors of the pp box (niv_pp) with the item's own LU factors and write
+ * out_pp [2][Q][w_pp][Mb][Mb] = beta^2 (delta c0 - c0 chi* c0), the chi* part of the vertex of
+ * create_full_vertex_q_r(_v2) (dgamore/eliashberg_solver.py:78-298), without a second factorisation.
+ * dga_eli_ladder_term_c128 adds the ladder term (U_r - U_r chi_r U_r) gamma_r gamma_r once the pass has the
+ * lambda-corrected chi_r and the three-leg vertex, giving the out of dga_eli_full_vertex_c128. */
+size_t dga_bse_eli_scratch_bytes(int N, int n2, int n_items);
+int dga_bse_solve_sum_eli_c128(int n_orb, int niv, int niw_half, int n_q, int n_ch, double beta, double inv_beta2,
+                               const void* gamma_cm, const void* chi0_inv, const void* uv, const int* work,
+                               int n_items, int niv_pp, int w_pp, void* out, void* out_pp, int* status, void* scratch,
+                               size_t scratch_bytes, dga_stream_t stream);
+int dga_eli_ladder_term_c128(const void* uv, const void* g3, const void* chi_phys, int n_orb, int niv, int niw_half,
+                             int n_q, int niv_pp, int w_pp, void* f, dga_stream_t stream);
+
 /* PH -> PP (w = 0) transform, singlet/triplet combination and gap-equation layout; replaces
  * _transform_vertex_frequencies_w0 and the Gamma_sing/trip sums (dgamore/eliashberg_solver.py:44-75, 620-628).
  * fph: [2][Q][w_pp][Mb][Mb] from dga_eli_full_vertex_c128; out [2 (sing, trip)][Q][Mb][Mb] with

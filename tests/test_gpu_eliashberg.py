@@ -95,3 +95,31 @@ def test_leading_eigenvalues_complex64_operator(solver, ch):
     assert status == 0
     expect = ref[f"lambdas_{ch}"]
     assert np.max(np.abs(vals[:3] - expect[:3])) < 1e-6
+
+
+@pytest.mark.parametrize("name", ELI)
+def test_vertex_fused_into_the_bse(name):
+    """A pass built with eliashberg_pp writes the chi* part of the full vertex from its own LU factors; the
+    Eliashberg stage then only adds the ladder term.  Pairing vertices equal the separate-kernel path (same
+    factors, same order of operations) and the upstream's, the pass's Sigma is unchanged and the buffer is
+    consumed by the stage."""
+    from dgamore_b200.eliashberg_solver import EliashbergSolver, default_niv_pp
+    from dgamore_b200.pipeline import LadderPass
+
+    inp, ref = load_golden(name)
+    plain = LadderPass(inp)
+    sig_plain = plain.run().cpu().numpy()
+    es_plain = EliashbergSolver(plain)
+    P = default_niv_pp(plain.sh.niw, plain.sh.niv)
+    lp = LadderPass(inp, eliashberg_pp=P)
+    sig = lp.run().cpu().numpy()
+    assert np.array_equal(sig, sig_plain)
+    assert lp.f_pp_ready
+    es = EliashbergSolver(lp)
+    torch.cuda.synchronize()
+    assert es.fused and not lp.f_pp_ready
+    assert int(es.vertex_status.abs().sum().item()) == 0
+    for st, ch in ((0, "sing"), (1, "trip")):
+        fused = es.pairing_vertex_ref_layout(st)
+        assert rel_err(fused, es_plain.pairing_vertex_ref_layout(st)) < 1e-14
+        assert rel_err(fused, ref[f"gamma_pp_{ch}"]) < 1e-10
