@@ -299,6 +299,101 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
 }
 
 // ------------------------------------------------------------------------------------------------
+// IBZ -> FBZ with the auto-mode orbital rotation (n_point_base.py:462-507, symmetry_reduction.py:791-902):
+//   dst[k](o1,o2,o3,o4; f) = sigma_k^2 sum U_{o1 p} U*_{o2 q} U_{o3 r} U*_{o4 s} [src[irrk_inv[k]](p,q,r,s; f)]^(*conj_k)
+// for four-orbital objects whose per-k block holds the orbital indices at strides st[0..3] and frequency pairs
+// (f1 < F1, f2 < F2) at f1 t1 + f2 t2.  One CTA per (k, chunk of frequency pairs): the chunk is staged in shared
+// memory and transformed one orbital index at a time (n-term sums); a point whose U_k is the identity without
+// conjugation is a plain copy.
+// ------------------------------------------------------------------------------------------------
+struct RotLayout {
+  long long st[4];
+  long long t1, t2;
+  int F1, F2;
+  long long block;  // elements per k
+};
+
+__global__ void __launch_bounds__(BZ_THREADS) fbz_rotate_kernel(const double2* __restrict__ src,
+                                                                 const int* __restrict__ irrk_inv,
+                                                                 const double2* __restrict__ us,
+                                                                 const double* __restrict__ sigmas,
+                                                                 const unsigned char* __restrict__ conjs, int n,
+                                                                 RotLayout L, int fc, double2* __restrict__ dst) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n4 = n * n * n * n;
+  double2* X = reinterpret_cast<double2*>(smem_raw);  // [fc][n4]
+  double2* Y = X + (size_t)fc * n4;
+  __shared__ double2 U[16];
+  __shared__ int ident;
+  const int k = blockIdx.y;
+  const long long nf = (long long)L.F1 * L.F2;
+  const long long f0 = (long long)blockIdx.x * fc;
+  if (f0 >= nf) return;
+  const int nfc = (int)min((long long)fc, nf - f0);
+  const int tid = threadIdx.x, T = blockDim.x;
+  if (tid < n * n) U[tid] = us[(size_t)k * n * n + tid];
+  __syncthreads();
+  if (tid == 0) {
+    int id = conjs[k] ? 0 : 1;
+    for (int a = 0; a < n; ++a)
+      for (int b = 0; b < n; ++b) {
+        const double2 u = U[a * n + b];
+        if (u.y != 0.0 || u.x != (a == b ? 1.0 : 0.0)) id = 0;
+      }
+    ident = id;
+  }
+  __syncthreads();
+  const double2* s = src + (size_t)irrk_inv[k] * L.block;
+  double2* d = dst + (size_t)k * L.block;
+  auto offset = [&](int fl, int e) -> long long {
+    const long long f = f0 + fl;
+    const int f1 = (int)(f / L.F2), f2 = (int)(f - (long long)f1 * L.F2);
+    const int o4 = e % n, o3 = (e / n) % n, o2 = (e / (n * n)) % n, o1 = e / (n * n * n);
+    return f1 * L.t1 + f2 * L.t2 + o1 * L.st[0] + o2 * L.st[1] + o3 * L.st[2] + o4 * L.st[3];
+  };
+  if (ident) {
+    for (int e = tid; e < nfc * n4; e += T) {
+      const long long off = offset(e / n4, e % n4);
+      d[off] = s[off];
+    }
+    return;
+  }
+  const bool cj = conjs[k] != 0;
+  for (int e = tid; e < nfc * n4; e += T) {
+    double2 v = s[offset(e / n4, e % n4)];
+    if (cj) v.y = -v.y;
+    X[e] = v;
+  }
+  __syncthreads();
+  // one orbital index at a time: position 0 and 2 with U, 1 and 3 with U*
+  int stride = n * n * n;
+  for (int pos = 0; pos < 4; ++pos) {
+    const bool dag = (pos & 1) != 0;
+    for (int e = tid; e < nfc * n4; e += T) {
+      const int fl = e / n4, r = e - fl * n4;
+      const int a = (r / stride) % n, base = r - a * stride;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int p = 0; p < n; ++p) {
+        double2 u = U[a * n + p];
+        if (dag) u.y = -u.y;
+        cfma(acc, u, X[(size_t)fl * n4 + base + p * stride]);
+      }
+      Y[e] = acc;
+    }
+    __syncthreads();
+    double2* t = X;
+    X = Y;
+    Y = t;
+    stride /= n;
+  }
+  const double sg = sigmas ? sigmas[k] * sigmas[k] : 1.0;
+  for (int e = tid; e < nfc * n4; e += T) {
+    const double2 v = X[e];
+    d[offset(e / n4, e % n4)] = make_double2(sg * v.x, sg * v.y);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
 // Sigma partial sums: CTA per (nu >= 0, i, j, w-chunk)
 //   kern: [Q][W][nv][n2][n2] irreducible kernel, matrix row (a,i), column (d,j); W = niw+1, nv = 2 niv
 //   g_r:  [T][n][n][Nk] with slot t = nu_index + niw, nu_index in [-niw, niv+niw)
@@ -499,6 +594,41 @@ int dga_bubble_c128(const void* g_r, int n_orb, int niv, int niw, int nx, int ny
   bubble_kernel<<<(int)(work < cap ? work : cap), BZ_THREADS, smem, stream>>>(
       (const double2*)g_r, n_orb, niv, niw, g, q_irr, n_qirr, (const double2*)tw, beta, (double2*)out, os);
   return launch_status("dga_bubble_c128");
+}
+
+// Expansion of a four-orbital object from the irreducible to the full zone with the auto-mode orbital rotation;
+// layout and arguments in include/dga_b200.h.
+int dga_fbz_rotate_c128(const void* src, const int* irrk_inv, int nk, const void* us, const double* sigmas,
+                        const unsigned char* conjs, int n_orb, const long long* orb_strides, long long f1_stride,
+                        int f1_count, long long f2_stride, int f2_count, long long block, void* dst,
+                        cudaStream_t stream) {
+  if (!src || !irrk_inv || !us || !conjs || !orb_strides || !dst || n_orb <= 0 || n_orb > 4 || nk <= 0 ||
+      nk > 65535 || f1_count <= 0 || f2_count <= 0 || block <= 0) {
+    dga_set_error("dga_fbz_rotate_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  RotLayout L;
+  for (int i = 0; i < 4; ++i) L.st[i] = orb_strides[i];
+  L.t1 = f1_stride;
+  L.t2 = f2_stride;
+  L.F1 = f1_count;
+  L.F2 = f2_count;
+  L.block = block;
+  const int n4 = n_orb * n_orb * n_orb * n_orb;
+  int fc = (int)((96 * 1024) / ((size_t)n4 * 2 * sizeof(double2)));
+  if (fc > 64) fc = 64;
+  if (fc < 1) fc = 1;
+  const long long nf = (long long)f1_count * f2_count;
+  const long long chunks = (nf + fc - 1) / fc;
+  if (chunks > 0x7fffffffLL) {
+    dga_set_error("dga_fbz_rotate_c128: too many frequency chunks");
+    return DGA_ERR_ARG;
+  }
+  const size_t smem = (size_t)fc * n4 * 2 * sizeof(double2);
+  cudaFuncSetAttribute(fbz_rotate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  fbz_rotate_kernel<<<dim3((unsigned)chunks, nk), BZ_THREADS, smem, stream>>>(
+      (const double2*)src, irrk_inv, (const double2*)us, sigmas, conjs, n_orb, L, fc, (double2*)dst);
+  return launch_status("dga_fbz_rotate_c128");
 }
 
 // Bytes of the partial-sum buffer of dga_sigma_c128.

@@ -28,7 +28,7 @@ import numpy as np
 import scipy.linalg as sla
 import torch
 
-from ._lib import call, lib
+from ._lib import call, lib, ll_array
 from .pipeline import LadderPass, _p, _s
 
 C128 = torch.complex128
@@ -115,9 +115,20 @@ class EliashbergSolver:
         # Gamma(R) = sign * FFT_q of the pairing vertex expanded to the full zone (eliashberg_solver.py:392-396)
         nx, ny, nz = sh.nk
         self.mat = torch.empty((2, sh.nk_tot, M, M), dtype=C128, device=dev)
+        full = torch.empty((sh.nk_tot, M, M), dtype=C128, device=dev) if sh.rotated else None
         for st, sign in ((0, 1.0), (1, -1.0)):
-            call("dga_dft_planes_gather_c128", _p(self.gamma_pp_irr[st]), 1, 0, M * M, _p(self.mat[st]), 1, 0, M * M,
-                 1, M * M, nx, ny, nz, _p(lp.tw_fwd), sign, _p(lp.irrk_inv), _s())
+            src, gather = self.gamma_pp_irr[st], lp.irrk_inv
+            if sh.rotated:
+                # auto-mode symmetries: each zone point's orbital rotation (U on the upstream positions o1, o3 =
+                # rows a, b; U* on o2, o4 = columns c, d of Mat[(a,b,nu)][(c,d,nu')] = Gamma[a,c,b,d])
+                P2 = 2 * P
+                call("dga_fbz_rotate_c128", _p(src), _p(lp.irrk_inv), sh.nk_tot, _p(lp.rot_us), _p(lp.rot_sigmas),
+                     _p(lp.rot_conjs), n, ll_array([n * P2 * M, n * P2, P2 * M, P2]), M, P2, 1, P2, M * M, _p(full),
+                     _s())
+                src, gather = full, lp.rot_ident
+            call("dga_dft_planes_gather_c128", _p(src), 1, 0, M * M, _p(self.mat[st]), 1, 0, M * M,
+                 1, M * M, nx, ny, nz, _p(lp.tw_fwd), sign, _p(gather), _s())
+        del full
         if precision == "mixed":
             mat64 = torch.empty((2, sh.nk_tot, M, M), dtype=torch.complex64, device=dev)
             call("dga_narrow_c128_to_c64", _p(self.mat), _p(mat64), self.mat.numel(), _s())

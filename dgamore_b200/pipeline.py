@@ -77,6 +77,7 @@ class PassShapes:
     niv_shell: int
     n_q: int
     niv_g: int
+    rotated: bool = False  # auto-mode symmetries with orbital rotations in the IBZ -> FBZ map
 
     @property
     def n2(self):
@@ -114,8 +115,18 @@ class PassShapes:
         return cls(
             n_orb=u.shape[0], nk=tuple(int(x) for x in inp["nk"]), beta=float(inp["beta"]), niw=int(inp["niw"]),
             niv=int(inp["niv_core"]), niv_shell=int(inp["niv_shell"]), n_q=len(inp["irrk_ind"]),
-            niv_g=np.shape(g_k)[-1] // 2,
+            niv_g=np.shape(g_k)[-1] // 2, rotated=needs_rotation(inp),
         )
+
+
+def needs_rotation(inp: dict) -> bool:
+    """True when the inputs carry auto-mode orbital rotations (``orbital_us``, ``orbital_conjs``) that are not all
+    the identity without conjugation (KGrid.specify_auto_symmetries, brillouin_zone.py:365-449)."""
+    if "orbital_us" not in inp:
+        return False
+    us = np.asarray(inp["orbital_us"])
+    conjs = np.asarray(inp["orbital_conjs"], dtype=bool)
+    return bool(conjs.any()) or not np.array_equal(us, np.broadcast_to(np.eye(us.shape[-1]), us.shape))
 
 
 _ALLOC_GRAIN = 512  # the caching allocator's block granularity
@@ -170,6 +181,8 @@ def estimate_device_bytes(sh: PassShapes, precision: str = "fp64", keep_intermed
         (chunks * sh.niv * n2 * nk * c * 2) // c * c + c,      # Sigma scratch
         nk * n * n * 2 * sh.niv * c,                           # Sigma
     ]
+    if sh.rotated:
+        sizes += [nk * n * n * c, nk * 8, nk, nk * 4, nk * W * nv * n2 * n2 * c]  # U_k, sigma_k, conj_k, map, K(FBZ)
     if keep_intermediates:
         sizes.append(2 * Q * W * nv * n2 * n2 * c)
     if own_bse_scratch:
@@ -211,6 +224,17 @@ class LadderPass:
         q_list = np.array(np.unravel_index(irr, nk)).T.astype(np.int32)
         self.q_irr = torch.from_numpy(np.ascontiguousarray(q_list)).to(dev)
         self.irrk_inv = torch.from_numpy(np.asarray(inp["irrk_inv"], dtype=np.int32)).to(dev)
+        # auto-mode symmetries (KGrid.specify_auto_symmetries): per-k orbital rotations of the IBZ -> FBZ map
+        self.rot_us = self.rot_sigmas = self.rot_conjs = self.rot_ident = self.k_full = None
+        if sh.rotated:
+            us = np.asarray(inp["orbital_us"], dtype=np.complex128).reshape(sh.nk_tot, n_orb, n_orb)
+            conjs = np.asarray(inp["orbital_conjs"], dtype=bool).ravel()
+            sig = np.asarray(inp.get("orbital_sigmas", np.ones(len(conjs))), dtype=np.float64).ravel()
+            self.rot_us = torch.from_numpy(np.ascontiguousarray(us)).to(dev)
+            self.rot_sigmas = torch.from_numpy(np.ascontiguousarray(sig)).to(dev)
+            self.rot_conjs = torch.from_numpy(conjs.astype(np.uint8)).to(dev)
+            self.rot_ident = torch.arange(sh.nk_tot, dtype=torch.int32, device=dev)
+            self.k_full = torch.empty((sh.nk_tot, sh.W, sh.nv, sh.n2, sh.n2), dtype=C128, device=dev)
         self.irrk_count = torch.from_numpy(np.asarray(inp["irrk_count"], dtype=np.int64)).to(dev)
         self.tw_fwd = torch.from_numpy(twiddles(nk, -1)).to(dev)
         self.tw_inv = torch.from_numpy(twiddles(nk, +1)).to(dev)
@@ -423,8 +447,16 @@ class LadderPass:
         sh = self.sh
         self._g_transform(self.g_r_sigma, -sh.niw, self.t_sigma)
         nx, ny, nz = sh.nk
-        call("dga_sigma_c128", _p(self.K), _p(self.g_r_sigma), sh.n_orb, sh.niv, sh.niw, sh.n_q, nx, ny, nz,
-             _p(self.irrk_inv), _p(self.tw_inv), sh.beta, self.sigma_chunks, _p(self.sigma), _p(self.sigma_scratch),
+        kern, n_q, inv = self.K, sh.n_q, self.irrk_inv
+        if sh.rotated:
+            # K(q) over the full zone with each point's orbital rotation, then the contraction without a gather
+            n, n2, W, nv = sh.n_orb, sh.n2, sh.W, sh.nv
+            call("dga_fbz_rotate_c128", _p(self.K), _p(self.irrk_inv), sh.nk_tot, _p(self.rot_us), _p(self.rot_sigmas),
+                 _p(self.rot_conjs), n, ll_array([n * n2, n2, 1, n]), n2 * n2, W * nv, 0, 1, W * nv * n2 * n2,
+                 _p(self.k_full), _s())
+            kern, n_q, inv = self.k_full, sh.nk_tot, self.rot_ident
+        call("dga_sigma_c128", _p(kern), _p(self.g_r_sigma), sh.n_orb, sh.niv, sh.niw, n_q, nx, ny, nz,
+             _p(inv), _p(self.tw_inv), sh.beta, self.sigma_chunks, _p(self.sigma), _p(self.sigma_scratch),
              self.sigma_scratch.numel() * 16, _s())
 
     def set_occupations(self, occ: np.ndarray, occ_k: np.ndarray, v_q_full: np.ndarray, u: np.ndarray) -> None:

@@ -44,6 +44,7 @@ class DgaConfig:
     u: float = 8.0
     j: float = 0.0
     t: tuple = (1.0,)  # nearest-neighbour hopping per orbital (isotropic)
+    t_aniso: tuple = ()  # per-orbital (t_x, t_y) nearest-neighbour hoppings; when given, they replace t
     tp: float = 0.0
     tpp: float = 0.0
     t_perp: float = 0.0  # on-site hopping between orbitals 0 and 1 (bilayer)
@@ -87,6 +88,10 @@ CONFIGS = {
     # Eliashberg parity cases (niv_pp = min(niw, niv) // 2 = 3)
     "t4e": DgaConfig("t4e", 2, (6, 6, 1), 15.0, 6, 6, 0, u=6.0, t=(1.0, 1.0), t_perp=0.8, n=1.8, seed=15),
     "t5e": DgaConfig("t5e", 1, (8, 8, 1), 10.0, 6, 6, 0, u=4.0, t=(1.0,), tp=-0.2, n=0.9, seed=16),
+    # t2g with the anisotropic d_xz / d_yz hoppings that the square lattice's x <-> y operations exchange: the
+    # irreducible wedge and the per-k orbital rotations come from the upstream's symmetry discovery (auto mode)
+    "t3a": DgaConfig("t3a", 3, (4, 4, 1), 20.0, 2, 2, 0, u=2.3, j=0.4, t_aniso=((0.5, 0.5), (0.5, 0.1), (0.1, 0.5)),
+                     n=1.0, seed=17, symmetries=()),
 }
 
 
@@ -96,14 +101,20 @@ CONFIGS = {
 
 
 def dispersion(cfg: DgaConfig, grid: KGrid) -> np.ndarray:
-    """e_k [kx,ky,kz,n,n] for isotropic square-lattice hoppings per orbital plus an on-site t_perp."""
+    """e_k [kx,ky,kz,n,n] for square-lattice hoppings per orbital (isotropic t, or (t_x, t_y) from t_aniso) plus
+    an on-site t_perp."""
     kx, ky = np.meshgrid(grid.kx, grid.ky, indexing="ij")
     nb = cfg.n_bands
     ek = np.zeros((*grid.nk, nb, nb), dtype=np.complex128)
     for a in range(nb):
         t = cfg.t[a] if a < len(cfg.t) else cfg.t[-1]
+        if cfg.t_aniso:
+            tx, ty = cfg.t_aniso[a]
+            nn = -2 * (tx * np.cos(kx) + ty * np.cos(ky))
+        else:
+            nn = -2 * t * (np.cos(kx) + np.cos(ky))
         e = (
-            -2 * t * (np.cos(kx) + np.cos(ky))
+            nn
             - 4 * cfg.tp * np.cos(kx) * np.cos(ky)
             - 2 * cfg.tpp * (np.cos(2 * kx) + np.cos(2 * ky))
         )

@@ -55,6 +55,18 @@ int dga_bse_block_ctas_per_sm(int n2);
 int dga_strided_copy_c128(const void* src, void* dst, int ndim, const long long* shape, const long long* src_stride,
                           const long long* dst_stride, double scale, dga_stream_t stream);
 
+/* IBZ -> FBZ expansion of a four-orbital object with the auto-mode orbital rotation (IAmNonLocal._map_to_full_bz,
+ * dgamore/n_point_base.py:462-507, through symmetry_reduction.apply_auto_orbital_transform, :791-902):
+ *   dst[k](o1,o2,o3,o4; f) = sigma_k^2 sum U_{o1 p} U*_{o2 q} U_{o3 r} U*_{o4 s} [src[irrk_inv[k]](p,q,r,s; f)]^(*conj_k)
+ * for k < nk.  A block of `block` elements per point holds orbital index i at orb_strides[i] and the frequency
+ * pairs (f1 < f1_count, f2 < f2_count) at f1 f1_stride + f2 f2_stride; us [nk][n][n], sigmas [nk] (may be null),
+ * conjs [nk] (bytes, nonzero = conjugate) are the per-k data of the upstream's symmetry discovery
+ * (KGrid.specify_auto_symmetries, brillouin_zone.py:365-449).  n_orb <= 4, nk <= 65535. */
+int dga_fbz_rotate_c128(const void* src, const int* irrk_inv, int nk, const void* us, const double* sigmas,
+                        const unsigned char* conjs, int n_orb, const long long* orb_strides, long long f1_stride,
+                        int f1_count, long long f2_stride, int f2_count, long long block, void* dst,
+                        dga_stream_t stream);
+
 /* Batched separable DFT of momentum planes; replaces IAmNonLocal.fft / ifft (dgamore/n_point_base.py:509-551).
  * Element (plane p = p_hi*n_lo + p_lo, point R) at p_hi*s_hi + p_lo*s_lo + R*s_r; tw = nx+ny+nz twiddles
  * e^{s 2 pi i m/n} (sign folded in by the caller); output multiplied by `scale`. */

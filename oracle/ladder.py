@@ -348,9 +348,21 @@ def sigma_dc_kernel(f_dc: np.ndarray, chi0_full: np.ndarray, u: np.ndarray, beta
 # ----------------------------------------------------------------------------------------------
 
 
-def map_to_full_bz(x_irr: np.ndarray, irrk_inv: np.ndarray) -> np.ndarray:
-    """x[k] = x_irr[irrk_inv[k]] (n_point_base.py:489-494), no orbital rotation (non-auto symmetries)."""
-    return np.take(x_irr, irrk_inv.ravel(), axis=0)
+def map_to_full_bz(x_irr: np.ndarray, irrk_inv: np.ndarray, rotations=None) -> np.ndarray:
+    """x[k] = x_irr[irrk_inv[k]] (n_point_base.py:489-494); with the auto-mode ``rotations`` = (us [Nk][n][n],
+    sigmas [Nk], conjs [Nk]) of a four-orbital object [k, a, b, c, d, ...] also
+    x_abcd(k) = sigma_k^2 U_ap U*_bq U_cr U*_ds [x_pqrs(k_rep)]^{(*conj_k)} (n_point_base.py:496-504,
+    symmetry_reduction.py:791-902)."""
+    x = np.take(x_irr, irrk_inv.ravel(), axis=0)
+    if rotations is None:
+        return x
+    us, sigmas, conjs = rotations
+    out = np.empty_like(x)
+    for k in range(x.shape[0]):
+        blk = np.conj(x[k]) if conjs[k] else x[k]
+        u = us[k]
+        out[k] = sigmas[k] ** 2 * np.einsum("ap,bq,cr,ds,pqrs...->abcd...", u, u.conj(), u, u.conj(), blk)
+    return out
 
 
 def sigma_from_kernel_fft(kernel_full: np.ndarray, g_k: np.ndarray, nk: tuple, beta: float, niv_core: int) -> np.ndarray:
@@ -468,7 +480,8 @@ def sde_pass(inp: dict, do_lambda: bool = True) -> dict:
         k_total = k_total + factor * k_r
     out["lambdas"] = lambdas
     out["kernel"] = k_total
-    k_full = map_to_full_bz(k_total, inp["irrk_inv"])
+    rot = (inp["orbital_us"], inp["orbital_sigmas"], inp["orbital_conjs"]) if "orbital_us" in inp else None
+    k_full = map_to_full_bz(k_total, inp["irrk_inv"], rot)
     out["sigma"] = sigma_from_kernel_fft(k_full, inp["g_k"], tuple(inp["nk"]), beta, niv_core)
     return out
 
@@ -543,10 +556,11 @@ def eliashberg_matvec(gamma_r_signed, gamma_flip, chi0pp, gap, beta, sign):
     return np.fft.ifftn(norm * new, axes=(0, 1, 2))
 
 
-def eliashberg_operator(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel):
-    """Gamma(R) and its flipped form for the matvec (eliashberg_solver.py:392-400); gamma_pp_irr [q_irr,...]."""
+def eliashberg_operator(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel, rotations=None):
+    """Gamma(R) and its flipped form for the matvec (eliashberg_solver.py:392-400); gamma_pp_irr [q_irr,...];
+    ``rotations``: the auto-mode per-k orbital rotations of the IBZ -> FBZ map (map_to_full_bz)."""
     sign = 1 if channel == "sing" else -1
-    full = map_to_full_bz(gamma_pp_irr, irrk_inv).reshape(*nk, *gamma_pp_irr.shape[1:])
+    full = map_to_full_bz(gamma_pp_irr, irrk_inv, rotations).reshape(*nk, *gamma_pp_irr.shape[1:])
     g_r = sign * sp_fft.fftn(full, axes=(0, 1, 2))
     flip = flip_momentum_axis(g_r)
     flip = np.flip(flip, axis=-1)
@@ -554,11 +568,11 @@ def eliashberg_operator(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel):
     return g_r, flip, sign
 
 
-def eliashberg_eigs(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel, v0, n_eig=4, tol=1e-10):
+def eliashberg_eigs(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel, v0, n_eig=4, tol=1e-10, rotations=None):
     """Leading eigenvalues via ARPACK eigsh(which='LA') as eliashberg_solver.py:430-452."""
     import scipy.sparse.linalg as spla
 
-    g_r, flip, sign = eliashberg_operator(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel)
+    g_r, flip, sign = eliashberg_operator(gamma_pp_irr, irrk_inv, nk, chi0pp, beta, channel, rotations)
     shape = v0.shape
 
     def mv(x):

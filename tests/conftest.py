@@ -38,4 +38,4 @@ def rel_err(a, b) -> float:
     return float(np.max(np.abs(a - b))) / scale
 
 
-GOLDEN_CONFIGS = ("t1", "t1b", "t2", "t3", "t4e", "t5e")
+GOLDEN_CONFIGS = ("t1", "t1b", "t2", "t3", "t4e", "t5e", "t3a")

@@ -5,7 +5,8 @@ variable (see _ref_harness.py); the sources are not needed where the tests run, 
 
     python tests/golden/make_golden.py
 
-For each small synthetic configuration (``dgamore_b200.synthetic.CONFIGS``: t1, t1b, t2, t3) it builds the
+For each small synthetic configuration (``dgamore_b200.synthetic.CONFIGS``: t1, t1b, t2, t3, and t3a, whose
+anisotropic t2g hoppings are reduced by the upstream's symmetry discovery with per-k orbital rotations) it builds the
 inputs of one nonlocal pass, then replays the upstream call sequence of ``calculate_self_energy_q``
 (dgamore/nonlocal_sde.py:786-879) with the upstream functions, in FP64 (``IHaveMat.mat`` patched to keep
 complex128), and stores inputs and every intermediate into ``<name>.npz``.
@@ -87,6 +88,21 @@ def run_reference_pass(name: str, variants: bool = True) -> dict:
     cfg = synthetic.CONFIGS[name]
     inp = synthetic.make_inputs(cfg)
     _setup_config(cfg, inp)
+    if name in AUTO_CONFIGS:
+        # the upstream's symmetry discovery on H(k) (brillouin_zone.py:365-449, DGAmore.py:98-109): its irreducible
+        # wedge and per-k orbital rotations replace the synthetic grid's and travel with the inputs
+        auto = bz.KGrid(tuple(cfg.nk), symmetries=bz.get_lattice_symmetries_from_string("auto"))
+        auto.specify_auto_symmetries(inp["ek"])
+        config.lattice.k_grid = auto
+        config.lattice.q_grid = auto
+        nk_tot, nb = int(np.prod(cfg.nk)), cfg.n_bands
+        inp["irrk_ind"] = np.asarray(auto.irrk_ind)
+        inp["irrk_inv"] = np.asarray(auto.irrk_inv).ravel()
+        inp["irrk_count"] = np.asarray(auto.irrk_count)
+        inp["v_q_irr"] = np.asarray(inp["v_q_full"])[inp["irrk_ind"]]
+        inp["orbital_us"] = np.asarray(auto._auto_us).reshape(nk_tot, nb, nb).astype(np.complex128)
+        inp["orbital_sigmas"] = np.asarray(auto._auto_sigmas).reshape(nk_tot).astype(np.float64)
+        inp["orbital_conjs"] = np.asarray(auto._auto_conjs).reshape(nk_tot).astype(bool)
     grid = config.lattice.q_grid
     assert np.array_equal(grid.irrk_ind, inp["irrk_ind"]), "irreducible wedge differs from upstream"
     assert np.array_equal(grid.irrk_inv.ravel(), inp["irrk_inv"]), "irreducible inverse map differs"
@@ -170,7 +186,8 @@ def run_reference_pass(name: str, variants: bool = True) -> dict:
     return save
 
 
-ELIASHBERG_CONFIGS = ("t4e", "t5e")
+ELIASHBERG_CONFIGS = ("t4e", "t5e", "t3a")
+AUTO_CONFIGS = ("t3a",)
 
 
 def run_reference_eliashberg(cfg, inp, giwk, u_loc, v_nonloc, gchi0_q_core_inv, keep, grid) -> dict:
@@ -305,6 +322,12 @@ def main():
     if "--only-hf" in sys.argv:
         np.savez_compressed(os.path.join(HERE, "hartree_fock.npz"), **hf_fixtures())
         print("wrote hartree_fock.npz")
+        return
+    if "--only" in sys.argv:
+        for name in sys.argv[sys.argv.index("--only") + 1:]:
+            data = run_reference_pass(name)
+            np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+            print("wrote", name, sorted(data.keys()))
         return
     np.savez_compressed(os.path.join(HERE, "hartree_fock.npz"), **hf_fixtures())
     for name in ("t1", "t1b", "t2", "t3") + ELIASHBERG_CONFIGS:

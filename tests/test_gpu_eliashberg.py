@@ -12,7 +12,7 @@ from conftest import load_golden, rel_err
 
 pytestmark = pytest.mark.gpu
 
-ELI = ("t4e", "t5e")
+ELI = ("t4e", "t5e", "t3a")  # t3a: auto-mode symmetries with per-k orbital rotations
 
 
 @pytest.fixture(scope="module", params=ELI)
@@ -52,7 +52,9 @@ def test_gap_operator_matches_oracle(solver, ch):
     P = es.P
     st = 0 if ch == "sing" else 1
     chi0pp = L.chi0_pp_full_grid(inp["g_k"], P)
-    g_r, flip, sign = L.eliashberg_operator(ref[f"gamma_pp_{ch}"], inp["irrk_inv"], inp["nk"], chi0pp, sh.beta, ch)
+    rot = (inp["orbital_us"], inp["orbital_sigmas"], inp["orbital_conjs"]) if "orbital_us" in inp else None
+    g_r, flip, sign = L.eliashberg_operator(ref[f"gamma_pp_{ch}"], inp["irrk_inv"], inp["nk"], chi0pp, sh.beta, ch,
+                                            rot)
     rng = np.random.default_rng(5)
     gap = rng.standard_normal((*inp["nk"], sh.n_orb, sh.n_orb, 2 * P)) + 1j * rng.standard_normal(
         (*inp["nk"], sh.n_orb, sh.n_orb, 2 * P))
@@ -68,6 +70,8 @@ def test_leading_eigenvalues(solver, ch):
     name, inp, ref, es = solver
     sh = es.lp.sh
     v0 = initial_gap(sh.nk, sh.n_orb, es.P, ch, "d-wave", inp["irrk_ind"], inp["irrk_inv"])
+    if "orbital_us" in inp:  # auto mode: a random start vector (the symmetrised d-wave form assumes no rotations)
+        v0 = np.random.default_rng(3).random(v0.shape) + 0j
     vals, vecs, status = es.eigs(ch, 4, 1e-12, v0.ravel())
     assert status == 0
     expect = ref[f"lambdas_{ch}"]

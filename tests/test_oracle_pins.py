@@ -119,7 +119,7 @@ def test_kgrid_irreducible_sizes():
     assert g.irrk_count.sum() == 48 * 48
 
 
-@pytest.mark.parametrize("name", ("t4e", "t5e"))
+@pytest.mark.parametrize("name", ("t4e", "t5e", "t3a"))
 def test_oracle_eliashberg_matches_upstream_fp64(name):
     """Full vertex in pp notation, chi0pp and the leading singlet/triplet eigenvalues (eliashberg_solver.py)."""
     inp, ref = load_golden(name)
@@ -139,7 +139,11 @@ def test_oracle_eliashberg_matches_upstream_fp64(name):
     for ch in ("sing", "trip"):
         assert rel_err(gam[ch], ref[f"gamma_pp_{ch}"]) < 1e-12
         v0 = L.symmetrise_gap(L.d_wave_gap(inp["nk"], nb, niv_pp, ch), inp["irrk_ind"], inp["irrk_inv"])
-        vals, _ = L.eliashberg_eigs(gam[ch], inp["irrk_inv"], inp["nk"], chi0pp, inp["beta"], ch, v0, 4, 1e-12)
+        rot = (inp["orbital_us"], inp["orbital_sigmas"], inp["orbital_conjs"]) if "orbital_us" in inp else None
+        if rot is not None:  # the upstream's auto-mode start vector is not the symmetrised d-wave form
+            v0 = np.random.default_rng(3).random(v0.shape) + 0j
+        vals, _ = L.eliashberg_eigs(gam[ch], inp["irrk_inv"], inp["nk"], chi0pp, inp["beta"], ch, v0, 4, 1e-12,
+                                    rotations=rot)
         assert np.max(np.abs(vals - ref[f"lambdas_{ch}"])) < 1e-9 * max(1.0, np.max(np.abs(vals)))
 
 
