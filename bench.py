@@ -390,6 +390,51 @@ def c4_batch_leg(precision: str, steps: int = 3) -> dict:
     return out
 
 
+def small_configs_leg(steps: int = 3, configs=("c1", "c2")) -> dict:
+    """The single-band configurations at their stated sizes (C1: 16x16, niv = niw = 20, N = 40; C2: 64x64,
+    niv = niw = 60, N = 120), both forms replayed from one CUDA graph each: solves/s, the mixed/FP64 ratio, the
+    Sigma error of the mixed form against the FP64 form and the difference of the lambdas."""
+    import torch
+
+    from dgamore_b200 import synthetic
+    from dgamore_b200.pipeline import LadderPass
+
+    out = {}
+    for name in configs:
+        inp = synthetic.make_inputs(name)
+        res = {}
+        sig = {}
+        lam = {}
+        for precision in ("mixed", "fp64"):
+            lp = LadderPass(inp, precision=precision, keep_intermediates=False)
+            lp.capture()
+            for _ in range(2):
+                lp.replay()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(steps):
+                lp.replay()
+            b.record()
+            b.synchronize()
+            ms = a.elapsed_time(b) / steps
+            res[precision] = {"ms_per_pass": ms, "solves_per_s": lp.sh.n_solves / (ms / 1e3),
+                              "bse_status_nonzero": int((lp.bse_status != 0).sum().item())}
+            sig[precision] = lp.sigma.cpu().numpy()
+            lam[precision] = lp.lambdas.cpu().numpy()
+            del lp
+            torch.cuda.empty_cache()
+        out[name] = {
+            "workload": f"{name}: 1-orbital {inp['nk'][0]}x{inp['nk'][1]}, niv = niw = {inp['niw']}, "
+                        f"N = {2 * inp['niv_core']}, {2 * len(inp['irrk_ind']) * (inp['niw'] + 1)} solves per pass",
+            "mixed": res["mixed"], "fp64": res["fp64"],
+            "mixed_vs_fp64": res["fp64"]["ms_per_pass"] / res["mixed"]["ms_per_pass"],
+            "sigma_rel_err_vs_fp64": float(np.abs(sig["mixed"] - sig["fp64"]).max() / np.abs(sig["fp64"]).max()),
+            "lambda_abs_diff_vs_fp64": float(np.abs(lam["mixed"] - lam["fp64"]).max()),
+        }
+    return out
+
+
 def eliashberg_leg(config: str = "c4_bilayer") -> dict:
     """Linearised Eliashberg on the bilayer configuration: pairing vertices from the FP64 pass, the gap-equation
     matvec timed with CUDA events (HBM roofline: it streams Gamma(R) [Nk][M][M] once per application), and the
@@ -559,6 +604,7 @@ def run_ours(args, rank: int, world: int, local: int):
         for prec in ("fp64", "mixed"):
             serving[prec] = serving_leg(prec, args.serve_requests)
     eliashberg = eliashberg_leg() if (args.eliashberg and rank == 0) else None
+    small = small_configs_leg() if (args.small and rank == 0) else None
     c4 = {}
     if args.c4 and rank == 0:
         for prec in ("fp64", "mixed"):
@@ -630,6 +676,7 @@ def run_ours(args, rank: int, world: int, local: int):
         "clocks": clocks.summary(),
         "serving": serving,
         "eliashberg": eliashberg,
+        "small_configs": small,
         "c4_batch": c4,
     }
     if rank == 0:
@@ -651,6 +698,7 @@ def main():
     ap.add_argument("--tune-cache", action="store_true", help="keep autotuner choices in _build/tuning.json")
     ap.add_argument("--eliashberg", type=int, default=1, help="run the Eliashberg leg (0: skip)")
     ap.add_argument("--c4", type=int, default=1, help="run the uneven-orbital batch leg under one graph (0: skip)")
+    ap.add_argument("--small", type=int, default=1, help="run the C1/C2 mixed-vs-FP64 leg (0: skip)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     try:

@@ -9,6 +9,11 @@ With ``--eliashberg K`` it then builds the pairing vertices of the same pass (FP
 applies the singlet gap-equation operator K times:
 
     python -m dgamore_b200.profile_case --config c4_bilayer --nk 48 --niw 30 --eliashberg 5
+
+With ``--local-sde`` it runs the local Schwinger-Dyson equation instead, on inputs made from the model vertex
+(synthetic.local_sde_inputs) with the configuration's fermionic box and ``--niw`` bosonic frequencies:
+
+    python -m dgamore_b200.profile_case --config c3 --niw 40 --local-sde --passes 2
 """
 
 from __future__ import annotations
@@ -36,7 +41,21 @@ def main(argv=None):
     ap.add_argument("--passes", type=int, default=1)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--eliashberg", type=int, default=0, help="gap-equation operator applications after the pass")
+    ap.add_argument("--local-sde", action="store_true", help="run the local Schwinger-Dyson equation instead")
     args = ap.parse_args(argv)
+    if args.local_sde:
+        from .local_sde import LocalSde
+
+        base = synthetic.CONFIGS[args.config]
+        lsi, _ = synthetic.local_sde_inputs(base, niw=args.niw)
+        sde = LocalSde(*lsi)
+        for _ in range(args.passes):
+            sde.run()
+        torch.cuda.synchronize()
+        sde.check()
+        print(json.dumps({"case": f"{args.config}_local_niw{args.niw}", "n_orb": sde.n, "N": sde.N, "Nf": sde.Nf,
+                          "matrices_per_lu": 2 * sde.W, "passes": args.passes}))
+        return
     cfg = reduced_config(args.config, args.nk, args.niw)
     inp = synthetic.make_inputs(cfg)
     lp = LadderPass(inp, keep_intermediates=args.eliashberg > 0, precision=args.precision)

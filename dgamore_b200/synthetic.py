@@ -380,3 +380,58 @@ def make_occupations(cfg: DgaConfig | str, seed_offset: int = 7919) -> tuple[np.
     occ_k += 0.5 * (pert + np.conj(np.swapaxes(pert, -1, -2)))
     occ = occ_k.mean(axis=(0, 1, 2))
     return occ, occ_k
+
+
+def local_sde_inputs(cfg: DgaConfig | str, niw: int | None = None, niv: int | None = None,
+                     niv_shell: int | None = None, nk: tuple = (8, 8, 1), seed_offset: int = 303) -> tuple:
+    """Inputs of the local Schwinger-Dyson equation (dgamore/local_sde.py:175) made from the model vertex: the
+    k-mean of the lattice G, and G2_r such that the equation returns gamma_model in the core box,
+
+        chi_r = [chi~_core^-1 + (Gamma_r - U_r)/beta^2]^-1,  G2_r = chi_r / beta (+ 2 G_ab(nu) G_cd(nu') at w = 0, dens),
+
+    with chi~_core^-1 the shell-corrected bubble term [(chi0^-1 + U_r/beta^2 over the full box)^-1]_core^-1, G2 in
+    the full w range.  Returns ((g, g2_dens, g2_magn, u, beta, niw, niv, niv_shell, occ), (gamma_dens, gamma_magn))."""
+    import dataclasses
+
+    if isinstance(cfg, str):
+        cfg = CONFIGS[cfg]
+    niw = cfg.niw if niw is None else niw
+    niv = cfg.niv if niv is None else niv
+    niv_shell = cfg.niv_shell if niv_shell is None else niv_shell
+    cfg = dataclasses.replace(cfg, nk=nk, niw=niw, niv=niv, niv_shell=niv_shell)
+    rng = np.random.default_rng(cfg.seed + seed_offset)
+    grid = KGrid(cfg.nk, cfg.symmetries)
+    ek = dispersion(cfg, grid)
+    mu = find_mu(cfg, ek)
+    niv_g = niv + niv_shell + niw + 4
+    g = g_lattice(ek, hubbard_i_sigma(cfg, mu, niv_g), mu, cfg.beta).mean(axis=(0, 1, 2))
+    u = kanamori_u(cfg)
+    beta = cfg.beta
+    nb, nvf, nv = cfg.n_bands, 2 * (niv + niv_shell), 2 * niv
+    n2 = nb * nb
+    chi0 = local_bubble(g, niw, niv + niv_shell, beta)  # [a,b,c,d,w,nu] full box, w >= 0
+    c0 = chi0.transpose(4, 5, 0, 1, 3, 2).reshape(niw + 1, nvf, n2, n2)  # [w][nu][(a,b)][(d,c)]
+    c0inv = np.linalg.inv(c0)
+    g2s, gammas = [], []
+    for ch in ("dens", "magn"):
+        u_r = u_channel(u, ch)
+        uc = _to_compound_orb(u_r)
+        # full-box dense chi~^-1 = blockdiag(chi0^-1) + U_r/beta^2 in every (nu, nu') block
+        dense = np.broadcast_to(uc[None, None, :, None, :] / beta**2, (niw + 1, nvf, n2, nvf, n2)).copy()
+        for v in range(nvf):
+            dense[:, v, :, v, :] += c0inv[:, v]
+        dense = dense.transpose(0, 2, 1, 4, 3).reshape(niw + 1, n2 * nvf, n2 * nvf)  # rows (p, nu)
+        idx = np.array([p * nvf + niv_shell + v for p in range(n2) for v in range(nv)])
+        tilde = np.linalg.inv(np.linalg.inv(dense)[:, idx][:, :, idx])
+        gamma = gamma_model(cfg, u, ch, rng, niv)
+        gm = (gamma - u_r[..., None, None, None]).transpose(4, 0, 1, 5, 3, 2, 6).reshape(niw + 1, n2 * nv, n2 * nv)
+        chi = np.linalg.inv(tilde + gm / beta**2)
+        g2 = chi.reshape(niw + 1, nb, nb, nv, nb, nb, nv).transpose(1, 2, 5, 4, 0, 3, 6) / beta  # [a,b,c,d,w,nu,nu']
+        if ch == "dens":
+            gs = g[..., g.shape[-1] // 2 - niv : g.shape[-1] // 2 + niv]
+            g2[:, :, :, :, 0] += 2.0 * gs[:, :, None, None, :, None] * gs[None, None, :, :, None, :]
+        neg = np.conj(np.flip(g2[:, :, :, :, 1:], axis=(4, 5, 6)))
+        g2s.append(np.concatenate([neg, g2], axis=4))
+        gammas.append(gamma)
+    occ = make_occupations(cfg)[0]
+    return (g, g2s[0], g2s[1], u, beta, niw, niv, niv_shell, occ), tuple(gammas)
