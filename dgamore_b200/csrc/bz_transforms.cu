@@ -299,6 +299,139 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
 }
 
 // ------------------------------------------------------------------------------------------------
+// Sigma through the irreducible wedge of real space.  Without per-k orbital rotations the full-zone kernel is
+// K(q) = K_irr(rep q), invariant under the grid's point group, and so is F(R) = sum_q K(q) e^{iqR}: it is needed
+// only at the irreducible R, where it is one complex GEMM over the irreducible q,
+//   Kw[plane][r] = sum_{q_irr} K[q_irr][plane] S[q_irr][r],   S[q_irr][r] = sum_{q in star(q_irr)} e^{i q R_r},
+// (plane = (w, nu, row, col)), and the contraction reads F(R) = Kw[plane][rep R] (w < 0: the conjugate, since
+// R and -R share a representative when the group holds the inversion).  Work: Q^2 per plane instead of a plane
+// transform of Nk (nx + ny + nz).
+// ------------------------------------------------------------------------------------------------
+constexpr int SW_TM = 64, SW_TN = 64, SW_TK = 16;
+
+// C[p][r] = sum_q A[q][p] B[q][r]: A = K [Q][P] (planes contiguous), B = S [Q][Q], C = Kw [P][Q].
+__global__ void __launch_bounds__(256, 2) sigma_wedge_gemm_kernel(const double2* __restrict__ A,
+                                                                  const double2* __restrict__ B, long long P, int Q,
+                                                                  double2* __restrict__ C) {
+  __shared__ double2 As[SW_TK][SW_TM + 1];
+  __shared__ double2 Bs[SW_TK][SW_TN];
+  const long long p0 = (long long)blockIdx.x * SW_TM;
+  const int r0 = blockIdx.y * SW_TN;
+  const int tid = threadIdx.x, ty = tid & 15, tx = tid >> 4;
+  // loads: A rows q = kq + 4 i of the tile, columns p0 + pa (64 consecutive planes per row); B rows kb + 4 i,
+  // columns r0 + rb
+  const int pa = tid & 63, kq = tid >> 6;
+  double2 ra[4], rb[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int q = k0 + kq + 4 * i;
+      const long long p = p0 + pa;
+      ra[i] = (q < Q && p < P) ? A[(size_t)q * P + p] : make_double2(0.0, 0.0);
+      const int r = r0 + pa;
+      rb[i] = (q < Q && r < Q) ? B[(size_t)q * Q + r] : make_double2(0.0, 0.0);
+    }
+  };
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+  load(0);
+  for (int k0 = 0; k0 < Q; k0 += SW_TK) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      As[kq + 4 * i][pa] = ra[i];
+      Bs[kq + 4 * i][pa] = rb[i];
+    }
+    __syncthreads();
+    if (k0 + SW_TK < Q) load(k0 + SW_TK);
+#pragma unroll
+    for (int kk = 0; kk < SW_TK; ++kk) {
+      double2 av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cfma(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const long long p = p0 + ty + 16 * i;
+    if (p >= P) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r0 + tx + 16 * j;
+      if (r < Q) C[(size_t)p * Q + r] = acc[i][j];
+    }
+  }
+}
+
+// Partial sums of the wedge form: as sigma_partial_kernel, with the plane K(-R) read from Kw through the
+// representative of each R instead of transformed.  kw: [W][nv][n2][n2][Q] (plane-major).
+template <int MAXR>
+__global__ void __launch_bounds__(BZ_THREADS, MAXR <= 4 ? 3 : 1)
+    sigma_wedge_partial_kernel(const double2* __restrict__ kw, const double2* __restrict__ g_r, int nb, int niv,
+                               int niw, int Q, int nk, const int* __restrict__ irrk_inv, int n_chunks,
+                               double2* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int* s_inv = reinterpret_cast<int*>(smem_raw);
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) s_inv[i] = irrk_inv[i];
+  __syncthreads();
+  const int n2 = nb * nb, nv = 2 * niv, nwf = 2 * niw + 1;
+  const int per_chunk = (nwf + n_chunks - 1) / n_chunks;
+  const int total = niv * n2 * n_chunks;
+  int rep[MAXR];
+#pragma unroll
+  for (int k = 0; k < MAXR; ++k) {
+    const int r = threadIdx.x + k * BZ_THREADS;
+    rep[k] = r < nk ? s_inv[r] : 0;
+  }
+  for (int blk = blockIdx.x; blk < total; blk += gridDim.x) {
+    const int chunk = blk % n_chunks;
+    const int ij = (blk / n_chunks) % n2;
+    const int v = blk / (n_chunks * n2);
+    const int i = ij / nb, j = ij - i * nb;
+    double2 acc[MAXR];
+#pragma unroll
+    for (int k = 0; k < MAXR; ++k) acc[k] = make_double2(0.0, 0.0);
+    const int wf0 = chunk * per_chunk, wf1 = min(nwf, wf0 + per_chunk);
+    for (int wf = wf0; wf < wf1; ++wf) {
+      const int w = wf - niw;
+      const bool neg = w < 0;
+      const int wa = neg ? -w : w;
+      const int vi = neg ? (niv - 1 - v) : (niv + v);
+      for (int ad = 0; ad < n2; ++ad) {
+        const int a = ad / nb, d = ad - a * nb;
+        const int row = a * nb + i, col = d * nb + j;
+        const double2* plane = kw + ((((size_t)wa * nv + vi) * n2 + row) * n2 + col) * Q;
+        const double2* gp = g_r + (((size_t)(v - w + niw) * nb + a) * nb + d) * nk;
+#pragma unroll
+        for (int k = 0; k < MAXR; ++k) {
+          const int r = threadIdx.x + k * BZ_THREADS;
+          if (r < nk) {
+            double2 kv = plane[rep[k]];
+            if (neg) kv.y = -kv.y;
+            cfma(acc[k], gp[r], kv);
+          }
+        }
+      }
+    }
+    double2* o = part + (((size_t)chunk * niv + v) * n2 + ij) * nk;
+#pragma unroll
+    for (int k = 0; k < MAXR; ++k) {
+      const int r = threadIdx.x + k * BZ_THREADS;
+      if (r < nk) o[r] = acc[k];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
 // IBZ -> FBZ with the auto-mode orbital rotation (n_point_base.py:462-507, symmetry_reduction.py:791-902):
 //   dst[k](o1,o2,o3,o4; f) = sigma_k^2 sum U_{o1 p} U*_{o2 q} U_{o3 r} U*_{o4 s} [src[irrk_inv[k]](p,q,r,s; f)]^(*conj_k)
 // for four-orbital objects whose per-k block holds the orbital indices at strides st[0..3] and frequency pairs
@@ -594,6 +727,65 @@ int dga_bubble_c128(const void* g_r, int n_orb, int niv, int niw, int nx, int ny
   bubble_kernel<<<(int)(work < cap ? work : cap), BZ_THREADS, smem, stream>>>(
       (const double2*)g_r, n_orb, niv, niw, g, q_irr, n_qirr, (const double2*)tw, beta, (double2*)out, os);
   return launch_status("dga_bubble_c128");
+}
+
+size_t dga_sigma_scratch_bytes(int n_orb, int niv, int nk, int n_chunks);
+
+// Scratch bytes of dga_sigma_wedge_c128: the partial sums of dga_sigma_c128 plus the wedge transform Kw.
+size_t dga_sigma_wedge_scratch_bytes(int n_orb, int niv, int niw, int n_q, int nk, int n_chunks) {
+  const size_t planes = (size_t)(niw + 1) * 2 * niv * n_orb * n_orb * n_orb * n_orb;
+  return dga_sigma_scratch_bytes(n_orb, niv, nk, n_chunks) + planes * (size_t)n_q * sizeof(double2);
+}
+
+// dga_sigma_c128 through the irreducible wedge of real space (see sigma_wedge_gemm_kernel); s_star [Q][Q] is
+// S[q_irr][r] = sum over the star of q_irr of e^{+i q R_r} for the irreducible R_r = the points irrk_ind names.
+int dga_sigma_wedge_c128(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, int nx, int ny,
+                         int nz, const int* irrk_inv, const void* s_star, const void* tw_inv, double beta,
+                         int n_chunks, void* out, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (check_grid(nx, ny, nz, "dga_sigma_wedge_c128")) return DGA_ERR_ARG;
+  if (!kern || !g_r || !irrk_inv || !s_star || !tw_inv || !out || !scratch || n_orb <= 0 || niv <= 0 || niw < 0 ||
+      n_q <= 0 || n_chunks <= 0) {
+    dga_set_error("dga_sigma_wedge_c128: invalid arguments");
+    return DGA_ERR_ARG;
+  }
+  Grid3 g{nx, ny, nz, nx * ny * nz};
+  const int n2 = n_orb * n_orb;
+  const size_t need = dga_sigma_wedge_scratch_bytes(n_orb, niv, niw, n_q, g.nk, n_chunks);
+  if (scratch_bytes < need) {
+    dga_set_error("dga_sigma_wedge_c128: scratch too small (%zu < %zu)", scratch_bytes, need);
+    return DGA_ERR_SCRATCH;
+  }
+  double2* part = (double2*)scratch;
+  double2* sig = part + (size_t)n_chunks * niv * n2 * g.nk;
+  double2* kw = sig + (size_t)niv * n2 * g.nk;
+  const long long P = (long long)(niw + 1) * 2 * niv * n2 * n2;
+  dim3 ggrid((unsigned)((P + SW_TM - 1) / SW_TM), (unsigned)((n_q + SW_TN - 1) / SW_TN));
+  sigma_wedge_gemm_kernel<<<ggrid, 256, 0, stream>>>((const double2*)kern, (const double2*)s_star, P, n_q, kw);
+  if (launch_status("dga_sigma_wedge_c128")) return DGA_ERR_LAUNCH;
+  const size_t smem = sizeof(int) * (size_t)g.nk;
+  const long long work = (long long)niv * n2 * n_chunks;
+  auto partial = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<grid_cap(work), BZ_THREADS, smem, stream>>>(kw, (const double2*)g_r, n_orb, niv, niw, n_q, g.nk,
+                                                         irrk_inv, n_chunks, part);
+  };
+  if (g.nk <= 4 * BZ_THREADS) partial(sigma_wedge_partial_kernel<4>);
+  else if (g.nk <= 8 * BZ_THREADS) partial(sigma_wedge_partial_kernel<8>);
+  else partial(sigma_wedge_partial_kernel<16>);
+  if (launch_status("dga_sigma_wedge_c128")) return DGA_ERR_LAUNCH;
+  const long long n_out = (long long)niv * n2 * g.nk;
+  sigma_reduce_kernel<<<grid_cap((n_out + 255) / 256), 256, 0, stream>>>(part, n_chunks, n_out,
+                                                                         -0.5 / beta / (double)g.nk, sig);
+  if (launch_status("dga_sigma_wedge_c128")) return DGA_ERR_LAUNCH;
+  const size_t dsmem = (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2);
+  cudaFuncSetAttribute(dft_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem);
+  PlaneAddr pa{(long long)g.nk, 0, 1, 1};
+  dft_planes_kernel<<<grid_cap(niv * n2), BZ_THREADS, dsmem, stream>>>(sig, pa, part, pa, niv * n2, g,
+                                                                       (const double2*)tw_inv, 1.0 / (double)g.nk,
+                                                                       nullptr);
+  if (launch_status("dga_sigma_wedge_c128")) return DGA_ERR_LAUNCH;
+  sigma_full_nu_kernel<<<grid_cap((n_out + 255) / 256), 256, 0, stream>>>(part, n_orb, niv, g.nk, (double2*)out);
+  return launch_status("dga_sigma_wedge_c128");
 }
 
 // Expansion of a four-orbital object from the irreducible to the full zone with the auto-mode orbital rotation;

@@ -78,6 +78,7 @@ class PassShapes:
     n_q: int
     niv_g: int
     rotated: bool = False  # auto-mode symmetries with orbital rotations in the IBZ -> FBZ map
+    wedge: bool = False  # Sigma through the irreducible wedge of real space (dga_sigma_wedge_c128)
 
     @property
     def n2(self):
@@ -116,7 +117,31 @@ class PassShapes:
             n_orb=u.shape[0], nk=tuple(int(x) for x in inp["nk"]), beta=float(inp["beta"]), niw=int(inp["niw"]),
             niv=int(inp["niv_core"]), niv_shell=int(inp["niv_shell"]), n_q=len(inp["irrk_ind"]),
             niv_g=np.shape(g_k)[-1] // 2, rotated=needs_rotation(inp),
+            wedge=not needs_rotation(inp) and inversion_shares_representatives(inp["irrk_inv"], inp["nk"]),
         )
+
+
+def inversion_shares_representatives(irrk_inv, nk) -> bool:
+    """True when every point and its inverse -k (per axis modulo the grid) map to the same irreducible point, the
+    condition of the wedge form of the Sigma contraction."""
+    inv = np.asarray(irrk_inv).reshape(tuple(int(x) for x in nk))
+    neg = inv[tuple(np.ix_(*[(-np.arange(n)) % n for n in inv.shape]))]
+    return bool(np.array_equal(inv, neg))
+
+
+def star_sums(irrk_ind, irrk_inv, nk) -> np.ndarray:
+    """S[q_irr][r] = sum over the points q with irrk_inv[q] = q_irr of e^{+i q R_r}, R_r = the point irrk_ind[r], from
+    the per-axis twiddles e^{+2 pi i m / n} (the s_star operand of dga_sigma_wedge_c128)."""
+    nk = tuple(int(x) for x in nk)
+    tw = [np.exp(2j * np.pi * np.arange(n) / n) for n in nk]
+    k = np.array(np.unravel_index(np.arange(int(np.prod(nk))), nk)).T  # [Nk][3]
+    r = np.array(np.unravel_index(np.asarray(irrk_ind), nk)).T  # [Q][3]
+    phase = np.ones((len(k), len(r)), dtype=np.complex128)
+    for ax in range(3):
+        phase *= tw[ax][(k[:, ax:ax + 1] * r[None, :, ax]) % nk[ax]]
+    s = np.zeros((len(r), len(r)), dtype=np.complex128)
+    np.add.at(s, np.asarray(irrk_inv).ravel(), phase)
+    return s
 
 
 def needs_rotation(inp: dict) -> bool:
@@ -178,9 +203,11 @@ def estimate_device_bytes(sh: PassShapes, precision: str = "fp64", keep_intermed
         2 * Q * W * n2 * n2 * c, 2 * Q * W * n2 * n2 * c,      # chi_phys, chi_lam
         2 * 8, 2 * 4, 4 * 4,                                   # lambdas, iterations, status
         Q * W * nv * n2 * n2 * c,                              # K
-        (chunks * sh.niv * n2 * nk * c * 2) // c * c + c,      # Sigma scratch
+        (chunks * sh.niv * n2 * nk * c * 2 + (W * nv * n2 * n2 * Q * c if sh.wedge else 0)) // c * c + c,  # Sigma scratch
         nk * n * n * 2 * sh.niv * c,                           # Sigma
     ]
+    if sh.wedge:
+        sizes.append(Q * Q * c)  # star sums
     if sh.rotated:
         sizes += [nk * n * n * c, nk * 8, nk, nk * 4, nk * W * nv * n2 * n2 * c]  # U_k, sigma_k, conj_k, map, K(FBZ)
     if keep_intermediates:
@@ -327,7 +354,13 @@ class LadderPass:
         if sigma_chunks is None:
             sigma_chunks = sigma_chunks_for(sh)
         self.sigma_chunks = sigma_chunks
-        self.sigma_scratch_bytes = int(lib().dga_sigma_scratch_bytes(n, sh.niv, nk_tot, sigma_chunks))
+        if sh.wedge:
+            self.s_star = torch.from_numpy(star_sums(inp["irrk_ind"], inp["irrk_inv"], sh.nk)).to(dev)
+            self.sigma_scratch_bytes = int(lib().dga_sigma_wedge_scratch_bytes(n, sh.niv, sh.niw, sh.n_q, nk_tot,
+                                                                               sigma_chunks))
+        else:
+            self.s_star = None
+            self.sigma_scratch_bytes = int(lib().dga_sigma_scratch_bytes(n, sh.niv, nk_tot, sigma_chunks))
         self.sigma_scratch = torch.empty(self.sigma_scratch_bytes // 16 + 1, dtype=C128, device=dev)
         self.sigma = torch.empty((nk_tot, n, n, 2 * sh.niv), dtype=C128, device=dev)
         self.g_k_host = torch.from_numpy(np.ascontiguousarray(g_k, dtype=np.complex128).reshape(sh.nk_tot, n, n, -1)).pin_memory()
@@ -447,6 +480,11 @@ class LadderPass:
         sh = self.sh
         self._g_transform(self.g_r_sigma, -sh.niw, self.t_sigma)
         nx, ny, nz = sh.nk
+        if sh.wedge:
+            call("dga_sigma_wedge_c128", _p(self.K), _p(self.g_r_sigma), sh.n_orb, sh.niv, sh.niw, sh.n_q, nx, ny, nz,
+                 _p(self.irrk_inv), _p(self.s_star), _p(self.tw_inv), sh.beta, self.sigma_chunks, _p(self.sigma),
+                 _p(self.sigma_scratch), self.sigma_scratch.numel() * 16, _s())
+            return
         kern, n_q, inv = self.K, sh.n_q, self.irrk_inv
         if sh.rotated:
             # K(q) over the full zone with each point's orbital rotation, then the contraction without a gather
