@@ -340,6 +340,38 @@ def serving_leg(precision: str, n_requests: int) -> dict:
     return out
 
 
+def serving_c5_leg(n_requests: int, rate_per_s: float = 25.0, seed: int = 11) -> dict:
+    """The continuous-batching server on a loaded stream of requests drawn from the mixed-request workload's shape
+    sets (serving.C5_SERVE_SHAPES: orbitals 1-3, grids 16^2-64^2, niv = niw 20-60, without the shapes whose inputs
+    take more than seconds to generate), beta ~ U[5,30], U ~ U[2,10], Poisson arrivals faster than the server
+    completes them; both forms on the same requests."""
+    from collections import Counter
+
+    from dgamore_b200.serving import C5_SERVE_SHAPES, LadderServer, serving_workload
+
+    base = serving_workload(n_requests, rate_per_s=rate_per_s, seed=seed, precision="fp64", shapes=C5_SERVE_SHAPES)
+    shapes = Counter((int(r.inp["u"].shape[0]), int(r.inp["nk"][0]), int(r.inp["niv_core"])) for r in base)
+    out = {"workload": f"{n_requests} requests from {len(C5_SERVE_SHAPES)} shapes (n_orb, nk, niv) of the mixed "
+                       f"workload's sets, Poisson arrivals at {rate_per_s}/s (seed {seed})",
+           "shapes_drawn": {f"{k[0]}orb_{k[1]}x{k[1]}_niv{k[2]}": v for k, v in sorted(shapes.items())}}
+    for precision in ("mixed", "fp64"):
+        reqs = [type(r)(r.inp, arrival=r.arrival, precision=precision) for r in base]
+        srv = LadderServer(hbm_budget=60 << 30, scratch_bytes=4 << 30, items_per_request=256)
+        seen, warm = set(), []
+        for r in reqs:
+            key = (r.inp["u"].shape[0], r.inp["niv_core"])
+            if key not in seen:
+                seen.add(key)
+                warm.append(type(r)(r.inp, precision=precision))
+        srv.serve(warm, realtime=False)
+        srv.stats = type(srv.stats)()
+        stats = srv.serve(reqs, realtime=True)
+        res = stats.summary()
+        res["bse_status_nonzero"] = int(sum(int(np.abs(r.bse_status).sum()) for r in stats.completed))
+        out[precision] = res
+    return out
+
+
 def c4_batch_leg(precision: str, steps: int = 3) -> dict:
     """The 2-orbital bilayer (48x48, niv = niw = 30, N = 240) and the 1-orbital lattice (32x32, niv = niw = 50,
     N = 100) as one device schedule: both passes' stages and ONE persistent BSE launch over the items of both,
@@ -605,6 +637,7 @@ def run_ours(args, rank: int, world: int, local: int):
             serving[prec] = serving_leg(prec, args.serve_requests)
     eliashberg = eliashberg_leg() if (args.eliashberg and rank == 0) else None
     small = small_configs_leg() if (args.small and rank == 0) else None
+    serving_c5 = serving_c5_leg(args.serve_c5) if (args.serve_c5 and rank == 0) else None
     c4 = {}
     if args.c4 and rank == 0:
         for prec in ("fp64", "mixed"):
@@ -677,6 +710,7 @@ def run_ours(args, rank: int, world: int, local: int):
         "serving": serving,
         "eliashberg": eliashberg,
         "small_configs": small,
+        "serving_c5": serving_c5,
         "c4_batch": c4,
     }
     if rank == 0:
@@ -699,6 +733,8 @@ def main():
     ap.add_argument("--eliashberg", type=int, default=1, help="run the Eliashberg leg (0: skip)")
     ap.add_argument("--c4", type=int, default=1, help="run the uneven-orbital batch leg under one graph (0: skip)")
     ap.add_argument("--small", type=int, default=1, help="run the C1/C2 mixed-vs-FP64 leg (0: skip)")
+    ap.add_argument("--serve-c5", type=int, default=0,
+                    help="requests of the loaded serving leg on the mixed-request workload's shapes (0: skip)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     try:

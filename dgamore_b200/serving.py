@@ -394,6 +394,11 @@ def poisson_arrivals(n: int, rate_per_s: float, seed: int = 0) -> np.ndarray:
 
 # (n_orb, nk, niv = niw) shapes of the serving mix: orbitals 1-3, small and mid momentum grids and boxes
 SERVE_SHAPES = ((1, 16, 10), (1, 16, 20), (2, 8, 10), (2, 16, 10), (3, 8, 8), (3, 8, 12))
+# The mixed-request workload's shape sets (orbitals {1, 2, 3} x grids {16^2, 32^2, 64^2} x boxes niv = niw
+# {20, 40, 60}) without the shapes whose seeded inputs take more than seconds to generate on the host (two
+# orbitals at niv = 60, three orbitals at niv >= 40): (n_orb, nk, niv).
+C5_SERVE_SHAPES = tuple((n, nk, niv) for n in (1, 2, 3) for nk in (16, 32, 64) for niv in (20, 40, 60)
+                        if not (n == 2 and niv == 60) and not (n == 3 and niv >= 40))
 
 
 def serving_workload(n_requests: int = 24, rate_per_s: float = 20.0, seed: int = 5, precision: str = "fp64",
