@@ -167,14 +167,15 @@ struct OutStrides7 {
 
 constexpr int BUB_GR = 4;  // (qy, qz) pairs per thread in the (y, z) sums
 
-__global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __restrict__ g_r, int nb, int niv,
+__global__ void __launch_bounds__(BZ_THREADS, 3) bubble_kernel(const double2* __restrict__ g_r, int nb, int niv,
                                                              int niw, Grid3 g, const int* __restrict__ q_irr,
                                                              int n_qirr, const double2* __restrict__ tw,
                                                              double beta, double2* __restrict__ out,
                                                              OutStrides7 os) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* P = reinterpret_cast<double2*>(smem_raw);  // [yz][x]
-  double2* Tt = P + g.nk;                               // [x][pair]
+  const int ldp = g.nx + 1;  // padded row: the transposed stores of one warp spread over all banks
+  double2* P = reinterpret_cast<double2*>(smem_raw);  // [yz][x], row stride ldp
+  double2* Tt = P + (size_t)ldp * g.ny * g.nz;          // [x][pair]
   double2* s_tw = Tt + g.nk;
   int* s_q = reinterpret_cast<int*>(s_tw + g.nx + g.ny + g.nz);  // [n_qirr][3]
   int* s_j = s_q + 3 * n_qirr;                                    // pair index of each q
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
       for (int r = threadIdx.x; r < g.nk; r += blockDim.x) {
         const int x = r / nyz, yz = r - x * nyz, y = yz / g.nz, z = yz - y * g.nz;
         const int xm = x ? g.nx - x : 0, ym = y ? g.ny - y : 0, zm = z ? g.nz - z : 0;
-        P[yz * g.nx + x] = cmul(gad[r], gcb[(xm * g.ny + ym) * g.nz + zm]);
+        P[yz * ldp + x] = cmul(gad[r], gcb[(xm * g.ny + ym) * g.nz + zm]);
       }
       __syncthreads();
       // T[x][j] for BUB_GR pairs j per thread: consecutive threads take consecutive x (conflict-free P reads)
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(BZ_THREADS) bubble_kernel(const double2* __res
 #pragma unroll
           for (int u = 0; u < BUB_GR; ++u) mz[u] = 0;
           for (int z = 0; z < g.nz; ++z) {
-            const double2 pv = P[(y * g.nz + z) * g.nx + x];
+            const double2 pv = P[(y * g.nz + z) * ldp + x];
 #pragma unroll
             for (int u = 0; u < BUB_GR; ++u) {
               const double2 tt = g.nz > 1 ? cmul(twy[my[u]], twz[mz[u]]) : twy[my[u]];
@@ -719,8 +720,8 @@ int dga_bubble_c128(const void* g_r, int n_orb, int niv, int niw, int nx, int ny
     dga_set_error("dga_bubble_c128: more irreducible q points (%d) than grid points", n_qirr);
     return DGA_ERR_ARG;
   }
-  const size_t smem =
-      (2 * (size_t)g.nk + nx + ny + nz) * sizeof(double2) + (6 * (size_t)n_qirr + 1) * sizeof(int);
+  const size_t smem = (2 * (size_t)g.nk + (size_t)ny * nz + nx + ny + nz) * sizeof(double2) +
+                      (6 * (size_t)n_qirr + 1) * sizeof(int);
   cudaFuncSetAttribute(bubble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long work = (long long)(niw + 1) * 2 * niv * n_orb * n_orb;
   const long long cap = 64LL * device_sm_count();
