@@ -583,6 +583,8 @@ def run_ours(args, rank: int, world: int, local: int):
     lp64 = LadderPass(inp, keep_intermediates=False, precision="fp64")
     lp64.pre_bse()
     tune64 = autotune.tune_bse(lp64, cache_path=cache)
+    lp64.run()
+    tune_sig = autotune.tune_sigma(lp64, cache_path=cache)  # the Sigma stage's tile and chunks, shared by both forms
     r64 = time_pass(lp64, args, world, local, sample_clocks=False)
     sigma64 = lp64.sigma.clone()
     del lp64
@@ -592,12 +594,13 @@ def run_ours(args, rank: int, world: int, local: int):
     sh = lp.sh
     lp.pre_bse()
     tune = autotune.tune_bse(lp, cache_path=cache)
+    autotune.tune_sigma(lp, cache_path=cache)
     res = time_pass(lp, args, world, local, sample_clocks=True)
     t, value, bse_ms, status, clocks = res["t"], res["value"], res["bse_ms"], res["status"], res["clocks"]
     sig_err = float((lp.sigma - sigma64).abs().max().item() / sigma64.abs().max().item())
     iters = lp.bse_iters.cpu().numpy() if args.precision == "mixed" else None
     kname = kernel_name(lp)
-    kernels_per_pass = (14 if lp.do_lambda else 13) + (1 if args.precision == "mixed" else 0)
+    kernels_per_pass = lp.kernels_per_pass()
 
     # end to end through the public API: host G(k) -> device pass (graph replay) -> host Sigma
     lp.run_e2e()
@@ -665,6 +668,7 @@ def run_ours(args, rank: int, world: int, local: int):
             "l2": "inputs larger than L2 (Gamma_r alone is %.0f MB)" % (2 * sh.W * sh.N * sh.N * 16 / 1e6),
             "parallelism": f"{world} independent replica(s)",
             "bse_launch": {"kernel": kname, "tuning": list(tune.choice), "tuning_times_ms": tune.times_ms},
+            "sigma_launch": {"tuning_tile_chunks": list(tune_sig.choice), "tuning_times_ms": tune_sig.times_ms},
         },
         "gpu_launches": kernels_per_pass * args.steps,
         "e2e": {

@@ -65,7 +65,7 @@ SIGNATURES = {
     "dga_bse_solve_sum_eli_c128": (I, [I, I, I, I, I, D, D, VP, VP, VP, PI, I, I, I, VP, VP, PI, VP, SZ, VP]),
     "dga_eli_ladder_term_c128": (I, [VP, VP, VP, I, I, I, I, I, I, VP, VP]),
     "dga_sigma_wedge_scratch_bytes": (SZ, [I, I, I, I, I, I]),
-    "dga_sigma_wedge_c128": (I, [VP, VP, I, I, I, I, I, I, I, PI, VP, VP, D, I, VP, VP, SZ, VP]),
+    "dga_sigma_wedge_c128": (I, [VP, VP, I, I, I, I, I, I, I, PI, VP, VP, D, I, I, VP, VP, SZ, VP]),
     "dga_fbz_rotate_c128": (I, [VP, PI, I, VP, PD, VP, I, PLL, LL, I, LL, I, LL, VP, VP]),
     "dga_lu_batched_c128": (I, [VP, I, I, LL, PI, PI, VP]),
     "dga_lu_solve_batched_c128": (I, [VP, PI, I, I, LL, VP, LL, LL, LL, I, VP, LL, PI, VP]),

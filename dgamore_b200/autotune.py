@@ -133,3 +133,60 @@ def tune_bse(lp, precision: str | None = None, sample_items: int | None = None, 
     save_cache(cache_path)
     lp.set_tuning(choice)
     return TuneResult(key, choice, {f"{k[0]}/{k[1]}": v for k, v in times.items()}, n)
+
+
+# wedge-Sigma launch choices: (GEMM output tile of dga_sigma_wedge_c128 (0 = 64 x 64, 1 = 128 x 32), bosonic chunks
+# of the contraction as a multiple of the pass's default)
+SIGMA_TILES = (0, 1)
+SIGMA_CHUNK_FACTORS = (0.5, 1.0, 2.0)
+
+
+def tune_sigma(lp, repeats: int = 2, cache_path: str | None = None, force: bool = False) -> TuneResult:
+    """Chooses the GEMM tile and the number of bosonic chunks of the wedge Sigma contraction for ``lp`` (a
+    LadderPass whose kernel K is computed: run a pass first) by timing ``lp.sigma_stage`` with each candidate (CUDA
+    events, best of ``repeats`` after a warm-up), installs the fastest and caches it per (device, shape).  Every
+    candidate computes the same Sigma up to the order of the bosonic partial sums.  Passes that do not take the
+    wedge form (orbital rotations, grids without the inversion) keep their defaults."""
+    from .pipeline import sigma_chunks_for
+
+    sh = lp.sh
+    if not sh.wedge:
+        return TuneResult("", (0, lp.sigma_chunks), {}, 0)
+    key = "sigma|" + shape_key(lp, "fp64")  # one choice per shape, shared by both forms of the pass
+    load_cache(cache_path)
+    if not force and key in _CACHE:
+        lp.sigma_tile, lp.sigma_chunks = _CACHE[key]
+        _ensure_sigma_scratch(lp)
+        return TuneResult(key, tuple(_CACHE[key]), {}, 0)
+    base = sigma_chunks_for(sh)
+    nwf = 2 * sh.niw + 1
+    chunks = sorted({max(1, min(nwf, int(round(base * f)))) for f in SIGMA_CHUNK_FACTORS})
+    stream = torch.cuda.current_stream()
+    times = {}
+    for tile in SIGMA_TILES:
+        for ch in chunks:
+            lp.sigma_tile, lp.sigma_chunks = tile, ch
+            _ensure_sigma_scratch(lp)
+            lp.sigma_stage()  # warm-up
+            best = float("inf")
+            for _ in range(repeats):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                lp.sigma_stage()
+                b.record(stream)
+                b.synchronize()
+                best = min(best, a.elapsed_time(b))
+            times[(tile, ch)] = best
+    choice = min(times, key=times.get)
+    lp.sigma_tile, lp.sigma_chunks = choice
+    _ensure_sigma_scratch(lp)
+    _CACHE[key] = choice
+    save_cache(cache_path)
+    return TuneResult(key, choice, {f"{k[0]}/{k[1]}": v for k, v in times.items()}, 0)
+
+
+def _ensure_sigma_scratch(lp) -> None:
+    sh = lp.sh
+    need = int(lib().dga_sigma_wedge_scratch_bytes(sh.n_orb, sh.niv, sh.niw, sh.n_q, sh.nk_tot, lp.sigma_chunks))
+    if lp.sigma_scratch.numel() * 16 < need:
+        lp.sigma_scratch = torch.empty(need // 16 + 1, dtype=C128, device=lp.dev)

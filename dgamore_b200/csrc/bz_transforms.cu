@@ -308,28 +308,33 @@ __global__ void __launch_bounds__(BZ_THREADS, 3) bubble_kernel(const double2* __
 // R and -R share a representative when the group holds the inversion).  Work: Q^2 per plane instead of a plane
 // transform of Nk (nx + ny + nz).
 // ------------------------------------------------------------------------------------------------
-constexpr int SW_TM = 64, SW_TN = 64, SW_TK = 16;
+constexpr int SW_TK = 16;
 
-// C[p][r] = sum_q A[q][p] B[q][r]: A = K [Q][P] (planes contiguous), B = S [Q][Q], C = Kw [P][Q].
+// C[p][r] = sum_q A[q][p] B[q][r]: A = K [Q][P] (planes contiguous), B = S [Q][Q], C = Kw [P][Q].  A TM x TN output
+// tile per 256-thread CTA, 4 x 4 per thread (TM * TN = 4096), K in steps of 16 with the next step's operands loaded
+// into registers while the current one multiplies.
+template <int TM, int TN>
 __global__ void __launch_bounds__(256, 2) sigma_wedge_gemm_kernel(const double2* __restrict__ A,
                                                                   const double2* __restrict__ B, long long P, int Q,
                                                                   double2* __restrict__ C) {
-  __shared__ double2 As[SW_TK][SW_TM + 1];
-  __shared__ double2 Bs[SW_TK][SW_TN];
-  const long long p0 = (long long)blockIdx.x * SW_TM;
-  const int r0 = blockIdx.y * SW_TN;
-  const int tid = threadIdx.x, ty = tid & 15, tx = tid >> 4;
-  // loads: A rows q = kq + 4 i of the tile, columns p0 + pa (64 consecutive planes per row); B rows kb + 4 i,
-  // columns r0 + rb
-  const int pa = tid & 63, kq = tid >> 6;
-  double2 ra[4], rb[4];
+  static_assert(TM * TN == 4096, "4 x 4 outputs per thread of 256");
+  constexpr int AL = TM * SW_TK / 256, BL = TN * SW_TK / 256;  // tile elements loaded per thread
+  __shared__ double2 As[SW_TK][TM + 1];
+  __shared__ double2 Bs[SW_TK][TN];
+  const long long p0 = (long long)blockIdx.x * TM;
+  const int r0 = blockIdx.y * TN;
+  const int tid = threadIdx.x, ty = tid % (TM / 4), tx = tid / (TM / 4);
+  double2 ra[AL], rb[BL];
   auto load = [&](int k0) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int q = k0 + kq + 4 * i;
-      const long long p = p0 + pa;
+    for (int i = 0; i < AL; ++i) {  // element e = tid + 256 i of the TK x TM tile: row q = e / TM, column e % TM
+      const int e = tid + 256 * i, q = k0 + e / TM;
+      const long long p = p0 + e % TM;
       ra[i] = (q < Q && p < P) ? A[(size_t)q * P + p] : make_double2(0.0, 0.0);
-      const int r = r0 + pa;
+    }
+#pragma unroll
+    for (int i = 0; i < BL; ++i) {
+      const int e = tid + 256 * i, q = k0 + e / TN, r = r0 + e % TN;
       rb[i] = (q < Q && r < Q) ? B[(size_t)q * Q + r] : make_double2(0.0, 0.0);
     }
   };
@@ -341,9 +346,14 @@ __global__ void __launch_bounds__(256, 2) sigma_wedge_gemm_kernel(const double2*
   load(0);
   for (int k0 = 0; k0 < Q; k0 += SW_TK) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      As[kq + 4 * i][pa] = ra[i];
-      Bs[kq + 4 * i][pa] = rb[i];
+    for (int i = 0; i < AL; ++i) {
+      const int e = tid + 256 * i;
+      As[e / TM][e % TM] = ra[i];
+    }
+#pragma unroll
+    for (int i = 0; i < BL; ++i) {
+      const int e = tid + 256 * i;
+      Bs[e / TN][e % TN] = rb[i];
     }
     __syncthreads();
     if (k0 + SW_TK < Q) load(k0 + SW_TK);
@@ -351,9 +361,9 @@ __global__ void __launch_bounds__(256, 2) sigma_wedge_gemm_kernel(const double2*
     for (int kk = 0; kk < SW_TK; ++kk) {
       double2 av[4], bv[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + (TM / 4) * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + (TN / 4) * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -363,11 +373,11 @@ __global__ void __launch_bounds__(256, 2) sigma_wedge_gemm_kernel(const double2*
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const long long p = p0 + ty + 16 * i;
+    const long long p = p0 + ty + (TM / 4) * i;
     if (p >= P) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int r = r0 + tx + 16 * j;
+      const int r = r0 + tx + (TN / 4) * j;
       if (r < Q) C[(size_t)p * Q + r] = acc[i][j];
     }
   }
@@ -742,10 +752,11 @@ size_t dga_sigma_wedge_scratch_bytes(int n_orb, int niv, int niw, int n_q, int n
 // S[q_irr][r] = sum over the star of q_irr of e^{+i q R_r} for the irreducible R_r = the points irrk_ind names.
 int dga_sigma_wedge_c128(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, int nx, int ny,
                          int nz, const int* irrk_inv, const void* s_star, const void* tw_inv, double beta,
-                         int n_chunks, void* out, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+                         int n_chunks, int gemm_tile, void* out, void* scratch, size_t scratch_bytes,
+                         cudaStream_t stream) {
   if (check_grid(nx, ny, nz, "dga_sigma_wedge_c128")) return DGA_ERR_ARG;
   if (!kern || !g_r || !irrk_inv || !s_star || !tw_inv || !out || !scratch || n_orb <= 0 || niv <= 0 || niw < 0 ||
-      n_q <= 0 || n_chunks <= 0) {
+      n_q <= 0 || n_chunks <= 0 || gemm_tile < 0 || gemm_tile > 1) {
     dga_set_error("dga_sigma_wedge_c128: invalid arguments");
     return DGA_ERR_ARG;
   }
@@ -760,8 +771,13 @@ int dga_sigma_wedge_c128(const void* kern, const void* g_r, int n_orb, int niv, 
   double2* sig = part + (size_t)n_chunks * niv * n2 * g.nk;
   double2* kw = sig + (size_t)niv * n2 * g.nk;
   const long long P = (long long)(niw + 1) * 2 * niv * n2 * n2;
-  dim3 ggrid((unsigned)((P + SW_TM - 1) / SW_TM), (unsigned)((n_q + SW_TN - 1) / SW_TN));
-  sigma_wedge_gemm_kernel<<<ggrid, 256, 0, stream>>>((const double2*)kern, (const double2*)s_star, P, n_q, kw);
+  // GEMM tile (rows of planes x columns of irreducible R): 0 = 64 x 64, 1 = 128 x 32
+  auto gemm = [&](auto kernel, int tm, int tn) {
+    dim3 ggrid((unsigned)((P + tm - 1) / tm), (unsigned)((n_q + tn - 1) / tn));
+    kernel<<<ggrid, 256, 0, stream>>>((const double2*)kern, (const double2*)s_star, P, n_q, kw);
+  };
+  if (gemm_tile == 0) gemm(sigma_wedge_gemm_kernel<64, 64>, 64, 64);
+  else gemm(sigma_wedge_gemm_kernel<128, 32>, 128, 32);
   if (launch_status("dga_sigma_wedge_c128")) return DGA_ERR_LAUNCH;
   const size_t smem = sizeof(int) * (size_t)g.nk;
   const long long work = (long long)niv * n2 * n_chunks;

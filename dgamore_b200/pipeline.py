@@ -354,6 +354,7 @@ class LadderPass:
         if sigma_chunks is None:
             sigma_chunks = sigma_chunks_for(sh)
         self.sigma_chunks = sigma_chunks
+        self.sigma_tile = 1  # wedge GEMM tile (dga_sigma_wedge_c128; autotune.tune_sigma picks it per shape)
         if sh.wedge:
             self.s_star = torch.from_numpy(star_sums(inp["irrk_ind"], inp["irrk_inv"], sh.nk)).to(dev)
             self.sigma_scratch_bytes = int(lib().dga_sigma_wedge_scratch_bytes(n, sh.niv, sh.niw, sh.n_q, nk_tot,
@@ -482,7 +483,8 @@ class LadderPass:
         nx, ny, nz = sh.nk
         if sh.wedge:
             call("dga_sigma_wedge_c128", _p(self.K), _p(self.g_r_sigma), sh.n_orb, sh.niv, sh.niw, sh.n_q, nx, ny, nz,
-                 _p(self.irrk_inv), _p(self.s_star), _p(self.tw_inv), sh.beta, self.sigma_chunks, _p(self.sigma),
+                 _p(self.irrk_inv), _p(self.s_star), _p(self.tw_inv), sh.beta, self.sigma_chunks, self.sigma_tile,
+                 _p(self.sigma),
                  _p(self.sigma_scratch), self.sigma_scratch.numel() * 16, _s())
             return
         kern, n_q, inv = self.K, sh.n_q, self.irrk_inv
@@ -567,6 +569,17 @@ class LadderPass:
         self.sigma_host.copy_(self.sigma, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return self.sigma_host.numpy()
+
+    def kernels_per_pass(self) -> int:
+        """Library kernel launches of one ``run()``: the G(R) transform, bubble, double counting (2), chi0^-1 and
+        sums (2); the BSE (mixed: solve + FP64 re-solve); chi_phys, lambda (single band), kernel assembly; the
+        Sigma stage's G(R) transform and contraction (wedge: GEMM, partial sums, reduction, inverse transform,
+        full-nu; otherwise the partial sums in place of the GEMM and partial sums, after the rotated expansion of K
+        when there is one); the Hartree-Fock term when occupations are set."""
+        n = 6 + (2 if self.precision == "mixed" else 1) + 2 + (1 if self.do_lambda else 0)
+        n += 1 + (5 if self.sh.wedge else 4 + (1 if self.sh.rotated else 0))
+        n += 1 if getattr(self, "hf_occ", None) is not None else 0
+        return n
 
     def device_bytes(self) -> int:
         """HBM held by this pass's device tensors, in caching-allocator blocks."""

@@ -59,12 +59,14 @@ int dga_strided_copy_c128(const void* src, void* dst, int ndim, const long long*
  * grid group holds the inversion (R and -R share a representative): F(R) = sum_q K(q) e^{iqR} is invariant under
  * the group, so it is formed only at the irreducible R as one complex GEMM over the irreducible q against
  * s_star [Q][Q], S[q_irr][r] = sum over the star of q_irr of e^{+i q R_r} (R_r = the point irrk_ind[r]), and the
- * contraction reads F at each R's representative (irrk_inv).  Same inputs and output as dga_sigma_c128 otherwise;
- * scratch: dga_sigma_wedge_scratch_bytes. */
+ * contraction reads F at each R's representative (irrk_inv).  gemm_tile: the GEMM's output tile (rows of kernel
+ * planes x columns of irreducible R; 0 = 64 x 64, 1 = 128 x 32), a choice of the autotuner.  Same
+ * inputs and output as dga_sigma_c128 otherwise; scratch: dga_sigma_wedge_scratch_bytes. */
 size_t dga_sigma_wedge_scratch_bytes(int n_orb, int niv, int niw, int n_q, int nk, int n_chunks);
 int dga_sigma_wedge_c128(const void* kern, const void* g_r, int n_orb, int niv, int niw, int n_q, int nx, int ny,
                          int nz, const int* irrk_inv, const void* s_star, const void* tw_inv, double beta,
-                         int n_chunks, void* out, void* scratch, size_t scratch_bytes, dga_stream_t stream);
+                         int n_chunks, int gemm_tile, void* out, void* scratch, size_t scratch_bytes,
+                         dga_stream_t stream);
 
 /* IBZ -> FBZ expansion of a four-orbital object with the auto-mode orbital rotation (IAmNonLocal._map_to_full_bz,
  * dgamore/n_point_base.py:462-507, through symmetry_reduction.apply_auto_orbital_transform, :791-902):

@@ -75,3 +75,20 @@ def test_tuner_picks_and_caches_a_choice(tmp_path):
     lp2.pre_bse()
     res2 = autotune.tune_bse(lp2, cache_path=path)
     assert res2.choice == res.choice and not res2.times_ms
+
+
+def test_sigma_tuning_keeps_sigma():
+    """The wedge-Sigma tuner (GEMM tile x bosonic chunks) installs a choice from its candidates and Sigma stays
+    the same up to the order of the bosonic partial sums."""
+    from dgamore_b200 import autotune
+    from dgamore_b200.pipeline import LadderPass
+
+    inp, ref = load_golden("t1b")
+    lp = LadderPass(inp, keep_intermediates=False)
+    assert lp.sh.wedge
+    sig0 = lp.run().cpu().numpy()
+    res = autotune.tune_sigma(lp, force=True)
+    assert res.choice[0] in autotune.SIGMA_TILES and len(res.times_ms) >= 2
+    sig1 = lp.run().cpu().numpy()
+    assert rel_err(sig1, sig0) < 1e-12
+    assert rel_err(sig1, ref["sigma"]) < 1e-10
