@@ -281,10 +281,18 @@ class LadderServer:
     items_per_request: BSE items each running request contributes to one iteration (None: all of them)."""
 
     def __init__(self, hbm_budget: int, scratch_bytes: int = 4 << 30, items_per_request: int | None = 256,
-                 device: str = "cuda", refine_max_iter: int = 6, refine_tol: float = 1e-10):
+                 device: str = "cuda", refine_max_iter: int = 6, refine_tol: float = 1e-10,
+                 reserve_bytes: int | None = None):
         self.dev = torch.device(device)
         with torch.cuda.device(self.dev):
             call("dga_bse_preload")  # the BSE kernels' code is loaded at start-up, not inside a request
+        # the requests' buffers are carved from one segment of the caching allocator reserved now (a block freed
+        # here stays cached and is split for later allocations), so that admitting a request does not pay a
+        # device-synchronising cudaMalloc
+        reserve = min(int(hbm_budget), 16 << 30) if reserve_bytes is None else int(reserve_bytes)
+        if reserve > 0:
+            block = torch.empty(reserve, dtype=torch.uint8, device=self.dev)
+            del block
         self.hbm_budget = int(hbm_budget)
         self.items_per_request = items_per_request
         self.refine_max_iter = refine_max_iter
