@@ -202,3 +202,32 @@ def test_local_results_feed_the_nonlocal_pass_on_the_device():
     ref = ladder.sde_pass(host_inp)
     assert rel_err(sig_dev, ref["sigma"]) < 1e-10
     assert rel_err(host_inp["gamma_magn"], base["gamma_magn"]) < 1e-10  # the round trip through the local ladder
+
+
+def test_whole_chain_on_the_device():
+    """Local SDE -> nonlocal pass (its vertices handed over on the device) with the Eliashberg vertex fused into the
+    FP64 BSE -> leading pairing eigenvalues, equal to the same chain with the separate vertex kernel."""
+    from dgamore_b200 import synthetic
+    from dgamore_b200.eliashberg_solver import EliashbergSolver, default_niv_pp
+    from dgamore_b200.local_sde import LocalSde
+    from dgamore_b200.pipeline import LadderPass
+
+    cfg = synthetic.CONFIGS["t4e"]  # 2 orbitals, 6x6, niw = niv = 6
+    base = synthetic.make_inputs(cfg)
+    lsi, _ = synthetic.local_sde_inputs(cfg)
+    sde = LocalSde(*lsi).run()
+    inputs = sde.nonlocal_inputs(base)
+    P = default_niv_pp(cfg.niw, cfg.niv)
+    lp = LadderPass(inputs, eliashberg_pp=P)
+    sig = lp.run()
+    es = EliashbergSolver(lp, P)
+    assert es.fused
+    ls, lt, _, _ = es.solve(n_eig=2, tol=1e-10)
+    plain = LadderPass({k: (v.clone() if isinstance(v, torch.Tensor) else v) for k, v in inputs.items()})
+    sig_plain = plain.run()
+    assert torch.equal(sig, sig_plain)
+    es_plain = EliashbergSolver(plain, P)
+    assert not es_plain.fused
+    ls_p, lt_p, _, _ = es_plain.solve(n_eig=2, tol=1e-10)
+    assert np.allclose(ls, ls_p, rtol=1e-9) and np.allclose(lt, lt_p, rtol=1e-9)
+    assert np.isfinite(ls).all() and np.isfinite(lt).all()
