@@ -6,7 +6,8 @@ wave of CTAs and an ncu capture of it holds about a gigabyte of device memory.
 
 Runs the passes and prints one JSON line with the shapes, the number of BSE items and the kernels launched.
 With ``--eliashberg K`` it then builds the pairing vertices of the same pass (FP64, three-leg vertex kept) and
-applies the singlet gap-equation operator K times:
+applies the singlet gap-equation operator K times.  The full vertex of the pp box comes out of the pass's own
+BSE (LadderPass(eliashberg_pp=niv_pp)); ``--separate-vertex`` builds it with the separate kernel instead:
 
     python -m dgamore_b200.profile_case --config c4_bilayer --nk 48 --niw 30 --eliashberg 5
 
@@ -41,6 +42,8 @@ def main(argv=None):
     ap.add_argument("--passes", type=int, default=1)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--eliashberg", type=int, default=0, help="gap-equation operator applications after the pass")
+    ap.add_argument("--separate-vertex", action="store_true",
+                    help="build the Eliashberg full vertex with its own kernel, not inside the pass's BSE")
     ap.add_argument("--local-sde", action="store_true", help="run the local Schwinger-Dyson equation instead")
     args = ap.parse_args(argv)
     if args.local_sde:
@@ -58,7 +61,13 @@ def main(argv=None):
         return
     cfg = reduced_config(args.config, args.nk, args.niw)
     inp = synthetic.make_inputs(cfg)
-    lp = LadderPass(inp, keep_intermediates=args.eliashberg > 0, precision=args.precision)
+    fuse = args.eliashberg > 0 and args.precision == "fp64" and not args.separate_vertex
+    eli_pp = None
+    if fuse:
+        from .eliashberg_solver import default_niv_pp
+
+        eli_pp = default_niv_pp(cfg.niw, cfg.niv)
+    lp = LadderPass(inp, keep_intermediates=args.eliashberg > 0, precision=args.precision, eliashberg_pp=eli_pp)
     for _ in range(args.passes):
         lp.run()
     torch.cuda.synchronize()
@@ -79,7 +88,7 @@ def main(argv=None):
         for _ in range(args.eliashberg):
             es.matvec("sing", x, out)
         torch.cuda.synchronize()
-        print(json.dumps({"eliashberg_M": es.M, "nk": lp.sh.nk_tot, "matvecs": args.eliashberg,
+        print(json.dumps({"eliashberg_M": es.M, "nk": lp.sh.nk_tot, "matvecs": args.eliashberg, "fused": es.fused,
                           "vertex_status": int(es.vertex_status.abs().sum())}))
 
 

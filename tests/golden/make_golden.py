@@ -82,9 +82,24 @@ def _setup_config(cfg: synthetic.DgaConfig, inp: dict):
     config.lambda_correction.perform_lambda_correction = False
 
 
-def run_reference_pass(name: str, variants: bool = True) -> dict:
+class _OnlyKeys(dict):
+    """A result dict that keeps only the named keys (the at-size fixtures store a few outputs; the upstream's
+    intermediates at the 3-orbital size are gigabytes each)."""
+
+    def __init__(self, keys):
+        super().__init__()
+        self._keys = set(keys)
+
+    def __setitem__(self, key, value):
+        if key in self._keys:
+            super().__setitem__(key, value)
+
+
+def run_reference_pass(name: str, variants: bool = True, bse_variant: str = "v1", keep_keys=None) -> dict:
     """The upstream pass in FP64; with ``variants`` also its alternative forms (direct-q bubble, v3 BSE, direct
-    Sigma), which the at-size fixtures skip because they cost far more than the pass at 64x64."""
+    Sigma), which the at-size fixtures skip because they cost far more than the pass at 64x64.  ``bse_variant``
+    "v3" takes the auxiliary sums from the upstream's q-by-q form (nonlocal_sde.py:129-156) instead of the
+    materialised v1 (nonlocal_sde.py:85-126); ``keep_keys`` names the outputs to keep."""
     cfg = synthetic.CONFIGS[name]
     inp = synthetic.make_inputs(cfg)
     _setup_config(cfg, inp)
@@ -116,7 +131,7 @@ def run_reference_pass(name: str, variants: bool = True) -> dict:
     irr_q_list = grid.get_irrq_list()
     v_nonloc = v_full.reduce_q(irr_q_list)
 
-    out = {}
+    out = {} if keep_keys is None else _OnlyKeys(keep_keys)
     # bubble (nonlocal_sde.py:801-809)
     gchi0_q = BubbleGenerator.create_generalized_chi0_q_fft_cpu(dist, giwk, cfg.niw, cfg.niv_full, grid, beta)
     out["chi0"] = gchi0_q.mat.copy()
@@ -143,7 +158,10 @@ def run_reference_pass(name: str, variants: bool = True) -> dict:
         gamma_r = LocalFourPoint(inp[f"gamma_{ch}"], chan, 1, 2, False, True)
         keep[ch] = {"gamma": gamma_r}
         # calculate_sigma_kernel_r_q (nonlocal_sde.py:257-336), both BSE variants
-        aux = nonlocal_sde.create_auxiliary_chi_r_q_sum_v1(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc)
+        if bse_variant == "v3":
+            aux = nonlocal_sde.create_auxiliary_chi_r_q_sum_v3(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc, dist)
+        else:
+            aux = nonlocal_sde.create_auxiliary_chi_r_q_sum_v1(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc)
         out[f"chi_aux_sum_{ch}"] = aux.mat.copy()
         if variants:
             aux3 = nonlocal_sde.create_auxiliary_chi_r_q_sum_v3(gamma_r, gchi0_q_core_inv, u_loc, v_nonloc, dist)
@@ -281,7 +299,12 @@ def hf_fixtures() -> dict:
     return out
 
 
-AT_SIZE_Q = {"c1": 45, "c2": 4}  # irreducible q whose X is stored (c1: all of them)
+AT_SIZE_Q = {"c1": 45, "c2": 4, "c3": 2}  # irreducible q whose X is stored (c1: all of them)
+# bosonic indices of X stored at the 3-orbital size (X of one q there is 81 x 41 x 80 complex128, 4.3 MB)
+AT_SIZE_W = {"c3": (0, 1, 20, 40)}
+# the 3-orbital box through the upstream's q-by-q BSE: v1 would hold 153 x 41 x 720^2 complex128 (52 GB) at once
+AT_SIZE_BSE = {"c3": "v3"}
+AT_SIZE_KEYS = ("sigma", "lambda_dens", "lambda_magn", "chi_aux_sum_dens", "chi_aux_sum_magn", "chi_phys_magn")
 
 
 def input_digest(inp: dict) -> dict:
@@ -293,22 +316,28 @@ def input_digest(inp: dict) -> dict:
 
 def run_reference_at_size(name: str) -> dict:
     """The upstream pass at a benchmark configuration's own size (c1: 1 orbital 16x16, niv = niw = 20 with the
-    spch lambda-correction; c2: 64x64, niv = niw = 60), in FP64.  Stored: Sigma on the irreducible k points,
-    lambda_d and lambda_m, X = sum_nu' chi* for the first AT_SIZE_Q[name] irreducible q, and the input digest;
-    the inputs themselves are regenerated from their seed by the tests."""
-    full = run_reference_pass(name, variants=False)
+    spch lambda-correction; c2: 64x64, niv = niw = 60; c3: 3 orbitals 32x32, niv = niw = 40, N = 720, no
+    lambda), in FP64.  Stored: Sigma on the irreducible k points, lambda_d and lambda_m (one orbital), X = sum_nu'
+    chi* (c3: at the bosonic indices AT_SIZE_W) and (c3) chi_phys_magn for the first AT_SIZE_Q[name] irreducible
+    q, and the input digest; the inputs themselves are regenerated from their seed by the tests."""
+    full = run_reference_pass(name, variants=False, bse_variant=AT_SIZE_BSE.get(name, "v1"), keep_keys=AT_SIZE_KEYS)
     ref = {k[4:]: v for k, v in full.items() if k.startswith("ref_")}
     inp = synthetic.make_inputs(synthetic.CONFIGS[name])
     nq = AT_SIZE_Q[name]
+    w_sel = AT_SIZE_W.get(name)
+    pick = (lambda x: x[:nq]) if w_sel is None else (lambda x: x[:nq][..., list(w_sel), :])
     out = {
         "sigma_irr": ref["sigma"][inp["irrk_ind"]],
-        "lambda_dens": ref["lambda_dens"],
-        "lambda_magn": ref["lambda_magn"],
-        "chi_aux_sum_dens_q": ref["chi_aux_sum_dens"][:nq],
-        "chi_aux_sum_magn_q": ref["chi_aux_sum_magn"][:nq],
-        "chi_phys_magn": ref["chi_phys_magn"],
+        "chi_aux_sum_dens_q": pick(ref["chi_aux_sum_dens"]),
+        "chi_aux_sum_magn_q": pick(ref["chi_aux_sum_magn"]),
+        "chi_phys_magn": ref["chi_phys_magn"] if name in ("c1", "c2") else ref["chi_phys_magn"][:nq],
         "n_q_stored": np.int64(nq),
     }
+    if w_sel is not None:
+        out["w_stored"] = np.asarray(w_sel, dtype=np.int64)
+    for key in ("lambda_dens", "lambda_magn"):
+        if key in ref:
+            out[key] = ref[key]
     out.update(input_digest(inp))
     return {f"ref_{k}": v for k, v in out.items()}
 
