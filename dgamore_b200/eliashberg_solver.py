@@ -177,7 +177,8 @@ class EliashbergSolver:
         rng = np.random.default_rng(seed)
         for ch in ("sing", "trip"):
             g0 = initial_gap(sh.nk, sh.n_orb, self.P, ch, symmetry, self.irrk_ind_host, self.irrk_inv_host, rng)
-            vals, vecs, status = self.eigs(ch, n_eig, tol, g0.ravel())
+            with torch.cuda.nvtx.range(f"dga.eliashberg.{ch}"):
+                vals, vecs, status = self.eigs(ch, n_eig, tol, g0.ravel())
             gaps = [v.reshape(*sh.nk, sh.n_orb, sh.n_orb, 2 * self.P) for v in vecs]
             out[ch] = (vals, gaps, status)
         self.status = {ch: out[ch][2] for ch in out}

@@ -92,6 +92,11 @@ class LocalSde:
 
     # ------------------------------------------------------------------ the pass
     def run(self) -> "LocalSde":
+        """Launches the whole equation on the device (no synchronisation), inside the NVTX range dga.local_sde."""
+        with torch.cuda.nvtx.range("dga.local_sde"):
+            return self._run()
+
+    def _run(self) -> "LocalSde":
         n, n2, W, N, Nf, nv, nvf = self.n, self.n2, self.W, self.N, self.Nf, self.nv, self.nvf
         dev, beta = self.dev, self.beta
         M = 2 * W

@@ -536,10 +536,14 @@ class LadderPass:
         return self.sigma
 
     def run(self):
-        """One device pass over the resident inputs (no host transfers, no synchronisation)."""
-        self.pre_bse()
-        self.bse()
-        return self.post_bse()
+        """One device pass over the resident inputs (no host transfers, no synchronisation).  The three phases are
+        NVTX ranges (dga.pre_bse, dga.bse, dga.post_bse) for timeline profilers; they cost nothing without one."""
+        with torch.cuda.nvtx.range("dga.pre_bse"):
+            self.pre_bse()
+        with torch.cuda.nvtx.range("dga.bse"):
+            self.bse()
+        with torch.cuda.nvtx.range("dga.post_bse"):
+            return self.post_bse()
 
     def capture(self) -> "torch.cuda.CUDAGraph":
         """Captures one device pass into a CUDA graph (``replay`` then re-runs all its kernels with one launch).
