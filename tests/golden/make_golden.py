@@ -299,11 +299,12 @@ def hf_fixtures() -> dict:
     return out
 
 
-AT_SIZE_Q = {"c1": 45, "c2": 4, "c3": 2}  # irreducible q whose X is stored (c1: all of them)
-# bosonic indices of X stored at the 3-orbital size (X of one q there is 81 x 41 x 80 complex128, 4.3 MB)
-AT_SIZE_W = {"c3": (0, 1, 20, 40)}
-# the 3-orbital box through the upstream's q-by-q BSE: v1 would hold 153 x 41 x 720^2 complex128 (52 GB) at once
-AT_SIZE_BSE = {"c3": "v3"}
+AT_SIZE_Q = {"c1": 45, "c2": 4, "c3": 2, "c4_bilayer": 2, "c4_single": 4}  # irreducible q whose X is stored
+# bosonic indices of X stored where X of one q is large (3 orbitals: 81 x 41 x 80 complex128, 4.3 MB)
+AT_SIZE_W = {"c3": (0, 1, 20, 40), "c4_bilayer": (0, 1, 15, 30)}
+# through the upstream's q-by-q BSE where v1 would hold every (q, w) matrix at once: 153 x 41 x 720^2 complex128
+# (52 GB) for the 3-orbital box, 325 x 31 x 240^2 (9.3 GB) for the bilayer
+AT_SIZE_BSE = {"c3": "v3", "c4_bilayer": "v3"}
 AT_SIZE_KEYS = ("sigma", "lambda_dens", "lambda_magn", "chi_aux_sum_dens", "chi_aux_sum_magn", "chi_phys_magn")
 
 
@@ -317,9 +318,10 @@ def input_digest(inp: dict) -> dict:
 def run_reference_at_size(name: str) -> dict:
     """The upstream pass at a benchmark configuration's own size (c1: 1 orbital 16x16, niv = niw = 20 with the
     spch lambda-correction; c2: 64x64, niv = niw = 60; c3: 3 orbitals 32x32, niv = niw = 40, N = 720, no
-    lambda), in FP64.  Stored: Sigma on the irreducible k points, lambda_d and lambda_m (one orbital), X = sum_nu'
-    chi* (c3: at the bosonic indices AT_SIZE_W) and (c3) chi_phys_magn for the first AT_SIZE_Q[name] irreducible
-    q, and the input digest; the inputs themselves are regenerated from their seed by the tests."""
+    lambda; the two requests of the batched pair, c4_bilayer: 2 orbitals 48x48, niv = niw = 30, N = 240, and
+    c4_single: 1 orbital 32x32, niv = niw = 50, with lambda), in FP64.  Stored: Sigma on the irreducible k points, lambda_d and lambda_m (one orbital), X = sum_nu'
+    chi* (at the bosonic indices AT_SIZE_W where given) and (c3, c4) chi_phys_magn for the first AT_SIZE_Q[name]
+    irreducible q, and the input digest; the inputs themselves are regenerated from their seed by the tests."""
     full = run_reference_pass(name, variants=False, bse_variant=AT_SIZE_BSE.get(name, "v1"), keep_keys=AT_SIZE_KEYS)
     ref = {k[4:]: v for k, v in full.items() if k.startswith("ref_")}
     inp = synthetic.make_inputs(synthetic.CONFIGS[name])

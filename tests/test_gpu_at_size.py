@@ -3,12 +3,15 @@
 * c1: 1 orbital, 16x16, niv = niw = 20, with the spch lambda-correction (the CPU-runnable configuration);
 * c2: 1 orbital, 64x64 reduced to its 561 irreducible q, niv = niw = 60 (the FP64 drop-in at scale);
 * c3: 3 orbitals (t2g, Kanamori), 32x32 reduced to its 153 irreducible q, niv = niw = 40, N = 720, no lambda (the
-  benchmark's own workload; the upstream ran its q-by-q BSE there).
+  benchmark's own workload; the upstream ran its q-by-q BSE there);
+* c4_bilayer (2 orbitals, 48x48, niv = niw = 30, N = 240) and c4_single (1 orbital, 32x32, niv = niw = 50, with
+  lambda): the two requests of the batched pair, each as its own pass.
 
-tests/golden/make_golden.py (``--at-size c1 c2 c3``) ran the upstream pass on the seeded inputs and stored Sigma
-on the irreducible k points, lambda_d and lambda_m (one orbital), X = sum_nu' chi* for some irreducible q (c3: at
-four bosonic indices), the physical magnetic susceptibility, and a digest of the inputs; the test regenerates the
-inputs from the same seed, checks the digest, and runs the device pass.
+tests/golden/make_golden.py (``--at-size c1 c2 c3 c4_single c4_bilayer``) ran the upstream pass on the seeded
+inputs and stored Sigma on the irreducible k points, lambda_d and lambda_m (one orbital), X = sum_nu' chi* for
+some irreducible q (at four bosonic indices for c3 and c4_bilayer), the physical magnetic susceptibility, and a
+digest of the inputs; the test regenerates the inputs from the same seed, checks the digest, and runs the device
+pass.
 Bounds: the FP64 drop-in form to 1e-10 relative (lambda to 1e-10 absolute); the mixed form Sigma to 1e-8 relative
 and lambda_d, lambda_m to 1e-6 absolute, the bounds the benchmark states for it.
 """
@@ -31,7 +34,7 @@ def _golden(name):
     return {k[4:]: v for k, v in np.load(path).items()}
 
 
-@pytest.fixture(scope="module", params=["c1", "c2", "c3"])
+@pytest.fixture(scope="module", params=["c1", "c2", "c3", "c4_bilayer", "c4_single"])
 def case(request):
     from dgamore_b200 import synthetic
 
