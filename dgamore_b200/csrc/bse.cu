@@ -339,11 +339,12 @@ __device__ bool lu_factor(C* __restrict__ A, int N, int ld, int* __restrict__ pi
 // block is solved by one warp per right-hand side (lane = row, the solved value broadcast by shuffle), the
 // rest of the rows are updated from the block copy in shared memory.
 // ----------------------------------------------------------------------------------------------
-constexpr int SOLVE_LOADS = 8;  // factor elements a thread has in flight in the row updates of lu_solve_inplace
-
 template <typename C, typename CY, int NR>
 __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __restrict__ Y, BseSmem<C>& sm) {
   constexpr int n_rhs = NR;
+  // factor elements a thread has in flight in the row updates: eight where each one feeds several right-hand
+  // sides; with one to three the registers go to the factorisation around the solve instead
+  constexpr int SOLVE_LOADS = NR >= 4 ? 8 : 1;
   using R = decltype(C::x);
   using RY = decltype(CY::x);
   const int tid = threadIdx.x, T = blockDim.x;
@@ -374,23 +375,32 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
       }
     }
     __syncthreads();
-    // rows below the block: one thread per row, every right-hand side at once (each L element read once, eight
-    // of them in flight; the products are summed in ascending r as before)
+    // rows below the block: one thread per row, every right-hand side at once (each L element read once,
+    // SOLVE_LOADS of them in flight; the products are summed in ascending r)
     for (int i = b0 + bn + tid; i < N; i += T) {
       CY acc[NR];
 #pragma unroll
       for (int s = 0; s < NR; ++s) acc[s] = Y[(size_t)s * N + i];
-      for (int r0 = 0; r0 < bn; r0 += SOLVE_LOADS) {
-        C l[SOLVE_LOADS];
+      if constexpr (SOLVE_LOADS == 1) {
+        for (int r = 0; r < bn; ++r) {
+          const C l = A[(size_t)(b0 + r) * ld + i];
+          const CY lw = cmake<CY>((RY)l.x, (RY)l.y);
 #pragma unroll
-        for (int u = 0; u < SOLVE_LOADS; ++u)
-          l[u] = (r0 + u < bn) ? A[(size_t)(b0 + r0 + u) * ld + i] : cmake<C>(R(0), R(0));
+          for (int s = 0; s < NR; ++s) cfms(acc[s], lw, yb[s * 32 + r]);
+        }
+      } else {
+        for (int r0 = 0; r0 < bn; r0 += SOLVE_LOADS) {
+          C l[SOLVE_LOADS];
 #pragma unroll
-        for (int u = 0; u < SOLVE_LOADS; ++u) {
-          if (r0 + u >= bn) break;
-          const CY lw = cmake<CY>((RY)l[u].x, (RY)l[u].y);
+          for (int u = 0; u < SOLVE_LOADS; ++u)
+            l[u] = (r0 + u < bn) ? A[(size_t)(b0 + r0 + u) * ld + i] : cmake<C>(R(0), R(0));
 #pragma unroll
-          for (int s = 0; s < NR; ++s) cfms(acc[s], lw, yb[s * 32 + r0 + u]);
+          for (int u = 0; u < SOLVE_LOADS; ++u) {
+            if (r0 + u >= bn) break;
+            const CY lw = cmake<CY>((RY)l[u].x, (RY)l[u].y);
+#pragma unroll
+            for (int s = 0; s < NR; ++s) cfms(acc[s], lw, yb[s * 32 + r0 + u]);
+          }
         }
       }
 #pragma unroll
@@ -429,23 +439,32 @@ __device__ void lu_solve_inplace(const C* __restrict__ A, int N, int ld, CY* __r
       }
     }
     __syncthreads();
-    // rows above the block: one thread per row, every right-hand side at once (each U element read once, eight
-    // of them in flight, summed in ascending r)
+    // rows above the block: one thread per row, every right-hand side at once (each U element read once,
+    // SOLVE_LOADS of them in flight, summed in ascending r)
     for (int i = tid; i < b0; i += T) {
       CY acc[NR];
 #pragma unroll
       for (int s = 0; s < NR; ++s) acc[s] = Y[(size_t)s * N + i];
-      for (int r0 = 0; r0 < bn; r0 += SOLVE_LOADS) {
-        C uu[SOLVE_LOADS];
+      if constexpr (SOLVE_LOADS == 1) {
+        for (int r = 0; r < bn; ++r) {
+          const C u = A[(size_t)(b0 + r) * ld + i];
+          const CY uw = cmake<CY>((RY)u.x, (RY)u.y);
 #pragma unroll
-        for (int u = 0; u < SOLVE_LOADS; ++u)
-          uu[u] = (r0 + u < bn) ? A[(size_t)(b0 + r0 + u) * ld + i] : cmake<C>(R(0), R(0));
+          for (int s = 0; s < NR; ++s) cfms(acc[s], uw, yb[s * 32 + r]);
+        }
+      } else {
+        for (int r0 = 0; r0 < bn; r0 += SOLVE_LOADS) {
+          C uu[SOLVE_LOADS];
 #pragma unroll
-        for (int u = 0; u < SOLVE_LOADS; ++u) {
-          if (r0 + u >= bn) break;
-          const CY uw = cmake<CY>((RY)uu[u].x, (RY)uu[u].y);
+          for (int u = 0; u < SOLVE_LOADS; ++u)
+            uu[u] = (r0 + u < bn) ? A[(size_t)(b0 + r0 + u) * ld + i] : cmake<C>(R(0), R(0));
 #pragma unroll
-          for (int s = 0; s < NR; ++s) cfms(acc[s], uw, yb[s * 32 + r0 + u]);
+          for (int u = 0; u < SOLVE_LOADS; ++u) {
+            if (r0 + u >= bn) break;
+            const CY uw = cmake<CY>((RY)uu[u].x, (RY)uu[u].y);
+#pragma unroll
+            for (int s = 0; s < NR; ++s) cfms(acc[s], uw, yb[s * 32 + r0 + u]);
+          }
         }
       }
 #pragma unroll
